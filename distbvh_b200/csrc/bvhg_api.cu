@@ -1,0 +1,853 @@
+// bvhg_api.cu — the C ABI declared in include/bvhg.h: contexts, objects and the per-object pipeline
+// K1 (centroids + Morton bounds) -> K2 (keys + digit histograms) -> K3 (radix passes) -> K4/K5 (leaf slabs, LBVH
+// build, refit) and the pairwise K6 (traversal) -> K7 (FP64 recheck, precision form) -> gid output.
+#include "../../include/bvhg.h"
+#include "bvhg_internal.cuh"
+#include "kdop_math.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace bvhg {
+cudaError_t launch_gid_pairs(const uint2 *pairs, uint64_t count, const uint64_t *gid_a, const uint64_t *gid_b,
+                             bool normalize, uint64_t *out, cudaStream_t s);
+int device_sm_count();
+}  // namespace bvhg
+
+using namespace bvhg;
+
+namespace {
+
+constexpr uint32_t kDefaultSpinLimit = 1u << 22;
+constexpr uint64_t kMaxElements = ( 1ull << 30 ) - 1;  // 30-bit radix status counters, int32 node links
+
+struct dev_buf
+{
+  void *p = nullptr;
+  size_t bytes = 0;
+  dev_buf() = default;
+  dev_buf(const dev_buf &) = delete;
+  dev_buf &operator=(const dev_buf &) = delete;
+  ~dev_buf()
+  {
+    if ( p ) cudaFree( p );
+  }
+  cudaError_t reserve(size_t b)
+  {
+    if ( b <= bytes ) return cudaSuccess;
+    if ( p ) cudaFree( p );
+    p = nullptr;
+    bytes = 0;
+    size_t want = b < 256 ? 256 : b;
+    cudaError_t e = cudaMalloc( &p, want );
+    if ( e != cudaSuccess )
+    {
+      p = nullptr;
+      return e;
+    }
+    bytes = want;
+    return cudaSuccess;
+  }
+  template< typename T >
+  T *as() const { return static_cast< T * >( p ); }
+};
+
+struct object
+{
+  uint64_t n = 0;
+  uint32_t V = 0;
+  const double *verts = nullptr;  // in use (owned copy or borrowed device pointer)
+  const uint64_t *gid = nullptr;
+  bool has_data = false;
+  bool built = false;  // slabs current for the present vertex data
+  bool topo = false;   // a rebuild's topology exists for the present n and V (refit allowed)
+  int sort_result_alt = 0;  // sorted keys/vals ended in the *_alt buffers
+  dev_buf verts_own, gid_own;
+  dev_buf cx, cy, cz;
+  dev_buf keys, keys_alt, vals, vals_alt;
+  dev_buf hist, status;
+  dev_buf leaf_box, node_box, child, range, parent, exch;
+  dev_buf scal;  // obj_scalars
+  obj_scalars *sc() const { return scal.as< obj_scalars >(); }
+  const uint64_t *sorted_keys() const { return sort_result_alt ? keys_alt.as< uint64_t >() : keys.as< uint64_t >(); }
+  const uint32_t *sorted_vals() const { return sort_result_alt ? vals_alt.as< uint32_t >() : vals.as< uint32_t >(); }
+};
+
+struct timed_stage
+{
+  int stage;
+  cudaEvent_t start, stop;
+};
+
+}  // namespace
+
+struct bvhg_ctx
+{
+  bvhg_config cfg{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  uint32_t spin_limit = kDefaultSpinLimit;
+  int stall_sort = 0;  // test hook: radix look-back polls a status row nobody publishes
+  std::vector< std::unique_ptr< object > > objs;
+  std::string err;
+  // pairs
+  dev_buf pairs, pairs2, pairs_out, pscal;
+  uint64_t pair_cap = 0, pair2_cap = 0;
+  pair_scalars *host_ps = nullptr;  // pinned: pair counters + the two objects' error words after a broadphase
+  int *host_err = nullptr;          // pinned [2]
+  obj_scalars *init_template = nullptr;  // pinned, constant: the reset state of an object's scalars
+  uint64_t last_candidates = 0;
+  // timing
+  std::vector< timed_stage > pending;
+  std::vector< cudaEvent_t > event_pool;
+  double stage_ms[BVHG_NUM_STAGES] = {};
+  uint64_t stage_launches[BVHG_NUM_STAGES] = {};
+  uint64_t launches = 0;
+};
+
+namespace {
+
+bvhg_status fail(bvhg_ctx *ctx, bvhg_status st, const std::string &msg)
+{
+  if ( ctx ) ctx->err = msg;
+  return st;
+}
+
+bvhg_status cuda_fail(bvhg_ctx *ctx, cudaError_t e, const char *where)
+{
+  std::string m = std::string( where ) + ": " + cudaGetErrorString( e );
+  return fail( ctx, e == cudaErrorMemoryAllocation ? BVHG_ERR_NOMEM : BVHG_ERR_CUDA, m );
+}
+
+#define BVHG_CUDA(ctx, call)                                                                                          \
+  do                                                                                                                  \
+  {                                                                                                                   \
+    cudaError_t e_ = ( call );                                                                                        \
+    if ( e_ != cudaSuccess ) return cuda_fail( ( ctx ), e_, #call );                                                  \
+  } while ( 0 )
+
+cudaEvent_t take_event(bvhg_ctx *ctx)
+{
+  if ( !ctx->event_pool.empty() )
+  {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate( &e );
+  return e;
+}
+
+struct stage_scope
+{
+  bvhg_ctx *ctx;
+  int stage;
+  cudaEvent_t start = nullptr;
+  stage_scope(bvhg_ctx *c, int s) : ctx( c ), stage( s )
+  {
+    if ( ctx->cfg.flags & BVHG_FLAG_STAGE_TIMING )
+    {
+      start = take_event( ctx );
+      cudaEventRecord( start, ctx->stream );
+    }
+  }
+  void launched(uint64_t k = 1)
+  {
+    ctx->launches += k;
+    ctx->stage_launches[stage] += k;
+  }
+  ~stage_scope()
+  {
+    if ( start )
+    {
+      cudaEvent_t stop = take_event( ctx );
+      cudaEventRecord( stop, ctx->stream );
+      ctx->pending.push_back( { stage, start, stop } );
+    }
+  }
+};
+
+void collect_timing(bvhg_ctx *ctx)
+{
+  for ( auto &t : ctx->pending )
+  {
+    float ms = 0.f;
+    if ( cudaEventSynchronize( t.stop ) == cudaSuccess && cudaEventElapsedTime( &ms, t.start, t.stop ) == cudaSuccess )
+      ctx->stage_ms[t.stage] += ms;
+    ctx->event_pool.push_back( t.start );
+    ctx->event_pool.push_back( t.stop );
+  }
+  ctx->pending.clear();
+}
+
+bool valid_obj(bvhg_ctx *ctx, int32_t obj)
+{
+  return ctx && obj >= 0 && static_cast< size_t >( obj ) < ctx->objs.size() && ctx->objs[obj];
+}
+
+size_t slab_bytes(const bvhg_ctx *ctx) { return ctx->cfg.precision == BVHG_FILTER_FP32 ? 4 : 8; }
+
+bvhg_status object_error(bvhg_ctx *ctx, int err)
+{
+  if ( err == kErrArg ) return fail( ctx, BVHG_ERR_ARG, "non-finite vertex coordinate in element data" );
+  if ( err == kErrTimeout ) return fail( ctx, BVHG_ERR_TIMEOUT, "radix sort look-back exceeded the spin limit" );
+  if ( err ) return fail( ctx, BVHG_ERR_CUDA, "device error " + std::to_string( err ) );
+  return BVHG_OK;
+}
+
+// Reads an object's device error word in stream order (synchronizes the stream).
+bvhg_status check_scalar_errors(bvhg_ctx *ctx, const object &o)
+{
+  BVHG_CUDA( ctx, cudaMemcpyAsync( ctx->host_err, &o.sc()->error, sizeof( int ), cudaMemcpyDeviceToHost, ctx->stream ) );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  return object_error( ctx, ctx->host_err[0] );
+}
+
+bvhg_status do_build(bvhg_ctx *ctx, object &o, int mode)
+{
+  const uint64_t n = o.n;
+  const int K = ctx->cfg.k;
+  const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
+  const int D = K / 2;
+  cudaStream_t s = ctx->stream;
+  if ( n == 0 )
+  {
+    o.built = true;
+    return BVHG_OK;
+  }
+  const size_t sb = slab_bytes( ctx );
+  if ( mode == BVHG_REFIT )
+  {
+    if ( !o.topo ) return fail( ctx, BVHG_ERR_STATE, "refit without a rebuild of this element count" );
+    stage_scope st( ctx, BVHG_STAGE_BUILD );
+    if ( n > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( n - 1 ) * sizeof( int ), s ) );
+    BVHG_CUDA( ctx, launch_refit( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.leaf_box.p,
+                                  o.node_box.p, o.parent.as< int >(), o.exch.as< int >(), o.sc(), s ) );
+    st.launched();
+    o.built = true;
+    return BVHG_OK;
+  }
+  const int bits = ctx->cfg.sort_digit_bits;
+  const int passes = sort_passes( bits );
+  const uint64_t radix = 1ull << bits;
+  const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
+  // capacity
+  BVHG_CUDA( ctx, o.scal.reserve( sizeof( obj_scalars ) ) );
+  BVHG_CUDA( ctx, o.cx.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.cy.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.cz.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.keys.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.keys_alt.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.vals.reserve( n * 4 ) );
+  BVHG_CUDA( ctx, o.vals_alt.reserve( n * 4 ) );
+  BVHG_CUDA( ctx, o.hist.reserve( passes * radix * 4 ) );
+  BVHG_CUDA( ctx, o.status.reserve( passes * ( tiles + 1 ) * radix * 4 ) );
+  BVHG_CUDA( ctx, o.leaf_box.reserve( n * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.node_box.reserve( ( n - 1 ) * D * 4 * sb + 16 ) );
+  BVHG_CUDA( ctx, o.child.reserve( ( n - 1 ) * 8 + 8 ) );
+  BVHG_CUDA( ctx, o.range.reserve( ( n - 1 ) * 8 + 8 ) );
+  BVHG_CUDA( ctx, o.parent.reserve( ( 2 * n ) * 4 ) );
+  BVHG_CUDA( ctx, o.exch.reserve( n * 4 ) );
+  {
+    stage_scope st( ctx, BVHG_STAGE_BOUNDS );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( o.sc(), ctx->init_template, sizeof( obj_scalars ), cudaMemcpyHostToDevice, s ) );
+    BVHG_CUDA( ctx, cudaMemsetAsync( o.hist.p, 0, passes * radix * 4, s ) );
+    BVHG_CUDA( ctx, cudaMemsetAsync( o.status.p, 0, passes * ( tiles + 1 ) * radix * 4, s ) );
+    if ( n > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( n - 1 ) * 4, s ) );
+    BVHG_CUDA( ctx, launch_centroid_bounds( K, o.verts, o.V, n, ctx->cfg.epsilon, o.cx.as< double >(),
+                                            o.cy.as< double >(), o.cz.as< double >(), o.sc(), s ) );
+    st.launched();
+  }
+  {
+    stage_scope st( ctx, BVHG_STAGE_KEYS );
+    BVHG_CUDA( ctx, launch_keys_hist( bits, o.cx.as< double >(), o.cy.as< double >(), o.cz.as< double >(), n, o.sc(),
+                                      o.keys.as< uint64_t >(), o.hist.as< uint32_t >(), s ) );
+    st.launched();
+  }
+  {
+    stage_scope st( ctx, BVHG_STAGE_SORT );
+    uint64_t *kin = o.keys.as< uint64_t >(), *kout = o.keys_alt.as< uint64_t >();
+    uint32_t *vin = nullptr, *vout = o.vals_alt.as< uint32_t >();
+    uint32_t *vother = o.vals.as< uint32_t >();
+    for ( int p = 0; p < passes; ++p )
+    {
+      BVHG_CUDA( ctx, launch_onesweep( bits, kin, vin, kout, vout, n, p, o.hist.as< uint32_t >(),
+                                       o.status.as< uint32_t >(), o.sc(), ctx->spin_limit, ctx->stall_sort, s ) );
+      st.launched();
+      std::swap( kin, kout );
+      uint32_t *next_out = vin ? vin : vother;
+      vin = vout;
+      vout = next_out;
+    }
+    o.sort_result_alt = ( passes & 1 ) ? 1 : 0;
+  }
+  {
+    stage_scope st( ctx, BVHG_STAGE_BUILD );
+    BVHG_CUDA( ctx, launch_build( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_keys(), o.sorted_vals(),
+                                  o.leaf_box.p, o.node_box.p, o.child.as< int2 >(), o.range.as< int2 >(),
+                                  o.parent.as< int >(), o.exch.as< int >(), o.sc(), s ) );
+    st.launched();
+  }
+  o.built = true;
+  o.topo = true;
+  return BVHG_OK;
+}
+
+tree_view view_of(const object &o)
+{
+  tree_view v;
+  v.node_box = o.node_box.p;
+  v.child = o.child.as< int2 >();
+  v.range = o.range.as< int2 >();
+  v.leaf_box = o.leaf_box.p;
+  v.perm = o.sorted_vals();
+  v.n = o.n;
+  v.sc = o.sc();
+  return v;
+}
+
+// Runs traversal (+ recheck) until both buffers were large enough; returns the final local pair buffer and count.
+// One host synchronization per attempt: the pair counters and both objects' error words come back together.
+bvhg_status find_pairs(bvhg_ctx *ctx, object &a, object &b, bool self, const uint2 **out_pairs, uint64_t *out_count)
+{
+  const int K = ctx->cfg.k;
+  const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
+  cudaStream_t s = ctx->stream;
+  BVHG_CUDA( ctx, ctx->pscal.reserve( sizeof( pair_scalars ) ) );
+  if ( ctx->pair_cap == 0 )
+  {
+    ctx->pair_cap = 1u << 20;
+    BVHG_CUDA( ctx, ctx->pairs.reserve( ctx->pair_cap * sizeof( uint2 ) ) );
+  }
+  if ( fp32 && ctx->pair2_cap == 0 )
+  {
+    ctx->pair2_cap = 1u << 20;
+    BVHG_CUDA( ctx, ctx->pairs2.reserve( ctx->pair2_cap * sizeof( uint2 ) ) );
+  }
+  pair_scalars *ps = ctx->pscal.as< pair_scalars >();
+  for ( int attempt = 0; attempt < 3; ++attempt )
+  {
+    BVHG_CUDA( ctx, cudaMemsetAsync( ps, 0, sizeof( pair_scalars ), s ) );
+    {
+      stage_scope st( ctx, BVHG_STAGE_TRAVERSE );
+      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( a ), view_of( b ), self, ctx->pairs.as< uint2 >(),
+                                       ctx->pair_cap, ps, s ) );
+      st.launched();
+    }
+    if ( fp32 )
+    {
+      stage_scope st( ctx, BVHG_STAGE_RECHECK );
+      BVHG_CUDA( ctx, launch_recheck( K, a.verts, a.V, b.verts, b.V, ctx->cfg.epsilon, ctx->pairs.as< uint2 >(),
+                                      ctx->pair_cap, ctx->pairs2.as< uint2 >(), ctx->pair2_cap, ps, s ) );
+      st.launched();
+    }
+    BVHG_CUDA( ctx, cudaMemcpyAsync( ctx->host_ps, ps, sizeof( pair_scalars ), cudaMemcpyDeviceToHost, s ) );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( ctx->host_err, &a.sc()->error, sizeof( int ), cudaMemcpyDeviceToHost, s ) );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( ctx->host_err + 1, &b.sc()->error, sizeof( int ), cudaMemcpyDeviceToHost, s ) );
+    BVHG_CUDA( ctx, cudaStreamSynchronize( s ) );
+    bvhg_status st = object_error( ctx, ctx->host_err[0] );
+    if ( st == BVHG_OK ) st = object_error( ctx, ctx->host_err[1] );
+    if ( st != BVHG_OK ) return st;
+    if ( ctx->host_ps->error ) return fail( ctx, BVHG_ERR_CUDA, "traversal stack overflow" );
+    const uint64_t ncand = ctx->host_ps->count;
+    ctx->last_candidates = ncand;
+    if ( ncand > ctx->pair_cap )
+    {
+      ctx->pair_cap = ncand + ncand / 8;
+      BVHG_CUDA( ctx, ctx->pairs.reserve( ctx->pair_cap * sizeof( uint2 ) ) );
+      continue;
+    }
+    if ( !fp32 )
+    {
+      *out_pairs = ctx->pairs.as< uint2 >();
+      *out_count = ncand;
+      return BVHG_OK;
+    }
+    const uint64_t nexact = ctx->host_ps->count2;
+    if ( nexact > ctx->pair2_cap )
+    {
+      ctx->pair2_cap = nexact + nexact / 8;
+      BVHG_CUDA( ctx, ctx->pairs2.reserve( ctx->pair2_cap * sizeof( uint2 ) ) );
+      continue;
+    }
+    *out_pairs = ctx->pairs2.as< uint2 >();
+    *out_count = nexact;
+    return BVHG_OK;
+  }
+  return fail( ctx, BVHG_ERR_CUDA, "pair buffer did not converge" );
+}
+
+bvhg_status emit_pairs(bvhg_ctx *ctx, const object &a, const object &b, bool self, const uint2 *pairs, uint64_t np,
+                       uint64_t *out, uint64_t capacity, uint64_t *count, int32_t mem)
+{
+  cudaStream_t s = ctx->stream;
+  *count = np;
+  const uint64_t nw = np < capacity ? np : capacity;
+  if ( nw > 0 && out )
+  {
+    stage_scope st( ctx, BVHG_STAGE_OUTPUT );
+    uint64_t *dst = out;
+    if ( mem == BVHG_MEM_HOST )
+    {
+      BVHG_CUDA( ctx, ctx->pairs_out.reserve( nw * 16 ) );
+      dst = ctx->pairs_out.as< uint64_t >();
+    }
+    BVHG_CUDA( ctx, launch_gid_pairs( pairs, nw, a.gid, b.gid, self, dst, s ) );
+    st.launched();
+    if ( mem == BVHG_MEM_HOST )
+      BVHG_CUDA( ctx, cudaMemcpyAsync( out, dst, nw * 16, cudaMemcpyDeviceToHost, s ) );
+  }
+  BVHG_CUDA( ctx, cudaStreamSynchronize( s ) );
+  if ( np > capacity ) return fail( ctx, BVHG_ERR_OVERFLOW, "pair buffer too small: " + std::to_string( np ) + " pairs" );
+  return BVHG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void bvhg_config_default(bvhg_config *cfg)
+{
+  if ( !cfg ) return;
+  std::memset( cfg, 0, sizeof( *cfg ) );
+  cfg->k = 18;
+  cfg->precision = BVHG_PLAIN_FP64;
+  cfg->sort_digit_bits = 8;
+  cfg->device = 0;
+  cfg->epsilon = 0.0;
+  cfg->stream = nullptr;
+  cfg->spin_limit = 0;
+  cfg->flags = 0;
+}
+
+bvhg_status bvhg_create(bvhg_ctx **out, const bvhg_config *cfg)
+{
+  if ( !out ) return BVHG_ERR_ARG;
+  *out = nullptr;
+  bvhg_config c;
+  bvhg_config_default( &c );
+  if ( cfg ) c = *cfg;
+  if ( c.k != 6 && c.k != 18 && c.k != 26 ) return BVHG_ERR_ARG;
+  if ( c.precision != BVHG_PLAIN_FP64 && c.precision != BVHG_FILTER_FP32 ) return BVHG_ERR_ARG;
+  if ( c.sort_digit_bits != 1 && c.sort_digit_bits != 2 && c.sort_digit_bits != 4 && c.sort_digit_bits != 8 )
+    return BVHG_ERR_ARG;
+  if ( !( c.epsilon >= 0.0 ) || c.epsilon > 1e300 ) return BVHG_ERR_ARG;
+  if ( cudaSetDevice( c.device ) != cudaSuccess ) return BVHG_ERR_CUDA;
+  auto ctx = std::make_unique< bvhg_ctx >();
+  ctx->cfg = c;
+  ctx->spin_limit = c.spin_limit ? c.spin_limit : kDefaultSpinLimit;
+  if ( c.stream )
+  {
+    ctx->stream = static_cast< cudaStream_t >( c.stream );
+  } else {
+    if ( cudaStreamCreateWithFlags( &ctx->stream, cudaStreamNonBlocking ) != cudaSuccess ) return BVHG_ERR_CUDA;
+    ctx->own_stream = true;
+  }
+  if ( cudaMallocHost( reinterpret_cast< void ** >( &ctx->host_ps ), sizeof( pair_scalars ) ) != cudaSuccess ||
+       cudaMallocHost( reinterpret_cast< void ** >( &ctx->host_err ), 2 * sizeof( int ) ) != cudaSuccess ||
+       cudaMallocHost( reinterpret_cast< void ** >( &ctx->init_template ), sizeof( obj_scalars ) ) != cudaSuccess )
+    return BVHG_ERR_CUDA;
+  std::memset( ctx->init_template, 0, sizeof( obj_scalars ) );
+  for ( int c = 0; c < 3; ++c )
+  {
+    ctx->init_template->bounds_enc[c] = ~0ull;  // min accumulators start at the largest encoding
+    ctx->init_template->bounds_enc[3 + c] = 0ull;
+  }
+  *out = ctx.release();
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_destroy(bvhg_ctx *ctx)
+{
+  if ( !ctx ) return BVHG_ERR_ARG;
+  cudaSetDevice( ctx->cfg.device );
+  cudaStreamSynchronize( ctx->stream );
+  collect_timing( ctx );
+  for ( auto e : ctx->event_pool ) cudaEventDestroy( e );
+  if ( ctx->host_ps ) cudaFreeHost( ctx->host_ps );
+  if ( ctx->host_err ) cudaFreeHost( ctx->host_err );
+  if ( ctx->init_template ) cudaFreeHost( ctx->init_template );
+  ctx->objs.clear();
+  if ( ctx->own_stream ) cudaStreamDestroy( ctx->stream );
+  delete ctx;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_object_create(bvhg_ctx *ctx, int32_t *obj)
+{
+  if ( !ctx || !obj ) return fail( ctx, BVHG_ERR_ARG, "null argument" );
+  cudaSetDevice( ctx->cfg.device );
+  auto o = std::make_unique< object >();
+  BVHG_CUDA( ctx, o->scal.reserve( sizeof( obj_scalars ) ) );
+  BVHG_CUDA( ctx, cudaMemsetAsync( o->scal.p, 0, sizeof( obj_scalars ), ctx->stream ) );
+  ctx->objs.push_back( std::move( o ) );
+  *obj = static_cast< int32_t >( ctx->objs.size() - 1 );
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_object_destroy(bvhg_ctx *ctx, int32_t obj)
+{
+  if ( !valid_obj( ctx, obj ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  cudaSetDevice( ctx->cfg.device );
+  cudaStreamSynchronize( ctx->stream );
+  ctx->objs[obj].reset();
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_set_elements(bvhg_ctx *ctx, int32_t obj, const double *xyz, uint32_t V, const uint64_t *gid,
+                              uint64_t n, int32_t mem)
+{
+  if ( !valid_obj( ctx, obj ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  if ( V == 0 || V > 32 ) return fail( ctx, BVHG_ERR_ARG, "verts_per_elem must be in [1, 32]" );
+  if ( n > kMaxElements ) return fail( ctx, BVHG_ERR_ARG, "too many elements (limit 2^30 - 1)" );
+  if ( n > 0 && !xyz ) return fail( ctx, BVHG_ERR_ARG, "null vertex pointer" );
+  if ( mem != BVHG_MEM_HOST && mem != BVHG_MEM_DEVICE ) return fail( ctx, BVHG_ERR_ARG, "bad memory kind" );
+  cudaSetDevice( ctx->cfg.device );
+  object &o = *ctx->objs[obj];
+  if ( n != o.n || V != o.V ) o.topo = false;
+  o.n = n;
+  o.V = V;
+  o.built = false;
+  o.has_data = true;
+  if ( n == 0 )
+  {
+    o.verts = nullptr;
+    o.gid = nullptr;
+    return BVHG_OK;
+  }
+  if ( mem == BVHG_MEM_DEVICE )
+  {
+    o.verts = xyz;
+    o.gid = gid;
+  } else {
+    const size_t vb = n * V * 3 * sizeof( double );
+    BVHG_CUDA( ctx, o.verts_own.reserve( vb ) );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( o.verts_own.p, xyz, vb, cudaMemcpyHostToDevice, ctx->stream ) );
+    o.verts = o.verts_own.as< double >();
+    if ( gid )
+    {
+      BVHG_CUDA( ctx, o.gid_own.reserve( n * 8 ) );
+      BVHG_CUDA( ctx, cudaMemcpyAsync( o.gid_own.p, gid, n * 8, cudaMemcpyHostToDevice, ctx->stream ) );
+      o.gid = o.gid_own.as< uint64_t >();
+    } else {
+      o.gid = nullptr;
+    }
+  }
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_build(bvhg_ctx *ctx, int32_t obj, int32_t mode)
+{
+  if ( !valid_obj( ctx, obj ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  if ( mode != BVHG_REBUILD && mode != BVHG_REFIT ) return fail( ctx, BVHG_ERR_ARG, "bad build mode" );
+  object &o = *ctx->objs[obj];
+  if ( !o.has_data ) return fail( ctx, BVHG_ERR_STATE, "build before set_elements" );
+  cudaSetDevice( ctx->cfg.device );
+  return do_build( ctx, o, mode );
+}
+
+bvhg_status bvhg_broadphase(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, uint64_t *pairs, uint64_t capacity,
+                            uint64_t *count, int32_t mem)
+{
+  if ( !valid_obj( ctx, obj_a ) || !valid_obj( ctx, obj_b ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  if ( !count ) return fail( ctx, BVHG_ERR_ARG, "null count" );
+  if ( capacity > 0 && !pairs ) return fail( ctx, BVHG_ERR_ARG, "null pair buffer" );
+  object &a = *ctx->objs[obj_a];
+  object &b = *ctx->objs[obj_b];
+  if ( !a.built || !b.built ) return fail( ctx, BVHG_ERR_STATE, "broadphase before build" );
+  cudaSetDevice( ctx->cfg.device );
+  *count = 0;
+  if ( a.n == 0 || b.n == 0 )
+  {
+    ctx->last_candidates = 0;
+    return BVHG_OK;
+  }
+  const uint2 *lp = nullptr;
+  uint64_t np = 0;
+  bvhg_status st = find_pairs( ctx, a, b, false, &lp, &np );
+  if ( st != BVHG_OK ) return st;
+  return emit_pairs( ctx, a, b, false, lp, np, pairs, capacity, count, mem );
+}
+
+bvhg_status bvhg_self_collision(bvhg_ctx *ctx, int32_t obj, uint64_t *pairs, uint64_t capacity, uint64_t *count,
+                                int32_t mem)
+{
+  if ( !valid_obj( ctx, obj ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  if ( !count ) return fail( ctx, BVHG_ERR_ARG, "null count" );
+  if ( capacity > 0 && !pairs ) return fail( ctx, BVHG_ERR_ARG, "null pair buffer" );
+  object &o = *ctx->objs[obj];
+  if ( !o.built ) return fail( ctx, BVHG_ERR_STATE, "self_collision before build" );
+  cudaSetDevice( ctx->cfg.device );
+  *count = 0;
+  if ( o.n < 2 )
+  {
+    ctx->last_candidates = 0;
+    return BVHG_OK;
+  }
+  const uint2 *lp = nullptr;
+  uint64_t np = 0;
+  bvhg_status st = find_pairs( ctx, o, o, true, &lp, &np );
+  if ( st != BVHG_OK ) return st;
+  return emit_pairs( ctx, o, o, true, lp, np, pairs, capacity, count, mem );
+}
+
+bvhg_status bvhg_get_morton(bvhg_ctx *ctx, int32_t obj, uint64_t *sorted_keys, uint32_t *perm, double *min3,
+                            double *inv3)
+{
+  if ( !valid_obj( ctx, obj ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  object &o = *ctx->objs[obj];
+  if ( !o.built ) return fail( ctx, BVHG_ERR_STATE, "probe before build" );
+  cudaSetDevice( ctx->cfg.device );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  if ( o.n == 0 ) return BVHG_OK;
+  bvhg_status st = check_scalar_errors( ctx, o );
+  if ( st != BVHG_OK ) return st;
+  if ( sorted_keys ) BVHG_CUDA( ctx, cudaMemcpy( sorted_keys, o.sorted_keys(), o.n * 8, cudaMemcpyDeviceToHost ) );
+  if ( perm ) BVHG_CUDA( ctx, cudaMemcpy( perm, o.sorted_vals(), o.n * 4, cudaMemcpyDeviceToHost ) );
+  obj_scalars h;
+  BVHG_CUDA( ctx, cudaMemcpy( &h, o.sc(), sizeof( h ), cudaMemcpyDeviceToHost ) );
+  if ( min3 ) std::memcpy( min3, h.min3, sizeof( h.min3 ) );
+  if ( inv3 ) std::memcpy( inv3, h.inv3, sizeof( h.inv3 ) );
+  return BVHG_OK;
+}
+
+static bvhg_status probe_kdops(bvhg_ctx *ctx, int32_t obj, void *out, bool fp32)
+{
+  if ( !valid_obj( ctx, obj ) || !out ) return fail( ctx, BVHG_ERR_ARG, "invalid argument" );
+  object &o = *ctx->objs[obj];
+  if ( !o.has_data ) return fail( ctx, BVHG_ERR_STATE, "probe before set_elements" );
+  cudaSetDevice( ctx->cfg.device );
+  if ( o.n == 0 ) return BVHG_OK;
+  const int D = ctx->cfg.k / 2;
+  const size_t bytes = o.n * D * 2 * ( fp32 ? 4 : 8 );
+  dev_buf tmp;
+  BVHG_CUDA( ctx, tmp.reserve( bytes ) );
+  BVHG_CUDA( ctx, launch_probe_kdops( ctx->cfg.k, fp32, o.verts, o.V, o.n, ctx->cfg.epsilon, tmp.p, ctx->stream ) );
+  ctx->launches += 1;
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  BVHG_CUDA( ctx, cudaMemcpy( out, tmp.p, bytes, cudaMemcpyDeviceToHost ) );
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_get_kdops(bvhg_ctx *ctx, int32_t obj, double *slabs)
+{
+  if ( ctx && ctx->cfg.precision != BVHG_PLAIN_FP64 ) return fail( ctx, BVHG_ERR_STATE, "FP64 slabs: FP64 form only" );
+  return probe_kdops( ctx, obj, slabs, false );
+}
+
+bvhg_status bvhg_get_kdops_f32(bvhg_ctx *ctx, int32_t obj, float *slabs)
+{
+  if ( ctx && ctx->cfg.precision != BVHG_FILTER_FP32 ) return fail( ctx, BVHG_ERR_STATE, "FP32 slabs: FP32 form only" );
+  return probe_kdops( ctx, obj, slabs, true );
+}
+
+bvhg_status bvhg_get_centroids(bvhg_ctx *ctx, int32_t obj, double *centroids)
+{
+  if ( !valid_obj( ctx, obj ) || !centroids ) return fail( ctx, BVHG_ERR_ARG, "invalid argument" );
+  object &o = *ctx->objs[obj];
+  if ( !o.built ) return fail( ctx, BVHG_ERR_STATE, "probe before build" );
+  cudaSetDevice( ctx->cfg.device );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  if ( o.n == 0 ) return BVHG_OK;
+  std::vector< double > x( o.n ), y( o.n ), z( o.n );
+  BVHG_CUDA( ctx, cudaMemcpy( x.data(), o.cx.p, o.n * 8, cudaMemcpyDeviceToHost ) );
+  BVHG_CUDA( ctx, cudaMemcpy( y.data(), o.cy.p, o.n * 8, cudaMemcpyDeviceToHost ) );
+  BVHG_CUDA( ctx, cudaMemcpy( z.data(), o.cz.p, o.n * 8, cudaMemcpyDeviceToHost ) );
+  for ( uint64_t i = 0; i < o.n; ++i )
+  {
+    centroids[3 * i] = x[i];
+    centroids[3 * i + 1] = y[i];
+    centroids[3 * i + 2] = z[i];
+  }
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
+{
+  if ( !valid_obj( ctx, obj ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  object &o = *ctx->objs[obj];
+  if ( !o.built ) return fail( ctx, BVHG_ERR_STATE, "validate before build" );
+  cudaSetDevice( ctx->cfg.device );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  if ( depth_out ) *depth_out = 0;
+  const uint64_t n = o.n;
+  if ( n <= 1 ) return BVHG_OK;
+  const int D = ctx->cfg.k / 2;
+  const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
+  const uint64_t m = n - 1;
+  std::vector< int2 > child( m ), range( m );
+  std::vector< uint32_t > perm( n );
+  std::vector< double > nb( m * D * 4 ), lb( n * D * 2 );
+  BVHG_CUDA( ctx, cudaMemcpy( child.data(), o.child.p, m * 8, cudaMemcpyDeviceToHost ) );
+  BVHG_CUDA( ctx, cudaMemcpy( range.data(), o.range.p, m * 8, cudaMemcpyDeviceToHost ) );
+  BVHG_CUDA( ctx, cudaMemcpy( perm.data(), o.sorted_vals(), n * 4, cudaMemcpyDeviceToHost ) );
+  if ( fp32 )
+  {
+    std::vector< float > f( m * D * 4 ), g( n * D * 2 );
+    BVHG_CUDA( ctx, cudaMemcpy( f.data(), o.node_box.p, f.size() * 4, cudaMemcpyDeviceToHost ) );
+    BVHG_CUDA( ctx, cudaMemcpy( g.data(), o.leaf_box.p, g.size() * 4, cudaMemcpyDeviceToHost ) );
+    for ( size_t k = 0; k < f.size(); ++k ) nb[k] = f[k];
+    for ( size_t k = 0; k < g.size(); ++k ) lb[k] = g[k];
+  } else {
+    BVHG_CUDA( ctx, cudaMemcpy( nb.data(), o.node_box.p, nb.size() * 8, cudaMemcpyDeviceToHost ) );
+    BVHG_CUDA( ctx, cudaMemcpy( lb.data(), o.leaf_box.p, lb.size() * 8, cudaMemcpyDeviceToHost ) );
+  }
+  obj_scalars h;
+  BVHG_CUDA( ctx, cudaMemcpy( &h, o.sc(), sizeof( h ), cudaMemcpyDeviceToHost ) );
+  if ( h.root < 0 || static_cast< uint64_t >( h.root ) >= m ) return fail( ctx, BVHG_ERR_STATE, "bad root" );
+  std::vector< uint32_t > rank_of( n );
+  for ( uint64_t r = 0; r < n; ++r ) rank_of[perm[r]] = static_cast< uint32_t >( r );
+  std::vector< uint8_t > seen_leaf( n, 0 ), seen_node( m, 0 );
+  // (node, depth); check each child box is inside the slot the parent stores and leaves match leaf_box
+  std::vector< std::pair< int, uint32_t > > st{ { h.root, 1u } };
+  uint32_t maxd = 0;
+  uint64_t leaves = 0, nodes = 0;
+  while ( !st.empty() )
+  {
+    auto [k, d] = st.back();
+    st.pop_back();
+    if ( seen_node[k] ) return fail( ctx, BVHG_ERR_STATE, "node reached twice" );
+    seen_node[k] = 1;
+    ++nodes;
+    const int c[2] = { child[k].x, child[k].y };
+    for ( int side = 0; side < 2; ++side )
+    {
+      const double *slot = &nb[( static_cast< size_t >( k ) * D ) * 4];
+      if ( c[side] < 0 )
+      {
+        const uint32_t e = static_cast< uint32_t >( ~c[side] );
+        if ( e >= n || seen_leaf[e] ) return fail( ctx, BVHG_ERR_STATE, "leaf missing or reached twice" );
+        seen_leaf[e] = 1;
+        ++leaves;
+        maxd = d + 1 > maxd ? d + 1 : maxd;
+        const double *l = &lb[static_cast< size_t >( rank_of[e] ) * D * 2];
+        for ( int a = 0; a < D; ++a )
+          if ( slot[a * 4 + side * 2] != l[2 * a] || slot[a * 4 + side * 2 + 1] != l[2 * a + 1] )
+            return fail( ctx, BVHG_ERR_STATE, "leaf slot differs from leaf slabs" );
+      } else {
+        if ( static_cast< uint64_t >( c[side] ) >= m ) return fail( ctx, BVHG_ERR_STATE, "bad child index" );
+        const double *cs = &nb[( static_cast< size_t >( c[side] ) * D ) * 4];
+        for ( int a = 0; a < D; ++a )
+        {
+          const double lo = slot[a * 4 + side * 2], hi = slot[a * 4 + side * 2 + 1];
+          for ( int g = 0; g < 2; ++g )
+            if ( cs[a * 4 + g * 2] < lo || cs[a * 4 + g * 2 + 1] > hi )
+              return fail( ctx, BVHG_ERR_STATE, "child slabs escape the parent's slot" );
+        }
+        st.push_back( { c[side], d + 1 } );
+      }
+    }
+  }
+  if ( leaves != n || nodes != m ) return fail( ctx, BVHG_ERR_STATE, "node count is not 2n - 1" );
+  if ( depth_out ) *depth_out = maxd;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_last_candidates(bvhg_ctx *ctx, uint64_t *candidates)
+{
+  if ( !ctx || !candidates ) return BVHG_ERR_ARG;
+  *candidates = ctx->last_candidates;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_get_stage_times(bvhg_ctx *ctx, double *ms, uint64_t *launches)
+{
+  if ( !ctx ) return BVHG_ERR_ARG;
+  cudaSetDevice( ctx->cfg.device );
+  collect_timing( ctx );
+  for ( int s = 0; s < BVHG_NUM_STAGES; ++s )
+  {
+    if ( ms ) ms[s] = ctx->stage_ms[s];
+    if ( launches ) launches[s] = ctx->stage_launches[s];
+    ctx->stage_ms[s] = 0.0;
+    ctx->stage_launches[s] = 0;
+  }
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_launch_count(bvhg_ctx *ctx, uint64_t *launches)
+{
+  if ( !ctx || !launches ) return BVHG_ERR_ARG;
+  *launches = ctx->launches;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_set_spin_limit(bvhg_ctx *ctx, uint32_t limit)
+{
+  if ( !ctx ) return BVHG_ERR_ARG;
+  ctx->spin_limit = limit ? limit : ( ctx->cfg.spin_limit ? ctx->cfg.spin_limit : kDefaultSpinLimit );
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_test_stall_sort(bvhg_ctx *ctx, int32_t enable)
+{
+  if ( !ctx ) return BVHG_ERR_ARG;
+  ctx->stall_sort = enable ? 1 : 0;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_debug_normal(int32_t k, int32_t axis, int32_t comp, double *value, float *lo, float *hi)
+{
+  if ( ( k != 6 && k != 18 && k != 26 ) || axis < 0 || axis >= k / 2 || comp < 0 || comp > 2 ) return BVHG_ERR_ARG;
+  double v = 0.0;
+  float l = 0.f, h = 0.f;
+  if ( k == 6 )
+  {
+    v = normal_comp< 6 >( axis, comp );
+    l = normal_lo< 6 >( axis, comp );
+    h = normal_hi< 6 >( axis, comp );
+  } else if ( k == 18 ) {
+    v = normal_comp< 18 >( axis, comp );
+    l = normal_lo< 18 >( axis, comp );
+    h = normal_hi< 18 >( axis, comp );
+  } else {
+    v = normal_comp< 26 >( axis, comp );
+    l = normal_lo< 26 >( axis, comp );
+    h = normal_hi< 26 >( axis, comp );
+  }
+  if ( value ) *value = v;
+  if ( lo ) *lo = l;
+  if ( hi ) *hi = h;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_synchronize(bvhg_ctx *ctx)
+{
+  if ( !ctx ) return BVHG_ERR_ARG;
+  cudaSetDevice( ctx->cfg.device );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  for ( auto &o : ctx->objs )
+    if ( o && o->built && o->n > 0 )
+    {
+      bvhg_status st = check_scalar_errors( ctx, *o );
+      if ( st != BVHG_OK ) return st;
+    }
+  return BVHG_OK;
+}
+
+const char *bvhg_last_error(const bvhg_ctx *ctx)
+{
+  if ( !ctx ) return "null context";
+  return ctx->err.c_str();
+}
+
+const char *bvhg_status_string(bvhg_status status)
+{
+  switch ( status )
+  {
+    case BVHG_OK: return "ok";
+    case BVHG_ERR_ARG: return "invalid argument";
+    case BVHG_ERR_CUDA: return "CUDA error";
+    case BVHG_ERR_OVERFLOW: return "pair buffer overflow";
+    case BVHG_ERR_TIMEOUT: return "device wait timed out";
+    case BVHG_ERR_STATE: return "invalid state";
+    case BVHG_ERR_NOMEM: return "out of device memory";
+  }
+  return "unknown status";
+}
+
+}  // extern "C"

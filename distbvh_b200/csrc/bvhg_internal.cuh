@@ -1,0 +1,131 @@
+// bvhg_internal.cuh — device data layout shared by the kernels and the C ABI implementation.
+//
+// Per object of n elements with V vertices each and D = K/2 slabs (T = double in the FP64 form, float in the
+// FP32 form), all in HBM:
+//   verts      n * V * 3 doubles, element-major (input, owned copy or borrowed device pointer)
+//   cx, cy, cz n doubles each: centroids, structure of arrays (coalesced write in K1, read in K2)
+//   keys/vals  n u64 Morton keys and n u32 element indices, ping-ponged by the radix passes; after the sort
+//              keys[r], vals[r] hold the key and original index of rank r (vals = the permutation)
+//   leaf_box   n * D * 2 T: slabs of the element at rank r, [r][a][min,max] (the query side of traversal)
+//   node_box   (n - 1) * D * 2 * 2 T: both children's slabs of internal node k, [k][a][child][min,max], so one
+//              32-byte (FP64) or 16-byte (FP32) sector per axis tests both children
+//   child      (n - 1) int2: child index, >= 0 internal node, < 0 leaf with ~child = original element index
+//   range      (n - 1) int2: [first rank, last rank] covered by the node (self-collision pruning)
+//   parent     n + (n - 1) int32: parent * 2 + side of every leaf (rank order) and internal node (refit)
+//   exch       n - 1 int32: the agglomerative build's exchange slot per internal node (-1 = empty)
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bvhg {
+
+// Device-side scalars of one object (one allocation, read back for probes).
+struct obj_scalars
+{
+  unsigned long long bounds_enc[6];  // order-preserving encodings: min x,y,z then max x,y,z of cardinal slabs
+  double min3[3];                    // Morton bounds min (contact_entity.hpp:136-148)
+  double inv3[3];                    // 1 / (max - min)
+  int root;                          // root internal node, or ~elem when n == 1
+  int error;                         // bvhg_status raised by a kernel (first one wins)
+  unsigned int sort_tile_counter[64];// tile dispenser per radix pass
+};
+
+// Candidate/pair accumulators of one broadphase.
+struct pair_scalars
+{
+  unsigned long long count;   // pairs found (may exceed capacity)
+  unsigned long long count2;  // pairs surviving the FP64 recheck
+  int error;
+  int pad;
+};
+
+constexpr int kErrArg = 1;
+constexpr int kErrTimeout = 4;
+constexpr int kErrOverflowStack = 7;
+
+__host__ __device__ inline unsigned long long ord_encode(double x)
+{
+  unsigned long long b;
+#ifdef __CUDA_ARCH__
+  b = static_cast< unsigned long long >( __double_as_longlong( x ) );
+#else
+  __builtin_memcpy( &b, &x, 8 );
+#endif
+  return ( b & 0x8000000000000000ull ) ? ~b : ( b | 0x8000000000000000ull );
+}
+
+__host__ __device__ inline double ord_decode(unsigned long long e)
+{
+  const unsigned long long b = ( e & 0x8000000000000000ull ) ? ( e & 0x7fffffffffffffffull ) : ~e;
+  double x;
+#ifdef __CUDA_ARCH__
+  x = __longlong_as_double( static_cast< long long >( b ) );
+#else
+  __builtin_memcpy( &x, &b, 8 );
+#endif
+  return x;
+}
+
+// Radix sort geometry: 63 significant key bits (morton64 never sets bit 63, hash.hpp:100-103).
+constexpr int kKeyBits = 63;
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+inline int sort_passes(int bits) { return ( kKeyBits + bits - 1 ) / bits; }
+
+// ---- launch wrappers (one per kernel family), implemented in the k_*.cu files ----
+// All return cudaGetLastError() of the launch.
+
+cudaError_t launch_centroid_bounds(int K, const double *verts, uint32_t V, uint64_t n, double eps, double *cx,
+                                   double *cy, double *cz, obj_scalars *sc, cudaStream_t s);
+
+cudaError_t launch_keys_hist(int bits, const double *cx, const double *cy, const double *cz, uint64_t n,
+                             obj_scalars *sc, uint64_t *keys, uint32_t *hist, cudaStream_t s);
+
+cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
+                            uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
+                            obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s);
+
+// Leaf slabs + agglomerative LBVH build + bottom-up refit in one pass (FP64 or FP32 slabs).
+cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
+                         const uint64_t *keys, const uint32_t *vals, void *leaf_box, void *node_box, int2 *child,
+                         int2 *range, int *parent, int *exch, obj_scalars *sc, cudaStream_t s);
+
+// Refit with the topology of the last build: recompute leaf slabs and every internal node.
+cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
+                         const uint32_t *vals, void *leaf_box, void *node_box, const int *parent, int *exch,
+                         obj_scalars *sc, cudaStream_t s);
+
+struct tree_view
+{
+  const void *node_box;
+  const int2 *child;
+  const int2 *range;
+  const void *leaf_box;
+  const uint32_t *perm;
+  uint64_t n;
+  const obj_scalars *sc;
+};
+
+// Queries every leaf of q against tree t; writes (q element, t element) local index pairs.
+cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, uint2 *pairs, uint64_t cap,
+                            pair_scalars *ps, cudaStream_t s);
+
+// FP64 recheck of FP32 candidates: keeps (a, b) iff the FP64 slabs of a and b overlap, compacted into out.
+// The candidate count is min(ps->count, cand_cap), read on the device.
+cudaError_t launch_recheck(int K, const double *verts_a, uint32_t Va, const double *verts_b, uint32_t Vb,
+                           double eps, const uint2 *cand, uint64_t cand_cap, uint2 *out, uint64_t cap,
+                           pair_scalars *ps, cudaStream_t s);
+
+// Writes pairs as global ids: out[2p] = gid_a[a] (or a), out[2p + 1] = gid_b[b] (or b); normalize orders each
+// pair by local index first (self-collision).
+cudaError_t launch_gid_pairs(const uint2 *pairs, uint64_t count, const uint64_t *gid_a, const uint64_t *gid_b,
+                             bool normalize, uint64_t *out, cudaStream_t s);
+
+// Original-order probes.
+cudaError_t launch_probe_kdops(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
+                               void *out, cudaStream_t s);
+
+}  // namespace bvhg

@@ -1,0 +1,232 @@
+// k_sort.cu — stable LSD radix sort of (63-bit Morton key, u32 element index) pairs.
+//
+// Replaces radix_sorter<T, Idx> (src/bvh/util/sort.hpp:75-144), which makes 8*sizeof(T) one-bit passes of
+// three kernels each (flag map, exclusive scan, split scatter). A stable sort's output is unique, so any digit
+// width yields the reference's permutation; BITS = 1 is the reference's one-bit-per-pass schedule, BITS = 8 the
+// fast one. Bit 63 of a morton64 key is always zero (hash.hpp:100-103), so ceil(63 / BITS) passes cover it.
+//
+// One kernel per pass, onesweep style: all digit histograms come from the key kernel (one read of the keys);
+// each block takes a tile of 4096 keys in launch order from an atomic tile counter, ranks them with warp-level
+// match (stable within the tile), publishes its per-digit counts, resolves its global offsets by decoupled
+// look-back over the preceding tiles' status words, reorders the tile in shared memory and writes contiguous
+// digit runs. Every look-back wait is bounded: past spin_limit polls the block records BVHG_ERR_TIMEOUT and
+// goes on with a garbage offset (the host reports the error; no thread waits forever).
+#include "bvhg_internal.cuh"
+
+namespace bvhg {
+namespace {
+
+constexpr uint32_t kFlagAggregate = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kValueMask = ( 1u << 30 ) - 1;
+constexpr int kWarps = kSortThreads / 32;
+
+// Exclusive scan of one value per thread over a 256-thread block.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s_warp)
+{
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for ( int o = 1; o < 32; o <<= 1 )
+  {
+    const uint32_t y = __shfl_up_sync( 0xffffffffu, inc, o );
+    if ( lane >= o ) inc += y;
+  }
+  if ( lane == 31 ) s_warp[w] = inc;
+  __syncthreads();
+  uint32_t wpre = 0;
+#pragma unroll
+  for ( int k = 0; k < kWarps; ++k )
+    if ( k < w ) wpre += s_warp[k];
+  __syncthreads();
+  return wpre + inc - x;
+}
+
+template< int BITS >
+__global__ void __launch_bounds__( kSortThreads ) k_onesweep(const uint64_t *__restrict__ keys_in,
+                                                           const uint32_t *__restrict__ vals_in,
+                                                           uint64_t *__restrict__ keys_out,
+                                                           uint32_t *__restrict__ vals_out, uint64_t n, int pass,
+                                                           const uint32_t *__restrict__ hist, uint32_t *status,
+                                                           obj_scalars *sc, uint32_t spin_limit, int stall)
+{
+  constexpr int RADIX = 1 << BITS;
+  constexpr uint32_t MASK = RADIX - 1;
+  extern __shared__ uint64_t s_keys[];  // kSortTile keys, then kSortTile vals
+  uint32_t *s_vals = reinterpret_cast< uint32_t * >( s_keys + kSortTile );
+  __shared__ uint32_t s_whist[kWarps][RADIX];
+  __shared__ uint32_t s_gbase[RADIX];
+  __shared__ uint32_t s_lstart[RADIX];
+  __shared__ uint32_t s_scan[kWarps];
+  __shared__ int s_tile;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int shift = pass * BITS;
+  if ( tid == 0 ) s_tile = static_cast< int >( atomicAdd( &sc->sort_tile_counter[pass], 1u ) );
+  for ( int k = tid; k < kWarps * RADIX; k += kSortThreads ) ( &s_whist[0][0] )[k] = 0;
+  __syncthreads();
+  const uint64_t tile = static_cast< uint64_t >( s_tile );
+  const uint64_t tile_base = tile * kSortTile;
+  const uint64_t wbase = tile_base + static_cast< uint64_t >( warp ) * ( kSortItems * 32 );
+
+  uint64_t k[kSortItems];
+  uint32_t v[kSortItems];
+  uint32_t rk[kSortItems];
+#pragma unroll
+  for ( int j = 0; j < kSortItems; ++j )
+  {
+    const uint64_t idx = wbase + j * 32 + lane;
+    if ( idx < n )
+    {
+      k[j] = keys_in[idx];
+      v[j] = vals_in ? vals_in[idx] : static_cast< uint32_t >( idx );
+    } else {
+      k[j] = 0;
+      v[j] = 0;
+    }
+  }
+  const unsigned lt_mask = ( 1u << lane ) - 1u;
+#pragma unroll
+  for ( int j = 0; j < kSortItems; ++j )
+  {
+    const bool valid = ( wbase + j * 32 + lane ) < n;
+    const uint32_t d = valid ? static_cast< uint32_t >( ( k[j] >> shift ) & MASK ) : RADIX;
+    const unsigned peers = __match_any_sync( 0xffffffffu, d );
+    const unsigned lower = peers & lt_mask;
+    const uint32_t base = valid ? s_whist[warp][d] : 0u;
+    __syncwarp();
+    if ( valid && lower == 0 ) s_whist[warp][d] = base + static_cast< uint32_t >( __popc( peers ) );
+    __syncwarp();
+    rk[j] = base + static_cast< uint32_t >( __popc( lower ) );
+  }
+  __syncthreads();
+
+  // Per digit: exclusive prefix over warps (in place) and the tile total.
+  uint32_t total = 0;
+  if ( tid < RADIX )
+  {
+#pragma unroll
+    for ( int w = 0; w < kWarps; ++w )
+    {
+      const uint32_t c = s_whist[w][tid];
+      s_whist[w][tid] = total;
+      total += c;
+    }
+    volatile uint32_t *st = status + tile * RADIX;
+    st[tid] = ( tile == 0 ? kFlagPrefix : kFlagAggregate ) | total;
+  }
+  const uint32_t g = ( tid < RADIX ) ? hist[tid] : 0u;
+  const uint32_t gexcl = block_exclusive_scan( g, s_scan );
+  const uint32_t lexcl = block_exclusive_scan( tid < RADIX ? total : 0u, s_scan );
+
+  if ( tid < RADIX )
+  {
+    uint32_t excl = 0;
+    if ( tile > 0 )
+    {
+      // Test hook: poll the spare status row after the last tile, which no block ever publishes.
+      int64_t p = stall ? static_cast< int64_t >( gridDim.x ) : static_cast< int64_t >( tile ) - 1;
+      uint32_t spins = 0;
+      while ( true )
+      {
+        const uint32_t s = reinterpret_cast< volatile uint32_t * >( status )[p * RADIX + tid];
+        const uint32_t flag = s & ~kValueMask;
+        if ( flag == 0 )
+        {
+          if ( ++spins > spin_limit )
+          {
+            atomicCAS( &sc->error, 0, kErrTimeout );
+            __threadfence();
+            break;
+          }
+          __nanosleep( 32 );
+          continue;
+        }
+        excl += s & kValueMask;
+        if ( flag == kFlagPrefix || p == 0 || stall ) break;
+        --p;
+      }
+      reinterpret_cast< volatile uint32_t * >( status )[tile * RADIX + tid] = kFlagPrefix | ( ( excl + total ) & kValueMask );
+    }
+    s_gbase[tid] = gexcl + excl - lexcl;
+    s_lstart[tid] = lexcl;
+  }
+  // A block that timed out published a garbage prefix (so that no successor waits forever) and raised the
+  // object's error word before doing so; every block that could have read such a prefix sees the word here and
+  // writes nothing.
+  __shared__ int s_err;
+  __syncthreads();
+  if ( tid == 0 )
+  {
+    __threadfence();
+    s_err = *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout;
+  }
+  __syncthreads();
+  if ( s_err ) return;
+
+#pragma unroll
+  for ( int j = 0; j < kSortItems; ++j )
+  {
+    if ( ( wbase + j * 32 + lane ) < n )
+    {
+      const uint32_t d = static_cast< uint32_t >( ( k[j] >> shift ) & MASK );
+      const uint32_t pos = s_lstart[d] + s_whist[warp][d] + rk[j];
+      s_keys[pos] = k[j];
+      s_vals[pos] = v[j];
+    }
+  }
+  __syncthreads();
+
+  const uint32_t cnt = static_cast< uint32_t >( min( static_cast< uint64_t >( kSortTile ), n - tile_base ) );
+  for ( uint32_t i = tid; i < cnt; i += kSortThreads )
+  {
+    const uint64_t key = s_keys[i];
+    const uint32_t d = static_cast< uint32_t >( ( key >> shift ) & MASK );
+    const uint32_t gp = s_gbase[d] + i;
+    if ( gp < n )
+    {
+      keys_out[gp] = key;
+      vals_out[gp] = s_vals[i];
+    }
+  }
+}
+
+template< int BITS >
+cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out, uint32_t *vals_out,
+                        uint64_t n, int pass, const uint32_t *hist, uint32_t *status, obj_scalars *sc,
+                        uint32_t spin_limit, int stall, cudaStream_t s)
+{
+  constexpr int RADIX = 1 << BITS;
+  const size_t smem = static_cast< size_t >( kSortTile ) * ( sizeof( uint64_t ) + sizeof( uint32_t ) );
+  static bool configured = false;
+  if ( !configured )
+  {
+    cudaError_t e = cudaFuncSetAttribute( k_onesweep< BITS >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast< int >( smem ) );
+    if ( e != cudaSuccess ) return e;
+    configured = true;
+  }
+  const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
+  k_onesweep< BITS ><<< static_cast< unsigned >( tiles ), kSortThreads, smem, s >>>(
+    keys_in, vals_in, keys_out, vals_out, n, pass, hist + static_cast< size_t >( pass ) * RADIX,
+    status + static_cast< size_t >( pass ) * ( tiles + 1 ) * RADIX, sc, spin_limit, stall );
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
+                            uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
+                            obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s)
+{
+  switch ( bits )
+  {
+    case 1: return launch_os_t< 1 >( keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc, spin_limit, stall, s );
+    case 2: return launch_os_t< 2 >( keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc, spin_limit, stall, s );
+    case 4: return launch_os_t< 4 >( keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc, spin_limit, stall, s );
+    case 8: return launch_os_t< 8 >( keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc, spin_limit, stall, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace bvhg

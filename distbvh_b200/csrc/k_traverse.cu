@@ -1,0 +1,293 @@
+// k_traverse.cu — tree traversal emitting candidate element pairs (K6), FP64 recheck (K7), gid output.
+//
+// The reference finds pairs with a 4-way simultaneous recursion over two trees (get_overlapping_indices,
+// src/bvh/collision_query.hpp:293-329) or a per-entity descent (query_tree, collision_query.hpp:166-213), both
+// pruning on the strict all-slab overlap (kdop.hpp:120-125, 538-549). Here each thread takes one leaf of the query
+// object, in Morton order so that a warp's queries are spatially coherent, and descends the other object's tree
+// with an explicit stack: both children of a node are tested from one 32-byte (FP64) / 16-byte (FP32) sector per
+// slab, with early exit on the first separating slab. Leaf-leaf overlaps are emitted as (query element, tree
+// element) local indices through a global atomic counter; pairs beyond capacity are counted but not stored, so
+// the host can grow the buffer and retry.
+//
+// Self-collision (self_collision_set, collision_query.hpp:331-368): the query leaf of rank i only visits
+// subtrees holding ranks > i (internal node k splits its range [l, r] into [l, k] and [k + 1, r]), so every
+// unordered pair is found once and no element is paired with itself.
+#include "bvhg_internal.cuh"
+#include "kdop_math.cuh"
+
+namespace bvhg {
+namespace {
+
+constexpr int kTravThreads = 128;
+constexpr int kStack = 96;  // radix tree over 96-bit (key, rank) pairs: at most 95 internal levels
+
+template< typename T >
+struct slab_pair;
+
+// Both children's (min, max) of one slab.
+template<>
+struct slab_pair< double >
+{
+  double min0, max0, min1, max1;
+  __device__ static slab_pair load(const double *p)
+  {
+    const double2 a = __ldg( reinterpret_cast< const double2 * >( p ) );
+    const double2 b = __ldg( reinterpret_cast< const double2 * >( p ) + 1 );
+    return { a.x, a.y, b.x, b.y };
+  }
+};
+
+template<>
+struct slab_pair< float >
+{
+  float min0, max0, min1, max1;
+  __device__ static slab_pair load(const float *p)
+  {
+    const float4 a = __ldg( reinterpret_cast< const float4 * >( p ) );
+    return { a.x, a.y, a.z, a.w };
+  }
+};
+
+__device__ __forceinline__ void emit(uint32_t a, uint32_t b, uint2 *pairs, uint64_t cap, pair_scalars *ps)
+{
+  const unsigned long long p = atomicAdd( &ps->count, 1ull );
+  if ( p < cap ) pairs[p] = make_uint2( a, b );
+}
+
+template< int K, typename T >
+__global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict__ qbox,
+                                                           const uint32_t *__restrict__ qperm, uint32_t nq,
+                                                           const int2 *__restrict__ child,
+                                                           const T *__restrict__ nbox,
+                                                           const int2 *__restrict__ range,
+                                                           const T *__restrict__ tleaf,
+                                                           const obj_scalars *__restrict__ tsc, uint32_t nt,
+                                                           const obj_scalars *__restrict__ qsc, int self,
+                                                           uint2 *pairs, uint64_t cap, pair_scalars *ps)
+{
+  constexpr int D = K / 2;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ( i >= nq ) return;
+  // No tree exists after a failed sort of either object.
+  if ( *reinterpret_cast< const volatile int * >( &tsc->error ) == kErrTimeout ||
+       *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
+    return;
+  T qlo[D], qhi[D];
+#pragma unroll
+  for ( int a = 0; a < D; ++a )
+  {
+    qlo[a] = __ldg( qbox + ( static_cast< size_t >( i ) * D + a ) * 2 );
+    qhi[a] = __ldg( qbox + ( static_cast< size_t >( i ) * D + a ) * 2 + 1 );
+  }
+  const uint32_t qe = __ldg( qperm + i );
+  const int root = tsc->root;
+  if ( nt == 1 )
+  {
+    if ( self ) return;
+    bool o = true;
+#pragma unroll
+    for ( int a = 0; a < D; ++a ) o = o && ( qlo[a] < tleaf[2 * a + 1] && tleaf[2 * a] < qhi[a] );
+    if ( o ) emit( qe, static_cast< uint32_t >( ~root ), pairs, cap, ps );
+    return;
+  }
+  int stack[kStack];
+  int sp = 0;
+  int node = root;
+  while ( true )
+  {
+    const int2 c = __ldg( child + node );
+    const T *nb = nbox + static_cast< size_t >( node ) * D * 4;
+    bool o0 = true, o1 = true;
+    if ( self )
+    {
+      // left child covers ranks [l, node], right child [node + 1, r]
+      o0 = node > static_cast< int >( i );
+      o1 = __ldg( &range[node].y ) > static_cast< int >( i );
+    }
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      if ( !( o0 || o1 ) ) break;
+      const slab_pair< T > s = slab_pair< T >::load( nb + a * 4 );
+      o0 = o0 && ( qlo[a] < s.max0 && s.min0 < qhi[a] );
+      o1 = o1 && ( qlo[a] < s.max1 && s.min1 < qhi[a] );
+    }
+    int next = -1;
+    if ( o0 )
+    {
+      if ( c.x < 0 ) emit( qe, static_cast< uint32_t >( ~c.x ), pairs, cap, ps );
+      else next = c.x;
+    }
+    if ( o1 )
+    {
+      if ( c.y < 0 ) emit( qe, static_cast< uint32_t >( ~c.y ), pairs, cap, ps );
+      else if ( next < 0 ) next = c.y;
+      else
+      {
+        if ( sp == kStack )
+        {
+          atomicCAS( &ps->error, 0, kErrOverflowStack );
+          return;
+        }
+        stack[sp++] = c.y;
+      }
+    }
+    if ( next < 0 )
+    {
+      if ( sp == 0 ) break;
+      next = stack[--sp];
+    }
+    node = next;
+  }
+}
+
+template< int K, typename T >
+cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, uint2 *pairs, uint64_t cap, pair_scalars *ps,
+                          cudaStream_t s)
+{
+  const unsigned grid = static_cast< unsigned >( ( q.n + kTravThreads - 1 ) / kTravThreads );
+  k_traverse< K, T ><<< grid, kTravThreads, 0, s >>>(
+    static_cast< const T * >( q.leaf_box ), q.perm, static_cast< uint32_t >( q.n ), t.child,
+    static_cast< const T * >( t.node_box ), t.range, static_cast< const T * >( t.leaf_box ), t.sc,
+    static_cast< uint32_t >( t.n ), q.sc, self ? 1 : 0, pairs, cap, ps );
+  return cudaGetLastError();
+}
+
+// K7: FP64 slabs of both elements from their vertices, slab by slab with early exit.
+template< int K, int VA, int VB >
+__global__ void __launch_bounds__( 256 ) k_recheck(const double *__restrict__ va, uint32_t Var,
+                                                 const double *__restrict__ vb, uint32_t Vbr, double eps,
+                                                 const uint2 *__restrict__ cand, uint64_t cand_cap, uint2 *out,
+                                                 uint64_t cap, pair_scalars *ps)
+{
+  constexpr int D = K / 2;
+  // The candidate count is read on the device: no host round trip between traversal and recheck.
+  const uint64_t ncand = min( static_cast< uint64_t >( *reinterpret_cast< volatile unsigned long long * >( &ps->count ) ),
+                              cand_cap );
+  const int Va = VA > 0 ? VA : static_cast< int >( Var );
+  const int Vb = VB > 0 ? VB : static_cast< int >( Vbr );
+  for ( uint64_t p = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; p < ncand;
+        p += static_cast< uint64_t >( gridDim.x ) * blockDim.x )
+  {
+    const uint2 c = __ldg( cand + p );
+    const double *pa = va + static_cast< size_t >( c.x ) * Va * 3;
+    const double *pb = vb + static_cast< size_t >( c.y ) * Vb * 3;
+    double xa[VA > 0 ? VA * 3 : 24], xb[VB > 0 ? VB * 3 : 24];
+    bool ok = true;
+    if constexpr ( VA > 0 && VB > 0 )
+    {
+#pragma unroll
+      for ( int k = 0; k < VA * 3; ++k ) xa[k] = __ldg( pa + k );
+#pragma unroll
+      for ( int k = 0; k < VB * 3; ++k ) xb[k] = __ldg( pb + k );
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
+      {
+        if ( !ok ) break;
+        double alo, ahi, blo, bhi;
+        slab64< K >( xa, VA, a, eps, alo, ahi );
+        slab64< K >( xb, VB, a, eps, blo, bhi );
+        ok = alo < bhi && blo < ahi;
+      }
+    } else {
+      (void)xa;
+      (void)xb;
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
+      {
+        if ( !ok ) break;
+        double alo = 0, ahi = 0, blo = 0, bhi = 0;
+        for ( int v = 0; v < Va; ++v )
+        {
+          const double q[3] = { __ldg( pa + 3 * v ), __ldg( pa + 3 * v + 1 ), __ldg( pa + 3 * v + 2 ) };
+          double l, h;
+          slab64< K >( q, 1, a, eps, l, h );
+          alo = v ? std_min( alo, l ) : l;
+          ahi = v ? std_max( ahi, h ) : h;
+        }
+        for ( int v = 0; v < Vb; ++v )
+        {
+          const double q[3] = { __ldg( pb + 3 * v ), __ldg( pb + 3 * v + 1 ), __ldg( pb + 3 * v + 2 ) };
+          double l, h;
+          slab64< K >( q, 1, a, eps, l, h );
+          blo = v ? std_min( blo, l ) : l;
+          bhi = v ? std_max( bhi, h ) : h;
+        }
+        ok = alo < bhi && blo < ahi;
+      }
+    }
+    if ( ok )
+    {
+      const unsigned long long o = atomicAdd( &ps->count2, 1ull );
+      if ( o < cap ) out[o] = c;
+    }
+  }
+}
+
+template< int K >
+cudaError_t recheck_k(const double *va, uint32_t Va, const double *vb, uint32_t Vb, double eps, const uint2 *cand,
+                      uint64_t ncand, uint2 *out, uint64_t cap, pair_scalars *ps, cudaStream_t s)
+{
+  const unsigned grid = 148 * 8;
+  if ( Va == 3 && Vb == 3 ) k_recheck< K, 3, 3 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
+  else if ( Va == 4 && Vb == 4 ) k_recheck< K, 4, 4 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
+  else if ( Va == 8 && Vb == 8 ) k_recheck< K, 8, 8 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
+  else k_recheck< K, 0, 0 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
+  return cudaGetLastError();
+}
+
+__global__ void k_gid_pairs(const uint2 *__restrict__ pairs, uint64_t count, const uint64_t *__restrict__ gid_a,
+                            const uint64_t *__restrict__ gid_b, int normalize, uint64_t *__restrict__ out)
+{
+  for ( uint64_t p = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; p < count;
+        p += static_cast< uint64_t >( gridDim.x ) * blockDim.x )
+  {
+    uint2 c = pairs[p];
+    if ( normalize && c.x > c.y ) c = make_uint2( c.y, c.x );
+    const uint64_t a = gid_a ? __ldg( gid_a + c.x ) : c.x;
+    const uint64_t b = gid_b ? __ldg( gid_b + c.y ) : c.y;
+    reinterpret_cast< ulonglong2 * >( out )[p] = make_ulonglong2( a, b );
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, uint2 *pairs, uint64_t cap,
+                            pair_scalars *ps, cudaStream_t s)
+{
+  switch ( K )
+  {
+    case 6: return fp32 ? launch_trav_t< 6, float >( q, t, self, pairs, cap, ps, s )
+                        : launch_trav_t< 6, double >( q, t, self, pairs, cap, ps, s );
+    case 18: return fp32 ? launch_trav_t< 18, float >( q, t, self, pairs, cap, ps, s )
+                         : launch_trav_t< 18, double >( q, t, self, pairs, cap, ps, s );
+    case 26: return fp32 ? launch_trav_t< 26, float >( q, t, self, pairs, cap, ps, s )
+                         : launch_trav_t< 26, double >( q, t, self, pairs, cap, ps, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_recheck(int K, const double *verts_a, uint32_t Va, const double *verts_b, uint32_t Vb, double eps,
+                           const uint2 *cand, uint64_t ncand, uint2 *out, uint64_t cap, pair_scalars *ps,
+                           cudaStream_t s)
+{
+  switch ( K )
+  {
+    case 6: return recheck_k< 6 >( verts_a, Va, verts_b, Vb, eps, cand, ncand, out, cap, ps, s );
+    case 18: return recheck_k< 18 >( verts_a, Va, verts_b, Vb, eps, cand, ncand, out, cap, ps, s );
+    case 26: return recheck_k< 26 >( verts_a, Va, verts_b, Vb, eps, cand, ncand, out, cap, ps, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_gid_pairs(const uint2 *pairs, uint64_t count, const uint64_t *gid_a, const uint64_t *gid_b,
+                             bool normalize, uint64_t *out, cudaStream_t s)
+{
+  if ( count == 0 ) return cudaSuccess;
+  const uint64_t blocks = ( count + 255 ) / 256;
+  const unsigned grid = static_cast< unsigned >( blocks < 148 * 8 ? blocks : 148 * 8 );
+  k_gid_pairs<<< grid, 256, 0, s >>>( pairs, count, gid_a, gid_b, normalize ? 1 : 0, out );
+  return cudaGetLastError();
+}
+
+}  // namespace bvhg

@@ -1,0 +1,395 @@
+// k_tree.cu — leaf slabs, LBVH build and bottom-up k-DOP refit in one kernel (K4 + K5).
+//
+// The reference builds its element trees on the host, top-down (top_down_builder, src/bvh/bvh_build.hpp:55-139,
+// mean split on the longest axis) or with a serial Morton bottom-up builder (bvh_build.hpp:145-296). Both give
+// one element per leaf and node k-DOP = union of the subtree (bvh_build.hpp:109-124; kdop merge, kdop.hpp:558-569),
+// so the pair set of a strict-overlap traversal does not depend on the tree shape. Here the tree is the binary
+// radix tree over the sorted Morton keys (Karras), built bottom-up agglomeratively (Apetrei): one thread per leaf
+// climbs while it is the second of two children to arrive at a node, merging ranges by comparing the
+// dissimilarity of the keys just outside its range, and writes each subtree's slabs into its parent as it goes.
+// Ties among equal keys are broken by rank, i.e. the tree is the radix tree of the 96-bit (key, rank) pairs.
+//
+// No thread ever waits: the first arrival at a node leaves, the second continues. Writes of the first arrival
+// are published with __threadfence before its atomicExch; the second arrival fences and reads them through L2.
+#include "bvhg_internal.cuh"
+#include "kdop_math.cuh"
+
+namespace bvhg {
+
+namespace {
+
+constexpr int kBuildThreads = 256;
+
+// epsilon rounded up to FP32 (host side).
+float f32_up(double x)
+{
+  if ( x == 0.0 ) return 0.f;
+  float f = static_cast< float >( x );
+  if ( static_cast< double >( f ) < x ) f = nextafterf( f, INFINITY );
+  return f;
+}
+
+// Dissimilarity of ranks j and j + 1: 33 + highest differing key bit when the keys differ, else
+// 1 + highest differing bit of the ranks. Larger = more different.
+__device__ __forceinline__ int delta(const uint64_t *__restrict__ keys, int j)
+{
+  const uint64_t x = __ldg( keys + j ) ^ __ldg( keys + j + 1 );
+  if ( x ) return 96 - __clzll( static_cast< long long >( x ) );
+  return 32 - __clz( j ^ ( j + 1 ) );
+}
+
+template< typename T >
+struct box_io;
+
+template<>
+struct box_io< double >
+{
+  __device__ static void store2(double *p, double lo, double hi) { *reinterpret_cast< double2 * >( p ) = make_double2( lo, hi ); }
+  __device__ static void load2_cg(const double *p, double &lo, double &hi)
+  {
+    const double2 v = __ldcg( reinterpret_cast< const double2 * >( p ) );
+    lo = v.x;
+    hi = v.y;
+  }
+  __device__ static double mn(double a, double b) { return ( b < a ) ? b : a; }
+  __device__ static double mx(double a, double b) { return ( a < b ) ? b : a; }
+};
+
+template<>
+struct box_io< float >
+{
+  __device__ static void store2(float *p, float lo, float hi) { *reinterpret_cast< float2 * >( p ) = make_float2( lo, hi ); }
+  __device__ static void load2_cg(const float *p, float &lo, float &hi)
+  {
+    const float2 v = __ldcg( reinterpret_cast< const float2 * >( p ) );
+    lo = v.x;
+    hi = v.y;
+  }
+  __device__ static float mn(float a, float b) { return fminf( a, b ); }
+  __device__ static float mx(float a, float b) { return fmaxf( a, b ); }
+};
+
+// Slabs of element e (gathered vertices) into lo/hi.
+template< int K, typename T, int VT >
+__device__ __forceinline__ void leaf_slabs(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
+                                           float eps_hi, T *lo, T *hi)
+{
+  constexpr int D = K / 2;
+  constexpr int VMAX = VT > 0 ? VT : 32;
+  const int V = VT > 0 ? VT : static_cast< int >( Vrt );
+  double p[VT > 0 ? VT * 3 : 3];
+  const double *src = verts + static_cast< size_t >( e ) * V * 3;
+  if constexpr ( VT > 0 )
+  {
+#pragma unroll
+    for ( int k = 0; k < VT * 3; ++k ) p[k] = __ldg( src + k );
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      if constexpr ( sizeof( T ) == 8 )
+      {
+        double l, h;
+        slab64< K >( p, VT, a, eps, l, h );
+        lo[a] = l;
+        hi[a] = h;
+      } else {
+        float l, h;
+        slab32< K >( p, VT, a, eps_hi, l, h );
+        lo[a] = l;
+        hi[a] = h;
+      }
+    }
+  } else {
+    (void)VMAX;
+    (void)p;
+    // Generic vertex count: one vertex at a time, slab by slab (vertices re-read from L1).
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      if constexpr ( sizeof( T ) == 8 )
+      {
+        double l = 0, h = 0;
+        for ( int v = 0; v < V; ++v )
+        {
+          const double q[3] = { __ldg( src + 3 * v ), __ldg( src + 3 * v + 1 ), __ldg( src + 3 * v + 2 ) };
+          double vl, vh;
+          slab64< K >( q, 1, a, eps, vl, vh );
+          if ( v == 0 )
+          {
+            l = vl;
+            h = vh;
+          } else {
+            l = std_min( l, vl );
+            h = std_max( h, vh );
+          }
+        }
+        lo[a] = l;
+        hi[a] = h;
+      } else {
+        float l = 0, h = 0;
+        for ( int v = 0; v < V; ++v )
+        {
+          const double q[3] = { __ldg( src + 3 * v ), __ldg( src + 3 * v + 1 ), __ldg( src + 3 * v + 2 ) };
+          float vl, vh;
+          slab32< K >( q, 1, a, eps_hi, vl, vh );
+          if ( v == 0 )
+          {
+            l = vl;
+            h = vh;
+          } else {
+            l = fminf( l, vl );
+            h = fmaxf( h, vh );
+          }
+        }
+        lo[a] = l;
+        hi[a] = h;
+      }
+    }
+  }
+}
+
+template< int K, typename T, int VT >
+__global__ void __launch_bounds__( kBuildThreads ) k_build(const double *__restrict__ verts, uint32_t Vrt, int n,
+                                                         double eps, float eps_hi,
+                                                         const uint64_t *__restrict__ keys,
+                                                         const uint32_t *__restrict__ vals, T *__restrict__ leaf_box,
+                                                         T *node_box, int *child, int2 *__restrict__ range,
+                                                         int *__restrict__ parent, int *exch, obj_scalars *sc)
+{
+  constexpr int D = K / 2;
+  using io = box_io< T >;
+  const int i = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
+  if ( i >= n ) return;
+  // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word).
+  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
+  const uint32_t e = __ldg( vals + i );
+  if ( e >= static_cast< uint32_t >( n ) )
+  {
+    atomicCAS( &sc->error, 0, kErrTimeout );
+    return;
+  }
+  T lo[D], hi[D];
+  leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
+#pragma unroll
+  for ( int a = 0; a < D; ++a ) io::store2( leaf_box + ( static_cast< size_t >( i ) * D + a ) * 2, lo[a], hi[a] );
+  if ( n == 1 )
+  {
+    sc->root = ~static_cast< int >( e );
+    return;
+  }
+  int l = i, r = i;
+  int node = ~static_cast< int >( e );
+  int self_slot = i;  // index into parent[]: leaves [0, n), internal nodes n + k
+  while ( true )
+  {
+    bool left_child;  // true: this subtree is the left child of internal node r
+    if ( l == 0 ) left_child = true;
+    else if ( r == n - 1 ) left_child = false;
+    else left_child = delta( keys, r ) < delta( keys, l - 1 );
+    const int par = left_child ? r : l - 1;
+    const int side = left_child ? 0 : 1;
+    T *pb = node_box + static_cast< size_t >( par ) * D * 4;
+#pragma unroll
+    for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
+    child[2 * par + side] = node;
+    parent[self_slot] = 2 * par + side;
+    __threadfence();
+    const int other = atomicExch( exch + par, left_child ? l : r );
+    if ( other < 0 ) return;  // first arrival: the sibling's thread finishes this node
+    __threadfence();
+    if ( left_child ) r = other;
+    else l = other;
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      T sl, sh;
+      io::load2_cg( pb + a * 4 + ( 1 - side ) * 2, sl, sh );
+      lo[a] = io::mn( lo[a], sl );
+      hi[a] = io::mx( hi[a], sh );
+    }
+    range[par] = make_int2( l, r );
+    node = par;
+    self_slot = n + par;
+    if ( l == 0 && r == n - 1 )
+    {
+      sc->root = par;
+      return;
+    }
+  }
+}
+
+// Refit with a fixed topology: leaf slabs again (elements keep their ranks), then the same first/second arrival
+// climb along the stored parent links. exch must be reset to -1 before the launch.
+template< int K, typename T, int VT >
+__global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restrict__ verts, uint32_t Vrt, int n,
+                                                         double eps, float eps_hi, const uint32_t *__restrict__ vals,
+                                                         T *__restrict__ leaf_box, T *node_box,
+                                                         const int *__restrict__ parent, int *exch,
+                                                         const obj_scalars *__restrict__ sc)
+{
+  constexpr int D = K / 2;
+  using io = box_io< T >;
+  const int i = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
+  if ( i >= n ) return;
+  const uint32_t e = __ldg( vals + i );
+  T lo[D], hi[D];
+  leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
+#pragma unroll
+  for ( int a = 0; a < D; ++a ) io::store2( leaf_box + ( static_cast< size_t >( i ) * D + a ) * 2, lo[a], hi[a] );
+  if ( n == 1 ) return;
+  const int root = sc->root;
+  int slot = i;
+  while ( true )
+  {
+    const int ps = __ldg( parent + slot );
+    const int par = ps >> 1, side = ps & 1;
+    T *pb = node_box + static_cast< size_t >( par ) * D * 4;
+#pragma unroll
+    for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
+    __threadfence();
+    const int other = atomicExch( exch + par, 1 );
+    if ( other < 0 ) return;
+    __threadfence();
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      T sl, sh;
+      io::load2_cg( pb + a * 4 + ( 1 - side ) * 2, sl, sh );
+      lo[a] = io::mn( lo[a], sl );
+      hi[a] = io::mx( hi[a], sh );
+    }
+    if ( par == root ) return;
+    slot = n + par;
+  }
+}
+
+template< int K, typename T, int VT >
+cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys,
+                           const uint32_t *vals, void *leaf_box, void *node_box, int2 *child, int2 *range, int *parent,
+                           int *exch, obj_scalars *sc, cudaStream_t s)
+{
+  const float eps_hi = f32_up( eps );
+  const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
+  k_build< K, T, VT ><<< grid, kBuildThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals,
+                                                       static_cast< T * >( leaf_box ), static_cast< T * >( node_box ),
+                                                       reinterpret_cast< int * >( child ), range, parent, exch, sc );
+  return cudaGetLastError();
+}
+
+template< int K, typename T, int VT >
+cudaError_t launch_refit_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
+                           void *leaf_box, void *node_box, const int *parent, int *exch, const obj_scalars *sc,
+                           cudaStream_t s)
+{
+  const float eps_hi = f32_up( eps );
+  const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
+  k_refit< K, T, VT ><<< grid, kBuildThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, eps_hi, vals,
+                                                       static_cast< T * >( leaf_box ), static_cast< T * >( node_box ),
+                                                       parent, exch, sc );
+  return cudaGetLastError();
+}
+
+template< int K, typename T >
+cudaError_t build_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys, const uint32_t *vals,
+                    void *lb, void *nb, int2 *child, int2 *range, int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
+{
+  switch ( V )
+  {
+    case 3: return launch_build_t< K, T, 3 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, sc, s );
+    case 4: return launch_build_t< K, T, 4 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, sc, s );
+    case 8: return launch_build_t< K, T, 8 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, sc, s );
+    default: return launch_build_t< K, T, 0 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, sc, s );
+  }
+}
+
+template< int K, typename T >
+cudaError_t refit_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *lb, void *nb,
+                    const int *parent, int *exch, const obj_scalars *sc, cudaStream_t s)
+{
+  switch ( V )
+  {
+    case 3: return launch_refit_t< K, T, 3 >( verts, V, n, eps, vals, lb, nb, parent, exch, sc, s );
+    case 4: return launch_refit_t< K, T, 4 >( verts, V, n, eps, vals, lb, nb, parent, exch, sc, s );
+    case 8: return launch_refit_t< K, T, 8 >( verts, V, n, eps, vals, lb, nb, parent, exch, sc, s );
+    default: return launch_refit_t< K, T, 0 >( verts, V, n, eps, vals, lb, nb, parent, exch, sc, s );
+  }
+}
+
+// Original-order slabs (parity probe).
+template< int K, typename T, int VT >
+__global__ void k_probe_kdops(const double *__restrict__ verts, uint32_t Vrt, uint64_t n, double eps, float eps_hi,
+                              T *__restrict__ out)
+{
+  constexpr int D = K / 2;
+  const uint64_t i = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
+  if ( i >= n ) return;
+  T lo[D], hi[D];
+  leaf_slabs< K, T, VT >( verts, Vrt, static_cast< uint32_t >( i ), eps, eps_hi, lo, hi );
+  for ( int a = 0; a < D; ++a )
+  {
+    out[( i * D + a ) * 2] = lo[a];
+    out[( i * D + a ) * 2 + 1] = hi[a];
+  }
+}
+
+template< int K, typename T >
+cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, void *out, cudaStream_t s)
+{
+  const float eps_hi = f32_up( eps );
+  const unsigned grid = static_cast< unsigned >( ( n + 255 ) / 256 );
+  if ( V == 3 ) k_probe_kdops< K, T, 3 ><<< grid, 256, 0, s >>>( verts, V, n, eps, eps_hi, static_cast< T * >( out ) );
+  else if ( V == 4 ) k_probe_kdops< K, T, 4 ><<< grid, 256, 0, s >>>( verts, V, n, eps, eps_hi, static_cast< T * >( out ) );
+  else if ( V == 8 ) k_probe_kdops< K, T, 8 ><<< grid, 256, 0, s >>>( verts, V, n, eps, eps_hi, static_cast< T * >( out ) );
+  else k_probe_kdops< K, T, 0 ><<< grid, 256, 0, s >>>( verts, V, n, eps, eps_hi, static_cast< T * >( out ) );
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
+                         const uint64_t *keys, const uint32_t *vals, void *leaf_box, void *node_box, int2 *child,
+                         int2 *range, int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
+{
+#define BVHG_BUILD_CASE( KK )                                                                                           \
+  case KK:                                                                                                             \
+    return fp32 ? build_v< KK, float >( verts, V, n, eps, keys, vals, leaf_box, node_box, child, range, parent, exch, sc, s ) \
+                : build_v< KK, double >( verts, V, n, eps, keys, vals, leaf_box, node_box, child, range, parent, exch, sc, s );
+  switch ( K )
+  {
+    BVHG_BUILD_CASE( 6 )
+    BVHG_BUILD_CASE( 18 )
+    BVHG_BUILD_CASE( 26 )
+    default: return cudaErrorInvalidValue;
+  }
+#undef BVHG_BUILD_CASE
+}
+
+cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
+                         const uint32_t *vals, void *leaf_box, void *node_box, const int *parent, int *exch,
+                         obj_scalars *sc, cudaStream_t s)
+{
+  switch ( K )
+  {
+    case 6: return fp32 ? refit_v< 6, float >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s )
+                        : refit_v< 6, double >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s );
+    case 18: return fp32 ? refit_v< 18, float >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s )
+                         : refit_v< 18, double >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s );
+    case 26: return fp32 ? refit_v< 26, float >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s )
+                         : refit_v< 26, double >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_probe_kdops(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps, void *out,
+                               cudaStream_t s)
+{
+  switch ( K )
+  {
+    case 6: return fp32 ? probe_v< 6, float >( verts, V, n, eps, out, s ) : probe_v< 6, double >( verts, V, n, eps, out, s );
+    case 18: return fp32 ? probe_v< 18, float >( verts, V, n, eps, out, s ) : probe_v< 18, double >( verts, V, n, eps, out, s );
+    case 26: return fp32 ? probe_v< 26, float >( verts, V, n, eps, out, s ) : probe_v< 26, double >( verts, V, n, eps, out, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace bvhg

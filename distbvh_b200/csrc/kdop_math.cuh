@@ -1,0 +1,190 @@
+// kdop_math.cuh — k-DOP slab arithmetic on the device.
+//
+// FP64 slabs follow kdop_base::from_vertices (src/bvh/kdop.hpp:238-264) bit for bit: every projection is
+// ((v0 * n0) + (v1 * n1)) + (v2 * n2) (kdop.hpp:223-227) with each product and sum rounded separately
+// (__dmul_rn / __dadd_rn stop nvcc from contracting them into FMAs), then proj - eps / proj + eps, then
+// std::min / std::max over the vertices.
+//
+// FP32 slabs (precision form) enclose the FP64 slabs: lo32 <= lo64 and hi32 >= hi64 for every element and
+// slab, computed with FP32 directed rounding only (interval products and sums, then a widening by an explicit
+// bound on the FP64 evaluation error). Strict overlap then carries over: a64.min < b64.max implies
+// a32.min <= a64.min < b64.max <= b32.max, so the FP32 candidate set is a superset of the FP64 pair set.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bvhg {
+
+constexpr double kOverRoot2 = 0.7071067811865475;  // dop_18::over_root_2, dop_26::one_over_root_2 (kdop.hpp:608,659)
+constexpr double kOverRoot3 = 0.5773502691896258;  // dop_26::one_over_root_3 (kdop.hpp:660)
+
+// Component c of normal a of the K-DOP (the first K/2 normals: kdop.hpp:583-587, 613-624, 662-677).
+template< int K >
+__host__ __device__ constexpr double normal_comp(int a, int c)
+{
+  if ( a < 3 ) return a == c ? 1.0 : 0.0;
+  if ( K == 18 || ( K == 26 && a >= 7 ) )
+  {
+    const int e = ( K == 18 ) ? a - 3 : a - 7;  // edge normals
+    // (r,r,0) (r,0,r) (0,r,r) (r,-r,0) (r,0,-r) (0,r,-r)
+    const int zero_c = ( e % 3 == 0 ) ? 2 : ( ( e % 3 == 1 ) ? 1 : 0 );
+    if ( c == zero_c ) return 0.0;
+    const bool second = ( c == ( e % 3 == 2 ? 2 : ( e % 3 == 0 ? 1 : 2 ) ) );
+    if ( e >= 3 && second ) return -kOverRoot2;
+    return kOverRoot2;
+  }
+  // K == 26 corners, a in [3, 7): (s,s,s) (s,-s,s) (s,s,-s) (s,-s,-s)
+  const int cidx = a - 3;
+  if ( c == 0 ) return kOverRoot3;
+  if ( c == 1 ) return ( cidx & 1 ) ? -kOverRoot3 : kOverRoot3;
+  return ( cidx & 2 ) ? -kOverRoot3 : kOverRoot3;
+}
+
+// FP64 projection exactly as kdop.hpp:226 evaluates it (no FMA contraction).
+template< int K >
+__device__ __forceinline__ double project64(const double v0, const double v1, const double v2, const int a)
+{
+  const double t0 = __dmul_rn( v0, normal_comp< K >( a, 0 ) );
+  const double t1 = __dmul_rn( v1, normal_comp< K >( a, 1 ) );
+  const double t2 = __dmul_rn( v2, normal_comp< K >( a, 2 ) );
+  return __dadd_rn( __dadd_rn( t0, t1 ), t2 );
+}
+
+// std::min / std::max (libstdc++): min(a, b) = (b < a) ? b : a; max(a, b) = (a < b) ? b : a.
+__device__ __forceinline__ double std_min(double a, double b) { return ( b < a ) ? b : a; }
+__device__ __forceinline__ double std_max(double a, double b) { return ( a < b ) ? b : a; }
+
+// Slab a of one element from its V vertices (vertex v at p[3 v + c]), FP64, as from_vertices.
+template< int K >
+__device__ __forceinline__ void slab64(const double *p, int V, int a, double eps, double &mn, double &mx)
+{
+  double proj = project64< K >( p[0], p[1], p[2], a );
+  mn = __dsub_rn( proj, eps );
+  mx = __dadd_rn( proj, eps );
+  for ( int v = 1; v < V; ++v )
+  {
+    proj = project64< K >( p[3 * v], p[3 * v + 1], p[3 * v + 2], a );
+    mn = std_min( mn, __dsub_rn( proj, eps ) );
+    mx = std_max( mx, __dadd_rn( proj, eps ) );
+  }
+}
+
+// ---- FP32 enclosure ------------------------------------------------------------------------------------
+
+// Error bound constant: the FP64 value of ((t0 + t1) + t2), t_k = fl(v_k n_k), differs from the exact sum by
+// at most gamma_3 * sum |v_k n_k| with gamma_3 = 3u / (1 - 3u), u = 2^-53; 2^-51 > gamma_3.
+constexpr float kTwoPowM51 = 4.44089209850062616169452667236328125e-16f;  // 2^-51, exact in FP32
+constexpr float kTwoPowM52 = 2.220446049250313080847263336181640625e-16f; // 2^-52, exact in FP32
+
+// Product interval of an FP32 interval [alo, ahi] (both roundings of one FP64 value, so they never straddle 0)
+// with the FP32 interval [nlo, nhi] of a nonzero constant of known sign.
+__device__ __forceinline__ void mul_interval(float alo, float ahi, float nlo, float nhi, bool npos, float &lo,
+                                             float &hi)
+{
+  if ( npos )
+  {
+    lo = __fmul_rd( alo, alo >= 0.f ? nlo : nhi );
+    hi = __fmul_ru( ahi, ahi >= 0.f ? nhi : nlo );
+  } else {
+    lo = __fmul_rd( ahi, ahi >= 0.f ? nlo : nhi );
+    hi = __fmul_ru( alo, alo >= 0.f ? nhi : nlo );
+  }
+}
+
+// FP32 enclosures of the two irrational normal magnitudes: lo = the largest float <= c, hi = the smallest
+// float >= c (hex literals; bvhg_debug_normal_interval exposes them so a CPU test checks the bracketing).
+constexpr float kOverRoot2Lo = 0x1.6a09e6p-1f;
+constexpr float kOverRoot2Hi = 0x1.6a09e8p-1f;
+constexpr float kOverRoot3Lo = 0x1.279a74p-1f;
+constexpr float kOverRoot3Hi = 0x1.279a76p-1f;
+
+// FP32 interval [lo, hi] of normal component (a, c).
+template< int K >
+__host__ __device__ constexpr float normal_lo(int a, int c)
+{
+  const double v = normal_comp< K >( a, c );
+  if ( v == kOverRoot2 ) return kOverRoot2Lo;
+  if ( v == -kOverRoot2 ) return -kOverRoot2Hi;
+  if ( v == kOverRoot3 ) return kOverRoot3Lo;
+  if ( v == -kOverRoot3 ) return -kOverRoot3Hi;
+  return static_cast< float >( v );  // 0, 1, -1: exact
+}
+
+template< int K >
+__host__ __device__ constexpr float normal_hi(int a, int c)
+{
+  const double v = normal_comp< K >( a, c );
+  if ( v == kOverRoot2 ) return kOverRoot2Hi;
+  if ( v == -kOverRoot2 ) return -kOverRoot2Lo;
+  if ( v == kOverRoot3 ) return kOverRoot3Hi;
+  if ( v == -kOverRoot3 ) return -kOverRoot3Lo;
+  return static_cast< float >( v );
+}
+
+// FP32 enclosure of slab a of one element: lo <= the FP64 slab min and hi >= the FP64 slab max that slab64
+// computes for the same vertices and epsilon. eps_hi is epsilon rounded up to FP32 (0 when epsilon is 0).
+template< int K >
+__device__ __forceinline__ void slab32(const double *p, int V, int a, float eps_hi, float &lo, float &hi)
+{
+  const double n0 = normal_comp< K >( a, 0 ), n1 = normal_comp< K >( a, 1 ), n2 = normal_comp< K >( a, 2 );
+  const int nz = ( n0 != 0.0 ) + ( n1 != 0.0 ) + ( n2 != 0.0 );
+  // A single unit component: the FP64 projection is the coordinate itself, exactly.
+  const bool exact = ( nz == 1 ) && ( n0 == 1.0 || n0 == -1.0 || n1 == 1.0 || n1 == -1.0 || n2 == 1.0 || n2 == -1.0 );
+  const float inf = __int_as_float( 0x7f800000 );
+  lo = inf;
+  hi = -inf;
+  for ( int v = 0; v < V; ++v )
+  {
+    float slo = 0.f, shi = 0.f, mag = 0.f;
+    bool first = true;
+#pragma unroll
+    for ( int c = 0; c < 3; ++c )
+    {
+      const double nc = normal_comp< K >( a, c );
+      if ( nc == 0.0 ) continue;
+      const double x = p[3 * v + c];
+      const float xlo = __double2float_rd( x ), xhi = __double2float_ru( x );
+      float tlo, thi;
+      if ( nc == 1.0 )
+      {
+        tlo = xlo;
+        thi = xhi;
+      } else if ( nc == -1.0 ) {
+        tlo = -xhi;
+        thi = -xlo;
+      } else {
+        mul_interval( xlo, xhi, normal_lo< K >( a, c ), normal_hi< K >( a, c ), nc > 0.0, tlo, thi );
+      }
+      const float tmag = fmaxf( fabsf( tlo ), fabsf( thi ) );
+      if ( first )
+      {
+        slo = tlo;
+        shi = thi;
+        mag = tmag;
+        first = false;
+      } else {
+        slo = __fadd_rd( slo, tlo );
+        shi = __fadd_ru( shi, thi );
+        mag = __fadd_ru( mag, tmag );
+      }
+    }
+    if ( !exact )
+    {
+      const float e = __fmul_ru( mag, kTwoPowM51 );
+      slo = __fsub_rd( slo, e );
+      shi = __fadd_ru( shi, e );
+    }
+    if ( eps_hi != 0.f )
+    {
+      const float m2 = __fadd_ru( fmaxf( fabsf( slo ), fabsf( shi ) ), eps_hi );
+      const float e2 = __fmul_ru( m2, kTwoPowM52 );
+      slo = __fsub_rd( __fsub_rd( slo, eps_hi ), e2 );
+      shi = __fadd_ru( __fadd_ru( shi, eps_hi ), e2 );
+    }
+    lo = fminf( lo, slo );
+    hi = fmaxf( hi, shi );
+  }
+}
+
+}  // namespace bvhg

@@ -1,0 +1,299 @@
+"""GPU parity: every stage of the CUDA path against the CPU oracle, through the C ABI.
+
+Bit-exact for everything integer or FP64 (slabs, centroids, Morton bounds and keys, permutation, pair sets).
+The FP32 precision form must give the identical pair set after its FP64 recheck, and its FP32 slabs must
+enclose the FP64 slabs. Sizes keep the oracle to seconds; full-size properties are checked in test_gpu_scale.py.
+"""
+import numpy as np
+import pytest
+
+import distbvh_b200 as bvhg
+from distbvh_b200 import meshes
+from oracle import oracle as orc
+from tests.grids import element_grid
+
+pytestmark = pytest.mark.gpu
+
+
+def u64(a):
+    return np.ascontiguousarray(a).view(np.uint64)
+
+
+def build_pair(ctx, a, b, ga=None, gb=None):
+    oa, ob = ctx.object(), ctx.object()
+    ctx.set_elements(oa, a, gid=ga)
+    ctx.set_elements(ob, b, gid=gb)
+    ctx.build(oa)
+    ctx.build(ob)
+    return oa, ob
+
+
+def check_stages(ctx, obj, xyz, k, eps):
+    n = xyz.shape[0]
+    s = orc.kdops(xyz, k, eps)
+    c = orc.centroids(xyz)
+    assert np.array_equal(u64(ctx.kdops(obj, n)), u64(s)), "FP64 slabs differ from kdop_base::from_vertices"
+    assert np.array_equal(u64(ctx.centroids(obj, n)), u64(c)), "centroids differ"
+    mn, inv = orc.morton_bounds(s, k)
+    okeys = orc.morton_keys(c, mn, inv)
+    operm = orc.stable_perm(okeys)
+    keys, perm, gmn, ginv = ctx.morton(obj, n)
+    assert np.array_equal(gmn, mn) and np.array_equal(u64(ginv), u64(inv)), "Morton bounds differ"
+    assert np.array_equal(perm, operm), "permutation differs from the stable sort"
+    assert np.array_equal(keys, okeys[operm]), "sorted Morton keys differ"
+    ctx.validate_tree(obj)
+
+
+@pytest.mark.parametrize("k", [6, 18, 26])
+@pytest.mark.parametrize("V", [3, 4, 8])
+@pytest.mark.parametrize("eps", [0.0, 0.004])
+def test_stages_and_pairs(k, V, eps):
+    a = meshes.random_soup(3000, V, seed=100 + V, size=0.03)
+    b = meshes.random_soup(2500, V, seed=200 + V, size=0.03, stream=1)
+    with bvhg.Context(k=k, epsilon=eps) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        check_stages(ctx, oa, a, k, eps)
+        check_stages(ctx, ob, b, k, eps)
+        got = orc.canonical(ctx.broadphase(oa, ob))
+        want = orc.pair_set(a, b, k, eps)
+        assert want.shape[0] > 0
+        assert np.array_equal(got, want)
+        # swapped roles give the transposed set
+        got_ba = orc.canonical(ctx.broadphase(ob, oa))
+        assert np.array_equal(got_ba, orc.canonical(want[:, ::-1]))
+
+
+@pytest.mark.parametrize("bits", [1, 2, 4])
+def test_digit_width_gives_the_same_permutation(bits):
+    a = meshes.random_soup(20000, 3, seed=5, size=0.01)
+    b = meshes.random_soup(15000, 3, seed=6, size=0.01, stream=1)
+    with bvhg.Context(k=18, digit_bits=8) as c8, bvhg.Context(k=18, digit_bits=bits) as cb:
+        a8, b8 = build_pair(c8, a, b)
+        ab, bb = build_pair(cb, a, b)
+        k8, p8, _, _ = c8.morton(a8, a.shape[0])
+        kb, pb, _, _ = cb.morton(ab, a.shape[0])
+        assert np.array_equal(p8, pb) and np.array_equal(k8, kb)
+        assert np.array_equal(orc.canonical(c8.broadphase(a8, b8)), orc.canonical(cb.broadphase(ab, bb)))
+
+
+def test_many_tiles_sort():
+    a = meshes.random_soup(300000, 3, seed=9, size=0.002)
+    with bvhg.Context(k=18) as ctx:
+        oa = ctx.object()
+        ctx.set_elements(oa, a)
+        ctx.build(oa)
+        check_stages(ctx, oa, a, 18, 0.0)
+
+
+def test_two_plates_config():
+    a, b = meshes.two_plates()
+    eps = meshes.TWO_PLATES_EPSILON
+    with bvhg.Context(k=18, epsilon=eps) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        check_stages(ctx, oa, a, 18, eps)  # plate A is flat: the z axis takes the NaN -> 0 path
+        check_stages(ctx, ob, b, 18, eps)
+        got = orc.canonical(ctx.broadphase(oa, ob))
+    want = orc.pair_set(a, b, 18, eps)
+    assert want.shape[0] > 10000
+    assert np.array_equal(got, want)
+
+
+def test_sphere_plate_small():
+    s, p = meshes.sphere_plate(level=5, nx=256, ny=128)
+    with bvhg.Context(k=18) as ctx:
+        os_, op = build_pair(ctx, s, p)
+        check_stages(ctx, os_, s, 18, 0.0)
+        check_stages(ctx, op, p, 18, 0.0)
+        got = orc.canonical(ctx.broadphase(os_, op))
+    want = orc.pair_set(s, p, 18)
+    assert want.shape[0] > 0
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("k", [6, 18, 26])
+def test_self_collision(k):
+    a = meshes.random_soup(4000, 4, seed=31, size=0.03)
+    with bvhg.Context(k=k) as ctx:
+        oa = ctx.object()
+        ctx.set_elements(oa, a)
+        ctx.build(oa)
+        got = orc.canonical(ctx.self_collision(oa))
+    assert np.all(got[:, 0] < got[:, 1])
+    assert np.array_equal(got, orc.self_pair_set(a, k))
+
+
+def test_reference_grids():
+    # tests/CollisionTest.cpp:43-81 on the GPU: 64 pairs; 0 self pairs for touching cubes; 8 self pairs
+    a, ga = element_grid(4, 4, 4)
+    b, gb = element_grid(1, 1, 1, a.shape[0])
+    with bvhg.Context(k=26) as ctx:
+        oa, ob = build_pair(ctx, a, b, ga, gb)
+        got = orc.canonical(ctx.broadphase(oa, ob))
+        assert got.shape[0] == 64
+        assert np.array_equal(got, orc.pair_set(a, b, 26, gid_a=ga, gid_b=gb))
+        t = ctx.object()
+        x, _ = element_grid(2, 2, 1)
+        ctx.set_elements(t, x)
+        ctx.build(t)
+        assert ctx.self_collision(t).shape[0] == 0
+        u = ctx.object()
+        x2 = np.concatenate([element_grid(2, 2, 2)[0], element_grid(1, 1, 1)[0]])
+        ctx.set_elements(u, x2)
+        ctx.build(u)
+        assert ctx.self_collision(u).shape[0] == 8
+
+
+def test_duplicate_keys_and_dense_pairs():
+    tet = meshes.random_soup(1, 4, seed=3, size=0.1)
+    a = np.repeat(tet, 300, axis=0)
+    b = np.repeat(tet, 200, axis=0)
+    with bvhg.Context(k=18) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        check_stages(ctx, oa, a, 18, 0.0)
+        got = orc.canonical(ctx.broadphase(oa, ob))
+        assert got.shape[0] == 300 * 200
+        assert np.array_equal(got, orc.pair_set(a, b, 18, method="brute"))
+        assert ctx.self_collision(oa).shape[0] == 300 * 299 // 2
+
+
+@pytest.mark.parametrize("na,nb", [(0, 5), (5, 0), (1, 1), (1, 50), (2, 3), (50, 1)])
+def test_tiny_objects(na, nb):
+    a = meshes.random_soup(max(na, 1), 3, seed=41, size=0.4)[:na]
+    b = meshes.random_soup(max(nb, 1), 3, seed=42, size=0.4, stream=1)[:nb]
+    with bvhg.Context(k=18) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        got = orc.canonical(ctx.broadphase(oa, ob))
+        want = orc.pair_set(a, b, 18, method="brute") if na and nb else np.zeros((0, 2), np.uint64)
+        assert np.array_equal(got, want)
+        if na >= 2:
+            assert np.array_equal(orc.canonical(ctx.self_collision(oa)), orc.self_pair_set(a, 18, method="brute"))
+
+
+@pytest.mark.parametrize("k", [18, 26])
+def test_fp32_filter_exact_after_recheck(k):
+    a = meshes.random_soup(6000, 3, seed=51, size=0.02)
+    b = meshes.random_soup(5000, 3, seed=52, size=0.02, stream=1)
+    eps = 0.001
+    with bvhg.Context(k=k, precision=bvhg.FILTER_FP32, epsilon=eps) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        f32 = ctx.kdops(oa, a.shape[0]).astype(np.float64)
+        f64 = orc.kdops(a, k, eps)
+        assert np.all(f32[..., 0] <= f64[..., 0]) and np.all(f32[..., 1] >= f64[..., 1]), "FP32 slabs not enclosing"
+        got = orc.canonical(ctx.broadphase(oa, ob))
+        cand = ctx.last_candidates()
+        ctx.validate_tree(oa)
+    want = orc.pair_set(a, b, k, eps)
+    assert np.array_equal(got, want)
+    assert cand >= want.shape[0]
+
+
+def test_fp32_filter_touching_boundaries():
+    # Exactly touching elements (FP64 slabs equal at the boundary) are not pairs; the FP32 filter keeps them as
+    # candidates and the FP64 recheck removes them.
+    a, _ = element_grid(6, 6, 6)
+    b, _ = element_grid(6, 6, 6, origin_shift=1.0 / 6.0)
+    with bvhg.Context(k=26, precision=bvhg.FILTER_FP32) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        got = orc.canonical(ctx.broadphase(oa, ob))
+        cand = ctx.last_candidates()
+    want = orc.pair_set(a, b, 26)
+    assert np.array_equal(got, want)
+    assert cand > want.shape[0]
+
+
+def test_gid_mapping_and_device_input():
+    torch = pytest.importorskip("torch")
+    a = meshes.random_soup(2000, 3, seed=61, size=0.03)
+    b = meshes.random_soup(2000, 3, seed=62, size=0.03, stream=1)
+    rng = np.random.default_rng(0)
+    ga = rng.choice(1 << 40, a.shape[0], replace=False).astype(np.uint64)
+    gb = rng.choice(1 << 40, b.shape[0], replace=False).astype(np.uint64)
+    want = orc.pair_set(a, b, 18, gid_a=ga, gid_b=gb)
+    with bvhg.Context(k=18) as ctx:
+        oa, ob = build_pair(ctx, a, b, ga, gb)
+        assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), want)
+        da = torch.from_numpy(a).cuda()
+        db = torch.from_numpy(b).cuda()
+        dga = torch.from_numpy(ga.view(np.int64)).cuda()
+        dgb = torch.from_numpy(gb.view(np.int64)).cuda()
+        torch.cuda.synchronize()
+        ctx.set_elements(oa, da, gid=dga)
+        ctx.set_elements(ob, db, gid=dgb)
+        ctx.build(oa)
+        ctx.build(ob)
+        assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), want)
+        # device output buffer
+        out = torch.empty((want.shape[0], 2), dtype=torch.int64, device="cuda")
+        st, cnt = ctx.broadphase_raw(oa, ob, out.data_ptr(), want.shape[0], bvhg.MEM_DEVICE)
+        assert st == 0 and cnt == want.shape[0]
+        assert np.array_equal(orc.canonical(out.cpu().numpy().view(np.uint64)), want)
+
+
+def test_overflow_reports_required_count():
+    a = meshes.random_soup(3000, 3, seed=71, size=0.05)
+    b = meshes.random_soup(3000, 3, seed=72, size=0.05, stream=1)
+    want = orc.pair_set(a, b, 18)
+    with bvhg.Context(k=18) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        out = np.empty((10, 2), dtype=np.uint64)
+        st, cnt = ctx.broadphase_raw(oa, ob, out.ctypes.data, 10, bvhg.MEM_HOST)
+        assert st == 3 and cnt == want.shape[0]
+        # the first `capacity` pairs written are genuine pairs
+        wset = set(map(tuple, want.tolist()))
+        assert all(tuple(p) in wset for p in out.tolist())
+        assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob, capacity=cnt)), want)
+
+
+def test_non_finite_input_is_rejected():
+    a = meshes.random_soup(500, 3, seed=81)
+    a[17, 1, 2] = np.nan
+    b = meshes.random_soup(500, 3, seed=82, stream=1)
+    with bvhg.Context(k=18) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        with pytest.raises(bvhg.BvhgError) as e:
+            ctx.broadphase(oa, ob)
+        assert e.value.status == 1
+
+
+def test_bounded_lookback_times_out_and_context_recovers():
+    a = meshes.random_soup(50000, 3, seed=91, size=0.01)
+    b = meshes.random_soup(20000, 3, seed=92, size=0.01, stream=1)
+    with bvhg.Context(k=18) as ctx:
+        ctx.set_spin_limit(2000)
+        ctx.test_stall_sort(True)
+        oa, ob = build_pair(ctx, a, b)
+        with pytest.raises(bvhg.BvhgError) as e:
+            ctx.broadphase(oa, ob)
+        assert e.value.status == 4
+        ctx.test_stall_sort(False)
+        ctx.set_spin_limit(0)
+        ctx.build(oa)
+        ctx.build(ob)
+        assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b, 18))
+
+
+@pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
+def test_refit_after_motion(precision):
+    a = meshes.random_soup(4000, 3, seed=101, size=0.03)
+    b = meshes.random_soup(4000, 3, seed=102, size=0.03, stream=1)
+    with bvhg.Context(k=18, precision=precision) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        for step in range(3):
+            b2 = b + np.array([0.01 * (step + 1), -0.005 * step, 0.003])
+            ctx.set_elements(ob, b2)
+            ctx.build(ob, bvhg.REFIT)
+            ctx.validate_tree(ob)
+            assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b2, 18))
+
+
+def test_stage_timing_and_launch_count():
+    a = meshes.random_soup(10000, 3, seed=111, size=0.02)
+    with bvhg.Context(k=18, stage_timing=True) as ctx:
+        oa = ctx.object()
+        ctx.set_elements(oa, a)
+        ctx.build(oa)
+        ctx.self_collision(oa)
+        ms, launches = ctx.stage_times()
+        assert launches["sort"] == 8 and launches["build"] == 1 and launches["traverse"] >= 1
+        assert all(v >= 0 for v in ms.values()) and ms["sort"] > 0
+        assert ctx.launch_count() >= 12
