@@ -191,13 +191,19 @@ __global__ void __launch_bounds__( kElemThreads ) k_keys_hist(const double *__re
       key = ( expand64( qz ) << 2 ) | ( expand64( qy ) << 1 ) | expand64( qx );
       keys[i] = key;
     }
+    const unsigned vmask = __ballot_sync( 0xffffffffu, valid );
 #pragma unroll
     for ( int p = 0; p < PASSES; ++p )
     {
-      const unsigned d = valid ? static_cast< unsigned >( ( key >> ( p * BITS ) ) & ( RADIX - 1 ) ) : RADIX;
-      const unsigned peers = __match_any_sync( 0xffffffffu, d );
-      if ( valid && lane == static_cast< unsigned >( __ffs( peers ) - 1 ) )
-        atomicAdd( &s_hist[p * RADIX + d], static_cast< uint32_t >( __popc( peers ) ) );
+      const unsigned d = static_cast< unsigned >( ( key >> ( p * BITS ) ) & ( RADIX - 1 ) );
+      // Spatially coherent warps share their high digits: one atomic for a uniform warp, else one per lane.
+      const unsigned d0 = __shfl_sync( 0xffffffffu, d, 0 );
+      if ( __all_sync( 0xffffffffu, d == d0 || !valid ) && vmask == 0xffffffffu )
+      {
+        if ( lane == 0 ) atomicAdd( &s_hist[p * RADIX + d0], 32u );
+      } else if ( valid ) {
+        atomicAdd( &s_hist[p * RADIX + d], 1u );
+      }
     }
   }
   __syncthreads();
@@ -223,7 +229,8 @@ cudaError_t launch_cb_t(const double *verts, uint32_t V, uint64_t n, double eps,
                         obj_scalars *sc, cudaStream_t s)
 {
   const size_t smem = static_cast< size_t >( kElemThreads ) * V * 3 * sizeof( double );
-  if ( smem > 48 * 1024 )
+  // Static shared memory counts against the same 48 KB default: opt in whenever the tile is large.
+  if ( smem >= 40 * 1024 )
   {
     cudaError_t e = cudaFuncSetAttribute( k_centroid_bounds< K, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           static_cast< int >( smem ) );

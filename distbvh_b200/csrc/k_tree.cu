@@ -9,8 +9,10 @@
 // dissimilarity of the keys just outside its range, and writes each subtree's slabs into its parent as it goes.
 // Ties among equal keys are broken by rank, i.e. the tree is the radix tree of the 96-bit (key, rank) pairs.
 //
-// No thread ever waits: the first arrival at a node leaves, the second continues. Writes of the first arrival
-// are published with __threadfence before its atomicExch; the second arrival fences and reads them through L2.
+// No thread ever waits: the first arrival at a node leaves, the second continues. Most nodes have both children
+// finished inside one warp; those are merged in registers (warp-synchronous rounds, shuffles, no global
+// synchronization). The rest use a global exchange slot per node: the first arrival's slab stores are ordered
+// before its acq_rel atomic exchange, and the second arrival reads them through L2 after its own.
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
 
@@ -36,6 +38,15 @@ __device__ __forceinline__ int delta(const uint64_t *__restrict__ keys, int j)
   const uint64_t x = __ldg( keys + j ) ^ __ldg( keys + j + 1 );
   if ( x ) return 96 - __clzll( static_cast< long long >( x ) );
   return 32 - __clz( j ^ ( j + 1 ) );
+}
+
+// Exchange with acquire-release semantics at GPU scope (orders this thread's earlier stores before the exchange
+// and its later loads after it).
+__device__ __forceinline__ int atomic_exch_acq_rel(int *p, int v)
+{
+  int old;
+  asm volatile( "atom.acq_rel.gpu.global.exch.b32 %0, [%1], %2;" : "=r"( old ) : "l"( p ), "r"( v ) : "memory" );
+  return old;
 }
 
 template< typename T >
@@ -159,27 +170,97 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build(const double *__restr
   constexpr int D = K / 2;
   using io = box_io< T >;
   const int i = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
-  if ( i >= n ) return;
+  const int lane = threadIdx.x & 31;
   // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word).
-  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
-  const uint32_t e = __ldg( vals + i );
-  if ( e >= static_cast< uint32_t >( n ) )
+  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // grid-uniform
+  bool active = i < n;
+  const uint32_t e = active ? __ldg( vals + i ) : 0u;
+  if ( active && e >= static_cast< uint32_t >( n ) )
   {
     atomicCAS( &sc->error, 0, kErrTimeout );
-    return;
+    active = false;
   }
   T lo[D], hi[D];
-  leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
+  if ( active )
+  {
+    leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
 #pragma unroll
-  for ( int a = 0; a < D; ++a ) io::store2( leaf_box + ( static_cast< size_t >( i ) * D + a ) * 2, lo[a], hi[a] );
+    for ( int a = 0; a < D; ++a ) io::store2( leaf_box + ( static_cast< size_t >( i ) * D + a ) * 2, lo[a], hi[a] );
+  } else {
+#pragma unroll
+    for ( int a = 0; a < D; ++a ) lo[a] = hi[a] = T( 0 );
+  }
   if ( n == 1 )
   {
-    sc->root = ~static_cast< int >( e );
+    if ( active ) sc->root = ~static_cast< int >( e );
     return;
   }
   int l = i, r = i;
   int node = ~static_cast< int >( e );
   int self_slot = i;  // index into parent[]: leaves [0, n), internal nodes n + k
+
+  // Phase 1, warp-synchronous: a node whose two children are both finished by lanes of this warp is merged in
+  // registers (the two lanes meet on the same parent index; the left lane absorbs the right one's slabs by
+  // shuffle). Rounds continue while some pair meets; lanes left waiting go on to the global phase.
+  while ( true )
+  {
+    int par = 0, side = 0;
+    if ( active )
+    {
+      bool left_child;
+      if ( l == 0 ) left_child = true;
+      else if ( r == n - 1 ) left_child = false;
+      else left_child = delta( keys, r ) < delta( keys, l - 1 );
+      par = left_child ? r : l - 1;
+      side = left_child ? 0 : 1;
+    }
+    const unsigned peers = __match_any_sync( 0xffffffffu, active ? par : -2 - lane );
+    const bool paired = active && __popc( peers ) == 2;
+    if ( !__any_sync( 0xffffffffu, paired ) ) break;
+    const int src = paired ? __ffs( peers & ~( 1u << lane ) ) - 1 : lane;
+    if ( paired )
+    {
+      T *pb = node_box + static_cast< size_t >( par ) * D * 4;
+#pragma unroll
+      for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
+      child[2 * par + side] = node;
+      parent[self_slot] = 2 * par + side;
+    }
+    const int sr = __shfl_sync( 0xffffffffu, r, src );
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      const T sl = __shfl_sync( 0xffffffffu, lo[a], src );
+      const T sh = __shfl_sync( 0xffffffffu, hi[a], src );
+      if ( paired && side == 0 )
+      {
+        lo[a] = io::mn( lo[a], sl );
+        hi[a] = io::mx( hi[a], sh );
+      }
+    }
+    if ( paired )
+    {
+      if ( side == 0 )
+      {
+        r = sr;
+        range[par] = make_int2( l, r );
+        node = par;
+        self_slot = n + par;
+        if ( l == 0 && r == n - 1 )
+        {
+          sc->root = par;
+          active = false;
+        }
+      } else {
+        active = false;
+      }
+    }
+  }
+  if ( !active ) return;
+
+  // Phase 2, global: first arrival at a node publishes its slabs and leaves; the second merges and climbs on.
+  // The exchange is an acq_rel atomic: it orders the first arrival's slab stores before it and the second
+  // arrival's slab loads (through L2) after it.
   while ( true )
   {
     bool left_child;  // true: this subtree is the left child of internal node r
@@ -193,10 +274,8 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build(const double *__restr
     for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
     child[2 * par + side] = node;
     parent[self_slot] = 2 * par + side;
-    __threadfence();
-    const int other = atomicExch( exch + par, left_child ? l : r );
+    const int other = atomic_exch_acq_rel( exch + par, left_child ? l : r );
     if ( other < 0 ) return;  // first arrival: the sibling's thread finishes this node
-    __threadfence();
     if ( left_child ) r = other;
     else l = other;
 #pragma unroll
@@ -246,10 +325,8 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restr
     T *pb = node_box + static_cast< size_t >( par ) * D * 4;
 #pragma unroll
     for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
-    __threadfence();
-    const int other = atomicExch( exch + par, 1 );
+    const int other = atomic_exch_acq_rel( exch + par, 1 );
     if ( other < 0 ) return;
-    __threadfence();
 #pragma unroll
     for ( int a = 0; a < D; ++a )
     {
