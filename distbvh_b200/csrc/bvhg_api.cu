@@ -69,7 +69,7 @@ struct object
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
   dev_buf hist, status;
-  dev_buf leaf_box, node_box, child, range, parent, exch;
+  dev_buf leaf_box, node_box, child, range, parent, exch, queue;
   dev_buf scal;  // obj_scalars
   obj_scalars *sc() const { return scal.as< obj_scalars >(); }
   const uint64_t *sorted_keys() const { return sort_result_alt ? keys_alt.as< uint64_t >() : keys.as< uint64_t >(); }
@@ -252,6 +252,7 @@ bvhg_status do_build(bvhg_ctx *ctx, object &o, int mode)
   BVHG_CUDA( ctx, o.range.reserve( ( n - 1 ) * 8 + 8 ) );
   BVHG_CUDA( ctx, o.parent.reserve( ( 2 * n ) * 4 ) );
   BVHG_CUDA( ctx, o.exch.reserve( n * 4 ) );
+  BVHG_CUDA( ctx, o.queue.reserve( n * 16 ) );
   {
     stage_scope st( ctx, BVHG_STAGE_BOUNDS );
     BVHG_CUDA( ctx, cudaMemcpyAsync( o.sc(), ctx->init_template, sizeof( obj_scalars ), cudaMemcpyHostToDevice, s ) );
@@ -289,8 +290,8 @@ bvhg_status do_build(bvhg_ctx *ctx, object &o, int mode)
     stage_scope st( ctx, BVHG_STAGE_BUILD );
     BVHG_CUDA( ctx, launch_build( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_keys(), o.sorted_vals(),
                                   o.leaf_box.p, o.node_box.p, o.child.as< int2 >(), o.range.as< int2 >(),
-                                  o.parent.as< int >(), o.exch.as< int >(), o.sc(), s ) );
-    st.launched();
+                                  o.parent.as< int >(), o.exch.as< int >(), o.queue.as< int4 >(), o.sc(), s ) );
+    st.launched( n > 1 ? 2 : 1 );
   }
   o.built = true;
   o.topo = true;

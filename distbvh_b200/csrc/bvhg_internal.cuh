@@ -13,6 +13,7 @@
 //   range      (n - 1) int2: [first rank, last rank] covered by the node (self-collision pruning)
 //   parent     n + (n - 1) int32: parent * 2 + side of every leaf (rank order) and internal node (refit)
 //   exch       n - 1 int32: the agglomerative build's exchange slot per internal node (-1 = empty)
+//   queue      n int4: subtrees the warp-local build phase leaves to the global phase
 #pragma once
 
 #include <cstddef>
@@ -29,6 +30,8 @@ struct obj_scalars
   double inv3[3];                    // 1 / (max - min)
   int root;                          // root internal node, or ~elem when n == 1
   int error;                         // bvhg_status raised by a kernel (first one wins)
+  unsigned int climb_count;          // subtrees queued for the global phase of the tree build
+  alignas( 16 ) unsigned char root_box[26 * 8];  // the root's slabs, D (min, max) pairs of the slab type
   unsigned int sort_tile_counter[64];// tile dispenser per radix pass
 };
 
@@ -88,10 +91,11 @@ cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *v
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
                             obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s);
 
-// Leaf slabs + agglomerative LBVH build + bottom-up refit in one pass (FP64 or FP32 slabs).
+// Leaf slabs + agglomerative LBVH build with bottom-up refit (FP64 or FP32 slabs): two launches, a warp-local
+// phase that queues unfinished subtrees (queue: n int4) and a global climb over the queue.
 cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
                          const uint64_t *keys, const uint32_t *vals, void *leaf_box, void *node_box, int2 *child,
-                         int2 *range, int *parent, int *exch, obj_scalars *sc, cudaStream_t s);
+                         int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s);
 
 // Refit with the topology of the last build: recompute leaf slabs and every internal node.
 cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,

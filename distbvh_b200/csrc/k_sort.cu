@@ -43,7 +43,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s
 }
 
 template< int BITS >
-__global__ void __launch_bounds__( kSortThreads ) k_onesweep(const uint64_t *__restrict__ keys_in,
+__global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *__restrict__ keys_in,
                                                            const uint32_t *__restrict__ vals_in,
                                                            uint64_t *__restrict__ keys_out,
                                                            uint32_t *__restrict__ vals_out, uint64_t n, int pass,
@@ -69,21 +69,15 @@ __global__ void __launch_bounds__( kSortThreads ) k_onesweep(const uint64_t *__r
   const uint64_t tile_base = tile * kSortTile;
   const uint64_t wbase = tile_base + static_cast< uint64_t >( warp ) * ( kSortItems * 32 );
 
+  // Keys stay in registers through ranking; values are only loaded at scatter time (fewer live registers,
+  // three blocks per SM). Ranks within the warp are < 512 and kept two per register.
   uint64_t k[kSortItems];
-  uint32_t v[kSortItems];
-  uint32_t rk[kSortItems];
+  uint32_t rk[kSortItems / 2];
 #pragma unroll
   for ( int j = 0; j < kSortItems; ++j )
   {
     const uint64_t idx = wbase + j * 32 + lane;
-    if ( idx < n )
-    {
-      k[j] = keys_in[idx];
-      v[j] = vals_in ? vals_in[idx] : static_cast< uint32_t >( idx );
-    } else {
-      k[j] = 0;
-      v[j] = 0;
-    }
+    k[j] = idx < n ? keys_in[idx] : 0ull;
   }
   const unsigned lt_mask = ( 1u << lane ) - 1u;
 #pragma unroll
@@ -97,7 +91,9 @@ __global__ void __launch_bounds__( kSortThreads ) k_onesweep(const uint64_t *__r
     __syncwarp();
     if ( valid && lower == 0 ) s_whist[warp][d] = base + static_cast< uint32_t >( __popc( peers ) );
     __syncwarp();
-    rk[j] = base + static_cast< uint32_t >( __popc( lower ) );
+    const uint32_t rank = base + static_cast< uint32_t >( __popc( lower ) );
+    if ( j & 1 ) rk[j >> 1] |= rank << 16;
+    else rk[j >> 1] = rank;
   }
   __syncthreads();
 
@@ -167,12 +163,14 @@ __global__ void __launch_bounds__( kSortThreads ) k_onesweep(const uint64_t *__r
 #pragma unroll
   for ( int j = 0; j < kSortItems; ++j )
   {
-    if ( ( wbase + j * 32 + lane ) < n )
+    const uint64_t idx = wbase + j * 32 + lane;
+    if ( idx < n )
     {
       const uint32_t d = static_cast< uint32_t >( ( k[j] >> shift ) & MASK );
-      const uint32_t pos = s_lstart[d] + s_whist[warp][d] + rk[j];
+      const uint32_t rank = ( rk[j >> 1] >> ( ( j & 1 ) * 16 ) ) & 0xffffu;
+      const uint32_t pos = s_lstart[d] + s_whist[warp][d] + rank;
       s_keys[pos] = k[j];
-      s_vals[pos] = v[j];
+      s_vals[pos] = vals_in ? vals_in[idx] : static_cast< uint32_t >( idx );
     }
   }
   __syncthreads();

@@ -72,22 +72,34 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
   if ( *reinterpret_cast< const volatile int * >( &tsc->error ) == kErrTimeout ||
        *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
     return;
+  // The root box test first, on the first four slabs only (two sectors of the query's slabs in FP64, one in
+  // FP32): most queries of a contact scene end here without reading the rest of their slabs.
+  constexpr int D0 = D < 4 ? D : 4;
   T qlo[D], qhi[D];
+  const T *qb = qbox + static_cast< size_t >( i ) * D * 2;
+  const T *rb = reinterpret_cast< const T * >( tsc->root_box );
+  bool o = true;
 #pragma unroll
-  for ( int a = 0; a < D; ++a )
+  for ( int a = 0; a < D0; ++a )
   {
-    qlo[a] = __ldg( qbox + ( static_cast< size_t >( i ) * D + a ) * 2 );
-    qhi[a] = __ldg( qbox + ( static_cast< size_t >( i ) * D + a ) * 2 + 1 );
+    qlo[a] = __ldg( qb + 2 * a );
+    qhi[a] = __ldg( qb + 2 * a + 1 );
+    o = o && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
   }
+  if ( !o ) return;
+#pragma unroll
+  for ( int a = D0; a < D; ++a )
+  {
+    qlo[a] = __ldg( qb + 2 * a );
+    qhi[a] = __ldg( qb + 2 * a + 1 );
+    o = o && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
+  }
+  if ( !o ) return;
   const uint32_t qe = __ldg( qperm + i );
   const int root = tsc->root;
   if ( nt == 1 )
   {
-    if ( self ) return;
-    bool o = true;
-#pragma unroll
-    for ( int a = 0; a < D; ++a ) o = o && ( qlo[a] < tleaf[2 * a + 1] && tleaf[2 * a] < qhi[a] );
-    if ( o ) emit( qe, static_cast< uint32_t >( ~root ), pairs, cap, ps );
+    if ( !self ) emit( qe, static_cast< uint32_t >( ~root ), pairs, cap, ps );  // the root box is the leaf box
     return;
   }
   int stack[kStack];

@@ -159,20 +159,50 @@ __device__ __forceinline__ void leaf_slabs(const double *__restrict__ verts, uin
   }
 }
 
+// The root's slabs, for the traversal's first test.
+template< typename T, size_t D >
+__device__ __forceinline__ void store_root(obj_scalars *sc, const T ( &lo )[D], const T ( &hi )[D])
+{
+  T *rb = reinterpret_cast< T * >( sc->root_box );
+#pragma unroll
+  for ( size_t a = 0; a < D; ++a )
+  {
+    rb[2 * a] = lo[a];
+    rb[2 * a + 1] = hi[a];
+  }
+}
+
+// Dissimilarity from two adjacent keys (see delta()).
+__device__ __forceinline__ int delta_of(uint64_t a, uint64_t b, int j)
+{
+  const uint64_t x = a ^ b;
+  if ( x ) return 96 - __clzll( static_cast< long long >( x ) );
+  return 32 - __clz( j ^ ( j + 1 ) );
+}
+
+// Phase 1 (one thread per leaf rank i): the leaf's slabs (written to leaf_box in rank order), then
+// warp-synchronous agglomeration: a node whose two children are both finished by lanes of this warp is merged in
+// registers (the two lanes meet on the same parent index; the left lane absorbs the right one's slabs by
+// shuffle). The dissimilarities of the warp's adjacent keys live in registers, so this phase touches no global
+// state but its own outputs. Lanes left waiting when no pair meets any more publish their subtree's slabs into
+// their parent's slot and are queued for phase 2 as (parent * 2 + side, l, r, node).
 template< int K, typename T, int VT >
-__global__ void __launch_bounds__( kBuildThreads ) k_build(const double *__restrict__ verts, uint32_t Vrt, int n,
-                                                         double eps, float eps_hi,
-                                                         const uint64_t *__restrict__ keys,
-                                                         const uint32_t *__restrict__ vals, T *__restrict__ leaf_box,
-                                                         T *node_box, int *child, int2 *__restrict__ range,
-                                                         int *__restrict__ parent, int *exch, obj_scalars *sc)
+__global__ void __launch_bounds__( kBuildThreads ) k_build_leaf(const double *__restrict__ verts, uint32_t Vrt, int n,
+                                                              double eps, float eps_hi,
+                                                              const uint64_t *__restrict__ keys,
+                                                              const uint32_t *__restrict__ vals,
+                                                              T *__restrict__ leaf_box, T *__restrict__ node_box,
+                                                              int *__restrict__ child, int2 *__restrict__ range,
+                                                              int *__restrict__ parent, int4 *__restrict__ queue,
+                                                              obj_scalars *sc)
 {
   constexpr int D = K / 2;
   using io = box_io< T >;
   const int i = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
   const int lane = threadIdx.x & 31;
+  const int wbase = i - lane;
   // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word).
-  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // grid-uniform
+  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // same value for all lanes
   bool active = i < n;
   const uint32_t e = active ? __ldg( vals + i ) : 0u;
   if ( active && e >= static_cast< uint32_t >( n ) )
@@ -180,6 +210,15 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build(const double *__restr
     atomicCAS( &sc->error, 0, kErrTimeout );
     active = false;
   }
+  // dissimilarity of ranks (i, i + 1) and of (wbase - 1, wbase)
+  const uint64_t kself = active ? __ldg( keys + i ) : 0ull;
+  uint64_t knext = __shfl_down_sync( 0xffffffffu, kself, 1 );
+  if ( lane == 31 && i + 1 < n ) knext = __ldg( keys + i + 1 );
+  const int dself = ( i + 1 < n ) ? delta_of( kself, knext, i ) : 0;
+  int dleft = 0;
+  if ( lane == 0 && wbase >= 1 && wbase < n ) dleft = delta_of( __ldg( keys + wbase - 1 ), kself, wbase - 1 );
+  dleft = __shfl_sync( 0xffffffffu, dleft, 0 );
+
   T lo[D], hi[D];
   if ( active )
   {
@@ -192,25 +231,28 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build(const double *__restr
   }
   if ( n == 1 )
   {
-    if ( active ) sc->root = ~static_cast< int >( e );
+    if ( active )
+    {
+      sc->root = ~static_cast< int >( e );
+      store_root( sc, lo, hi );
+    }
     return;
   }
   int l = i, r = i;
   int node = ~static_cast< int >( e );
   int self_slot = i;  // index into parent[]: leaves [0, n), internal nodes n + k
-
-  // Phase 1, warp-synchronous: a node whose two children are both finished by lanes of this warp is merged in
-  // registers (the two lanes meet on the same parent index; the left lane absorbs the right one's slabs by
-  // shuffle). Rounds continue while some pair meets; lanes left waiting go on to the global phase.
+  int par = 0, side = 0;
   while ( true )
   {
-    int par = 0, side = 0;
+    // all lanes take part in the shuffles; ranges of active lanes stay inside [wbase, wbase + 31]
+    const int d_r = __shfl_sync( 0xffffffffu, dself, ( r - wbase ) & 31 );
+    const int d_lm1 = __shfl_sync( 0xffffffffu, dself, ( l - 1 - wbase ) & 31 );
     if ( active )
     {
       bool left_child;
       if ( l == 0 ) left_child = true;
       else if ( r == n - 1 ) left_child = false;
-      else left_child = delta( keys, r ) < delta( keys, l - 1 );
+      else left_child = d_r < ( l == wbase ? dleft : d_lm1 );
       par = left_child ? r : l - 1;
       side = left_child ? 0 : 1;
     }
@@ -249,6 +291,7 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build(const double *__restr
         if ( l == 0 && r == n - 1 )
         {
           sc->root = par;
+          store_root( sc, lo, hi );
           active = false;
         }
       } else {
@@ -256,43 +299,76 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build(const double *__restr
       }
     }
   }
+  // par/side hold this lane's parent from the last round (the round in which nothing paired).
+  const unsigned waiting = __ballot_sync( 0xffffffffu, active );
+  if ( !waiting ) return;
+  unsigned base = 0;
+  if ( lane == 0 ) base = atomicAdd( &sc->climb_count, static_cast< unsigned >( __popc( waiting ) ) );
+  base = __shfl_sync( 0xffffffffu, base, 0 );
   if ( !active ) return;
+  T *pb = node_box + static_cast< size_t >( par ) * D * 4;
+#pragma unroll
+  for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
+  child[2 * par + side] = node;
+  parent[self_slot] = 2 * par + side;
+  queue[base + __popc( waiting & ( ( 1u << lane ) - 1u ) )] = make_int4( 2 * par + side, l, r, node );
+}
 
-  // Phase 2, global: first arrival at a node publishes its slabs and leaves; the second merges and climbs on.
-  // The exchange is an acq_rel atomic: it orders the first arrival's slab stores before it and the second
-  // arrival's slab loads (through L2) after it.
-  while ( true )
+// Phase 2 (dense, one thread per queued subtree): the agglomerative climb with a global exchange slot per node.
+// The first arrival at a node leaves; the second merges and climbs on. The exchange is an acq_rel atomic:
+// it orders the first arrival's slab stores before it and the second arrival's slab loads (through L2) after
+// it. Slabs written by phase 1 are visible here (kernel boundary).
+template< int K, typename T >
+__global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__restrict__ keys, T *node_box,
+                                                     int *child, int2 *__restrict__ range, int *__restrict__ parent,
+                                                     int *exch, const int4 *__restrict__ queue, obj_scalars *sc)
+{
+  constexpr int D = K / 2;
+  using io = box_io< T >;
+  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
+  const unsigned count = *reinterpret_cast< volatile unsigned * >( &sc->climb_count );
+  for ( unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x )
   {
-    bool left_child;  // true: this subtree is the left child of internal node r
-    if ( l == 0 ) left_child = true;
-    else if ( r == n - 1 ) left_child = false;
-    else left_child = delta( keys, r ) < delta( keys, l - 1 );
-    const int par = left_child ? r : l - 1;
-    const int side = left_child ? 0 : 1;
+    const int4 w = queue[q];
+    int par = w.x >> 1, side = w.x & 1, l = w.y, r = w.z;
+    T lo[D], hi[D];
     T *pb = node_box + static_cast< size_t >( par ) * D * 4;
 #pragma unroll
-    for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
-    child[2 * par + side] = node;
-    parent[self_slot] = 2 * par + side;
-    const int other = atomic_exch_acq_rel( exch + par, left_child ? l : r );
-    if ( other < 0 ) return;  // first arrival: the sibling's thread finishes this node
-    if ( left_child ) r = other;
-    else l = other;
+    for ( int a = 0; a < D; ++a ) io::load2_cg( pb + a * 4 + side * 2, lo[a], hi[a] );
+    while ( true )
+    {
+      const int other = atomic_exch_acq_rel( exch + par, side == 0 ? l : r );
+      if ( other < 0 ) break;  // first arrival: the sibling's thread finishes this node
+      if ( side == 0 ) r = other;
+      else l = other;
 #pragma unroll
-    for ( int a = 0; a < D; ++a )
-    {
-      T sl, sh;
-      io::load2_cg( pb + a * 4 + ( 1 - side ) * 2, sl, sh );
-      lo[a] = io::mn( lo[a], sl );
-      hi[a] = io::mx( hi[a], sh );
-    }
-    range[par] = make_int2( l, r );
-    node = par;
-    self_slot = n + par;
-    if ( l == 0 && r == n - 1 )
-    {
-      sc->root = par;
-      return;
+      for ( int a = 0; a < D; ++a )
+      {
+        T sl, sh;
+        io::load2_cg( pb + a * 4 + ( 1 - side ) * 2, sl, sh );
+        lo[a] = io::mn( lo[a], sl );
+        hi[a] = io::mx( hi[a], sh );
+      }
+      range[par] = make_int2( l, r );
+      if ( l == 0 && r == n - 1 )
+      {
+        sc->root = par;
+        store_root( sc, lo, hi );
+        break;
+      }
+      const int node = par;
+      const int self_slot = n + par;
+      bool left_child;
+      if ( l == 0 ) left_child = true;
+      else if ( r == n - 1 ) left_child = false;
+      else left_child = delta( keys, r ) < delta( keys, l - 1 );
+      par = left_child ? r : l - 1;
+      side = left_child ? 0 : 1;
+      pb = node_box + static_cast< size_t >( par ) * D * 4;
+#pragma unroll
+      for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
+      child[2 * par + side] = node;
+      parent[self_slot] = 2 * par + side;
     }
   }
 }
@@ -304,7 +380,7 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restr
                                                          double eps, float eps_hi, const uint32_t *__restrict__ vals,
                                                          T *__restrict__ leaf_box, T *node_box,
                                                          const int *__restrict__ parent, int *exch,
-                                                         const obj_scalars *__restrict__ sc)
+                                                         obj_scalars *__restrict__ sc)
 {
   constexpr int D = K / 2;
   using io = box_io< T >;
@@ -315,7 +391,11 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restr
   leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
 #pragma unroll
   for ( int a = 0; a < D; ++a ) io::store2( leaf_box + ( static_cast< size_t >( i ) * D + a ) * 2, lo[a], hi[a] );
-  if ( n == 1 ) return;
+  if ( n == 1 )
+  {
+    store_root( sc, lo, hi );
+    return;
+  }
   const int root = sc->root;
   int slot = i;
   while ( true )
@@ -335,7 +415,11 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restr
       lo[a] = io::mn( lo[a], sl );
       hi[a] = io::mx( hi[a], sh );
     }
-    if ( par == root ) return;
+    if ( par == root )
+    {
+      store_root( sc, lo, hi );
+      return;
+    }
     slot = n + par;
   }
 }
@@ -343,19 +427,27 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restr
 template< int K, typename T, int VT >
 cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys,
                            const uint32_t *vals, void *leaf_box, void *node_box, int2 *child, int2 *range, int *parent,
-                           int *exch, obj_scalars *sc, cudaStream_t s)
+                           int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
   const float eps_hi = f32_up( eps );
   const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
-  k_build< K, T, VT ><<< grid, kBuildThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals,
-                                                       static_cast< T * >( leaf_box ), static_cast< T * >( node_box ),
-                                                       reinterpret_cast< int * >( child ), range, parent, exch, sc );
+  k_build_leaf< K, T, VT ><<< grid, kBuildThreads, 0, s >>>(
+    verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals, static_cast< T * >( leaf_box ),
+    static_cast< T * >( node_box ), reinterpret_cast< int * >( child ), range, parent, queue, sc );
+  cudaError_t e = cudaGetLastError();
+  if ( e != cudaSuccess || n < 2 ) return e;
+  // The queue length is known only on the device: a grid-stride grid covering the worst case n / 2 for the
+  // usual fraction (a few percent) in one sweep.
+  const uint64_t want = ( n / 16 + 127 ) / 128;
+  const unsigned cgrid = static_cast< unsigned >( want < 148 * 16 ? ( want ? want : 1 ) : 148 * 16 );
+  k_build_climb< K, T ><<< cgrid, 128, 0, s >>>( static_cast< int >( n ), keys, static_cast< T * >( node_box ),
+                                                reinterpret_cast< int * >( child ), range, parent, exch, queue, sc );
   return cudaGetLastError();
 }
 
 template< int K, typename T, int VT >
 cudaError_t launch_refit_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
-                           void *leaf_box, void *node_box, const int *parent, int *exch, const obj_scalars *sc,
+                           void *leaf_box, void *node_box, const int *parent, int *exch, obj_scalars *sc,
                            cudaStream_t s)
 {
   const float eps_hi = f32_up( eps );
@@ -368,20 +460,21 @@ cudaError_t launch_refit_t(const double *verts, uint32_t V, uint64_t n, double e
 
 template< int K, typename T >
 cudaError_t build_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys, const uint32_t *vals,
-                    void *lb, void *nb, int2 *child, int2 *range, int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
+                    void *lb, void *nb, int2 *child, int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc,
+                    cudaStream_t s)
 {
   switch ( V )
   {
-    case 3: return launch_build_t< K, T, 3 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, sc, s );
-    case 4: return launch_build_t< K, T, 4 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, sc, s );
-    case 8: return launch_build_t< K, T, 8 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, sc, s );
-    default: return launch_build_t< K, T, 0 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, sc, s );
+    case 3: return launch_build_t< K, T, 3 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, queue, sc, s );
+    case 4: return launch_build_t< K, T, 4 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, queue, sc, s );
+    case 8: return launch_build_t< K, T, 8 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, queue, sc, s );
+    default: return launch_build_t< K, T, 0 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, queue, sc, s );
   }
 }
 
 template< int K, typename T >
 cudaError_t refit_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *lb, void *nb,
-                    const int *parent, int *exch, const obj_scalars *sc, cudaStream_t s)
+                    const int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
 {
   switch ( V )
   {
@@ -425,12 +518,12 @@ cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, voi
 
 cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
                          const uint64_t *keys, const uint32_t *vals, void *leaf_box, void *node_box, int2 *child,
-                         int2 *range, int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
+                         int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
 #define BVHG_BUILD_CASE( KK )                                                                                           \
   case KK:                                                                                                             \
-    return fp32 ? build_v< KK, float >( verts, V, n, eps, keys, vals, leaf_box, node_box, child, range, parent, exch, sc, s ) \
-                : build_v< KK, double >( verts, V, n, eps, keys, vals, leaf_box, node_box, child, range, parent, exch, sc, s );
+    return fp32 ? build_v< KK, float >( verts, V, n, eps, keys, vals, leaf_box, node_box, child, range, parent, exch, queue, sc, s ) \
+                : build_v< KK, double >( verts, V, n, eps, keys, vals, leaf_box, node_box, child, range, parent, exch, queue, sc, s );
   switch ( K )
   {
     BVHG_BUILD_CASE( 6 )
