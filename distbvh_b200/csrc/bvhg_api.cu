@@ -5,6 +5,7 @@
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -69,8 +70,19 @@ struct object
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
   dev_buf hist, status;
-  dev_buf leaf_box, node_box, child, range, parent, exch, queue;
+  dev_buf warp_box, node_box, child, range, parent, exch, queue;
   dev_buf scal;  // obj_scalars
+  // Each object's build runs on its own stream, forked from and joined back into the context stream with
+  // events, so two objects' builds overlap (one's latency-bound tree climb beside the other's streaming kernels).
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+  ~object()
+  {
+    if ( st ) cudaStreamSynchronize( st );
+    if ( done ) cudaEventDestroy( done );
+    if ( st ) cudaStreamDestroy( st );
+  }
   obj_scalars *sc() const { return scal.as< obj_scalars >(); }
   const uint64_t *sorted_keys() const { return sort_result_alt ? keys_alt.as< uint64_t >() : keys.as< uint64_t >(); }
   const uint32_t *sorted_vals() const { return sort_result_alt ? vals_alt.as< uint32_t >() : vals.as< uint32_t >(); }
@@ -92,6 +104,7 @@ struct bvhg_ctx
   uint32_t spin_limit = kDefaultSpinLimit;
   int stall_sort = 0;  // test hook: radix look-back polls a status row nobody publishes
   std::vector< std::unique_ptr< object > > objs;
+  cudaEvent_t fork_evt = nullptr;
   std::string err;
   // pairs
   dev_buf pairs, pairs2, pairs_out, pscal;
@@ -184,6 +197,35 @@ void collect_timing(bvhg_ctx *ctx)
   ctx->pending.clear();
 }
 
+// The stream an object's build runs on: its own, ordered after everything already on the context stream.
+// With stage timing the context stream itself (stages then never overlap and their times are per kernel).
+cudaError_t fork_object(bvhg_ctx *ctx, object &o, cudaStream_t *out)
+{
+  if ( ctx->cfg.flags & BVHG_FLAG_STAGE_TIMING )
+  {
+    *out = ctx->stream;
+    return cudaSuccess;
+  }
+  cudaError_t e = cudaSuccess;
+  if ( !o.st ) e = cudaStreamCreateWithFlags( &o.st, cudaStreamNonBlocking );
+  if ( e == cudaSuccess && !o.done ) e = cudaEventCreateWithFlags( &o.done, cudaEventDisableTiming );
+  if ( e == cudaSuccess && !ctx->fork_evt ) e = cudaEventCreateWithFlags( &ctx->fork_evt, cudaEventDisableTiming );
+  if ( e == cudaSuccess ) e = cudaEventRecord( ctx->fork_evt, ctx->stream );
+  if ( e == cudaSuccess ) e = cudaStreamWaitEvent( o.st, ctx->fork_evt, 0 );
+  *out = o.st;
+  return e;
+}
+
+// Orders the context stream after the object's last build.
+void join_object(bvhg_ctx *ctx, object &o)
+{
+  if ( o.pending )
+  {
+    cudaStreamWaitEvent( ctx->stream, o.done, 0 );
+    o.pending = false;
+  }
+}
+
 bool valid_obj(bvhg_ctx *ctx, int32_t obj)
 {
   return ctx && obj >= 0 && static_cast< size_t >( obj ) < ctx->objs.size() && ctx->objs[obj];
@@ -207,25 +249,52 @@ bvhg_status check_scalar_errors(bvhg_ctx *ctx, const object &o)
   return object_error( ctx, ctx->host_err[0] );
 }
 
+bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s);
+
 bvhg_status do_build(bvhg_ctx *ctx, object &o, int mode)
 {
   const uint64_t n = o.n;
   const int K = ctx->cfg.k;
   const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
   const int D = K / 2;
-  cudaStream_t s = ctx->stream;
   if ( n == 0 )
   {
     o.built = true;
     return BVHG_OK;
   }
+  cudaStream_t s = nullptr;
+  BVHG_CUDA( ctx, fork_object( ctx, o, &s ) );
+  if ( s != ctx->stream )
+  {
+    // recorded when this call returns, whatever path it takes
+    struct recorder
+    {
+      object &o;
+      cudaStream_t s;
+      ~recorder()
+      {
+        cudaEventRecord( o.done, s );
+        o.pending = true;
+      }
+    } rec{ o, s };
+    return do_build_on( ctx, o, mode, s );
+  }
+  return do_build_on( ctx, o, mode, s );
+}
+
+bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
+{
+  const uint64_t n = o.n;
+  const int K = ctx->cfg.k;
+  const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
+  const int D = K / 2;
   const size_t sb = slab_bytes( ctx );
   if ( mode == BVHG_REFIT )
   {
     if ( !o.topo ) return fail( ctx, BVHG_ERR_STATE, "refit without a rebuild of this element count" );
     stage_scope st( ctx, BVHG_STAGE_BUILD );
     if ( n > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( n - 1 ) * sizeof( int ), s ) );
-    BVHG_CUDA( ctx, launch_refit( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.leaf_box.p,
+    BVHG_CUDA( ctx, launch_refit( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.warp_box.p,
                                   o.node_box.p, o.parent.as< int >(), o.exch.as< int >(), o.sc(), s ) );
     st.launched();
     o.built = true;
@@ -246,7 +315,7 @@ bvhg_status do_build(bvhg_ctx *ctx, object &o, int mode)
   BVHG_CUDA( ctx, o.vals_alt.reserve( n * 4 ) );
   BVHG_CUDA( ctx, o.hist.reserve( passes * radix * 4 ) );
   BVHG_CUDA( ctx, o.status.reserve( passes * ( tiles + 1 ) * radix * 4 ) );
-  BVHG_CUDA( ctx, o.leaf_box.reserve( n * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.node_box.reserve( ( n - 1 ) * D * 4 * sb + 16 ) );
   BVHG_CUDA( ctx, o.child.reserve( ( n - 1 ) * 8 + 8 ) );
   BVHG_CUDA( ctx, o.range.reserve( ( n - 1 ) * 8 + 8 ) );
@@ -289,7 +358,7 @@ bvhg_status do_build(bvhg_ctx *ctx, object &o, int mode)
   {
     stage_scope st( ctx, BVHG_STAGE_BUILD );
     BVHG_CUDA( ctx, launch_build( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_keys(), o.sorted_vals(),
-                                  o.leaf_box.p, o.node_box.p, o.child.as< int2 >(), o.range.as< int2 >(),
+                                  o.warp_box.p, o.node_box.p, o.child.as< int2 >(), o.range.as< int2 >(),
                                   o.parent.as< int >(), o.exch.as< int >(), o.queue.as< int4 >(), o.sc(), s ) );
     st.launched( n > 1 ? 2 : 1 );
   }
@@ -304,7 +373,8 @@ tree_view view_of(const object &o)
   v.node_box = o.node_box.p;
   v.child = o.child.as< int2 >();
   v.range = o.range.as< int2 >();
-  v.leaf_box = o.leaf_box.p;
+  v.warp_box = o.warp_box.p;
+  v.parent = o.parent.as< int >();
   v.perm = o.sorted_vals();
   v.n = o.n;
   v.sc = o.sc();
@@ -466,6 +536,8 @@ bvhg_status bvhg_destroy(bvhg_ctx *ctx)
 {
   if ( !ctx ) return BVHG_ERR_ARG;
   cudaSetDevice( ctx->cfg.device );
+  for ( auto &o : ctx->objs )
+    if ( o ) join_object( ctx, *o );
   cudaStreamSynchronize( ctx->stream );
   collect_timing( ctx );
   for ( auto e : ctx->event_pool ) cudaEventDestroy( e );
@@ -473,6 +545,7 @@ bvhg_status bvhg_destroy(bvhg_ctx *ctx)
   if ( ctx->host_err ) cudaFreeHost( ctx->host_err );
   if ( ctx->init_template ) cudaFreeHost( ctx->init_template );
   ctx->objs.clear();
+  if ( ctx->fork_evt ) cudaEventDestroy( ctx->fork_evt );
   if ( ctx->own_stream ) cudaStreamDestroy( ctx->stream );
   delete ctx;
   return BVHG_OK;
@@ -509,6 +582,7 @@ bvhg_status bvhg_set_elements(bvhg_ctx *ctx, int32_t obj, const double *xyz, uin
   if ( mem != BVHG_MEM_HOST && mem != BVHG_MEM_DEVICE ) return fail( ctx, BVHG_ERR_ARG, "bad memory kind" );
   cudaSetDevice( ctx->cfg.device );
   object &o = *ctx->objs[obj];
+  join_object( ctx, o );  // the last build may still read the owned vertex buffer
   if ( n != o.n || V != o.V ) o.topo = false;
   o.n = n;
   o.V = V;
@@ -561,6 +635,8 @@ bvhg_status bvhg_broadphase(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, uint64_
   object &b = *ctx->objs[obj_b];
   if ( !a.built || !b.built ) return fail( ctx, BVHG_ERR_STATE, "broadphase before build" );
   cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, a );
+  join_object( ctx, b );
   *count = 0;
   if ( a.n == 0 || b.n == 0 )
   {
@@ -583,6 +659,7 @@ bvhg_status bvhg_self_collision(bvhg_ctx *ctx, int32_t obj, uint64_t *pairs, uin
   object &o = *ctx->objs[obj];
   if ( !o.built ) return fail( ctx, BVHG_ERR_STATE, "self_collision before build" );
   cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, o );
   *count = 0;
   if ( o.n < 2 )
   {
@@ -603,6 +680,7 @@ bvhg_status bvhg_get_morton(bvhg_ctx *ctx, int32_t obj, uint64_t *sorted_keys, u
   object &o = *ctx->objs[obj];
   if ( !o.built ) return fail( ctx, BVHG_ERR_STATE, "probe before build" );
   cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, o );
   BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
   if ( o.n == 0 ) return BVHG_OK;
   bvhg_status st = check_scalar_errors( ctx, o );
@@ -622,6 +700,7 @@ static bvhg_status probe_kdops(bvhg_ctx *ctx, int32_t obj, void *out, bool fp32)
   object &o = *ctx->objs[obj];
   if ( !o.has_data ) return fail( ctx, BVHG_ERR_STATE, "probe before set_elements" );
   cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, o );
   if ( o.n == 0 ) return BVHG_OK;
   const int D = ctx->cfg.k / 2;
   const size_t bytes = o.n * D * 2 * ( fp32 ? 4 : 8 );
@@ -652,6 +731,7 @@ bvhg_status bvhg_get_centroids(bvhg_ctx *ctx, int32_t obj, double *centroids)
   object &o = *ctx->objs[obj];
   if ( !o.built ) return fail( ctx, BVHG_ERR_STATE, "probe before build" );
   cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, o );
   BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
   if ( o.n == 0 ) return BVHG_OK;
   std::vector< double > x( o.n ), y( o.n ), z( o.n );
@@ -673,37 +753,75 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
   object &o = *ctx->objs[obj];
   if ( !o.built ) return fail( ctx, BVHG_ERR_STATE, "validate before build" );
   cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, o );
   BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
   if ( depth_out ) *depth_out = 0;
   const uint64_t n = o.n;
-  if ( n <= 1 ) return BVHG_OK;
+  if ( n == 0 ) return BVHG_OK;
   const int D = ctx->cfg.k / 2;
   const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
+  const size_t sb = fp32 ? 4 : 8;
   const uint64_t m = n - 1;
-  std::vector< int2 > child( m ), range( m );
-  std::vector< uint32_t > perm( n );
-  std::vector< double > nb( m * D * 4 ), lb( n * D * 2 );
-  BVHG_CUDA( ctx, cudaMemcpy( child.data(), o.child.p, m * 8, cudaMemcpyDeviceToHost ) );
-  BVHG_CUDA( ctx, cudaMemcpy( range.data(), o.range.p, m * 8, cudaMemcpyDeviceToHost ) );
-  BVHG_CUDA( ctx, cudaMemcpy( perm.data(), o.sorted_vals(), n * 4, cudaMemcpyDeviceToHost ) );
-  if ( fp32 )
-  {
-    std::vector< float > f( m * D * 4 ), g( n * D * 2 );
-    BVHG_CUDA( ctx, cudaMemcpy( f.data(), o.node_box.p, f.size() * 4, cudaMemcpyDeviceToHost ) );
-    BVHG_CUDA( ctx, cudaMemcpy( g.data(), o.leaf_box.p, g.size() * 4, cudaMemcpyDeviceToHost ) );
-    for ( size_t k = 0; k < f.size(); ++k ) nb[k] = f[k];
-    for ( size_t k = 0; k < g.size(); ++k ) lb[k] = g[k];
-  } else {
-    BVHG_CUDA( ctx, cudaMemcpy( nb.data(), o.node_box.p, nb.size() * 8, cudaMemcpyDeviceToHost ) );
-    BVHG_CUDA( ctx, cudaMemcpy( lb.data(), o.leaf_box.p, lb.size() * 8, cudaMemcpyDeviceToHost ) );
-  }
+  const uint64_t nw = ( n + 31 ) / 32;
+  auto fetch = [&](const void *src, size_t count, std::vector< double > &dst) -> cudaError_t {
+    dst.resize( count );
+    if ( !count ) return cudaSuccess;
+    if ( fp32 )
+    {
+      std::vector< float > f( count );
+      cudaError_t e = cudaMemcpy( f.data(), src, count * 4, cudaMemcpyDeviceToHost );
+      for ( size_t k = 0; k < count; ++k ) dst[k] = f[k];
+      return e;
+    }
+    return cudaMemcpy( dst.data(), src, count * 8, cudaMemcpyDeviceToHost );
+  };
+  // element slabs recomputed from the vertices, original order
+  dev_buf tmp;
+  BVHG_CUDA( ctx, tmp.reserve( n * D * 2 * sb ) );
+  BVHG_CUDA( ctx, launch_probe_kdops( ctx->cfg.k, fp32, o.verts, o.V, n, ctx->cfg.epsilon, tmp.p, ctx->stream ) );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  std::vector< double > lb, nb, wb, rootb;
+  BVHG_CUDA( ctx, fetch( tmp.p, n * D * 2, lb ) );
+  BVHG_CUDA( ctx, fetch( o.node_box.p, m * D * 4, nb ) );
+  BVHG_CUDA( ctx, fetch( o.warp_box.p, nw * D * 2, wb ) );
   obj_scalars h;
   BVHG_CUDA( ctx, cudaMemcpy( &h, o.sc(), sizeof( h ), cudaMemcpyDeviceToHost ) );
+  BVHG_CUDA( ctx, fetch( o.sc()->root_box, D * 2, rootb ) );
+  std::vector< uint32_t > perm( n );
+  BVHG_CUDA( ctx, cudaMemcpy( perm.data(), o.sorted_vals(), n * 4, cudaMemcpyDeviceToHost ) );
+  // every warp box is the union of its ranks' slabs
+  for ( uint64_t w = 0; w < nw; ++w )
+    for ( int a = 0; a < D; ++a )
+    {
+      double lo = 0, hi = 0;
+      for ( uint64_t r = 32 * w; r < n && r < 32 * w + 32; ++r )
+      {
+        const double *l = &lb[static_cast< size_t >( perm[r] ) * D * 2];
+        lo = r == 32 * w ? l[2 * a] : std::min( lo, l[2 * a] );
+        hi = r == 32 * w ? l[2 * a + 1] : std::max( hi, l[2 * a + 1] );
+      }
+      if ( wb[( w * D + a ) * 2] != lo || wb[( w * D + a ) * 2 + 1] != hi )
+        return fail( ctx, BVHG_ERR_STATE, "warp box is not the union of its ranks' slabs" );
+    }
+  if ( n == 1 )
+  {
+    for ( int a = 0; a < 2 * D; ++a )
+      if ( rootb[a] != lb[a] ) return fail( ctx, BVHG_ERR_STATE, "single-element root box differs" );
+    if ( depth_out ) *depth_out = 1;
+    return BVHG_OK;
+  }
+  std::vector< int2 > child( m );
+  BVHG_CUDA( ctx, cudaMemcpy( child.data(), o.child.p, m * 8, cudaMemcpyDeviceToHost ) );
   if ( h.root < 0 || static_cast< uint64_t >( h.root ) >= m ) return fail( ctx, BVHG_ERR_STATE, "bad root" );
-  std::vector< uint32_t > rank_of( n );
-  for ( uint64_t r = 0; r < n; ++r ) rank_of[perm[r]] = static_cast< uint32_t >( r );
+  for ( int a = 0; a < D; ++a )
+  {
+    const double *slot = &nb[static_cast< size_t >( h.root ) * D * 4];
+    if ( rootb[2 * a] != std::min( slot[a * 4], slot[a * 4 + 2] ) ||
+         rootb[2 * a + 1] != std::max( slot[a * 4 + 1], slot[a * 4 + 3] ) )
+      return fail( ctx, BVHG_ERR_STATE, "root box is not the union of the root's children" );
+  }
   std::vector< uint8_t > seen_leaf( n, 0 ), seen_node( m, 0 );
-  // (node, depth); check each child box is inside the slot the parent stores and leaves match leaf_box
+  // (node, depth): every child's slabs lie inside the slot its parent stores for it; leaf slots equal the slabs
   std::vector< std::pair< int, uint32_t > > st{ { h.root, 1u } };
   uint32_t maxd = 0;
   uint64_t leaves = 0, nodes = 0;
@@ -715,9 +833,9 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
     seen_node[k] = 1;
     ++nodes;
     const int c[2] = { child[k].x, child[k].y };
+    const double *slot = &nb[static_cast< size_t >( k ) * D * 4];
     for ( int side = 0; side < 2; ++side )
     {
-      const double *slot = &nb[( static_cast< size_t >( k ) * D ) * 4];
       if ( c[side] < 0 )
       {
         const uint32_t e = static_cast< uint32_t >( ~c[side] );
@@ -725,13 +843,13 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
         seen_leaf[e] = 1;
         ++leaves;
         maxd = d + 1 > maxd ? d + 1 : maxd;
-        const double *l = &lb[static_cast< size_t >( rank_of[e] ) * D * 2];
+        const double *l = &lb[static_cast< size_t >( e ) * D * 2];
         for ( int a = 0; a < D; ++a )
           if ( slot[a * 4 + side * 2] != l[2 * a] || slot[a * 4 + side * 2 + 1] != l[2 * a + 1] )
-            return fail( ctx, BVHG_ERR_STATE, "leaf slot differs from leaf slabs" );
+            return fail( ctx, BVHG_ERR_STATE, "leaf slot differs from the element's slabs" );
       } else {
         if ( static_cast< uint64_t >( c[side] ) >= m ) return fail( ctx, BVHG_ERR_STATE, "bad child index" );
-        const double *cs = &nb[( static_cast< size_t >( c[side] ) * D ) * 4];
+        const double *cs = &nb[static_cast< size_t >( c[side] ) * D * 4];
         for ( int a = 0; a < D; ++a )
         {
           const double lo = slot[a * 4 + side * 2], hi = slot[a * 4 + side * 2 + 1];
@@ -820,6 +938,8 @@ bvhg_status bvhg_synchronize(bvhg_ctx *ctx)
 {
   if ( !ctx ) return BVHG_ERR_ARG;
   cudaSetDevice( ctx->cfg.device );
+  for ( auto &o : ctx->objs )
+    if ( o ) join_object( ctx, *o );
   BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
   for ( auto &o : ctx->objs )
     if ( o && o->built && o->n > 0 )

@@ -6,7 +6,8 @@
 //   cx, cy, cz n doubles each: centroids, structure of arrays (coalesced write in K1, read in K2)
 //   keys/vals  n u64 Morton keys and n u32 element indices, ping-ponged by the radix passes; after the sort
 //              keys[r], vals[r] hold the key and original index of rank r (vals = the permutation)
-//   leaf_box   n * D * 2 T: slabs of the element at rank r, [r][a][min,max] (the query side of traversal)
+//   warp_box   ceil(n / 32) * D * 2 T: union of the slabs of ranks [32 w, 32 w + 31], [w][a][min,max] (the
+//              query side's first cull); a leaf's own slabs are read from its slot in its parent
 //   node_box   (n - 1) * D * 2 * 2 T: both children's slabs of internal node k, [k][a][child][min,max], so one
 //              32-byte (FP64) or 16-byte (FP32) sector per axis tests both children
 //   child      (n - 1) int2: child index, >= 0 internal node, < 0 leaf with ~child = original element index
@@ -94,12 +95,12 @@ cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *v
 // Leaf slabs + agglomerative LBVH build with bottom-up refit (FP64 or FP32 slabs): two launches, a warp-local
 // phase that queues unfinished subtrees (queue: n int4) and a global climb over the queue.
 cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint64_t *keys, const uint32_t *vals, void *leaf_box, void *node_box, int2 *child,
+                         const uint64_t *keys, const uint32_t *vals, void *warp_box, void *node_box, int2 *child,
                          int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s);
 
 // Refit with the topology of the last build: recompute leaf slabs and every internal node.
 cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *leaf_box, void *node_box, const int *parent, int *exch,
+                         const uint32_t *vals, void *warp_box, void *node_box, const int *parent, int *exch,
                          obj_scalars *sc, cudaStream_t s);
 
 struct tree_view
@@ -107,7 +108,8 @@ struct tree_view
   const void *node_box;
   const int2 *child;
   const int2 *range;
-  const void *leaf_box;
+  const void *warp_box;
+  const int *parent;
   const uint32_t *perm;
   uint64_t n;
   const obj_scalars *sc;

@@ -55,46 +55,63 @@ __device__ __forceinline__ void emit(uint32_t a, uint32_t b, uint2 *pairs, uint6
 }
 
 template< int K, typename T >
-__global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict__ qbox,
+__global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict__ qwarp,
+                                                           const T *__restrict__ qnode,
+                                                           const int *__restrict__ qparent,
                                                            const uint32_t *__restrict__ qperm, uint32_t nq,
                                                            const int2 *__restrict__ child,
                                                            const T *__restrict__ nbox,
                                                            const int2 *__restrict__ range,
-                                                           const T *__restrict__ tleaf,
                                                            const obj_scalars *__restrict__ tsc, uint32_t nt,
                                                            const obj_scalars *__restrict__ qsc, int self,
                                                            uint2 *pairs, uint64_t cap, pair_scalars *ps)
 {
   constexpr int D = K / 2;
+  constexpr int D0 = D < 4 ? D : 4;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if ( i >= nq ) return;
   // No tree exists after a failed sort of either object.
   if ( *reinterpret_cast< const volatile int * >( &tsc->error ) == kErrTimeout ||
        *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
     return;
-  // The root box test first, on the first four slabs only (two sectors of the query's slabs in FP64, one in
-  // FP32): most queries of a contact scene end here without reading the rest of their slabs.
-  constexpr int D0 = D < 4 ? D : 4;
-  T qlo[D], qhi[D];
-  const T *qb = qbox + static_cast< size_t >( i ) * D * 2;
+  if ( ( i & ~31u ) >= nq ) return;  // warps entirely past the last rank have no warp box
   const T *rb = reinterpret_cast< const T * >( tsc->root_box );
-  bool o = true;
-#pragma unroll
-  for ( int a = 0; a < D0; ++a )
+  // 1. The union box of this warp's 32 query ranks against the target's root box, first four slabs first: a warp
+  //    of queries far from the other object stops after one broadcast load.
   {
-    qlo[a] = __ldg( qb + 2 * a );
-    qhi[a] = __ldg( qb + 2 * a + 1 );
-    o = o && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
-  }
-  if ( !o ) return;
+    const T *wb = qwarp + static_cast< size_t >( i >> 5 ) * D * 2;
+    bool o = true;
 #pragma unroll
-  for ( int a = D0; a < D; ++a )
-  {
-    qlo[a] = __ldg( qb + 2 * a );
-    qhi[a] = __ldg( qb + 2 * a + 1 );
-    o = o && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
+    for ( int a = 0; a < D0; ++a ) o = o && ( __ldg( wb + 2 * a ) < rb[2 * a + 1] && rb[2 * a] < __ldg( wb + 2 * a + 1 ) );
+    if ( !o ) return;
+#pragma unroll
+    for ( int a = D0; a < D; ++a ) o = o && ( __ldg( wb + 2 * a ) < rb[2 * a + 1] && rb[2 * a] < __ldg( wb + 2 * a + 1 ) );
+    if ( !o ) return;
   }
-  if ( !o ) return;
+  if ( i >= nq ) return;
+  // 2. The query's own slabs: from its slot in its parent (or the root box of a one-element object).
+  T qlo[D], qhi[D];
+  {
+    const T *qs;
+    int stride;
+    if ( nq == 1 )
+    {
+      qs = reinterpret_cast< const T * >( qsc->root_box );
+      stride = 2;
+    } else {
+      const int pp = __ldg( qparent + i );
+      qs = qnode + static_cast< size_t >( pp >> 1 ) * D * 4 + ( pp & 1 ) * 2;
+      stride = 4;
+    }
+    bool o = true;
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      qlo[a] = __ldg( qs + stride * a );
+      qhi[a] = __ldg( qs + stride * a + 1 );
+      o = o && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
+    }
+    if ( !o ) return;
+  }
   const uint32_t qe = __ldg( qperm + i );
   const int root = tsc->root;
   if ( nt == 1 )
@@ -159,8 +176,8 @@ cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, uint2 *pairs, uin
 {
   const unsigned grid = static_cast< unsigned >( ( q.n + kTravThreads - 1 ) / kTravThreads );
   k_traverse< K, T ><<< grid, kTravThreads, 0, s >>>(
-    static_cast< const T * >( q.leaf_box ), q.perm, static_cast< uint32_t >( q.n ), t.child,
-    static_cast< const T * >( t.node_box ), t.range, static_cast< const T * >( t.leaf_box ), t.sc,
+    static_cast< const T * >( q.warp_box ), static_cast< const T * >( q.node_box ), q.parent, q.perm,
+    static_cast< uint32_t >( q.n ), t.child, static_cast< const T * >( t.node_box ), t.range, t.sc,
     static_cast< uint32_t >( t.n ), q.sc, self ? 1 : 0, pairs, cap, ps );
   return cudaGetLastError();
 }

@@ -159,6 +159,28 @@ __device__ __forceinline__ void leaf_slabs(const double *__restrict__ verts, uin
   }
 }
 
+// Union of the slabs of the warp's 32 consecutive ranks (lanes past n contribute nothing), one box per warp.
+template< typename T, int D >
+__device__ __forceinline__ void store_warp_box(T *warp_box, int wbase, int n, bool active, const T *lo, const T *hi)
+{
+  using io = box_io< T >;
+  const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for ( int a = 0; a < D; ++a )
+  {
+    T l = active ? lo[a] : inf;
+    T h = active ? hi[a] : -inf;
+#pragma unroll
+    for ( int o = 16; o > 0; o >>= 1 )
+    {
+      l = io::mn( l, __shfl_xor_sync( 0xffffffffu, l, o ) );
+      h = io::mx( h, __shfl_xor_sync( 0xffffffffu, h, o ) );
+    }
+    if ( lane == 0 && wbase < n ) io::store2( warp_box + ( static_cast< size_t >( wbase >> 5 ) * D + a ) * 2, l, h );
+  }
+}
+
 // The root's slabs, for the traversal's first test.
 template< typename T, size_t D >
 __device__ __forceinline__ void store_root(obj_scalars *sc, const T ( &lo )[D], const T ( &hi )[D])
@@ -180,7 +202,8 @@ __device__ __forceinline__ int delta_of(uint64_t a, uint64_t b, int j)
   return 32 - __clz( j ^ ( j + 1 ) );
 }
 
-// Phase 1 (one thread per leaf rank i): the leaf's slabs (written to leaf_box in rank order), then
+// Phase 1 (one thread per leaf rank i): the leaf's slabs (their union over the warp's 32 ranks goes to warp_box,
+// the traversal's first cull), then
 // warp-synchronous agglomeration: a node whose two children are both finished by lanes of this warp is merged in
 // registers (the two lanes meet on the same parent index; the left lane absorbs the right one's slabs by
 // shuffle). The dissimilarities of the warp's adjacent keys live in registers, so this phase touches no global
@@ -191,7 +214,7 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build_leaf(const double *__
                                                               double eps, float eps_hi,
                                                               const uint64_t *__restrict__ keys,
                                                               const uint32_t *__restrict__ vals,
-                                                              T *__restrict__ leaf_box, T *__restrict__ node_box,
+                                                              T *__restrict__ warp_box, T *__restrict__ node_box,
                                                               int *__restrict__ child, int2 *__restrict__ range,
                                                               int *__restrict__ parent, int4 *__restrict__ queue,
                                                               obj_scalars *sc)
@@ -223,12 +246,11 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build_leaf(const double *__
   if ( active )
   {
     leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
-#pragma unroll
-    for ( int a = 0; a < D; ++a ) io::store2( leaf_box + ( static_cast< size_t >( i ) * D + a ) * 2, lo[a], hi[a] );
   } else {
 #pragma unroll
     for ( int a = 0; a < D; ++a ) lo[a] = hi[a] = T( 0 );
   }
+  store_warp_box< T, D >( warp_box, wbase, n, active, lo, hi );
   if ( n == 1 )
   {
     if ( active )
@@ -378,19 +400,25 @@ __global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__
 template< int K, typename T, int VT >
 __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restrict__ verts, uint32_t Vrt, int n,
                                                          double eps, float eps_hi, const uint32_t *__restrict__ vals,
-                                                         T *__restrict__ leaf_box, T *node_box,
+                                                         T *__restrict__ warp_box, T *node_box,
                                                          const int *__restrict__ parent, int *exch,
                                                          obj_scalars *__restrict__ sc)
 {
   constexpr int D = K / 2;
   using io = box_io< T >;
   const int i = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
-  if ( i >= n ) return;
-  const uint32_t e = __ldg( vals + i );
+  const bool active = i < n;
+  const uint32_t e = active ? __ldg( vals + i ) : 0u;
   T lo[D], hi[D];
-  leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
+  if ( active )
+  {
+    leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
+  } else {
 #pragma unroll
-  for ( int a = 0; a < D; ++a ) io::store2( leaf_box + ( static_cast< size_t >( i ) * D + a ) * 2, lo[a], hi[a] );
+    for ( int a = 0; a < D; ++a ) lo[a] = hi[a] = T( 0 );
+  }
+  store_warp_box< T, D >( warp_box, i - ( static_cast< int >( threadIdx.x ) & 31 ), n, active, lo, hi );
+  if ( !active ) return;
   if ( n == 1 )
   {
     store_root( sc, lo, hi );
@@ -426,13 +454,13 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restr
 
 template< int K, typename T, int VT >
 cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys,
-                           const uint32_t *vals, void *leaf_box, void *node_box, int2 *child, int2 *range, int *parent,
+                           const uint32_t *vals, void *warp_box, void *node_box, int2 *child, int2 *range, int *parent,
                            int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
   const float eps_hi = f32_up( eps );
   const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
   k_build_leaf< K, T, VT ><<< grid, kBuildThreads, 0, s >>>(
-    verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals, static_cast< T * >( leaf_box ),
+    verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals, static_cast< T * >( warp_box ),
     static_cast< T * >( node_box ), reinterpret_cast< int * >( child ), range, parent, queue, sc );
   cudaError_t e = cudaGetLastError();
   if ( e != cudaSuccess || n < 2 ) return e;
@@ -447,13 +475,13 @@ cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double e
 
 template< int K, typename T, int VT >
 cudaError_t launch_refit_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
-                           void *leaf_box, void *node_box, const int *parent, int *exch, obj_scalars *sc,
+                           void *warp_box, void *node_box, const int *parent, int *exch, obj_scalars *sc,
                            cudaStream_t s)
 {
   const float eps_hi = f32_up( eps );
   const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
   k_refit< K, T, VT ><<< grid, kBuildThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, eps_hi, vals,
-                                                       static_cast< T * >( leaf_box ), static_cast< T * >( node_box ),
+                                                       static_cast< T * >( warp_box ), static_cast< T * >( node_box ),
                                                        parent, exch, sc );
   return cudaGetLastError();
 }
@@ -517,13 +545,13 @@ cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, voi
 }  // namespace
 
 cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint64_t *keys, const uint32_t *vals, void *leaf_box, void *node_box, int2 *child,
+                         const uint64_t *keys, const uint32_t *vals, void *warp_box, void *node_box, int2 *child,
                          int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
 #define BVHG_BUILD_CASE( KK )                                                                                           \
   case KK:                                                                                                             \
-    return fp32 ? build_v< KK, float >( verts, V, n, eps, keys, vals, leaf_box, node_box, child, range, parent, exch, queue, sc, s ) \
-                : build_v< KK, double >( verts, V, n, eps, keys, vals, leaf_box, node_box, child, range, parent, exch, queue, sc, s );
+    return fp32 ? build_v< KK, float >( verts, V, n, eps, keys, vals, warp_box, node_box, child, range, parent, exch, queue, sc, s ) \
+                : build_v< KK, double >( verts, V, n, eps, keys, vals, warp_box, node_box, child, range, parent, exch, queue, sc, s );
   switch ( K )
   {
     BVHG_BUILD_CASE( 6 )
@@ -535,17 +563,17 @@ cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint
 }
 
 cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *leaf_box, void *node_box, const int *parent, int *exch,
+                         const uint32_t *vals, void *warp_box, void *node_box, const int *parent, int *exch,
                          obj_scalars *sc, cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return fp32 ? refit_v< 6, float >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s )
-                        : refit_v< 6, double >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s );
-    case 18: return fp32 ? refit_v< 18, float >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s )
-                         : refit_v< 18, double >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s );
-    case 26: return fp32 ? refit_v< 26, float >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s )
-                         : refit_v< 26, double >( verts, V, n, eps, vals, leaf_box, node_box, parent, exch, sc, s );
+    case 6: return fp32 ? refit_v< 6, float >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s )
+                        : refit_v< 6, double >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s );
+    case 18: return fp32 ? refit_v< 18, float >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s )
+                         : refit_v< 18, double >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s );
+    case 26: return fp32 ? refit_v< 26, float >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s )
+                         : refit_v< 26, double >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s );
     default: return cudaErrorInvalidValue;
   }
 }
