@@ -20,6 +20,7 @@ constexpr uint32_t kFlagAggregate = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kValueMask = ( 1u << 30 ) - 1;
 constexpr int kWarps = kSortThreads / 32;
+constexpr int kLookback = 8;  // predecessor status words fetched per look-back step
 
 // Exclusive scan of one value per thread over a 256-thread block.
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s_warp)
@@ -120,14 +121,12 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
     uint32_t excl = 0;
     if ( tile > 0 )
     {
-      // Test hook: poll the spare status row after the last tile, which no block ever publishes.
-      int64_t p = stall ? static_cast< int64_t >( gridDim.x ) : static_cast< int64_t >( tile ) - 1;
+      const volatile uint32_t *vs = reinterpret_cast< const volatile uint32_t * >( status );
       uint32_t spins = 0;
-      while ( true )
+      if ( stall )
       {
-        const uint32_t s = reinterpret_cast< volatile uint32_t * >( status )[p * RADIX + tid];
-        const uint32_t flag = s & ~kValueMask;
-        if ( flag == 0 )
+        // Test hook: poll the spare status row after the last tile, which no block ever publishes.
+        while ( ( vs[static_cast< uint64_t >( gridDim.x ) * RADIX + tid] & ~kValueMask ) == 0 )
         {
           if ( ++spins > spin_limit )
           {
@@ -136,11 +135,41 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
             break;
           }
           __nanosleep( 32 );
-          continue;
         }
-        excl += s & kValueMask;
-        if ( flag == kFlagPrefix || p == 0 || stall ) break;
-        --p;
+      } else {
+        // Look back over a window of kLookback predecessors per step: their status words are fetched together
+        // (independent loads in flight) and consumed nearest first until an inclusive prefix is found.
+        int64_t p = static_cast< int64_t >( tile ) - 1;
+        bool done = false;
+        while ( !done )
+        {
+          uint32_t w[kLookback];
+#pragma unroll
+          for ( int q = 0; q < kLookback; ++q ) w[q] = ( p - q >= 0 ) ? vs[( p - q ) * RADIX + tid] : kFlagPrefix;
+          int consumed = 0;
+#pragma unroll
+          for ( int q = 0; q < kLookback; ++q )
+          {
+            if ( done || consumed < q ) break;  // stop at the first word that was not ready
+            const uint32_t flag = w[q] & ~kValueMask;
+            if ( flag == 0 ) break;
+            excl += w[q] & kValueMask;
+            consumed = q + 1;
+            if ( flag == kFlagPrefix ) done = true;
+          }
+          if ( done ) break;
+          p -= consumed;
+          if ( consumed == 0 )
+          {
+            if ( ++spins > spin_limit )
+            {
+              atomicCAS( &sc->error, 0, kErrTimeout );
+              __threadfence();
+              break;
+            }
+            __nanosleep( 32 );
+          }
+        }
       }
       reinterpret_cast< volatile uint32_t * >( status )[tile * RADIX + tid] = kFlagPrefix | ( ( excl + total ) & kValueMask );
     }

@@ -210,7 +210,7 @@ __device__ __forceinline__ int delta_of(uint64_t a, uint64_t b, int j)
 // state but its own outputs. Lanes left waiting when no pair meets any more publish their subtree's slabs into
 // their parent's slot and are queued for phase 2 as (parent * 2 + side, l, r, node).
 template< int K, typename T, int VT >
-__global__ void __launch_bounds__( kBuildThreads ) k_build_leaf(const double *__restrict__ verts, uint32_t Vrt, int n,
+__global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double *__restrict__ verts, uint32_t Vrt, int n,
                                                               double eps, float eps_hi,
                                                               const uint64_t *__restrict__ keys,
                                                               const uint32_t *__restrict__ vals,
@@ -322,6 +322,119 @@ __global__ void __launch_bounds__( kBuildThreads ) k_build_leaf(const double *__
     }
   }
   // par/side hold this lane's parent from the last round (the round in which nothing paired).
+
+  // Phase 1b, block-level: the waiting subtrees of all warps of the block meet through shared-memory tables
+  // indexed by the first and the last rank of each subtree. A left child (parent r) looks for a subtree starting
+  // at r + 1 that targets the same parent as right child, a right child (parent l - 1) for one ending at l - 1.
+  // Rounds (each behind block barriers) continue while some pair meets.
+  {
+    extern __shared__ unsigned char s_raw[];
+    T *s_box = reinterpret_cast< T * >( s_raw );  // [kBuildThreads][2 D]
+    __shared__ short s_start[kBuildThreads], s_end[kBuildThreads];
+    __shared__ int s_par[kBuildThreads], s_r[kBuildThreads];
+    __shared__ int s_delta[kBuildThreads + 1];  // dissimilarity of ranks (bbase - 1 + k, bbase + k)
+    const int tid = threadIdx.x;
+    const int bbase = i - tid;
+    s_start[tid] = -1;
+    s_end[tid] = -1;
+    s_delta[tid + 1] = dself;
+    if ( tid == 0 ) s_delta[0] = ( bbase >= 1 && bbase < n ) ? delta( keys, bbase - 1 ) : 0;
+    __syncthreads();
+    while ( true )
+    {
+      if ( active )
+      {
+        s_start[l - bbase] = static_cast< short >( tid );
+        s_end[r - bbase] = static_cast< short >( tid );
+        s_par[tid] = 2 * par + side;
+        s_r[tid] = r;
+#pragma unroll
+        for ( int a = 0; a < D; ++a )
+        {
+          s_box[tid * 2 * D + 2 * a] = lo[a];
+          s_box[tid * 2 * D + 2 * a + 1] = hi[a];
+        }
+      }
+      __syncthreads();
+      int partner = -1;
+      if ( active )
+      {
+        if ( side == 0 )
+        {
+          const int q = r + 1;
+          if ( q < bbase + kBuildThreads && q < n )
+          {
+            const int c = s_start[q - bbase];
+            if ( c >= 0 && s_par[c] == 2 * par + 1 ) partner = c;
+          }
+        } else {
+          const int q = l - 1;
+          if ( q >= bbase )
+          {
+            const int c = s_end[q - bbase];
+            if ( c >= 0 && s_par[c] == 2 * par ) partner = c;
+          }
+        }
+      }
+      const bool paired = partner >= 0;
+      int r2 = r;
+      if ( paired && side == 0 )
+      {
+        r2 = s_r[partner];
+#pragma unroll
+        for ( int a = 0; a < D; ++a )
+        {
+          lo[a] = io::mn( lo[a], s_box[partner * 2 * D + 2 * a] );
+          hi[a] = io::mx( hi[a], s_box[partner * 2 * D + 2 * a + 1] );
+        }
+      }
+      if ( paired )
+      {
+        // both children write the slot their parent keeps for them (own slabs: the pre-merge values, still in
+        // shared memory for the left lane)
+        T *pb = node_box + static_cast< size_t >( par ) * D * 4;
+#pragma unroll
+        for ( int a = 0; a < D; ++a )
+          io::store2( pb + a * 4 + side * 2, s_box[tid * 2 * D + 2 * a], s_box[tid * 2 * D + 2 * a + 1] );
+        child[2 * par + side] = node;
+        parent[self_slot] = 2 * par + side;
+      }
+      const int any = __syncthreads_or( paired );
+      if ( active )
+      {
+        s_start[l - bbase] = -1;
+        s_end[r - bbase] = -1;
+      }
+      if ( paired )
+      {
+        if ( side == 0 )
+        {
+          r = r2;
+          range[par] = make_int2( l, r );
+          node = par;
+          self_slot = n + par;
+          if ( l == 0 && r == n - 1 )
+          {
+            sc->root = par;
+            store_root( sc, lo, hi );
+            active = false;
+          } else {
+            bool left_child;
+            if ( l == 0 ) left_child = true;
+            else if ( r == n - 1 ) left_child = false;
+            else left_child = s_delta[r - bbase + 1] < s_delta[l - bbase];
+            par = left_child ? r : l - 1;
+            side = left_child ? 0 : 1;
+          }
+        } else {
+          active = false;
+        }
+      }
+      __syncthreads();
+      if ( !any ) break;
+    }
+  }
+
   const unsigned waiting = __ballot_sync( 0xffffffffu, active );
   if ( !waiting ) return;
   unsigned base = 0;
@@ -459,7 +572,16 @@ cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double e
 {
   const float eps_hi = f32_up( eps );
   const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
-  k_build_leaf< K, T, VT ><<< grid, kBuildThreads, 0, s >>>(
+  const size_t smem = static_cast< size_t >( kBuildThreads ) * 2 * ( K / 2 ) * sizeof( T );
+  static bool configured = false;
+  if ( !configured )
+  {
+    cudaError_t e0 = cudaFuncSetAttribute( k_build_leaf< K, T, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast< int >( smem ) );
+    if ( e0 != cudaSuccess ) return e0;
+    configured = true;
+  }
+  k_build_leaf< K, T, VT ><<< grid, kBuildThreads, smem, s >>>(
     verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals, static_cast< T * >( warp_box ),
     static_cast< T * >( node_box ), reinterpret_cast< int * >( child ), range, parent, queue, sc );
   cudaError_t e = cudaGetLastError();
