@@ -202,13 +202,22 @@ __device__ __forceinline__ int delta_of(uint64_t a, uint64_t b, int j)
   return 32 - __clz( j ^ ( j + 1 ) );
 }
 
-// Phase 1 (one thread per leaf rank i): the leaf's slabs (their union over the warp's 32 ranks goes to warp_box,
-// the traversal's first cull), then
-// warp-synchronous agglomeration: a node whose two children are both finished by lanes of this warp is merged in
-// registers (the two lanes meet on the same parent index; the left lane absorbs the right one's slabs by
-// shuffle). The dissimilarities of the warp's adjacent keys live in registers, so this phase touches no global
-// state but its own outputs. Lanes left waiting when no pair meets any more publish their subtree's slabs into
-// their parent's slot and are queued for phase 2 as (parent * 2 + side, l, r, node).
+// Phase 1 (one thread per leaf rank i, blocks of 256 consecutive ranks).
+//
+// a. Each thread computes its leaf's slabs and stores them into its column of the warp's component table in
+//    shared memory: comp[c][lane], c = 2 * axis + {0 min, 1 max}. From here on boxes never move through registers:
+//    a subtree's box lives in the column of the lane that holds the subtree.
+// b. Warp rounds (topology only): every lane holding an unfinished subtree [l, r] picks its parent from the
+//    dissimilarities just outside the range (registers, shuffled); two lanes meeting on the same parent are its
+//    two children. Each pair is merged with the lanes acting as slab components: lane c reads component c of both
+//    children, writes both into the parent's slot in node_box and keeps the min (or max) in the left column.
+//    Rounds continue while some pair meets.
+// c. The union of the warp's remaining subtrees is the warp box (the traversal's cull for these 32 queries).
+// d. Block rounds: the warps' remaining subtrees meet through shared tables indexed by the first and the last
+//    rank of each subtree (a left child with parent r looks for a subtree starting at r + 1 that targets the same
+//    parent as right child; a right child with parent l - 1 for one ending at l - 1); merged the same way.
+// e. Subtrees still unfinished publish their box into their parent's slot and are queued for phase 2 as
+//    (parent * 2 + side, l, r, node).
 template< int K, typename T, int VT >
 __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double *__restrict__ verts, uint32_t Vrt, int n,
                                                               double eps, float eps_hi,
@@ -220,12 +229,23 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
                                                               obj_scalars *sc)
 {
   constexpr int D = K / 2;
+  constexpr int C = 2 * D;
+  constexpr int W = kBuildThreads / 32;
   using io = box_io< T >;
-  const int i = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
-  const int lane = threadIdx.x & 31;
-  const int wbase = i - lane;
+  extern __shared__ unsigned char s_raw[];
+  T *s_comp = reinterpret_cast< T * >( s_raw );  // [W][C][32]
+  __shared__ short s_start[kBuildThreads], s_end[kBuildThreads];
+  __shared__ int s_par[kBuildThreads], s_r[kBuildThreads];
+  __shared__ int s_delta[kBuildThreads + 1];  // dissimilarity of ranks (bbase - 1 + k, bbase + k)
+  __shared__ int3 s_pairs[kBuildThreads / 2];
+  __shared__ int s_npairs, s_root_tid;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i = static_cast< int >( blockIdx.x * blockDim.x ) + tid;
+  const int wbase = i - lane, bbase = i - tid;
+  T *sw = s_comp + warp * C * 32;
   // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word).
-  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // same value for all lanes
+  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // same value for all threads
   bool active = i < n;
   const uint32_t e = active ? __ldg( vals + i ) : 0u;
   if ( active && e >= static_cast< uint32_t >( n ) )
@@ -242,28 +262,43 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
   if ( lane == 0 && wbase >= 1 && wbase < n ) dleft = delta_of( __ldg( keys + wbase - 1 ), kself, wbase - 1 );
   dleft = __shfl_sync( 0xffffffffu, dleft, 0 );
 
-  T lo[D], hi[D];
-  if ( active )
+  // a. leaf slabs into the component table
   {
-    leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
-  } else {
-#pragma unroll
-    for ( int a = 0; a < D; ++a ) lo[a] = hi[a] = T( 0 );
-  }
-  store_warp_box< T, D >( warp_box, wbase, n, active, lo, hi );
-  if ( n == 1 )
-  {
+    T lo[D], hi[D];
+    if ( active ) leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
+    if ( n == 1 )
+    {
+      if ( active )
+      {
+        sc->root = ~static_cast< int >( e );
+        store_root( sc, lo, hi );
+      }
+      return;  // n is uniform
+    }
     if ( active )
     {
-      sc->root = ~static_cast< int >( e );
-      store_root( sc, lo, hi );
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
+      {
+        sw[( 2 * a ) * 32 + lane] = lo[a];
+        sw[( 2 * a + 1 ) * 32 + lane] = hi[a];
+      }
     }
-    return;
   }
+  if ( tid == 0 )
+  {
+    s_npairs = 0;
+    s_root_tid = -1;
+  }
+  __syncthreads();  // the returns above are uniform over the grid
+
   int l = i, r = i;
   int node = ~static_cast< int >( e );
   int self_slot = i;  // index into parent[]: leaves [0, n), internal nodes n + k
   int par = 0, side = 0;
+  const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
+
+  // b. warp rounds
   while ( true )
   {
     // all lanes take part in the shuffles; ranges of active lanes stay inside [wbase, wbase + 31]
@@ -280,28 +315,31 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
     }
     const unsigned peers = __match_any_sync( 0xffffffffu, active ? par : -2 - lane );
     const bool paired = active && __popc( peers ) == 2;
-    if ( !__any_sync( 0xffffffffu, paired ) ) break;
+    const unsigned lefts = __ballot_sync( 0xffffffffu, paired && side == 0 );
+    if ( !lefts ) break;
     const int src = paired ? __ffs( peers & ~( 1u << lane ) ) - 1 : lane;
     if ( paired )
     {
-      T *pb = node_box + static_cast< size_t >( par ) * D * 4;
-#pragma unroll
-      for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
       child[2 * par + side] = node;
       parent[self_slot] = 2 * par + side;
     }
-    const int sr = __shfl_sync( 0xffffffffu, r, src );
-#pragma unroll
-    for ( int a = 0; a < D; ++a )
+    // merges, lanes as slab components
+    for ( unsigned m = lefts; m; m &= m - 1 )
     {
-      const T sl = __shfl_sync( 0xffffffffu, lo[a], src );
-      const T sh = __shfl_sync( 0xffffffffu, hi[a], src );
-      if ( paired && side == 0 )
+      const int L = __ffs( m ) - 1;
+      const int R = __shfl_sync( 0xffffffffu, src, L );
+      const int p = __shfl_sync( 0xffffffffu, par, L );
+      if ( lane < C )
       {
-        lo[a] = io::mn( lo[a], sl );
-        hi[a] = io::mx( hi[a], sh );
+        const T x = sw[lane * 32 + L], y = sw[lane * 32 + R];
+        T *pb = node_box + static_cast< size_t >( p ) * D * 4 + ( lane >> 1 ) * 4 + ( lane & 1 );
+        pb[0] = x;
+        pb[2] = y;
+        sw[lane * 32 + L] = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
       }
     }
+    __syncwarp();
+    const int sr = __shfl_sync( 0xffffffffu, r, src );
     if ( paired )
     {
       if ( side == 0 )
@@ -313,7 +351,7 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
         if ( l == 0 && r == n - 1 )
         {
           sc->root = par;
-          store_root( sc, lo, hi );
+          s_root_tid = tid;
           active = false;
         }
       } else {
@@ -321,129 +359,136 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
       }
     }
   }
-  // par/side hold this lane's parent from the last round (the round in which nothing paired).
 
-  // Phase 1b, block-level: the waiting subtrees of all warps of the block meet through shared-memory tables
-  // indexed by the first and the last rank of each subtree. A left child (parent r) looks for a subtree starting
-  // at r + 1 that targets the same parent as right child, a right child (parent l - 1) for one ending at l - 1.
-  // Rounds (each behind block barriers) continue while some pair meets.
+  // c. warp box: union of the subtrees the warp's lanes still hold (and of the root, when the tree ends here)
   {
-    extern __shared__ unsigned char s_raw[];
-    T *s_box = reinterpret_cast< T * >( s_raw );  // [kBuildThreads][2 D]
-    __shared__ short s_start[kBuildThreads], s_end[kBuildThreads];
-    __shared__ int s_par[kBuildThreads], s_r[kBuildThreads];
-    __shared__ int s_delta[kBuildThreads + 1];  // dissimilarity of ranks (bbase - 1 + k, bbase + k)
-    const int tid = threadIdx.x;
-    const int bbase = i - tid;
-    s_start[tid] = -1;
-    s_end[tid] = -1;
-    s_delta[tid + 1] = dself;
-    if ( tid == 0 ) s_delta[0] = ( bbase >= 1 && bbase < n ) ? delta( keys, bbase - 1 ) : 0;
-    __syncthreads();
-    while ( true )
+    const bool holds = active || ( s_root_tid == tid );
+    const unsigned hm = __ballot_sync( 0xffffffffu, holds );
+    if ( lane < C && wbase < n )
     {
-      if ( active )
+      T u = ( lane & 1 ) ? -inf : inf;
+      for ( unsigned m = hm; m; m &= m - 1 )
       {
-        s_start[l - bbase] = static_cast< short >( tid );
-        s_end[r - bbase] = static_cast< short >( tid );
-        s_par[tid] = 2 * par + side;
-        s_r[tid] = r;
-#pragma unroll
-        for ( int a = 0; a < D; ++a )
-        {
-          s_box[tid * 2 * D + 2 * a] = lo[a];
-          s_box[tid * 2 * D + 2 * a + 1] = hi[a];
-        }
+        const T x = sw[lane * 32 + __ffs( m ) - 1];
+        u = ( lane & 1 ) ? io::mx( u, x ) : io::mn( u, x );
       }
-      __syncthreads();
-      int partner = -1;
-      if ( active )
-      {
-        if ( side == 0 )
-        {
-          const int q = r + 1;
-          if ( q < bbase + kBuildThreads && q < n )
-          {
-            const int c = s_start[q - bbase];
-            if ( c >= 0 && s_par[c] == 2 * par + 1 ) partner = c;
-          }
-        } else {
-          const int q = l - 1;
-          if ( q >= bbase )
-          {
-            const int c = s_end[q - bbase];
-            if ( c >= 0 && s_par[c] == 2 * par ) partner = c;
-          }
-        }
-      }
-      const bool paired = partner >= 0;
-      int r2 = r;
-      if ( paired && side == 0 )
-      {
-        r2 = s_r[partner];
-#pragma unroll
-        for ( int a = 0; a < D; ++a )
-        {
-          lo[a] = io::mn( lo[a], s_box[partner * 2 * D + 2 * a] );
-          hi[a] = io::mx( hi[a], s_box[partner * 2 * D + 2 * a + 1] );
-        }
-      }
-      if ( paired )
-      {
-        // both children write the slot their parent keeps for them (own slabs: the pre-merge values, still in
-        // shared memory for the left lane)
-        T *pb = node_box + static_cast< size_t >( par ) * D * 4;
-#pragma unroll
-        for ( int a = 0; a < D; ++a )
-          io::store2( pb + a * 4 + side * 2, s_box[tid * 2 * D + 2 * a], s_box[tid * 2 * D + 2 * a + 1] );
-        child[2 * par + side] = node;
-        parent[self_slot] = 2 * par + side;
-      }
-      const int any = __syncthreads_or( paired );
-      if ( active )
-      {
-        s_start[l - bbase] = -1;
-        s_end[r - bbase] = -1;
-      }
-      if ( paired )
-      {
-        if ( side == 0 )
-        {
-          r = r2;
-          range[par] = make_int2( l, r );
-          node = par;
-          self_slot = n + par;
-          if ( l == 0 && r == n - 1 )
-          {
-            sc->root = par;
-            store_root( sc, lo, hi );
-            active = false;
-          } else {
-            bool left_child;
-            if ( l == 0 ) left_child = true;
-            else if ( r == n - 1 ) left_child = false;
-            else left_child = s_delta[r - bbase + 1] < s_delta[l - bbase];
-            par = left_child ? r : l - 1;
-            side = left_child ? 0 : 1;
-          }
-        } else {
-          active = false;
-        }
-      }
-      __syncthreads();
-      if ( !any ) break;
+      warp_box[static_cast< size_t >( wbase >> 5 ) * C + lane] = u;
     }
   }
 
+  // d. block rounds
+  s_start[tid] = -1;
+  s_end[tid] = -1;
+  s_delta[tid + 1] = dself;
+  if ( tid == 0 ) s_delta[0] = ( bbase >= 1 && bbase < n ) ? delta( keys, bbase - 1 ) : 0;
+  __syncthreads();
+  while ( true )
+  {
+    if ( active )
+    {
+      s_start[l - bbase] = static_cast< short >( tid );
+      s_end[r - bbase] = static_cast< short >( tid );
+      s_par[tid] = 2 * par + side;
+      s_r[tid] = r;
+    }
+    __syncthreads();
+    int partner = -1;
+    if ( active )
+    {
+      if ( side == 0 )
+      {
+        const int q = r + 1;
+        if ( q < bbase + kBuildThreads && q < n )
+        {
+          const int c = s_start[q - bbase];
+          if ( c >= 0 && s_par[c] == 2 * par + 1 ) partner = c;
+        }
+      } else {
+        const int q = l - 1;
+        if ( q >= bbase )
+        {
+          const int c = s_end[q - bbase];
+          if ( c >= 0 && s_par[c] == 2 * par ) partner = c;
+        }
+      }
+    }
+    const bool paired = partner >= 0;
+    if ( paired && side == 0 ) s_pairs[atomicAdd( &s_npairs, 1 )] = make_int3( tid, partner, par );
+    if ( paired )
+    {
+      child[2 * par + side] = node;
+      parent[self_slot] = 2 * par + side;
+    }
+    const int any = __syncthreads_or( paired );
+    if ( !any ) break;
+    // merges: warp w takes pairs w, w + W, ...; lanes as slab components
+    const int np = s_npairs;
+    for ( int k = warp; k < np; k += W )
+    {
+      const int3 pr = s_pairs[k];
+      if ( lane < C )
+      {
+        T *cl = s_comp + ( ( pr.x >> 5 ) * C + lane ) * 32 + ( pr.x & 31 );
+        const T x = *cl;
+        const T y = s_comp[( ( pr.y >> 5 ) * C + lane ) * 32 + ( pr.y & 31 )];
+        T *pb = node_box + static_cast< size_t >( pr.z ) * D * 4 + ( lane >> 1 ) * 4 + ( lane & 1 );
+        pb[0] = x;
+        pb[2] = y;
+        *cl = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
+      }
+    }
+    if ( active )
+    {
+      s_start[l - bbase] = -1;
+      s_end[r - bbase] = -1;
+    }
+    if ( paired )
+    {
+      if ( side == 0 )
+      {
+        r = s_r[partner];
+        range[par] = make_int2( l, r );
+        node = par;
+        self_slot = n + par;
+        if ( l == 0 && r == n - 1 )
+        {
+          sc->root = par;
+          s_root_tid = tid;
+          active = false;
+        } else {
+          bool left_child;
+          if ( l == 0 ) left_child = true;
+          else if ( r == n - 1 ) left_child = false;
+          else left_child = s_delta[r - bbase + 1] < s_delta[l - bbase];
+          par = left_child ? r : l - 1;
+          side = left_child ? 0 : 1;
+        }
+      } else {
+        active = false;
+      }
+    }
+    __syncthreads();
+    if ( tid == 0 ) s_npairs = 0;
+  }
+  // the root's box, when the whole tree closed inside this block
+  if ( s_root_tid >= 0 && warp == ( s_root_tid >> 5 ) && lane < C )
+    reinterpret_cast< T * >( sc->root_box )[lane] = s_comp[( warp * C + lane ) * 32 + ( s_root_tid & 31 )];
+
+  // e. unfinished subtrees: publish into the parent's slot, queue for phase 2
   const unsigned waiting = __ballot_sync( 0xffffffffu, active );
   if ( !waiting ) return;
+  for ( unsigned m = waiting; m; m &= m - 1 )
+  {
+    const int j = __ffs( m ) - 1;
+    const int p = __shfl_sync( 0xffffffffu, par, j );
+    const int sd = __shfl_sync( 0xffffffffu, side, j );
+    if ( lane < C )
+      node_box[static_cast< size_t >( p ) * D * 4 + ( lane >> 1 ) * 4 + sd * 2 + ( lane & 1 )] = sw[lane * 32 + j];
+  }
   unsigned base = 0;
   if ( lane == 0 ) base = atomicAdd( &sc->climb_count, static_cast< unsigned >( __popc( waiting ) ) );
   base = __shfl_sync( 0xffffffffu, base, 0 );
   if ( !active ) return;
-  T *pb = node_box + static_cast< size_t >( par ) * D * 4;
-#pragma unroll
-  for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
   child[2 * par + side] = node;
   parent[self_slot] = 2 * par + side;
   queue[base + __popc( waiting & ( ( 1u << lane ) - 1u ) )] = make_int4( 2 * par + side, l, r, node );
@@ -572,7 +617,7 @@ cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double e
 {
   const float eps_hi = f32_up( eps );
   const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
-  const size_t smem = static_cast< size_t >( kBuildThreads ) * 2 * ( K / 2 ) * sizeof( T );
+  const size_t smem = static_cast< size_t >( kBuildThreads ) * 2 * ( K / 2 ) * sizeof( T );  // [W][C][32]
   static bool configured = false;
   if ( !configured )
   {
