@@ -202,24 +202,25 @@ __device__ __forceinline__ int delta_of(uint64_t a, uint64_t b, int j)
   return 32 - __clz( j ^ ( j + 1 ) );
 }
 
-// Phase 1 (one thread per leaf rank i, blocks of 256 consecutive ranks).
+// Phase 1 (one thread per leaf rank i, blocks of 256 consecutive ranks). Everything a block decides about the
+// nodes it closes is staged in shared memory and written out once at the end, as whole 16-byte-aligned rows of
+// node_box (both children's slabs of consecutive nodes are contiguous), child, range and parent.
 //
-// a. Each thread computes its leaf's slabs and stores them into its column of the warp's component table in
-//    shared memory: comp[c][lane], c = 2 * axis + {0 min, 1 max}. From here on boxes never move through registers:
-//    a subtree's box lives in the column of the lane that holds the subtree.
-// b. Warp rounds (topology only): every lane holding an unfinished subtree [l, r] picks its parent from the
-//    dissimilarities just outside the range (registers, shuffled); two lanes meeting on the same parent are its
-//    two children. Each pair is merged with the lanes acting as slab components: lane c reads component c of both
-//    children, writes both into the parent's slot in node_box and keeps the min (or max) in the left column.
-//    Rounds continue while some pair meets.
-// c. The union of the warp's remaining subtrees is the warp box (the traversal's cull for these 32 queries).
+// a. Each thread computes its leaf's slabs into the warp's box table, column = lane (component c = 2 axis +
+//    {0 min, 1 max}). A table has 64 columns: 32 leaves and 32 internal nodes (node p of the block lives in the
+//    table of warp (p - bbase) / 32, column 32 + (p - bbase) % 32).
+// b. Warp rounds (topology in registers): every lane holding an unfinished subtree [l, r] picks its parent from
+//    the dissimilarities just outside the range; two lanes meeting on one parent are its children. The parent's
+//    box is formed with the lanes acting as slab components (one min or max per lane).
+// c. The union of the subtrees the warp still holds is the warp box (the traversal's cull for these 32 queries).
 // d. Block rounds: the warps' remaining subtrees meet through shared tables indexed by the first and the last
 //    rank of each subtree (a left child with parent r looks for a subtree starting at r + 1 that targets the same
-//    parent as right child; a right child with parent l - 1 for one ending at l - 1); merged the same way.
+//    parent as right child; a right child with parent l - 1 for one ending at l - 1).
 // e. Subtrees still unfinished publish their box into their parent's slot and are queued for phase 2 as
 //    (parent * 2 + side, l, r, node).
+// f. Coalesced write-out of every node closed in the block.
 template< int K, typename T, int VT >
-__global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double *__restrict__ verts, uint32_t Vrt, int n,
+__global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double *__restrict__ verts, uint32_t Vrt, int n,
                                                               double eps, float eps_hi,
                                                               const uint64_t *__restrict__ keys,
                                                               const uint32_t *__restrict__ vals,
@@ -233,17 +234,24 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
   constexpr int W = kBuildThreads / 32;
   using io = box_io< T >;
   extern __shared__ unsigned char s_raw[];
-  T *s_comp = reinterpret_cast< T * >( s_raw );  // [W][C][32]
+  T *s_box = reinterpret_cast< T * >( s_raw );  // [W][C][64]
+  __shared__ int2 s_child[kBuildThreads];       // closed node p - bbase: global child encodings
+  __shared__ int2 s_cref[kBuildThreads];        // closed node p - bbase: box table refs of its children
+  __shared__ int2 s_rng[kBuildThreads];
+  __shared__ int s_pnode[kBuildThreads];        // parent entry of node p - bbase, -1 when not closed here
+  __shared__ int s_pleaf[kBuildThreads];        // parent entry of leaf bbase + k
   __shared__ short s_start[kBuildThreads], s_end[kBuildThreads];
-  __shared__ int s_par[kBuildThreads], s_r[kBuildThreads];
+  __shared__ int s_par[kBuildThreads], s_r[kBuildThreads], s_ref[kBuildThreads], s_gn[kBuildThreads];
   __shared__ int s_delta[kBuildThreads + 1];  // dissimilarity of ranks (bbase - 1 + k, bbase + k)
-  __shared__ int3 s_pairs[kBuildThreads / 2];
+  __shared__ int4 s_pairs[kBuildThreads / 2];
   __shared__ int s_npairs, s_root_tid;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int i = static_cast< int >( blockIdx.x * blockDim.x ) + tid;
   const int wbase = i - lane, bbase = i - tid;
-  T *sw = s_comp + warp * C * 32;
+  // box table element of ref (table * 64 + column), component c
+  auto box = [&](int ref, int c) -> T & { return s_box[( ( ref >> 6 ) * C + c ) * 64 + ( ref & 63 )]; };
+  auto node_ref = [&](int p) { const int q = p - bbase; return ( q >> 5 ) * 64 + 32 + ( q & 31 ); };
   // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word).
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // same value for all threads
   bool active = i < n;
@@ -262,7 +270,7 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
   if ( lane == 0 && wbase >= 1 && wbase < n ) dleft = delta_of( __ldg( keys + wbase - 1 ), kself, wbase - 1 );
   dleft = __shfl_sync( 0xffffffffu, dleft, 0 );
 
-  // a. leaf slabs into the component table
+  // a. leaf slabs into the box table
   {
     T lo[D], hi[D];
     if ( active ) leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
@@ -280,28 +288,39 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
 #pragma unroll
       for ( int a = 0; a < D; ++a )
       {
-        sw[( 2 * a ) * 32 + lane] = lo[a];
-        sw[( 2 * a + 1 ) * 32 + lane] = hi[a];
+        box( warp * 64 + lane, 2 * a ) = lo[a];
+        box( warp * 64 + lane, 2 * a + 1 ) = hi[a];
       }
     }
   }
+  s_pnode[tid] = -1;
+  s_pleaf[tid] = -1;
+  s_rng[tid] = make_int2( -1, -1 );  // x >= 0 marks a node closed in this block
+  s_start[tid] = -1;
+  s_end[tid] = -1;
+  s_delta[tid + 1] = dself;
   if ( tid == 0 )
   {
     s_npairs = 0;
     s_root_tid = -1;
+    s_delta[0] = ( bbase >= 1 && bbase < n ) ? delta( keys, bbase - 1 ) : 0;
   }
   __syncthreads();  // the returns above are uniform over the grid
 
   int l = i, r = i;
-  int node = ~static_cast< int >( e );
-  int self_slot = i;  // index into parent[]: leaves [0, n), internal nodes n + k
+  int gnode = ~static_cast< int >( e );  // child encoding of the subtree this lane holds
+  int ref = warp * 64 + lane;            // its box in the tables
+  int selfp = -1 - tid;                  // its parent entry: leaf (-1 - k) or closed node (p - bbase)
   int par = 0, side = 0;
   const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
+  auto set_parent = [&](int entry) {
+    if ( selfp < 0 ) s_pleaf[-1 - selfp] = entry;
+    else s_pnode[selfp] = entry;
+  };
 
   // b. warp rounds
   while ( true )
   {
-    // all lanes take part in the shuffles; ranges of active lanes stay inside [wbase, wbase + 31]
     const int d_r = __shfl_sync( 0xffffffffu, dself, ( r - wbase ) & 31 );
     const int d_lm1 = __shfl_sync( 0xffffffffu, dself, ( l - 1 - wbase ) & 31 );
     if ( active )
@@ -318,36 +337,39 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
     const unsigned lefts = __ballot_sync( 0xffffffffu, paired && side == 0 );
     if ( !lefts ) break;
     const int src = paired ? __ffs( peers & ~( 1u << lane ) ) - 1 : lane;
-    if ( paired )
+    const int sref = __shfl_sync( 0xffffffffu, ref, src );
+    const int sgnode = __shfl_sync( 0xffffffffu, gnode, src );
+    const int sr = __shfl_sync( 0xffffffffu, r, src );
+    if ( paired ) set_parent( 2 * par + side );
+    if ( paired && side == 0 )
     {
-      child[2 * par + side] = node;
-      parent[self_slot] = 2 * par + side;
+      const int q = par - bbase;
+      s_child[q] = make_int2( gnode, sgnode );
+      s_cref[q] = make_int2( ref, sref );
+      s_rng[q] = make_int2( l, sr );
     }
-    // merges, lanes as slab components
+    // merged boxes, lanes as slab components
     for ( unsigned m = lefts; m; m &= m - 1 )
     {
       const int L = __ffs( m ) - 1;
-      const int R = __shfl_sync( 0xffffffffu, src, L );
       const int p = __shfl_sync( 0xffffffffu, par, L );
+      const int rl = __shfl_sync( 0xffffffffu, ref, L );
+      const int rr = __shfl_sync( 0xffffffffu, sref, L );
       if ( lane < C )
       {
-        const T x = sw[lane * 32 + L], y = sw[lane * 32 + R];
-        T *pb = node_box + static_cast< size_t >( p ) * D * 4 + ( lane >> 1 ) * 4 + ( lane & 1 );
-        pb[0] = x;
-        pb[2] = y;
-        sw[lane * 32 + L] = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
+        const T x = box( rl, lane ), y = box( rr, lane );
+        box( node_ref( p ), lane ) = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
       }
     }
     __syncwarp();
-    const int sr = __shfl_sync( 0xffffffffu, r, src );
     if ( paired )
     {
       if ( side == 0 )
       {
         r = sr;
-        range[par] = make_int2( l, r );
-        node = par;
-        self_slot = n + par;
+        gnode = par;
+        ref = node_ref( par );
+        selfp = par - bbase;
         if ( l == 0 && r == n - 1 )
         {
           sc->root = par;
@@ -364,24 +386,21 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
   {
     const bool holds = active || ( s_root_tid == tid );
     const unsigned hm = __ballot_sync( 0xffffffffu, holds );
-    if ( lane < C && wbase < n )
+    T u = ( lane & 1 ) ? -inf : inf;
+    for ( unsigned m = hm; m; m &= m - 1 )
     {
-      T u = ( lane & 1 ) ? -inf : inf;
-      for ( unsigned m = hm; m; m &= m - 1 )
+      const int hr = __shfl_sync( 0xffffffffu, ref, __ffs( m ) - 1 );
+      if ( lane < C )
       {
-        const T x = sw[lane * 32 + __ffs( m ) - 1];
+        const T x = box( hr, lane );
         u = ( lane & 1 ) ? io::mx( u, x ) : io::mn( u, x );
       }
-      warp_box[static_cast< size_t >( wbase >> 5 ) * C + lane] = u;
     }
+    if ( lane < C && wbase < n ) warp_box[static_cast< size_t >( wbase >> 5 ) * C + lane] = u;
   }
+  __syncthreads();
 
   // d. block rounds
-  s_start[tid] = -1;
-  s_end[tid] = -1;
-  s_delta[tid + 1] = dself;
-  if ( tid == 0 ) s_delta[0] = ( bbase >= 1 && bbase < n ) ? delta( keys, bbase - 1 ) : 0;
-  __syncthreads();
   while ( true )
   {
     if ( active )
@@ -390,6 +409,8 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
       s_end[r - bbase] = static_cast< short >( tid );
       s_par[tid] = 2 * par + side;
       s_r[tid] = r;
+      s_ref[tid] = ref;
+      s_gn[tid] = gnode;
     }
     __syncthreads();
     int partner = -1;
@@ -413,30 +434,30 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
       }
     }
     const bool paired = partner >= 0;
-    if ( paired && side == 0 ) s_pairs[atomicAdd( &s_npairs, 1 )] = make_int3( tid, partner, par );
-    if ( paired )
-    {
-      child[2 * par + side] = node;
-      parent[self_slot] = 2 * par + side;
-    }
+    if ( paired ) set_parent( 2 * par + side );
+    if ( paired && side == 0 ) s_pairs[atomicAdd( &s_npairs, 1 )] = make_int4( tid, partner, par, 0 );
     const int any = __syncthreads_or( paired );
     if ( !any ) break;
-    // merges: warp w takes pairs w, w + W, ...; lanes as slab components
     const int np = s_npairs;
+    // closed nodes' boxes, lanes as slab components (warp w takes pairs w, w + W, ...)
     for ( int k = warp; k < np; k += W )
     {
-      const int3 pr = s_pairs[k];
+      const int4 pr = s_pairs[k];
+      const int rl = s_ref[pr.x], rr = s_ref[pr.y];
       if ( lane < C )
       {
-        T *cl = s_comp + ( ( pr.x >> 5 ) * C + lane ) * 32 + ( pr.x & 31 );
-        const T x = *cl;
-        const T y = s_comp[( ( pr.y >> 5 ) * C + lane ) * 32 + ( pr.y & 31 )];
-        T *pb = node_box + static_cast< size_t >( pr.z ) * D * 4 + ( lane >> 1 ) * 4 + ( lane & 1 );
-        pb[0] = x;
-        pb[2] = y;
-        *cl = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
+        const T x = box( rl, lane ), y = box( rr, lane );
+        box( node_ref( pr.z ), lane ) = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
+      }
+      if ( lane == 0 )
+      {
+        const int q = pr.z - bbase;
+        s_child[q] = make_int2( s_gn[pr.x], s_gn[pr.y] );
+        s_cref[q] = make_int2( rl, rr );
       }
     }
+    const int r2 = ( paired && side == 0 ) ? s_r[partner] : r;
+    __syncthreads();
     if ( active )
     {
       s_start[l - bbase] = -1;
@@ -446,10 +467,11 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
     {
       if ( side == 0 )
       {
-        r = s_r[partner];
-        range[par] = make_int2( l, r );
-        node = par;
-        self_slot = n + par;
+        r = r2;
+        s_rng[par - bbase] = make_int2( l, r );
+        gnode = par;
+        ref = node_ref( par );
+        selfp = par - bbase;
         if ( l == 0 && r == n - 1 )
         {
           sc->root = par;
@@ -467,31 +489,58 @@ __global__ void __launch_bounds__( kBuildThreads, 3 ) k_build_leaf(const double 
         active = false;
       }
     }
-    __syncthreads();
     if ( tid == 0 ) s_npairs = 0;
+    __syncthreads();
   }
   // the root's box, when the whole tree closed inside this block
-  if ( s_root_tid >= 0 && warp == ( s_root_tid >> 5 ) && lane < C )
-    reinterpret_cast< T * >( sc->root_box )[lane] = s_comp[( warp * C + lane ) * 32 + ( s_root_tid & 31 )];
+  if ( s_root_tid >= 0 && lane < C && warp == ( s_root_tid >> 5 ) )
+    reinterpret_cast< T * >( sc->root_box )[lane] = box( node_ref( sc->root ), lane );
 
-  // e. unfinished subtrees: publish into the parent's slot, queue for phase 2
+  // e. unfinished subtrees: publish their box into the parent's slot and queue them for phase 2
   const unsigned waiting = __ballot_sync( 0xffffffffu, active );
-  if ( !waiting ) return;
   for ( unsigned m = waiting; m; m &= m - 1 )
   {
     const int j = __ffs( m ) - 1;
     const int p = __shfl_sync( 0xffffffffu, par, j );
     const int sd = __shfl_sync( 0xffffffffu, side, j );
+    const int rf = __shfl_sync( 0xffffffffu, ref, j );
     if ( lane < C )
-      node_box[static_cast< size_t >( p ) * D * 4 + ( lane >> 1 ) * 4 + sd * 2 + ( lane & 1 )] = sw[lane * 32 + j];
+      node_box[static_cast< size_t >( p ) * D * 4 + ( lane >> 1 ) * 4 + sd * 2 + ( lane & 1 )] = box( rf, lane );
   }
-  unsigned base = 0;
-  if ( lane == 0 ) base = atomicAdd( &sc->climb_count, static_cast< unsigned >( __popc( waiting ) ) );
-  base = __shfl_sync( 0xffffffffu, base, 0 );
-  if ( !active ) return;
-  child[2 * par + side] = node;
-  parent[self_slot] = 2 * par + side;
-  queue[base + __popc( waiting & ( ( 1u << lane ) - 1u ) )] = make_int4( 2 * par + side, l, r, node );
+  if ( waiting )
+  {
+    unsigned base = 0;
+    if ( lane == 0 ) base = atomicAdd( &sc->climb_count, static_cast< unsigned >( __popc( waiting ) ) );
+    base = __shfl_sync( 0xffffffffu, base, 0 );
+    if ( active )
+    {
+      child[2 * par + side] = gnode;
+      parent[selfp < 0 ? i : n + bbase + selfp] = 2 * par + side;
+      queue[base + __popc( waiting & ( ( 1u << lane ) - 1u ) )] =
+        make_int4( 2 * par + side, l, r, gnode );
+    }
+  }
+
+  // f. coalesced write-out of the nodes closed in this block: node_box rows (16-byte pairs), child, range, parent
+  const int nclosed = min( kBuildThreads, n - 1 - bbase );  // internal nodes bbase .. bbase + nclosed - 1
+  for ( int k = tid; k < nclosed * C; k += kBuildThreads )
+  {
+    // the row of node q = k / C holds C 16-byte (min, max) pairs in the order (axis, side); pair t = k % C
+    const int q = k / C, t = k % C;
+    if ( s_rng[q].x < 0 ) continue;
+    const int2 cr = s_cref[q];
+    const int a = t >> 1, sd = t & 1;
+    const int rf = sd ? cr.y : cr.x;
+    io::store2( node_box + ( static_cast< size_t >( bbase + q ) * D + a ) * 4 + sd * 2, box( rf, 2 * a ),
+                box( rf, 2 * a + 1 ) );
+  }
+  if ( tid < nclosed && s_rng[tid].x >= 0 )
+  {
+    reinterpret_cast< int2 * >( child )[bbase + tid] = s_child[tid];
+    range[bbase + tid] = s_rng[tid];
+    if ( s_pnode[tid] >= 0 ) parent[n + bbase + tid] = s_pnode[tid];
+  }
+  if ( i < n && s_pleaf[tid] >= 0 ) parent[i] = s_pleaf[tid];
 }
 
 // Phase 2 (dense, one thread per queued subtree): the agglomerative climb with a global exchange slot per node.
@@ -617,7 +666,7 @@ cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double e
 {
   const float eps_hi = f32_up( eps );
   const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
-  const size_t smem = static_cast< size_t >( kBuildThreads ) * 2 * ( K / 2 ) * sizeof( T );  // [W][C][32]
+  const size_t smem = static_cast< size_t >( 2 * kBuildThreads ) * ( 2 * ( K / 2 ) ) * sizeof( T );  // [W][C][64]
   static bool configured = false;
   if ( !configured )
   {
