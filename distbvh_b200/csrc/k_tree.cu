@@ -234,7 +234,7 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
   constexpr int W = kBuildThreads / 32;
   using io = box_io< T >;
   extern __shared__ unsigned char s_raw[];
-  T *s_box = reinterpret_cast< T * >( s_raw );  // [W][C][64]
+  T *s_box = reinterpret_cast< T * >( s_raw );  // [W * 64][C + 1]
   __shared__ int2 s_child[kBuildThreads];       // closed node p - bbase: global child encodings
   __shared__ int2 s_cref[kBuildThreads];        // closed node p - bbase: box table refs of its children
   __shared__ int2 s_rng[kBuildThreads];
@@ -249,8 +249,9 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int i = static_cast< int >( blockIdx.x * blockDim.x ) + tid;
   const int wbase = i - lane, bbase = i - tid;
-  // box table element of ref (table * 64 + column), component c
-  auto box = [&](int ref, int c) -> T & { return s_box[( ( ref >> 6 ) * C + c ) * 64 + ( ref & 63 )]; };
+  // box table element of ref (table * 64 + column), component c: one padded row of C + 1 per box, so lanes
+  // acting as components touch consecutive words and a lane writing its own row strides by an odd count
+  auto box = [&](int ref, int c) -> T & { return s_box[ref * ( C + 1 ) + c]; };
   auto node_ref = [&](int p) { const int q = p - bbase; return ( q >> 5 ) * 64 + 32 + ( q & 31 ); };
   // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word).
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // same value for all threads
@@ -666,7 +667,7 @@ cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double e
 {
   const float eps_hi = f32_up( eps );
   const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
-  const size_t smem = static_cast< size_t >( 2 * kBuildThreads ) * ( 2 * ( K / 2 ) ) * sizeof( T );  // [W][C][64]
+  const size_t smem = static_cast< size_t >( 2 * kBuildThreads ) * ( 2 * ( K / 2 ) + 1 ) * sizeof( T );  // [W * 64][C + 1]
   static bool configured = false;
   if ( !configured )
   {
