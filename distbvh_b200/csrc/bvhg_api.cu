@@ -70,7 +70,7 @@ struct object
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
   dev_buf hist, status;
-  dev_buf warp_box, node_box, child, range, parent, exch, queue;
+  dev_buf elem_box, warp_box, node_box, child, range, parent, exch, queue;
   dev_buf scal;  // obj_scalars
   // Each object's build runs on its own stream, forked from and joined back into the context stream with
   // events, so two objects' builds overlap (one's latency-bound tree climb beside the other's streaming kernels).
@@ -293,9 +293,10 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   {
     if ( !o.topo ) return fail( ctx, BVHG_ERR_STATE, "refit without a rebuild of this element count" );
     stage_scope st( ctx, BVHG_STAGE_BUILD );
-    if ( n > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( n - 1 ) * sizeof( int ), s ) );
-    BVHG_CUDA( ctx, launch_refit( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.warp_box.p,
-                                  o.node_box.p, o.parent.as< int >(), o.exch.as< int >(), o.sc(), s ) );
+    const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
+    if ( m > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( m - 1 ) * sizeof( int ), s ) );
+    BVHG_CUDA( ctx, launch_refit( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.elem_box.p,
+                                  o.warp_box.p, o.node_box.p, o.parent.as< int >(), o.exch.as< int >(), o.sc(), s ) );
     st.launched();
     o.built = true;
     return BVHG_OK;
@@ -315,19 +316,21 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   BVHG_CUDA( ctx, o.vals_alt.reserve( n * 4 ) );
   BVHG_CUDA( ctx, o.hist.reserve( passes * radix * 4 ) );
   BVHG_CUDA( ctx, o.status.reserve( passes * ( tiles + 1 ) * radix * 4 ) );
+  const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;  // leaf buckets
+  BVHG_CUDA( ctx, o.elem_box.reserve( n * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
-  BVHG_CUDA( ctx, o.node_box.reserve( ( n - 1 ) * D * 4 * sb + 16 ) );
-  BVHG_CUDA( ctx, o.child.reserve( ( n - 1 ) * 8 + 8 ) );
-  BVHG_CUDA( ctx, o.range.reserve( ( n - 1 ) * 8 + 8 ) );
-  BVHG_CUDA( ctx, o.parent.reserve( ( 2 * n ) * 4 ) );
-  BVHG_CUDA( ctx, o.exch.reserve( n * 4 ) );
-  BVHG_CUDA( ctx, o.queue.reserve( n * 16 ) );
+  BVHG_CUDA( ctx, o.node_box.reserve( ( m - 1 ) * D * 4 * sb + 16 ) );
+  BVHG_CUDA( ctx, o.child.reserve( ( m - 1 ) * 8 + 8 ) );
+  BVHG_CUDA( ctx, o.range.reserve( ( m - 1 ) * 8 + 8 ) );
+  BVHG_CUDA( ctx, o.parent.reserve( ( 2 * m ) * 4 ) );
+  BVHG_CUDA( ctx, o.exch.reserve( m * 4 ) );
+  BVHG_CUDA( ctx, o.queue.reserve( m * 16 ) );
   {
     stage_scope st( ctx, BVHG_STAGE_BOUNDS );
     BVHG_CUDA( ctx, cudaMemcpyAsync( o.sc(), ctx->init_template, sizeof( obj_scalars ), cudaMemcpyHostToDevice, s ) );
     BVHG_CUDA( ctx, cudaMemsetAsync( o.hist.p, 0, passes * radix * 4, s ) );
     BVHG_CUDA( ctx, cudaMemsetAsync( o.status.p, 0, passes * ( tiles + 1 ) * radix * 4, s ) );
-    if ( n > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( n - 1 ) * 4, s ) );
+    if ( m > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( m - 1 ) * 4, s ) );
     BVHG_CUDA( ctx, launch_centroid_bounds( K, o.verts, o.V, n, ctx->cfg.epsilon, o.cx.as< double >(),
                                             o.cy.as< double >(), o.cz.as< double >(), o.sc(), s ) );
     st.launched();
@@ -358,9 +361,10 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   {
     stage_scope st( ctx, BVHG_STAGE_BUILD );
     BVHG_CUDA( ctx, launch_build( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_keys(), o.sorted_vals(),
-                                  o.warp_box.p, o.node_box.p, o.child.as< int2 >(), o.range.as< int2 >(),
-                                  o.parent.as< int >(), o.exch.as< int >(), o.queue.as< int4 >(), o.sc(), s ) );
-    st.launched( n > 1 ? 2 : 1 );
+                                  o.elem_box.p, o.warp_box.p, o.node_box.p, o.child.as< int2 >(),
+                                  o.range.as< int2 >(), o.parent.as< int >(), o.exch.as< int >(),
+                                  o.queue.as< int4 >(), o.sc(), s ) );
+    st.launched( m > 1 ? 2 : 1 );
   }
   o.built = true;
   o.topo = true;
@@ -374,7 +378,7 @@ tree_view view_of(const object &o)
   v.child = o.child.as< int2 >();
   v.range = o.range.as< int2 >();
   v.warp_box = o.warp_box.p;
-  v.parent = o.parent.as< int >();
+  v.elem_box = o.elem_box.p;
   v.perm = o.sorted_vals();
   v.n = o.n;
   v.sc = o.sc();
@@ -761,7 +765,7 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
   const int D = ctx->cfg.k / 2;
   const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
   const size_t sb = fp32 ? 4 : 8;
-  const uint64_t m = n - 1;
+  const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
   const uint64_t nw = ( n + 31 ) / 32;
   auto fetch = [&](const void *src, size_t count, std::vector< double > &dst) -> cudaError_t {
     dst.resize( count );
@@ -780,39 +784,56 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
   BVHG_CUDA( ctx, tmp.reserve( n * D * 2 * sb ) );
   BVHG_CUDA( ctx, launch_probe_kdops( ctx->cfg.k, fp32, o.verts, o.V, n, ctx->cfg.epsilon, tmp.p, ctx->stream ) );
   BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
-  std::vector< double > lb, nb, wb, rootb;
+  std::vector< double > lb, eb, nb, wb, rootb;
   BVHG_CUDA( ctx, fetch( tmp.p, n * D * 2, lb ) );
-  BVHG_CUDA( ctx, fetch( o.node_box.p, m * D * 4, nb ) );
+  BVHG_CUDA( ctx, fetch( o.elem_box.p, n * D * 2, eb ) );
+  BVHG_CUDA( ctx, fetch( o.node_box.p, ( m - 1 ) * D * 4, nb ) );
   BVHG_CUDA( ctx, fetch( o.warp_box.p, nw * D * 2, wb ) );
   obj_scalars h;
   BVHG_CUDA( ctx, cudaMemcpy( &h, o.sc(), sizeof( h ), cudaMemcpyDeviceToHost ) );
   BVHG_CUDA( ctx, fetch( o.sc()->root_box, D * 2, rootb ) );
   std::vector< uint32_t > perm( n );
   BVHG_CUDA( ctx, cudaMemcpy( perm.data(), o.sorted_vals(), n * 4, cudaMemcpyDeviceToHost ) );
-  // every warp box is the union of its ranks' slabs
-  for ( uint64_t w = 0; w < nw; ++w )
+  // rank-order element slabs are the elements' slabs
+  for ( uint64_t r = 0; r < n; ++r )
+    for ( int k = 0; k < 2 * D; ++k )
+      if ( eb[r * D * 2 + k] != lb[static_cast< size_t >( perm[r] ) * D * 2 + k] )
+        return fail( ctx, BVHG_ERR_STATE, "rank-order element slabs differ from the elements' slabs" );
+  // union of ranks [lo, hi) into out (2 D values)
+  auto unite = [&](uint64_t lo, uint64_t hi, std::vector< double > &out) {
+    out.assign( 2 * D, 0.0 );
     for ( int a = 0; a < D; ++a )
     {
-      double lo = 0, hi = 0;
-      for ( uint64_t r = 32 * w; r < n && r < 32 * w + 32; ++r )
+      double mn = eb[lo * D * 2 + 2 * a], mx = eb[lo * D * 2 + 2 * a + 1];
+      for ( uint64_t r = lo + 1; r < hi; ++r )
       {
-        const double *l = &lb[static_cast< size_t >( perm[r] ) * D * 2];
-        lo = r == 32 * w ? l[2 * a] : std::min( lo, l[2 * a] );
-        hi = r == 32 * w ? l[2 * a + 1] : std::max( hi, l[2 * a + 1] );
+        mn = std::min( mn, eb[r * D * 2 + 2 * a] );
+        mx = std::max( mx, eb[r * D * 2 + 2 * a + 1] );
       }
-      if ( wb[( w * D + a ) * 2] != lo || wb[( w * D + a ) * 2 + 1] != hi )
-        return fail( ctx, BVHG_ERR_STATE, "warp box is not the union of its ranks' slabs" );
+      out[2 * a] = mn;
+      out[2 * a + 1] = mx;
     }
-  if ( n == 1 )
+  };
+  std::vector< double > u;
+  for ( uint64_t w = 0; w < nw; ++w )
   {
-    for ( int a = 0; a < 2 * D; ++a )
-      if ( rootb[a] != lb[a] ) return fail( ctx, BVHG_ERR_STATE, "single-element root box differs" );
+    unite( 32 * w, std::min< uint64_t >( n, 32 * w + 32 ), u );
+    for ( int k = 0; k < 2 * D; ++k )
+      if ( wb[w * D * 2 + k] != u[k] ) return fail( ctx, BVHG_ERR_STATE, "query group box is not the union of its ranks" );
+  }
+  std::vector< std::vector< double > > bucket( m );
+  for ( uint64_t b = 0; b < m; ++b ) unite( kLeafSize * b, std::min< uint64_t >( n, kLeafSize * b + kLeafSize ), bucket[b] );
+  if ( m == 1 )
+  {
+    if ( h.root != ~0 ) return fail( ctx, BVHG_ERR_STATE, "bad root of a one-bucket tree" );
+    for ( int k = 0; k < 2 * D; ++k )
+      if ( rootb[k] != bucket[0][k] ) return fail( ctx, BVHG_ERR_STATE, "one-bucket root box differs" );
     if ( depth_out ) *depth_out = 1;
     return BVHG_OK;
   }
-  std::vector< int2 > child( m );
-  BVHG_CUDA( ctx, cudaMemcpy( child.data(), o.child.p, m * 8, cudaMemcpyDeviceToHost ) );
-  if ( h.root < 0 || static_cast< uint64_t >( h.root ) >= m ) return fail( ctx, BVHG_ERR_STATE, "bad root" );
+  std::vector< int2 > child( m - 1 );
+  BVHG_CUDA( ctx, cudaMemcpy( child.data(), o.child.p, ( m - 1 ) * 8, cudaMemcpyDeviceToHost ) );
+  if ( h.root < 0 || static_cast< uint64_t >( h.root ) >= m - 1 ) return fail( ctx, BVHG_ERR_STATE, "bad root" );
   for ( int a = 0; a < D; ++a )
   {
     const double *slot = &nb[static_cast< size_t >( h.root ) * D * 4];
@@ -820,8 +841,8 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
          rootb[2 * a + 1] != std::max( slot[a * 4 + 1], slot[a * 4 + 3] ) )
       return fail( ctx, BVHG_ERR_STATE, "root box is not the union of the root's children" );
   }
-  std::vector< uint8_t > seen_leaf( n, 0 ), seen_node( m, 0 );
-  // (node, depth): every child's slabs lie inside the slot its parent stores for it; leaf slots equal the slabs
+  std::vector< uint8_t > seen_leaf( m, 0 ), seen_node( m - 1, 0 );
+  // (node, depth): every child's slot is the exact union of what it covers; buckets reached once
   std::vector< std::pair< int, uint32_t > > st{ { h.root, 1u } };
   uint32_t maxd = 0;
   uint64_t leaves = 0, nodes = 0;
@@ -838,30 +859,26 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
     {
       if ( c[side] < 0 )
       {
-        const uint32_t e = static_cast< uint32_t >( ~c[side] );
-        if ( e >= n || seen_leaf[e] ) return fail( ctx, BVHG_ERR_STATE, "leaf missing or reached twice" );
-        seen_leaf[e] = 1;
+        const uint64_t bb = static_cast< uint64_t >( ~c[side] );
+        if ( bb >= m || seen_leaf[bb] ) return fail( ctx, BVHG_ERR_STATE, "bucket missing or reached twice" );
+        seen_leaf[bb] = 1;
         ++leaves;
         maxd = d + 1 > maxd ? d + 1 : maxd;
-        const double *l = &lb[static_cast< size_t >( e ) * D * 2];
         for ( int a = 0; a < D; ++a )
-          if ( slot[a * 4 + side * 2] != l[2 * a] || slot[a * 4 + side * 2 + 1] != l[2 * a + 1] )
-            return fail( ctx, BVHG_ERR_STATE, "leaf slot differs from the element's slabs" );
+          if ( slot[a * 4 + side * 2] != bucket[bb][2 * a] || slot[a * 4 + side * 2 + 1] != bucket[bb][2 * a + 1] )
+            return fail( ctx, BVHG_ERR_STATE, "bucket slot differs from the union of its elements" );
       } else {
-        if ( static_cast< uint64_t >( c[side] ) >= m ) return fail( ctx, BVHG_ERR_STATE, "bad child index" );
+        if ( static_cast< uint64_t >( c[side] ) >= m - 1 ) return fail( ctx, BVHG_ERR_STATE, "bad child index" );
         const double *cs = &nb[static_cast< size_t >( c[side] ) * D * 4];
         for ( int a = 0; a < D; ++a )
-        {
-          const double lo = slot[a * 4 + side * 2], hi = slot[a * 4 + side * 2 + 1];
-          for ( int g = 0; g < 2; ++g )
-            if ( cs[a * 4 + g * 2] < lo || cs[a * 4 + g * 2 + 1] > hi )
-              return fail( ctx, BVHG_ERR_STATE, "child slabs escape the parent's slot" );
-        }
+          if ( slot[a * 4 + side * 2] != std::min( cs[a * 4], cs[a * 4 + 2] ) ||
+               slot[a * 4 + side * 2 + 1] != std::max( cs[a * 4 + 1], cs[a * 4 + 3] ) )
+            return fail( ctx, BVHG_ERR_STATE, "node slot is not the union of the child's children" );
         st.push_back( { c[side], d + 1 } );
       }
     }
   }
-  if ( leaves != n || nodes != m ) return fail( ctx, BVHG_ERR_STATE, "node count is not 2n - 1" );
+  if ( leaves != m || nodes != m - 1 ) return fail( ctx, BVHG_ERR_STATE, "tree does not cover every bucket once" );
   if ( depth_out ) *depth_out = maxd;
   return BVHG_OK;
 }

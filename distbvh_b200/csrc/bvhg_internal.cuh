@@ -1,20 +1,21 @@
 // bvhg_internal.cuh — device data layout shared by the kernels and the C ABI implementation.
 //
 // Per object of n elements with V vertices each and D = K/2 slabs (T = double in the FP64 form, float in the
-// FP32 form), all in HBM:
+// FP32 form), all in HBM. The tree's leaves are buckets of kLeafSize consecutive Morton ranks (m = ceil(n /
+// kLeafSize) buckets, m - 1 internal nodes); the pair set does not depend on the tree shape.
 //   verts      n * V * 3 doubles, element-major (input, owned copy or borrowed device pointer)
 //   cx, cy, cz n doubles each: centroids, structure of arrays (coalesced write in K1, read in K2)
 //   keys/vals  n u64 Morton keys and n u32 element indices, ping-ponged by the radix passes; after the sort
 //              keys[r], vals[r] hold the key and original index of rank r (vals = the permutation)
-//   warp_box   ceil(n / 32) * D * 2 T: union of the slabs of ranks [32 w, 32 w + 31], [w][a][min,max] (the
-//              query side's first cull); a leaf's own slabs are read from its slot in its parent
-//   node_box   (n - 1) * D * 2 * 2 T: both children's slabs of internal node k, [k][a][child][min,max], so one
+//   elem_box   n * D * 2 T: slabs of the element of rank r, [r][a][min,max] (leaf tests and queries)
+//   warp_box   ceil(n / 32) * D * 2 T: union of the slabs of ranks [32 w, 32 w + 31] (the query side's cull)
+//   node_box   (m - 1) * D * 2 * 2 T: both children's slabs of internal node k, [k][a][child][min,max], so one
 //              32-byte (FP64) or 16-byte (FP32) sector per axis tests both children
-//   child      (n - 1) int2: child index, >= 0 internal node, < 0 leaf with ~child = original element index
-//   range      (n - 1) int2: [first rank, last rank] covered by the node (self-collision pruning)
-//   parent     n + (n - 1) int32: parent * 2 + side of every leaf (rank order) and internal node (refit)
-//   exch       n - 1 int32: the agglomerative build's exchange slot per internal node (-1 = empty)
-//   queue      n int4: subtrees the warp-local build phase leaves to the global phase
+//   child      (m - 1) int2: child index, >= 0 internal node, < 0 bucket with ~child = bucket index
+//   range      (m - 1) int2: [first bucket, last bucket] covered by the node (self-collision pruning)
+//   parent     m + (m - 1) int32: parent * 2 + side of every bucket and internal node (refit)
+//   exch       m - 1 int32: the agglomerative build's exchange slot per internal node (-1 = empty)
+//   queue      m int4: subtrees the block-local build phases leave to the global phase
 #pragma once
 
 #include <cstddef>
@@ -44,6 +45,8 @@ struct pair_scalars
   int error;
   int pad;
 };
+
+constexpr int kLeafSize = 8;  // elements per tree leaf (consecutive Morton ranks)
 
 constexpr int kErrArg = 1;
 constexpr int kErrTimeout = 4;
@@ -92,16 +95,17 @@ cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *v
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
                             obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s);
 
-// Leaf slabs + agglomerative LBVH build with bottom-up refit (FP64 or FP32 slabs): two launches, a warp-local
-// phase that queues unfinished subtrees (queue: n int4) and a global climb over the queue.
+// Element slabs + agglomerative LBVH build over leaf buckets with bottom-up refit (FP64 or FP32 slabs): two
+// launches, a block-local phase that queues unfinished subtrees and a global climb over the queue.
 cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint64_t *keys, const uint32_t *vals, void *warp_box, void *node_box, int2 *child,
-                         int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s);
+                         const uint64_t *keys, const uint32_t *vals, void *elem_box, void *warp_box, void *node_box,
+                         int2 *child, int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc,
+                         cudaStream_t s);
 
-// Refit with the topology of the last build: recompute leaf slabs and every internal node.
+// Refit with the topology of the last build: recompute element slabs, bucket boxes and every internal node.
 cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *warp_box, void *node_box, const int *parent, int *exch,
-                         obj_scalars *sc, cudaStream_t s);
+                         const uint32_t *vals, void *elem_box, void *warp_box, void *node_box, const int *parent,
+                         int *exch, obj_scalars *sc, cudaStream_t s);
 
 struct tree_view
 {
@@ -109,7 +113,7 @@ struct tree_view
   const int2 *child;
   const int2 *range;
   const void *warp_box;
-  const int *parent;
+  const void *elem_box;
   const uint32_t *perm;
   uint64_t n;
   const obj_scalars *sc;

@@ -5,13 +5,14 @@
 // pruning on the strict all-slab overlap (kdop.hpp:120-125, 538-549). Here each thread takes one leaf of the query
 // object, in Morton order so that a warp's queries are spatially coherent, and descends the other object's tree
 // with an explicit stack: both children of a node are tested from one 32-byte (FP64) / 16-byte (FP32) sector per
-// slab, with early exit on the first separating slab. Leaf-leaf overlaps are emitted as (query element, tree
-// element) local indices through a global atomic counter; pairs beyond capacity are counted but not stored, so
-// the host can grow the buffer and retry.
+// slab, with early exit on the first separating slab. At a leaf bucket the query is tested against each of the
+// bucket's elements. Overlaps are emitted as (query element, tree element) local indices through a global atomic
+// counter; pairs beyond capacity are counted but not stored, so the host can grow the buffer and retry.
 //
 // Self-collision (self_collision_set, collision_query.hpp:331-368): the query leaf of rank i only visits
-// subtrees holding ranks > i (internal node k splits its range [l, r] into [l, k] and [k + 1, r]), so every
-// unordered pair is found once and no element is paired with itself.
+// subtrees holding ranks > i (internal node k splits its bucket range [l, r] into [l, k] and [k + 1, r]) and
+// tests only bucket elements of rank > i, so every unordered pair is found once and no element is paired with
+// itself.
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
 
@@ -54,14 +55,37 @@ __device__ __forceinline__ void emit(uint32_t a, uint32_t b, uint2 *pairs, uint6
   if ( p < cap ) pairs[p] = make_uint2( a, b );
 }
 
+// The elements of target bucket bb against the query slabs (ranks > skip only, for self-collision).
+template< int D, typename T >
+__device__ __forceinline__ void test_bucket(const T *qlo, const T *qhi, uint32_t qe, int bb, int nt, int skip,
+                                            const T *__restrict__ telem, const uint32_t *__restrict__ tperm,
+                                            uint2 *pairs, uint64_t cap, pair_scalars *ps)
+{
+  const int r0 = max( kLeafSize * bb, skip + 1 );
+  const int r1 = min( kLeafSize * bb + kLeafSize, nt );
+  for ( int r = r0; r < r1; ++r )
+  {
+    const T *eb = telem + static_cast< size_t >( r ) * D * 2;
+    bool o = true;
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      if ( !o ) break;
+      o = qlo[a] < __ldg( eb + 2 * a + 1 ) && __ldg( eb + 2 * a ) < qhi[a];
+    }
+    if ( o ) emit( qe, __ldg( tperm + r ), pairs, cap, ps );
+  }
+}
+
 template< int K, typename T >
 __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict__ qwarp,
-                                                           const T *__restrict__ qnode,
-                                                           const int *__restrict__ qparent,
+                                                           const T *__restrict__ qelem,
                                                            const uint32_t *__restrict__ qperm, uint32_t nq,
                                                            const int2 *__restrict__ child,
                                                            const T *__restrict__ nbox,
                                                            const int2 *__restrict__ range,
+                                                           const T *__restrict__ telem,
+                                                           const uint32_t *__restrict__ tperm,
                                                            const obj_scalars *__restrict__ tsc, uint32_t nt,
                                                            const obj_scalars *__restrict__ qsc, int self,
                                                            uint2 *pairs, uint64_t cap, pair_scalars *ps)
@@ -73,7 +97,7 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
   if ( *reinterpret_cast< const volatile int * >( &tsc->error ) == kErrTimeout ||
        *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
     return;
-  if ( ( i & ~31u ) >= nq ) return;  // warps entirely past the last rank have no warp box
+  if ( ( i & ~31u ) >= nq ) return;  // warps entirely past the last rank have no group box
   const T *rb = reinterpret_cast< const T * >( tsc->root_box );
   // 1. The union box of this warp's 32 query ranks against the target's root box, first four slabs first: a warp
   //    of queries far from the other object stops after one broadcast load.
@@ -88,35 +112,26 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
     if ( !o ) return;
   }
   if ( i >= nq ) return;
-  // 2. The query's own slabs: from its slot in its parent (or the root box of a one-element object).
+  // 2. The query's own slabs against the root box.
   T qlo[D], qhi[D];
   {
-    const T *qs;
-    int stride;
-    if ( nq == 1 )
-    {
-      qs = reinterpret_cast< const T * >( qsc->root_box );
-      stride = 2;
-    } else {
-      const int pp = __ldg( qparent + i );
-      qs = qnode + static_cast< size_t >( pp >> 1 ) * D * 4 + ( pp & 1 ) * 2;
-      stride = 4;
-    }
+    const T *qs = qelem + static_cast< size_t >( i ) * D * 2;
     bool o = true;
 #pragma unroll
     for ( int a = 0; a < D; ++a )
     {
-      qlo[a] = __ldg( qs + stride * a );
-      qhi[a] = __ldg( qs + stride * a + 1 );
+      qlo[a] = __ldg( qs + 2 * a );
+      qhi[a] = __ldg( qs + 2 * a + 1 );
       o = o && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
     }
     if ( !o ) return;
   }
   const uint32_t qe = __ldg( qperm + i );
+  const int skip = self ? static_cast< int >( i ) : -1;  // self-collision: only ranks above the query's
   const int root = tsc->root;
-  if ( nt == 1 )
+  if ( root < 0 )
   {
-    if ( !self ) emit( qe, static_cast< uint32_t >( ~root ), pairs, cap, ps );  // the root box is the leaf box
+    test_bucket< D >( qlo, qhi, qe, ~root, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
     return;
   }
   int stack[kStack];
@@ -129,9 +144,9 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
     bool o0 = true, o1 = true;
     if ( self )
     {
-      // left child covers ranks [l, node], right child [node + 1, r]
-      o0 = node > static_cast< int >( i );
-      o1 = __ldg( &range[node].y ) > static_cast< int >( i );
+      // left child covers buckets [l, node], right child [node + 1, r]; skip subtrees whose last rank <= i
+      o0 = kLeafSize * node + kLeafSize - 1 > static_cast< int >( i );
+      o1 = min( kLeafSize * __ldg( &range[node].y ) + kLeafSize - 1, static_cast< int >( nt ) - 1 ) > static_cast< int >( i );
     }
 #pragma unroll
     for ( int a = 0; a < D; ++a )
@@ -144,12 +159,12 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
     int next = -1;
     if ( o0 )
     {
-      if ( c.x < 0 ) emit( qe, static_cast< uint32_t >( ~c.x ), pairs, cap, ps );
+      if ( c.x < 0 ) test_bucket< D >( qlo, qhi, qe, ~c.x, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
       else next = c.x;
     }
     if ( o1 )
     {
-      if ( c.y < 0 ) emit( qe, static_cast< uint32_t >( ~c.y ), pairs, cap, ps );
+      if ( c.y < 0 ) test_bucket< D >( qlo, qhi, qe, ~c.y, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
       else if ( next < 0 ) next = c.y;
       else
       {
@@ -176,9 +191,10 @@ cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, uint2 *pairs, uin
 {
   const unsigned grid = static_cast< unsigned >( ( q.n + kTravThreads - 1 ) / kTravThreads );
   k_traverse< K, T ><<< grid, kTravThreads, 0, s >>>(
-    static_cast< const T * >( q.warp_box ), static_cast< const T * >( q.node_box ), q.parent, q.perm,
-    static_cast< uint32_t >( q.n ), t.child, static_cast< const T * >( t.node_box ), t.range, t.sc,
-    static_cast< uint32_t >( t.n ), q.sc, self ? 1 : 0, pairs, cap, ps );
+    static_cast< const T * >( q.warp_box ), static_cast< const T * >( q.elem_box ), q.perm,
+    static_cast< uint32_t >( q.n ), t.child, static_cast< const T * >( t.node_box ), t.range,
+    static_cast< const T * >( t.elem_box ), t.perm, t.sc, static_cast< uint32_t >( t.n ), q.sc, self ? 1 : 0, pairs,
+    cap, ps );
   return cudaGetLastError();
 }
 

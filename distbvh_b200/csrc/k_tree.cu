@@ -1,18 +1,17 @@
-// k_tree.cu — leaf slabs, LBVH build and bottom-up k-DOP refit in one kernel (K4 + K5).
+// k_tree.cu — element slabs, LBVH build and bottom-up k-DOP refit (K4 + K5).
 //
 // The reference builds its element trees on the host, top-down (top_down_builder, src/bvh/bvh_build.hpp:55-139,
-// mean split on the longest axis) or with a serial Morton bottom-up builder (bvh_build.hpp:145-296). Both give
-// one element per leaf and node k-DOP = union of the subtree (bvh_build.hpp:109-124; kdop merge, kdop.hpp:558-569),
-// so the pair set of a strict-overlap traversal does not depend on the tree shape. Here the tree is the binary
-// radix tree over the sorted Morton keys (Karras), built bottom-up agglomeratively (Apetrei): one thread per leaf
-// climbs while it is the second of two children to arrive at a node, merging ranges by comparing the
-// dissimilarity of the keys just outside its range, and writes each subtree's slabs into its parent as it goes.
-// Ties among equal keys are broken by rank, i.e. the tree is the radix tree of the 96-bit (key, rank) pairs.
+// mean split on the longest axis) or with a serial Morton bottom-up builder (bvh_build.hpp:145-296), one element
+// per leaf, node k-DOP = union of the subtree (bvh_build.hpp:109-124; kdop merge, kdop.hpp:558-569). The pair set
+// of a strict-overlap traversal does not depend on the tree shape, so here the leaves are buckets of kLeafSize
+// consecutive Morton ranks (the traversal tests a bucket's elements one by one) and the tree over the buckets is
+// the radix tree of the bucket-boundary keys, built bottom-up agglomeratively (Apetrei): a subtree [l, r] joins
+// the neighbour across its more similar boundary.
 //
-// No thread ever waits: the first arrival at a node leaves, the second continues. Most nodes have both children
-// finished inside one warp; those are merged in registers (warp-synchronous rounds, shuffles, no global
-// synchronization). The rest use a global exchange slot per node: the first arrival's slab stores are ordered
-// before its acq_rel atomic exchange, and the second arrival reads them through L2 after its own.
+// No thread ever waits. Nodes whose two children close inside a block of 256 buckets are merged in shared memory
+// (warp rounds, then block rounds) and written out coalesced; the rest use a global exchange slot per node: the
+// first arrival's slab stores are ordered before its acq_rel atomic exchange, and the second arrival reads them
+// through L2 after its own.
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
 
@@ -159,28 +158,6 @@ __device__ __forceinline__ void leaf_slabs(const double *__restrict__ verts, uin
   }
 }
 
-// Union of the slabs of the warp's 32 consecutive ranks (lanes past n contribute nothing), one box per warp.
-template< typename T, int D >
-__device__ __forceinline__ void store_warp_box(T *warp_box, int wbase, int n, bool active, const T *lo, const T *hi)
-{
-  using io = box_io< T >;
-  const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for ( int a = 0; a < D; ++a )
-  {
-    T l = active ? lo[a] : inf;
-    T h = active ? hi[a] : -inf;
-#pragma unroll
-    for ( int o = 16; o > 0; o >>= 1 )
-    {
-      l = io::mn( l, __shfl_xor_sync( 0xffffffffu, l, o ) );
-      h = io::mx( h, __shfl_xor_sync( 0xffffffffu, h, o ) );
-    }
-    if ( lane == 0 && wbase < n ) io::store2( warp_box + ( static_cast< size_t >( wbase >> 5 ) * D + a ) * 2, l, h );
-  }
-}
-
 // The root's slabs, for the traversal's first test.
 template< typename T, size_t D >
 __device__ __forceinline__ void store_root(obj_scalars *sc, const T ( &lo )[D], const T ( &hi )[D])
@@ -202,32 +179,105 @@ __device__ __forceinline__ int delta_of(uint64_t a, uint64_t b, int j)
   return 32 - __clz( j ^ ( j + 1 ) );
 }
 
-// Phase 1 (one thread per leaf rank i, blocks of 256 consecutive ranks). Everything a block decides about the
-// nodes it closes is staged in shared memory and written out once at the end, as whole 16-byte-aligned rows of
-// node_box (both children's slabs of consecutive nodes are contiguous), child, range and parent.
+// Dissimilarity of leaf buckets b and b + 1: the element dissimilarity across the bucket boundary, ties broken by
+// position, so that the values are distinct and the agglomerative rule builds a well-defined binary tree (the
+// Cartesian tree of these values, i.e. the radix tree of the boundary keys).
+__device__ __forceinline__ long long bdelta(const uint64_t *__restrict__ keys, int b)
+{
+  return ( static_cast< long long >( delta( keys, kLeafSize * b + kLeafSize - 1 ) ) << 32 ) | static_cast< unsigned >( b );
+}
+
+// Slabs of the elements of leaf bucket b (ranks kLeafSize * b .. + kLeafSize - 1, < n): each element's slabs go to
+// elem_box in rank order, their union to lo/hi. Returns false when the permutation is not one.
+template< int K, typename T, int VT >
+__device__ __forceinline__ bool bucket_slabs(const double *__restrict__ verts, uint32_t Vrt, int n, int b, double eps,
+                                             float eps_hi, const uint32_t *__restrict__ vals, T *__restrict__ elem_box,
+                                             T *lo, T *hi)
+{
+  constexpr int D = K / 2;
+  using io = box_io< T >;
+  const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
+#pragma unroll
+  for ( int a = 0; a < D; ++a )
+  {
+    lo[a] = inf;
+    hi[a] = -inf;
+  }
+  const int r0 = kLeafSize * b;
+  const int r1 = min( r0 + kLeafSize, n );
+  bool ok = true;
+  for ( int r = r0; r < r1; ++r )
+  {
+    const uint32_t e = __ldg( vals + r );
+    if ( e >= static_cast< uint32_t >( n ) )
+    {
+      ok = false;
+      continue;
+    }
+    T el[D], eh[D];
+    leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, el, eh );
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      io::store2( elem_box + ( static_cast< size_t >( r ) * D + a ) * 2, el[a], eh[a] );
+      lo[a] = io::mn( lo[a], el[a] );
+      hi[a] = io::mx( hi[a], eh[a] );
+    }
+  }
+  return ok;
+}
+
+// Union boxes of 32 consecutive ranks (kQueryGroup / kLeafSize buckets, adjacent lanes): the traversal culls a
+// warp of 32 queries with one of them.
+template< typename T, int D >
+__device__ __forceinline__ void store_query_group_box(T *warp_box, int b, int m, bool active, const T *lo, const T *hi)
+{
+  using io = box_io< T >;
+  constexpr int G = 32 / kLeafSize;  // buckets per group
+  const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for ( int a = 0; a < D; ++a )
+  {
+    T l = active ? lo[a] : inf;
+    T h = active ? hi[a] : -inf;
+#pragma unroll
+    for ( int o = 1; o < G; o <<= 1 )
+    {
+      l = io::mn( l, __shfl_xor_sync( 0xffffffffu, l, o ) );
+      h = io::mx( h, __shfl_xor_sync( 0xffffffffu, h, o ) );
+    }
+    if ( ( lane & ( G - 1 ) ) == 0 && b < m )
+      io::store2( warp_box + ( static_cast< size_t >( b / G ) * D + a ) * 2, l, h );
+  }
+}
+
+// Phase 1 (one thread per leaf bucket b, blocks of 256 consecutive buckets). Everything a block decides about the
+// nodes it closes is staged in shared memory and written out once at the end, as whole rows of node_box (both
+// children's slabs of consecutive nodes are contiguous), child, range and parent.
 //
-// a. Each thread computes its leaf's slabs into the warp's box table, column = lane (component c = 2 axis +
-//    {0 min, 1 max}). A table has 64 columns: 32 leaves and 32 internal nodes (node p of the block lives in the
-//    table of warp (p - bbase) / 32, column 32 + (p - bbase) % 32).
-// b. Warp rounds (topology in registers): every lane holding an unfinished subtree [l, r] picks its parent from
-//    the dissimilarities just outside the range; two lanes meeting on one parent are its children. The parent's
-//    box is formed with the lanes acting as slab components (one min or max per lane).
-// c. The union of the subtrees the warp still holds is the warp box (the traversal's cull for these 32 queries).
-// d. Block rounds: the warps' remaining subtrees meet through shared tables indexed by the first and the last
-//    rank of each subtree (a left child with parent r looks for a subtree starting at r + 1 that targets the same
-//    parent as right child; a right child with parent l - 1 for one ending at l - 1).
-// e. Subtrees still unfinished publish their box into their parent's slot and are queued for phase 2 as
+// a. Each thread computes the slabs of its bucket's elements (written to elem_box in rank order), their union
+//    (the bucket box, into the warp's box table in shared memory) and the 32-rank query-group boxes. A table has
+//    64 rows: 32 buckets and 32 internal nodes (node p of the block lives in the table of warp (p - bbase) / 32,
+//    row 32 + (p - bbase) % 32); a row holds the C = 2 D components, padded to C + 1 against bank conflicts.
+// b. Warp rounds (topology in registers): every lane holding an unfinished subtree [l, r] (in buckets) picks its
+//    parent from the dissimilarities just outside the range; two lanes meeting on one parent are its children.
+//    The parent's box is formed with the lanes acting as slab components (one min or max per lane).
+// c. Block rounds: the warps' remaining subtrees meet through shared tables indexed by the first and the last
+//    bucket of each subtree (a left child with parent r looks for a subtree starting at r + 1 that targets the
+//    same parent as right child; a right child with parent l - 1 for one ending at l - 1).
+// d. Subtrees still unfinished publish their box into their parent's slot and are queued for phase 2 as
 //    (parent * 2 + side, l, r, node).
-// f. Coalesced write-out of every node closed in the block.
+// e. Coalesced write-out of every node closed in the block.
 template< int K, typename T, int VT >
 __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double *__restrict__ verts, uint32_t Vrt, int n,
                                                               double eps, float eps_hi,
                                                               const uint64_t *__restrict__ keys,
                                                               const uint32_t *__restrict__ vals,
-                                                              T *__restrict__ warp_box, T *__restrict__ node_box,
-                                                              int *__restrict__ child, int2 *__restrict__ range,
-                                                              int *__restrict__ parent, int4 *__restrict__ queue,
-                                                              obj_scalars *sc)
+                                                              T *__restrict__ elem_box, T *__restrict__ warp_box,
+                                                              T *__restrict__ node_box, int *__restrict__ child,
+                                                              int2 *__restrict__ range, int *__restrict__ parent,
+                                                              int4 *__restrict__ queue, obj_scalars *sc)
 {
   constexpr int D = K / 2;
   constexpr int C = 2 * D;
@@ -237,52 +287,40 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
   T *s_box = reinterpret_cast< T * >( s_raw );  // [W * 64][C + 1]
   __shared__ int2 s_child[kBuildThreads];       // closed node p - bbase: global child encodings
   __shared__ int2 s_cref[kBuildThreads];        // closed node p - bbase: box table refs of its children
-  __shared__ int2 s_rng[kBuildThreads];
+  __shared__ int2 s_rng[kBuildThreads];         // closed node p - bbase: bucket range (x < 0: not closed here)
   __shared__ int s_pnode[kBuildThreads];        // parent entry of node p - bbase, -1 when not closed here
-  __shared__ int s_pleaf[kBuildThreads];        // parent entry of leaf bbase + k
+  __shared__ int s_pleaf[kBuildThreads];        // parent entry of bucket bbase + k
   __shared__ short s_start[kBuildThreads], s_end[kBuildThreads];
   __shared__ int s_par[kBuildThreads], s_r[kBuildThreads], s_ref[kBuildThreads], s_gn[kBuildThreads];
-  __shared__ int s_delta[kBuildThreads + 1];  // dissimilarity of ranks (bbase - 1 + k, bbase + k)
+  __shared__ long long s_delta[kBuildThreads + 1];  // dissimilarity of buckets (bbase - 1 + k, bbase + k)
   __shared__ int4 s_pairs[kBuildThreads / 2];
   __shared__ int s_npairs, s_root_tid;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int i = static_cast< int >( blockIdx.x * blockDim.x ) + tid;
-  const int wbase = i - lane, bbase = i - tid;
-  // box table element of ref (table * 64 + column), component c: one padded row of C + 1 per box, so lanes
-  // acting as components touch consecutive words and a lane writing its own row strides by an odd count
+  const int b = static_cast< int >( blockIdx.x * blockDim.x ) + tid;
+  const int wbase = b - lane, bbase = b - tid;
+  const int m = ( n + kLeafSize - 1 ) / kLeafSize;  // buckets
+  // box table element of ref (table * 64 + row), component c
   auto box = [&](int ref, int c) -> T & { return s_box[ref * ( C + 1 ) + c]; };
   auto node_ref = [&](int p) { const int q = p - bbase; return ( q >> 5 ) * 64 + 32 + ( q & 31 ); };
   // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word).
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // same value for all threads
-  bool active = i < n;
-  const uint32_t e = active ? __ldg( vals + i ) : 0u;
-  if ( active && e >= static_cast< uint32_t >( n ) )
-  {
-    atomicCAS( &sc->error, 0, kErrTimeout );
-    active = false;
-  }
-  // dissimilarity of ranks (i, i + 1) and of (wbase - 1, wbase)
-  const uint64_t kself = active ? __ldg( keys + i ) : 0ull;
-  uint64_t knext = __shfl_down_sync( 0xffffffffu, kself, 1 );
-  if ( lane == 31 && i + 1 < n ) knext = __ldg( keys + i + 1 );
-  const int dself = ( i + 1 < n ) ? delta_of( kself, knext, i ) : 0;
-  int dleft = 0;
-  if ( lane == 0 && wbase >= 1 && wbase < n ) dleft = delta_of( __ldg( keys + wbase - 1 ), kself, wbase - 1 );
-  dleft = __shfl_sync( 0xffffffffu, dleft, 0 );
+  bool active = b < m;
 
-  // a. leaf slabs into the box table
+  // a. element slabs, bucket box, query-group boxes
   {
     T lo[D], hi[D];
-    if ( active ) leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
-    if ( n == 1 )
+    if ( active && !bucket_slabs< K, T, VT >( verts, Vrt, n, b, eps, eps_hi, vals, elem_box, lo, hi ) )
+      atomicCAS( &sc->error, 0, kErrTimeout );
+    store_query_group_box< T, D >( warp_box, b, m, active, lo, hi );
+    if ( m == 1 )
     {
-      if ( active )
+      if ( b == 0 )
       {
-        sc->root = ~static_cast< int >( e );
+        sc->root = ~0;
         store_root( sc, lo, hi );
       }
-      return;  // n is uniform
+      return;  // m is uniform
     }
     if ( active )
     {
@@ -294,9 +332,13 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
       }
     }
   }
+  const long long dself = ( b + 1 < m ) ? bdelta( keys, b ) : 0ll;
+  long long dleft = 0;
+  if ( lane == 0 && wbase >= 1 && wbase < m ) dleft = bdelta( keys, wbase - 1 );
+  dleft = __shfl_sync( 0xffffffffu, dleft, 0 );
   s_pnode[tid] = -1;
   s_pleaf[tid] = -1;
-  s_rng[tid] = make_int2( -1, -1 );  // x >= 0 marks a node closed in this block
+  s_rng[tid] = make_int2( -1, -1 );
   s_start[tid] = -1;
   s_end[tid] = -1;
   s_delta[tid + 1] = dself;
@@ -304,16 +346,15 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
   {
     s_npairs = 0;
     s_root_tid = -1;
-    s_delta[0] = ( bbase >= 1 && bbase < n ) ? delta( keys, bbase - 1 ) : 0;
+    s_delta[0] = ( bbase >= 1 && bbase < m ) ? bdelta( keys, bbase - 1 ) : 0ll;
   }
   __syncthreads();  // the returns above are uniform over the grid
 
-  int l = i, r = i;
-  int gnode = ~static_cast< int >( e );  // child encoding of the subtree this lane holds
-  int ref = warp * 64 + lane;            // its box in the tables
-  int selfp = -1 - tid;                  // its parent entry: leaf (-1 - k) or closed node (p - bbase)
+  int l = b, r = b;
+  int gnode = ~b;             // child encoding of the subtree this lane holds (bucket: ~bucket)
+  int ref = warp * 64 + lane; // its box in the tables
+  int selfp = -1 - tid;       // its parent entry: bucket (-1 - k) or closed node (p - bbase)
   int par = 0, side = 0;
-  const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
   auto set_parent = [&](int entry) {
     if ( selfp < 0 ) s_pleaf[-1 - selfp] = entry;
     else s_pnode[selfp] = entry;
@@ -322,13 +363,13 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
   // b. warp rounds
   while ( true )
   {
-    const int d_r = __shfl_sync( 0xffffffffu, dself, ( r - wbase ) & 31 );
-    const int d_lm1 = __shfl_sync( 0xffffffffu, dself, ( l - 1 - wbase ) & 31 );
+    const long long d_r = __shfl_sync( 0xffffffffu, dself, ( r - wbase ) & 31 );
+    const long long d_lm1 = __shfl_sync( 0xffffffffu, dself, ( l - 1 - wbase ) & 31 );
     if ( active )
     {
       bool left_child;
       if ( l == 0 ) left_child = true;
-      else if ( r == n - 1 ) left_child = false;
+      else if ( r == m - 1 ) left_child = false;
       else left_child = d_r < ( l == wbase ? dleft : d_lm1 );
       par = left_child ? r : l - 1;
       side = left_child ? 0 : 1;
@@ -350,9 +391,9 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
       s_rng[q] = make_int2( l, sr );
     }
     // merged boxes, lanes as slab components
-    for ( unsigned m = lefts; m; m &= m - 1 )
+    for ( unsigned mm = lefts; mm; mm &= mm - 1 )
     {
-      const int L = __ffs( m ) - 1;
+      const int L = __ffs( mm ) - 1;
       const int p = __shfl_sync( 0xffffffffu, par, L );
       const int rl = __shfl_sync( 0xffffffffu, ref, L );
       const int rr = __shfl_sync( 0xffffffffu, sref, L );
@@ -371,7 +412,7 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
         gnode = par;
         ref = node_ref( par );
         selfp = par - bbase;
-        if ( l == 0 && r == n - 1 )
+        if ( l == 0 && r == m - 1 )
         {
           sc->root = par;
           s_root_tid = tid;
@@ -382,26 +423,9 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
       }
     }
   }
-
-  // c. warp box: union of the subtrees the warp's lanes still hold (and of the root, when the tree ends here)
-  {
-    const bool holds = active || ( s_root_tid == tid );
-    const unsigned hm = __ballot_sync( 0xffffffffu, holds );
-    T u = ( lane & 1 ) ? -inf : inf;
-    for ( unsigned m = hm; m; m &= m - 1 )
-    {
-      const int hr = __shfl_sync( 0xffffffffu, ref, __ffs( m ) - 1 );
-      if ( lane < C )
-      {
-        const T x = box( hr, lane );
-        u = ( lane & 1 ) ? io::mx( u, x ) : io::mn( u, x );
-      }
-    }
-    if ( lane < C && wbase < n ) warp_box[static_cast< size_t >( wbase >> 5 ) * C + lane] = u;
-  }
   __syncthreads();
 
-  // d. block rounds
+  // c. block rounds
   while ( true )
   {
     if ( active )
@@ -420,7 +444,7 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
       if ( side == 0 )
       {
         const int q = r + 1;
-        if ( q < bbase + kBuildThreads && q < n )
+        if ( q < bbase + kBuildThreads && q < m )
         {
           const int c = s_start[q - bbase];
           if ( c >= 0 && s_par[c] == 2 * par + 1 ) partner = c;
@@ -473,7 +497,7 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
         gnode = par;
         ref = node_ref( par );
         selfp = par - bbase;
-        if ( l == 0 && r == n - 1 )
+        if ( l == 0 && r == m - 1 )
         {
           sc->root = par;
           s_root_tid = tid;
@@ -481,7 +505,7 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
         } else {
           bool left_child;
           if ( l == 0 ) left_child = true;
-          else if ( r == n - 1 ) left_child = false;
+          else if ( r == m - 1 ) left_child = false;
           else left_child = s_delta[r - bbase + 1] < s_delta[l - bbase];
           par = left_child ? r : l - 1;
           side = left_child ? 0 : 1;
@@ -497,11 +521,11 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
   if ( s_root_tid >= 0 && lane < C && warp == ( s_root_tid >> 5 ) )
     reinterpret_cast< T * >( sc->root_box )[lane] = box( node_ref( sc->root ), lane );
 
-  // e. unfinished subtrees: publish their box into the parent's slot and queue them for phase 2
+  // d. unfinished subtrees: publish their box into the parent's slot and queue them for phase 2
   const unsigned waiting = __ballot_sync( 0xffffffffu, active );
-  for ( unsigned m = waiting; m; m &= m - 1 )
+  for ( unsigned mm = waiting; mm; mm &= mm - 1 )
   {
-    const int j = __ffs( m ) - 1;
+    const int j = __ffs( mm ) - 1;
     const int p = __shfl_sync( 0xffffffffu, par, j );
     const int sd = __shfl_sync( 0xffffffffu, side, j );
     const int rf = __shfl_sync( 0xffffffffu, ref, j );
@@ -516,17 +540,16 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
     if ( active )
     {
       child[2 * par + side] = gnode;
-      parent[selfp < 0 ? i : n + bbase + selfp] = 2 * par + side;
-      queue[base + __popc( waiting & ( ( 1u << lane ) - 1u ) )] =
-        make_int4( 2 * par + side, l, r, gnode );
+      parent[selfp < 0 ? b : m + bbase + selfp] = 2 * par + side;
+      queue[base + __popc( waiting & ( ( 1u << lane ) - 1u ) )] = make_int4( 2 * par + side, l, r, gnode );
     }
   }
 
-  // f. coalesced write-out of the nodes closed in this block: node_box rows (16-byte pairs), child, range, parent
-  const int nclosed = min( kBuildThreads, n - 1 - bbase );  // internal nodes bbase .. bbase + nclosed - 1
+  // e. coalesced write-out of the nodes closed in this block: node_box rows (16-byte pairs), child, range, parent
+  const int nclosed = min( kBuildThreads, m - 1 - bbase );  // internal nodes bbase .. bbase + nclosed - 1
   for ( int k = tid; k < nclosed * C; k += kBuildThreads )
   {
-    // the row of node q = k / C holds C 16-byte (min, max) pairs in the order (axis, side); pair t = k % C
+    // the row of node q = k / C holds C (min, max) pairs in the order (axis, side); pair t = k % C
     const int q = k / C, t = k % C;
     if ( s_rng[q].x < 0 ) continue;
     const int2 cr = s_cref[q];
@@ -539,9 +562,9 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
   {
     reinterpret_cast< int2 * >( child )[bbase + tid] = s_child[tid];
     range[bbase + tid] = s_rng[tid];
-    if ( s_pnode[tid] >= 0 ) parent[n + bbase + tid] = s_pnode[tid];
+    if ( s_pnode[tid] >= 0 ) parent[m + bbase + tid] = s_pnode[tid];
   }
-  if ( i < n && s_pleaf[tid] >= 0 ) parent[i] = s_pleaf[tid];
+  if ( b < m && s_pleaf[tid] >= 0 ) parent[b] = s_pleaf[tid];
 }
 
 // Phase 2 (dense, one thread per queued subtree): the agglomerative climb with a global exchange slot per node.
@@ -556,6 +579,7 @@ __global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__
   constexpr int D = K / 2;
   using io = box_io< T >;
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
+  const int m = ( n + kLeafSize - 1 ) / kLeafSize;
   const unsigned count = *reinterpret_cast< volatile unsigned * >( &sc->climb_count );
   for ( unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x )
   {
@@ -580,18 +604,18 @@ __global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__
         hi[a] = io::mx( hi[a], sh );
       }
       range[par] = make_int2( l, r );
-      if ( l == 0 && r == n - 1 )
+      if ( l == 0 && r == m - 1 )
       {
         sc->root = par;
         store_root( sc, lo, hi );
         break;
       }
       const int node = par;
-      const int self_slot = n + par;
+      const int self_slot = m + par;
       bool left_child;
       if ( l == 0 ) left_child = true;
-      else if ( r == n - 1 ) left_child = false;
-      else left_child = delta( keys, r ) < delta( keys, l - 1 );
+      else if ( r == m - 1 ) left_child = false;
+      else left_child = bdelta( keys, r ) < bdelta( keys, l - 1 );
       par = left_child ? r : l - 1;
       side = left_child ? 0 : 1;
       pb = node_box + static_cast< size_t >( par ) * D * 4;
@@ -603,37 +627,31 @@ __global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__
   }
 }
 
-// Refit with a fixed topology: leaf slabs again (elements keep their ranks), then the same first/second arrival
-// climb along the stored parent links. exch must be reset to -1 before the launch.
+// Refit with a fixed topology (one thread per bucket): the elements' slabs and the bucket box again (elements keep
+// their ranks), then the first/second-arrival climb along the stored parent links. exch must hold -1.
 template< int K, typename T, int VT >
 __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restrict__ verts, uint32_t Vrt, int n,
                                                          double eps, float eps_hi, const uint32_t *__restrict__ vals,
-                                                         T *__restrict__ warp_box, T *node_box,
-                                                         const int *__restrict__ parent, int *exch,
+                                                         T *__restrict__ elem_box, T *__restrict__ warp_box,
+                                                         T *node_box, const int *__restrict__ parent, int *exch,
                                                          obj_scalars *__restrict__ sc)
 {
   constexpr int D = K / 2;
   using io = box_io< T >;
-  const int i = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
-  const bool active = i < n;
-  const uint32_t e = active ? __ldg( vals + i ) : 0u;
+  const int b = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
+  const int m = ( n + kLeafSize - 1 ) / kLeafSize;
+  const bool active = b < m;
   T lo[D], hi[D];
-  if ( active )
-  {
-    leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
-  } else {
-#pragma unroll
-    for ( int a = 0; a < D; ++a ) lo[a] = hi[a] = T( 0 );
-  }
-  store_warp_box< T, D >( warp_box, i - ( static_cast< int >( threadIdx.x ) & 31 ), n, active, lo, hi );
+  if ( active ) bucket_slabs< K, T, VT >( verts, Vrt, n, b, eps, eps_hi, vals, elem_box, lo, hi );
+  store_query_group_box< T, D >( warp_box, b, m, active, lo, hi );
   if ( !active ) return;
-  if ( n == 1 )
+  if ( m == 1 )
   {
     store_root( sc, lo, hi );
     return;
   }
   const int root = sc->root;
-  int slot = i;
+  int slot = b;
   while ( true )
   {
     const int ps = __ldg( parent + slot );
@@ -656,34 +674,30 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restr
       store_root( sc, lo, hi );
       return;
     }
-    slot = n + par;
+    slot = m + par;
   }
 }
 
 template< int K, typename T, int VT >
 cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys,
-                           const uint32_t *vals, void *warp_box, void *node_box, int2 *child, int2 *range, int *parent,
-                           int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s)
+                           const uint32_t *vals, void *elem_box, void *warp_box, void *node_box, int2 *child,
+                           int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
   const float eps_hi = f32_up( eps );
-  const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
+  const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
+  const unsigned grid = static_cast< unsigned >( ( m + kBuildThreads - 1 ) / kBuildThreads );
   const size_t smem = static_cast< size_t >( 2 * kBuildThreads ) * ( 2 * ( K / 2 ) + 1 ) * sizeof( T );  // [W * 64][C + 1]
-  static bool configured = false;
-  if ( !configured )
-  {
-    cudaError_t e0 = cudaFuncSetAttribute( k_build_leaf< K, T, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast< int >( smem ) );
-    if ( e0 != cudaSuccess ) return e0;
-    configured = true;
-  }
+  cudaError_t e = cudaFuncSetAttribute( k_build_leaf< K, T, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast< int >( smem ) );
+  if ( e != cudaSuccess ) return e;
   k_build_leaf< K, T, VT ><<< grid, kBuildThreads, smem, s >>>(
-    verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals, static_cast< T * >( warp_box ),
-    static_cast< T * >( node_box ), reinterpret_cast< int * >( child ), range, parent, queue, sc );
-  cudaError_t e = cudaGetLastError();
-  if ( e != cudaSuccess || n < 2 ) return e;
-  // The queue length is known only on the device: a grid-stride grid covering the worst case n / 2 for the
-  // usual fraction (a few percent) in one sweep.
-  const uint64_t want = ( n / 16 + 127 ) / 128;
+    verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals, static_cast< T * >( elem_box ),
+    static_cast< T * >( warp_box ), static_cast< T * >( node_box ), reinterpret_cast< int * >( child ), range, parent,
+    queue, sc );
+  e = cudaGetLastError();
+  if ( e != cudaSuccess || m < 2 ) return e;
+  // The queue length is known only on the device: a grid-stride grid sized for the usual fraction.
+  const uint64_t want = ( m / 8 + 127 ) / 128;
   const unsigned cgrid = static_cast< unsigned >( want < 148 * 16 ? ( want ? want : 1 ) : 148 * 16 );
   k_build_climb< K, T ><<< cgrid, 128, 0, s >>>( static_cast< int >( n ), keys, static_cast< T * >( node_box ),
                                                 reinterpret_cast< int * >( child ), range, parent, exch, queue, sc );
@@ -692,41 +706,42 @@ cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double e
 
 template< int K, typename T, int VT >
 cudaError_t launch_refit_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
-                           void *warp_box, void *node_box, const int *parent, int *exch, obj_scalars *sc,
-                           cudaStream_t s)
+                           void *elem_box, void *warp_box, void *node_box, const int *parent, int *exch,
+                           obj_scalars *sc, cudaStream_t s)
 {
   const float eps_hi = f32_up( eps );
-  const unsigned grid = static_cast< unsigned >( ( n + kBuildThreads - 1 ) / kBuildThreads );
+  const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
+  const unsigned grid = static_cast< unsigned >( ( m + kBuildThreads - 1 ) / kBuildThreads );
   k_refit< K, T, VT ><<< grid, kBuildThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, eps_hi, vals,
-                                                       static_cast< T * >( warp_box ), static_cast< T * >( node_box ),
-                                                       parent, exch, sc );
+                                                       static_cast< T * >( elem_box ), static_cast< T * >( warp_box ),
+                                                       static_cast< T * >( node_box ), parent, exch, sc );
   return cudaGetLastError();
 }
 
 template< int K, typename T >
 cudaError_t build_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys, const uint32_t *vals,
-                    void *lb, void *nb, int2 *child, int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc,
-                    cudaStream_t s)
+                    void *eb, void *wb, void *nb, int2 *child, int2 *range, int *parent, int *exch, int4 *queue,
+                    obj_scalars *sc, cudaStream_t s)
 {
   switch ( V )
   {
-    case 3: return launch_build_t< K, T, 3 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, queue, sc, s );
-    case 4: return launch_build_t< K, T, 4 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, queue, sc, s );
-    case 8: return launch_build_t< K, T, 8 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, queue, sc, s );
-    default: return launch_build_t< K, T, 0 >( verts, V, n, eps, keys, vals, lb, nb, child, range, parent, exch, queue, sc, s );
+    case 3: return launch_build_t< K, T, 3 >( verts, V, n, eps, keys, vals, eb, wb, nb, child, range, parent, exch, queue, sc, s );
+    case 4: return launch_build_t< K, T, 4 >( verts, V, n, eps, keys, vals, eb, wb, nb, child, range, parent, exch, queue, sc, s );
+    case 8: return launch_build_t< K, T, 8 >( verts, V, n, eps, keys, vals, eb, wb, nb, child, range, parent, exch, queue, sc, s );
+    default: return launch_build_t< K, T, 0 >( verts, V, n, eps, keys, vals, eb, wb, nb, child, range, parent, exch, queue, sc, s );
   }
 }
 
 template< int K, typename T >
-cudaError_t refit_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *lb, void *nb,
-                    const int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
+cudaError_t refit_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *eb, void *wb,
+                    void *nb, const int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
 {
   switch ( V )
   {
-    case 3: return launch_refit_t< K, T, 3 >( verts, V, n, eps, vals, lb, nb, parent, exch, sc, s );
-    case 4: return launch_refit_t< K, T, 4 >( verts, V, n, eps, vals, lb, nb, parent, exch, sc, s );
-    case 8: return launch_refit_t< K, T, 8 >( verts, V, n, eps, vals, lb, nb, parent, exch, sc, s );
-    default: return launch_refit_t< K, T, 0 >( verts, V, n, eps, vals, lb, nb, parent, exch, sc, s );
+    case 3: return launch_refit_t< K, T, 3 >( verts, V, n, eps, vals, eb, wb, nb, parent, exch, sc, s );
+    case 4: return launch_refit_t< K, T, 4 >( verts, V, n, eps, vals, eb, wb, nb, parent, exch, sc, s );
+    case 8: return launch_refit_t< K, T, 8 >( verts, V, n, eps, vals, eb, wb, nb, parent, exch, sc, s );
+    default: return launch_refit_t< K, T, 0 >( verts, V, n, eps, vals, eb, wb, nb, parent, exch, sc, s );
   }
 }
 
@@ -762,13 +777,16 @@ cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, voi
 }  // namespace
 
 cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint64_t *keys, const uint32_t *vals, void *warp_box, void *node_box, int2 *child,
-                         int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s)
+                         const uint64_t *keys, const uint32_t *vals, void *elem_box, void *warp_box, void *node_box,
+                         int2 *child, int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc,
+                         cudaStream_t s)
 {
-#define BVHG_BUILD_CASE( KK )                                                                                           \
-  case KK:                                                                                                             \
-    return fp32 ? build_v< KK, float >( verts, V, n, eps, keys, vals, warp_box, node_box, child, range, parent, exch, queue, sc, s ) \
-                : build_v< KK, double >( verts, V, n, eps, keys, vals, warp_box, node_box, child, range, parent, exch, queue, sc, s );
+#define BVHG_BUILD_CASE( KK )                                                                                      \
+  case KK:                                                                                                        \
+    return fp32 ? build_v< KK, float >( verts, V, n, eps, keys, vals, elem_box, warp_box, node_box, child, range,  \
+                                        parent, exch, queue, sc, s )                                               \
+                : build_v< KK, double >( verts, V, n, eps, keys, vals, elem_box, warp_box, node_box, child, range, \
+                                         parent, exch, queue, sc, s );
   switch ( K )
   {
     BVHG_BUILD_CASE( 6 )
@@ -780,17 +798,17 @@ cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint
 }
 
 cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *warp_box, void *node_box, const int *parent, int *exch,
-                         obj_scalars *sc, cudaStream_t s)
+                         const uint32_t *vals, void *elem_box, void *warp_box, void *node_box, const int *parent,
+                         int *exch, obj_scalars *sc, cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return fp32 ? refit_v< 6, float >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s )
-                        : refit_v< 6, double >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s );
-    case 18: return fp32 ? refit_v< 18, float >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s )
-                         : refit_v< 18, double >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s );
-    case 26: return fp32 ? refit_v< 26, float >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s )
-                         : refit_v< 26, double >( verts, V, n, eps, vals, warp_box, node_box, parent, exch, sc, s );
+    case 6: return fp32 ? refit_v< 6, float >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s )
+                        : refit_v< 6, double >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s );
+    case 18: return fp32 ? refit_v< 18, float >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s )
+                         : refit_v< 18, double >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s );
+    case 26: return fp32 ? refit_v< 26, float >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s )
+                         : refit_v< 26, double >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s );
     default: return cudaErrorInvalidValue;
   }
 }
