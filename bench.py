@@ -139,15 +139,22 @@ def peaks():
     return 6650.0, "fallback"
 
 
-# Algorithmic DRAM bytes per element of each stage for triangles (V = 3) with D = K/2 slabs of S bytes:
-#   bounds   read 72 (vertices) + write 24 (centroid, SoA)                               = 96
-#   keys     read 24 (centroid) + write 8 (key)                                          = 32
-#   sort     per pass read 12 + write 12 (key + index)                                   = 24 per pass
-#   build    read 72 (vertices, gathered) + 8 (key) + 4 (index) + write leaf slabs D*2*S + node slots
-#            2*D*2*S (one per child) + 8 (child) + 8 (range) + 8 (parent) + 4 (exchange)  = 112 + 6*D*S
-#   traverse read D*2*S (query slabs) + 4 (index)                                        = 4 + 2*D*S
+# Algorithmic DRAM bytes per element of each stage for triangles (V = 3) with D = K/2 slabs of S bytes and leaf
+# buckets of 8 elements:
+#   bounds   read 72 (vertices) + write 24 (centroid, SoA)                                      = 96
+#   keys     read 24 (centroid) + write 8 (key)                                                 = 32
+#   sort     per pass read 12 + write 12 (key + index)                                          = 24 per pass
+#   build    read 72 (vertices, gathered) + 4 (index) + 2 (boundary keys) + write 2 D S (element slabs in rank
+#            order) + 2 D S / 32 (query-group boxes) + (4 D S + 8 child + 8 range + 8 parent) / 8 (internal node
+#            per bucket)                                                                        = 78 + 2DS(1 + 1/32) + (4DS + 24)/8
+#   traverse read 2 D S / 32 (query-group box) per query; survivors read their slabs and the tree
+LEAF = 8
+
+
 def stage_bytes(D, S, passes):
-    return {"bounds": 96, "keys": 32, "sort": 24 * passes, "build": 112 + 6 * D * S, "traverse": 4 + 2 * D * S}
+    return {"bounds": 96, "keys": 32, "sort": 24 * passes,
+            "build": 78 + 2 * D * S * (1 + 1 / 32) + (4 * D * S + 24) / LEAF,
+            "traverse": 2 * D * S / 32}
 
 
 def run_gpu(args, world, rank, local):

@@ -364,7 +364,14 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
                                   o.elem_box.p, o.warp_box.p, o.node_box.p, o.child.as< int2 >(),
                                   o.range.as< int2 >(), o.parent.as< int >(), o.exch.as< int >(),
                                   o.queue.as< int4 >(), o.sc(), s ) );
-    st.launched( m > 1 ? 2 : 1 );
+    st.launched();
+  }
+  if ( m > 1 )
+  {
+    stage_scope st( ctx, BVHG_STAGE_CLIMB );
+    BVHG_CUDA( ctx, launch_climb( K, fp32, n, o.sorted_keys(), o.node_box.p, o.child.as< int2 >(), o.range.as< int2 >(),
+                                  o.parent.as< int >(), o.exch.as< int >(), o.queue.as< int4 >(), o.sc(), s ) );
+    st.launched();
   }
   o.built = true;
   o.topo = true;

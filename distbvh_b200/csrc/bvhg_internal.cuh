@@ -95,12 +95,16 @@ cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *v
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
                             obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s);
 
-// Element slabs + agglomerative LBVH build over leaf buckets with bottom-up refit (FP64 or FP32 slabs): two
-// launches, a block-local phase that queues unfinished subtrees and a global climb over the queue.
+// Element slabs + agglomerative LBVH build over leaf buckets with bottom-up refit (FP64 or FP32 slabs): the
+// block-local phase, which queues unfinished subtrees for launch_climb.
 cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
                          const uint64_t *keys, const uint32_t *vals, void *elem_box, void *warp_box, void *node_box,
                          int2 *child, int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc,
                          cudaStream_t s);
+
+// Global climb of the build (subtrees the block-local phase queued); after launch_build, only when m > 1.
+cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint64_t *keys, void *node_box, int2 *child, int2 *range,
+                         int *parent, int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s);
 
 // Refit with the topology of the last build: recompute element slabs, bucket boxes and every internal node.
 cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,

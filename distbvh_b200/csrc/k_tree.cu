@@ -687,15 +687,21 @@ cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double e
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
   const unsigned grid = static_cast< unsigned >( ( m + kBuildThreads - 1 ) / kBuildThreads );
   const size_t smem = static_cast< size_t >( 2 * kBuildThreads ) * ( 2 * ( K / 2 ) + 1 ) * sizeof( T );  // [W * 64][C + 1]
-  cudaError_t e = cudaFuncSetAttribute( k_build_leaf< K, T, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast< int >( smem ) );
+  const cudaError_t e = cudaFuncSetAttribute( k_build_leaf< K, T, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast< int >( smem ) );
   if ( e != cudaSuccess ) return e;
   k_build_leaf< K, T, VT ><<< grid, kBuildThreads, smem, s >>>(
     verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals, static_cast< T * >( elem_box ),
     static_cast< T * >( warp_box ), static_cast< T * >( node_box ), reinterpret_cast< int * >( child ), range, parent,
     queue, sc );
-  e = cudaGetLastError();
-  if ( e != cudaSuccess || m < 2 ) return e;
+  return cudaGetLastError();
+}
+
+template< int K, typename T >
+cudaError_t launch_climb_t(uint64_t n, const uint64_t *keys, void *node_box, int2 *child, int2 *range, int *parent,
+                           int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s)
+{
+  const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
   // The queue length is known only on the device: a grid-stride grid sized for the usual fraction.
   const uint64_t want = ( m / 8 + 127 ) / 128;
   const unsigned cgrid = static_cast< unsigned >( want < 148 * 16 ? ( want ? want : 1 ) : 148 * 16 );
@@ -795,6 +801,21 @@ cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint
     default: return cudaErrorInvalidValue;
   }
 #undef BVHG_BUILD_CASE
+}
+
+cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint64_t *keys, void *node_box, int2 *child, int2 *range,
+                         int *parent, int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s)
+{
+  switch ( K )
+  {
+    case 6: return fp32 ? launch_climb_t< 6, float >( n, keys, node_box, child, range, parent, exch, queue, sc, s )
+                        : launch_climb_t< 6, double >( n, keys, node_box, child, range, parent, exch, queue, sc, s );
+    case 18: return fp32 ? launch_climb_t< 18, float >( n, keys, node_box, child, range, parent, exch, queue, sc, s )
+                         : launch_climb_t< 18, double >( n, keys, node_box, child, range, parent, exch, queue, sc, s );
+    case 26: return fp32 ? launch_climb_t< 26, float >( n, keys, node_box, child, range, parent, exch, queue, sc, s )
+                         : launch_climb_t< 26, double >( n, keys, node_box, child, range, parent, exch, queue, sc, s );
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
