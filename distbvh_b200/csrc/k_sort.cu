@@ -13,6 +13,8 @@
 // goes on with a garbage offset (the host reports the error; no thread waits forever).
 #include "bvhg_internal.cuh"
 
+#include <atomic>
+
 namespace bvhg {
 namespace {
 
@@ -225,13 +227,18 @@ cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64
 {
   constexpr int RADIX = 1 << BITS;
   const size_t smem = static_cast< size_t >( kSortTile ) * ( sizeof( uint64_t ) + sizeof( uint32_t ) );
-  static bool configured = false;
-  if ( !configured )
+  // The attribute is per device: set it once for each device this process launches on.
+  static std::atomic< unsigned long long > configured{ 0 };
+  int dev = 0;
+  cudaError_t e = cudaGetDevice( &dev );
+  if ( e != cudaSuccess ) return e;
+  const unsigned long long bit = 1ull << ( dev & 63 );
+  if ( !( configured.load() & bit ) )
   {
-    cudaError_t e = cudaFuncSetAttribute( k_onesweep< BITS >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast< int >( smem ) );
+    e = cudaFuncSetAttribute( k_onesweep< BITS >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast< int >( smem ) );
     if ( e != cudaSuccess ) return e;
-    configured = true;
+    configured.fetch_or( bit );
   }
   const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
   k_onesweep< BITS ><<< static_cast< unsigned >( tiles ), kSortThreads, smem, s >>>(
