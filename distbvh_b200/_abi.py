@@ -24,8 +24,7 @@ EXPORTS = (
     "bvhg_set_elements", "bvhg_build", "bvhg_broadphase", "bvhg_self_collision", "bvhg_get_morton",
     "bvhg_get_kdops", "bvhg_get_kdops_f32", "bvhg_get_centroids", "bvhg_validate_tree", "bvhg_last_candidates",
     "bvhg_get_stage_times", "bvhg_launch_count", "bvhg_set_spin_limit", "bvhg_test_stall_sort", "bvhg_debug_normal",
-    "bvhg_synchronize",
-    "bvhg_last_error", "bvhg_status_string",
+    "bvhg_synchronize", "bvhg_last_error", "bvhg_status_string", "bvhg_radix_sort_noalloc",
 )
 
 
@@ -77,6 +76,7 @@ def _load():
         "bvhg_synchronize": (I32, [P]),
         "bvhg_last_error": (ctypes.c_char_p, [P]),
         "bvhg_status_string": (ctypes.c_char_p, [I32]),
+        "bvhg_radix_sort_noalloc": (I32, [P, P, P, U64, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
