@@ -49,28 +49,37 @@ template< int BITS >
 __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *__restrict__ keys_in,
                                                            const uint32_t *__restrict__ vals_in,
                                                            uint64_t *__restrict__ keys_out,
-                                                           uint32_t *__restrict__ vals_out, uint64_t n, int pass,
+                                                           uint32_t *__restrict__ vals_out, uint64_t n64, int pass,
                                                            const uint32_t *__restrict__ hist, uint32_t *status,
                                                            obj_scalars *sc, uint32_t spin_limit, int stall)
 {
   constexpr int RADIX = 1 << BITS;
   constexpr uint32_t MASK = RADIX - 1;
-  extern __shared__ uint64_t s_keys[];  // kSortTile keys, then kSortTile vals
+  extern __shared__ uint64_t s_keys[];  // kSortTile keys, then kSortTile vals, then kSortTile digits
   uint32_t *s_vals = reinterpret_cast< uint32_t * >( s_keys + kSortTile );
+  uint8_t *s_dig = reinterpret_cast< uint8_t * >( s_vals + kSortTile );
   __shared__ uint32_t s_whist[kWarps][RADIX];
   __shared__ uint32_t s_gbase[RADIX];
   __shared__ uint32_t s_lstart[RADIX];
   __shared__ uint32_t s_scan[kWarps];
   __shared__ int s_tile;
 
+  const uint32_t n = static_cast< uint32_t >( n64 );  // n < 2^30
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int shift = pass * BITS;
+  // digits never straddle the two 32-bit halves of a key (BITS divides 32)
+  const bool high = shift >= 32;
+  const int sh = shift & 31;
+  auto digit = [&](uint64_t key) -> uint32_t {
+    const uint32_t w = high ? static_cast< uint32_t >( key >> 32 ) : static_cast< uint32_t >( key );
+    return ( w >> sh ) & MASK;
+  };
   if ( tid == 0 ) s_tile = static_cast< int >( atomicAdd( &sc->sort_tile_counter[pass], 1u ) );
   for ( int k = tid; k < kWarps * RADIX; k += kSortThreads ) ( &s_whist[0][0] )[k] = 0;
   __syncthreads();
-  const uint64_t tile = static_cast< uint64_t >( s_tile );
-  const uint64_t tile_base = tile * kSortTile;
-  const uint64_t wbase = tile_base + static_cast< uint64_t >( warp ) * ( kSortItems * 32 );
+  const uint32_t tile = static_cast< uint32_t >( s_tile );
+  const uint32_t tile_base = tile * kSortTile;
+  const uint32_t wbase = tile_base + static_cast< uint32_t >( warp ) * ( kSortItems * 32 );
 
   // Keys stay in registers through ranking; values are only loaded at scatter time (fewer live registers,
   // three blocks per SM). Ranks within the warp are < 512 and kept two per register.
@@ -79,22 +88,24 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
 #pragma unroll
   for ( int j = 0; j < kSortItems; ++j )
   {
-    const uint64_t idx = wbase + j * 32 + lane;
+    const uint32_t idx = wbase + j * 32 + lane;
     k[j] = idx < n ? keys_in[idx] : 0ull;
   }
+  // Stable warp-level ranking: the lanes holding one digit meet by match; their leader takes the group's slots
+  // with one shared-memory atomic (a warp's atomics on one address retire in program order, so earlier items
+  // rank first) and hands the base back by shuffle.
   const unsigned lt_mask = ( 1u << lane ) - 1u;
 #pragma unroll
   for ( int j = 0; j < kSortItems; ++j )
   {
     const bool valid = ( wbase + j * 32 + lane ) < n;
-    const uint32_t d = valid ? static_cast< uint32_t >( ( k[j] >> shift ) & MASK ) : RADIX;
+    const uint32_t d = valid ? digit( k[j] ) : RADIX;
     const unsigned peers = __match_any_sync( 0xffffffffu, d );
-    const unsigned lower = peers & lt_mask;
-    const uint32_t base = valid ? s_whist[warp][d] : 0u;
-    __syncwarp();
-    if ( valid && lower == 0 ) s_whist[warp][d] = base + static_cast< uint32_t >( __popc( peers ) );
-    __syncwarp();
-    const uint32_t rank = base + static_cast< uint32_t >( __popc( lower ) );
+    const int leader = __ffs( peers ) - 1;
+    uint32_t base = 0;
+    if ( valid && lane == leader ) base = atomicAdd( &s_whist[warp][d], static_cast< uint32_t >( __popc( peers ) ) );
+    base = __shfl_sync( 0xffffffffu, base, leader );
+    const uint32_t rank = base + static_cast< uint32_t >( __popc( peers & lt_mask ) );
     if ( j & 1 ) rk[j >> 1] |= rank << 16;
     else rk[j >> 1] = rank;
   }
@@ -111,7 +122,7 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
       s_whist[w][tid] = total;
       total += c;
     }
-    volatile uint32_t *st = status + tile * RADIX;
+    volatile uint32_t *st = status + static_cast< size_t >( tile ) * RADIX;
     st[tid] = ( tile == 0 ? kFlagPrefix : kFlagAggregate ) | total;
   }
   const uint32_t g = ( tid < RADIX ) ? hist[tid] : 0u;
@@ -141,13 +152,13 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
       } else {
         // Look back over a window of kLookback predecessors per step: their status words are fetched together
         // (independent loads in flight) and consumed nearest first until an inclusive prefix is found.
-        int64_t p = static_cast< int64_t >( tile ) - 1;
+        int p = static_cast< int >( tile ) - 1;
         bool done = false;
         while ( !done )
         {
           uint32_t w[kLookback];
 #pragma unroll
-          for ( int q = 0; q < kLookback; ++q ) w[q] = ( p - q >= 0 ) ? vs[( p - q ) * RADIX + tid] : kFlagPrefix;
+          for ( int q = 0; q < kLookback; ++q ) w[q] = ( p - q >= 0 ) ? vs[static_cast< size_t >( p - q ) * RADIX + tid] : kFlagPrefix;
           int consumed = 0;
 #pragma unroll
           for ( int q = 0; q < kLookback; ++q )
@@ -173,7 +184,8 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
           }
         }
       }
-      reinterpret_cast< volatile uint32_t * >( status )[tile * RADIX + tid] = kFlagPrefix | ( ( excl + total ) & kValueMask );
+      reinterpret_cast< volatile uint32_t * >( status )[static_cast< size_t >( tile ) * RADIX + tid] =
+        kFlagPrefix | ( ( excl + total ) & kValueMask );
     }
     s_gbase[tid] = gexcl + excl - lexcl;
     s_lstart[tid] = lexcl;
@@ -194,27 +206,26 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
 #pragma unroll
   for ( int j = 0; j < kSortItems; ++j )
   {
-    const uint64_t idx = wbase + j * 32 + lane;
+    const uint32_t idx = wbase + j * 32 + lane;
     if ( idx < n )
     {
-      const uint32_t d = static_cast< uint32_t >( ( k[j] >> shift ) & MASK );
+      const uint32_t d = digit( k[j] );
       const uint32_t rank = ( rk[j >> 1] >> ( ( j & 1 ) * 16 ) ) & 0xffffu;
       const uint32_t pos = s_lstart[d] + s_whist[warp][d] + rank;
       s_keys[pos] = k[j];
-      s_vals[pos] = vals_in ? vals_in[idx] : static_cast< uint32_t >( idx );
+      s_dig[pos] = static_cast< uint8_t >( d );
+      s_vals[pos] = vals_in ? vals_in[idx] : idx;
     }
   }
   __syncthreads();
 
-  const uint32_t cnt = static_cast< uint32_t >( min( static_cast< uint64_t >( kSortTile ), n - tile_base ) );
+  const uint32_t cnt = min( static_cast< uint32_t >( kSortTile ), n - tile_base );
   for ( uint32_t i = tid; i < cnt; i += kSortThreads )
   {
-    const uint64_t key = s_keys[i];
-    const uint32_t d = static_cast< uint32_t >( ( key >> shift ) & MASK );
-    const uint32_t gp = s_gbase[d] + i;
+    const uint32_t gp = s_gbase[s_dig[i]] + i;
     if ( gp < n )
     {
-      keys_out[gp] = key;
+      keys_out[gp] = s_keys[i];
       vals_out[gp] = s_vals[i];
     }
   }
@@ -226,7 +237,7 @@ cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64
                         uint32_t spin_limit, int stall, cudaStream_t s)
 {
   constexpr int RADIX = 1 << BITS;
-  const size_t smem = static_cast< size_t >( kSortTile ) * ( sizeof( uint64_t ) + sizeof( uint32_t ) );
+  const size_t smem = static_cast< size_t >( kSortTile ) * ( sizeof( uint64_t ) + sizeof( uint32_t ) + 1 );
   // The attribute is per device: set it once for each device this process launches on.
   static std::atomic< unsigned long long > configured{ 0 };
   int dev = 0;
