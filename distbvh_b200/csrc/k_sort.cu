@@ -16,6 +16,7 @@
 #include <atomic>
 
 namespace bvhg {
+int device_sm_count();
 namespace {
 
 constexpr uint32_t kFlagAggregate = 1u << 30;
@@ -45,26 +46,71 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s
   return wpre + inc - x;
 }
 
+// Shared-memory address of a pointer into shared memory (PTX operand form).
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+  return static_cast< uint32_t >( __cvta_generic_to_shared( p ) );
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+  asm volatile( "mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"( smem_addr( bar ) ), "r"( count ) : "memory" );
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+  asm volatile( "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"( smem_addr( bar ) ), "r"( bytes )
+                : "memory" );
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase)
+{
+  uint32_t ok;
+  asm volatile( "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                : "=r"( ok )
+                : "r"( smem_addr( bar ) ), "r"( phase )
+                : "memory" );
+  return ok != 0;
+}
+
+// One-dimensional bulk copy global -> shared (TMA), completing on an mbarrier. Both addresses 16-byte aligned,
+// size a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile( "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                  smem_addr( dst ) ),
+                "l"( src ), "r"( bytes ), "r"( smem_addr( bar ) )
+                : "memory" );
+}
+
+// Persistent radix pass. A block keeps taking tiles from the pass's tile counter; while it ranks, resolves and
+// writes one tile, the next one is already streaming into the other half of its double-buffered shared memory
+// (TMA bulk copies on an mbarrier). Per tile: keys and indices to registers, stable warp-level ranking (the lanes
+// holding one digit meet by match; their leader takes the group's slots with one shared-memory atomic, which
+// retire in program order within the warp, and hands the base back by shuffle), per-digit tile counts published
+// for the decoupled look-back, the tile reordered in the shared buffer it came from, contiguous digit runs
+// written out. Every wait is bounded (look-back polls and mbarrier waits); on a timeout the block raises the
+// object's error word and stops, and blocks that may have read a garbage prefix write nothing.
 template< int BITS >
-__global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *__restrict__ keys_in,
+__global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *__restrict__ keys_in,
                                                            const uint32_t *__restrict__ vals_in,
                                                            uint64_t *__restrict__ keys_out,
                                                            uint32_t *__restrict__ vals_out, uint64_t n64, int pass,
                                                            const uint32_t *__restrict__ hist, uint32_t *status,
-                                                           obj_scalars *sc, uint32_t spin_limit, int stall)
+                                                           obj_scalars *sc, uint32_t spin_limit, int stall, int use_tma)
 {
   constexpr int RADIX = 1 << BITS;
   constexpr uint32_t MASK = RADIX - 1;
-  extern __shared__ uint64_t s_keys[];  // kSortTile keys, then kSortTile vals, then kSortTile digits
-  uint32_t *s_vals = reinterpret_cast< uint32_t * >( s_keys + kSortTile );
-  uint8_t *s_dig = reinterpret_cast< uint8_t * >( s_vals + kSortTile );
+  extern __shared__ __align__( 128 ) unsigned char s_raw[];  // 2 stages of [kSortTile keys][kSortTile indices]
+  __shared__ __align__( 8 ) uint64_t s_mbar[2];
   __shared__ uint32_t s_whist[kWarps][RADIX];
   __shared__ uint32_t s_gbase[RADIX];
   __shared__ uint32_t s_lstart[RADIX];
   __shared__ uint32_t s_scan[kWarps];
-  __shared__ int s_tile;
+  __shared__ int s_next, s_err;
 
   const uint32_t n = static_cast< uint32_t >( n64 );  // n < 2^30
+  const uint32_t tiles = ( n + kSortTile - 1 ) / kSortTile;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int shift = pass * BITS;
   // digits never straddle the two 32-bit halves of a key (BITS divides 32)
@@ -74,105 +120,128 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
     const uint32_t w = high ? static_cast< uint32_t >( key >> 32 ) : static_cast< uint32_t >( key );
     return ( w >> sh ) & MASK;
   };
-  if ( tid == 0 ) s_tile = static_cast< int >( atomicAdd( &sc->sort_tile_counter[pass], 1u ) );
-  for ( int k = tid; k < kWarps * RADIX; k += kSortThreads ) ( &s_whist[0][0] )[k] = 0;
-  __syncthreads();
-  const uint32_t tile = static_cast< uint32_t >( s_tile );
-  const uint32_t tile_base = tile * kSortTile;
-  const uint32_t wbase = tile_base + static_cast< uint32_t >( warp ) * ( kSortItems * 32 );
+  auto stage_keys = [&](int st) { return reinterpret_cast< uint64_t * >( s_raw + st * kSortTile * 12 ); };
+  auto stage_vals = [&](int st) { return reinterpret_cast< uint32_t * >( s_raw + st * kSortTile * 12 + kSortTile * 8 ); };
 
-  // Keys stay in registers through ranking; values are only loaded at scatter time (fewer live registers,
-  // three blocks per SM). Ranks within the warp are < 512 and kept two per register.
-  uint64_t k[kSortItems];
-  uint32_t rk[kSortItems / 2];
-#pragma unroll
-  for ( int j = 0; j < kSortItems; ++j )
+  // global exclusive offsets of the digits (the same for every tile of the pass)
+  const uint32_t gexcl = block_exclusive_scan( ( tid < RADIX ) ? hist[tid] : 0u, s_scan );
+  if ( tid == 0 )
   {
-    const uint32_t idx = wbase + j * 32 + lane;
-    k[j] = idx < n ? keys_in[idx] : 0ull;
+    mbar_init( &s_mbar[0], 1 );
+    mbar_init( &s_mbar[1], 1 );
+    asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+    s_next = static_cast< int >( atomicAdd( &sc->sort_tile_counter[pass], 1u ) );
+    s_err = 0;
   }
-  // Stable warp-level ranking: the lanes holding one digit meet by match; their leader takes the group's slots
-  // with one shared-memory atomic (a warp's atomics on one address retire in program order, so earlier items
-  // rank first) and hands the base back by shuffle.
+  __syncthreads();
+  uint32_t tile = static_cast< uint32_t >( s_next );
+  // a tile goes through the bulk copy when it is full and the arrays are 16-byte aligned
+  auto tma_tile = [&](uint32_t t) { return use_tma && ( t + 1 ) * kSortTile <= n; };
+  auto issue = [&](uint32_t t, int st) {
+    const uint32_t bytes = kSortTile * 8 + ( vals_in ? kSortTile * 4 : 0 );
+    mbar_expect_tx( &s_mbar[st], bytes );
+    bulk_load( stage_keys( st ), keys_in + static_cast< size_t >( t ) * kSortTile, kSortTile * 8, &s_mbar[st] );
+    if ( vals_in )
+      bulk_load( stage_vals( st ), vals_in + static_cast< size_t >( t ) * kSortTile, kSortTile * 4, &s_mbar[st] );
+  };
+  if ( tid == 0 && tile < tiles && tma_tile( tile ) ) issue( tile, 0 );
+  uint32_t phases = 0u;  // bit s: parity of stage s's mbarrier phase to wait for
+  int st = 0;
   const unsigned lt_mask = ( 1u << lane ) - 1u;
-#pragma unroll
-  for ( int j = 0; j < kSortItems; ++j )
-  {
-    const bool valid = ( wbase + j * 32 + lane ) < n;
-    const uint32_t d = valid ? digit( k[j] ) : RADIX;
-    const unsigned peers = __match_any_sync( 0xffffffffu, d );
-    const int leader = __ffs( peers ) - 1;
-    uint32_t base = 0;
-    if ( valid && lane == leader ) base = atomicAdd( &s_whist[warp][d], static_cast< uint32_t >( __popc( peers ) ) );
-    base = __shfl_sync( 0xffffffffu, base, leader );
-    const uint32_t rank = base + static_cast< uint32_t >( __popc( peers & lt_mask ) );
-    if ( j & 1 ) rk[j >> 1] |= rank << 16;
-    else rk[j >> 1] = rank;
-  }
-  __syncthreads();
 
-  // Per digit: exclusive prefix over warps (in place) and the tile total.
-  uint32_t total = 0;
-  if ( tid < RADIX )
+  while ( tile < tiles )
   {
-#pragma unroll
-    for ( int w = 0; w < kWarps; ++w )
+    const uint32_t tile_base = tile * kSortTile;
+    const uint32_t cnt = min( static_cast< uint32_t >( kSortTile ), n - tile_base );
+    const bool bulk = tma_tile( tile );
+    uint64_t *sk = stage_keys( st );
+    uint32_t *sv = stage_vals( st );
+    if ( bulk )
     {
-      const uint32_t c = s_whist[w][tid];
-      s_whist[w][tid] = total;
-      total += c;
-    }
-    volatile uint32_t *st = status + static_cast< size_t >( tile ) * RADIX;
-    st[tid] = ( tile == 0 ? kFlagPrefix : kFlagAggregate ) | total;
-  }
-  const uint32_t g = ( tid < RADIX ) ? hist[tid] : 0u;
-  const uint32_t gexcl = block_exclusive_scan( g, s_scan );
-  const uint32_t lexcl = block_exclusive_scan( tid < RADIX ? total : 0u, s_scan );
-
-  if ( tid < RADIX )
-  {
-    uint32_t excl = 0;
-    if ( tile > 0 )
-    {
-      const volatile uint32_t *vs = reinterpret_cast< const volatile uint32_t * >( status );
       uint32_t spins = 0;
-      if ( stall )
-      {
-        // Test hook: poll the spare status row after the last tile, which no block ever publishes.
-        while ( ( vs[static_cast< uint64_t >( gridDim.x ) * RADIX + tid] & ~kValueMask ) == 0 )
+      bool ok = true;
+      const uint32_t ph = ( phases >> st ) & 1u;
+      while ( !mbar_try_wait( &s_mbar[st], ph ) )
+        if ( ++spins > spin_limit )
         {
-          if ( ++spins > spin_limit )
-          {
-            atomicCAS( &sc->error, 0, kErrTimeout );
-            __threadfence();
-            break;
-          }
-          __nanosleep( 32 );
+          ok = false;
+          break;
         }
-      } else {
-        // Look back over a window of kLookback predecessors per step: their status words are fetched together
-        // (independent loads in flight) and consumed nearest first until an inclusive prefix is found.
-        int p = static_cast< int >( tile ) - 1;
-        bool done = false;
-        while ( !done )
+      phases ^= 1u << st;
+      if ( __syncthreads_or( !ok ) )
+      {
+        // the copy did not complete in time: give it one more bounded wait, raise the error and stop
+        if ( tid == 0 )
         {
-          uint32_t w[kLookback];
+          for ( uint32_t k = 0; k < spin_limit && !mbar_try_wait( &s_mbar[st], ph ); ++k ) {}
+          atomicCAS( &sc->error, 0, kErrTimeout );
+        }
+        return;
+      }
+    }
+    // keys and indices of the tile to registers, warp-striped (item j of lane l: local 512 w + 32 j + l)
+    uint64_t k[kSortItems];
+    uint32_t v[kSortItems];
+    uint32_t rk[kSortItems / 2];
+    const uint32_t wl = static_cast< uint32_t >( warp ) * ( kSortItems * 32 );
 #pragma unroll
-          for ( int q = 0; q < kLookback; ++q ) w[q] = ( p - q >= 0 ) ? vs[static_cast< size_t >( p - q ) * RADIX + tid] : kFlagPrefix;
-          int consumed = 0;
+    for ( int j = 0; j < kSortItems; ++j )
+    {
+      const uint32_t li = wl + j * 32 + lane;
+      const bool valid = li < cnt;
+      if ( bulk )
+      {
+        k[j] = sk[li];
+        v[j] = vals_in ? sv[li] : tile_base + li;
+      } else {
+        k[j] = valid ? keys_in[tile_base + li] : 0ull;
+        v[j] = valid ? ( vals_in ? vals_in[tile_base + li] : tile_base + li ) : 0u;
+      }
+    }
+    for ( int q = lane; q < RADIX; q += 32 ) s_whist[warp][q] = 0;
+    __syncwarp();
 #pragma unroll
-          for ( int q = 0; q < kLookback; ++q )
-          {
-            if ( done || consumed < q ) break;  // stop at the first word that was not ready
-            const uint32_t flag = w[q] & ~kValueMask;
-            if ( flag == 0 ) break;
-            excl += w[q] & kValueMask;
-            consumed = q + 1;
-            if ( flag == kFlagPrefix ) done = true;
-          }
-          if ( done ) break;
-          p -= consumed;
-          if ( consumed == 0 )
+    for ( int j = 0; j < kSortItems; ++j )
+    {
+      const bool valid = ( wl + j * 32 + lane ) < cnt;
+      const uint32_t d = valid ? digit( k[j] ) : RADIX;
+      const unsigned peers = __match_any_sync( 0xffffffffu, d );
+      const int leader = __ffs( peers ) - 1;
+      uint32_t base = 0;
+      if ( valid && lane == leader ) base = atomicAdd( &s_whist[warp][d], static_cast< uint32_t >( __popc( peers ) ) );
+      base = __shfl_sync( 0xffffffffu, base, leader );
+      const uint32_t rank = base + static_cast< uint32_t >( __popc( peers & lt_mask ) );
+      if ( j & 1 ) rk[j >> 1] |= rank << 16;
+      else rk[j >> 1] = rank;
+    }
+    __syncthreads();
+
+    // per digit: exclusive prefix over warps (in place) and the tile total, published for the look-back
+    uint32_t total = 0;
+    if ( tid < RADIX )
+    {
+#pragma unroll
+      for ( int w = 0; w < kWarps; ++w )
+      {
+        const uint32_t c = s_whist[w][tid];
+        s_whist[w][tid] = total;
+        total += c;
+      }
+      reinterpret_cast< volatile uint32_t * >( status )[static_cast< size_t >( tile ) * RADIX + tid] =
+        ( tile == 0 ? kFlagPrefix : kFlagAggregate ) | total;
+    }
+    const uint32_t lexcl = block_exclusive_scan( tid < RADIX ? total : 0u, s_scan );
+    if ( tid < RADIX )
+    {
+      uint32_t excl = 0;
+      if ( tile > 0 )
+      {
+        const volatile uint32_t *vs = reinterpret_cast< const volatile uint32_t * >( status );
+        uint32_t spins = 0;
+        if ( stall )
+        {
+          // Test hook: poll the spare status row after the last tile, which no block ever publishes.
+          while ( ( vs[static_cast< size_t >( tiles ) * RADIX + tid] & ~kValueMask ) == 0 )
           {
             if ( ++spins > spin_limit )
             {
@@ -182,52 +251,93 @@ __global__ void __launch_bounds__( kSortThreads, 3 ) k_onesweep(const uint64_t *
             }
             __nanosleep( 32 );
           }
-        }
-      }
-      reinterpret_cast< volatile uint32_t * >( status )[static_cast< size_t >( tile ) * RADIX + tid] =
-        kFlagPrefix | ( ( excl + total ) & kValueMask );
-    }
-    s_gbase[tid] = gexcl + excl - lexcl;
-    s_lstart[tid] = lexcl;
-  }
-  // A block that timed out published a garbage prefix (so that no successor waits forever) and raised the
-  // object's error word before doing so; every block that could have read such a prefix sees the word here and
-  // writes nothing.
-  __shared__ int s_err;
-  __syncthreads();
-  if ( tid == 0 )
-  {
-    __threadfence();
-    s_err = *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout;
-  }
-  __syncthreads();
-  if ( s_err ) return;
-
+        } else {
+          // a window of kLookback predecessors per step, fetched together and consumed nearest first
+          int p = static_cast< int >( tile ) - 1;
+          bool done = false;
+          while ( !done )
+          {
+            uint32_t w[kLookback];
 #pragma unroll
-  for ( int j = 0; j < kSortItems; ++j )
-  {
-    const uint32_t idx = wbase + j * 32 + lane;
-    if ( idx < n )
-    {
-      const uint32_t d = digit( k[j] );
-      const uint32_t rank = ( rk[j >> 1] >> ( ( j & 1 ) * 16 ) ) & 0xffffu;
-      const uint32_t pos = s_lstart[d] + s_whist[warp][d] + rank;
-      s_keys[pos] = k[j];
-      s_dig[pos] = static_cast< uint8_t >( d );
-      s_vals[pos] = vals_in ? vals_in[idx] : idx;
+            for ( int q = 0; q < kLookback; ++q )
+              w[q] = ( p - q >= 0 ) ? vs[static_cast< size_t >( p - q ) * RADIX + tid] : kFlagPrefix;
+            int consumed = 0;
+#pragma unroll
+            for ( int q = 0; q < kLookback; ++q )
+            {
+              if ( done || consumed < q ) break;  // stop at the first word that was not ready
+              const uint32_t flag = w[q] & ~kValueMask;
+              if ( flag == 0 ) break;
+              excl += w[q] & kValueMask;
+              consumed = q + 1;
+              if ( flag == kFlagPrefix ) done = true;
+            }
+            if ( done ) break;
+            p -= consumed;
+            if ( consumed == 0 )
+            {
+              if ( ++spins > spin_limit )
+              {
+                atomicCAS( &sc->error, 0, kErrTimeout );
+                __threadfence();
+                break;
+              }
+              __nanosleep( 32 );
+            }
+          }
+        }
+        reinterpret_cast< volatile uint32_t * >( status )[static_cast< size_t >( tile ) * RADIX + tid] =
+          kFlagPrefix | ( ( excl + total ) & kValueMask );
+      }
+      s_gbase[tid] = gexcl + excl - lexcl;
+      s_lstart[tid] = lexcl;
     }
-  }
-  __syncthreads();
-
-  const uint32_t cnt = min( static_cast< uint32_t >( kSortTile ), n - tile_base );
-  for ( uint32_t i = tid; i < cnt; i += kSortThreads )
-  {
-    const uint32_t gp = s_gbase[s_dig[i]] + i;
-    if ( gp < n )
+    __syncthreads();
+    // A block that timed out published a garbage prefix (so that no successor waits forever) and raised the
+    // object's error word before doing so; every block that could have read such a prefix sees it here, writes
+    // nothing and stops (no bulk copy is in flight at this point).
+    if ( tid == 0 )
     {
-      keys_out[gp] = s_keys[i];
-      vals_out[gp] = s_vals[i];
+      __threadfence();
+      s_err = *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout;
+      s_next = static_cast< int >( atomicAdd( &sc->sort_tile_counter[pass], 1u ) );
     }
+    __syncthreads();
+    if ( s_err ) return;
+    const uint32_t next = static_cast< uint32_t >( s_next );
+    // the other stage was drained by the previous iteration's write-out (barrier below): refill it
+    if ( tid == 0 && next < tiles && tma_tile( next ) )
+    {
+      asm volatile( "fence.proxy.async.shared::cta;" ::: "memory" );
+      issue( next, st ^ 1 );
+    }
+    // reorder the tile into its own stage buffer (its data now lives in registers)
+#pragma unroll
+    for ( int j = 0; j < kSortItems; ++j )
+    {
+      if ( ( wl + j * 32 + lane ) < cnt )
+      {
+        const uint32_t d = digit( k[j] );
+        const uint32_t rank = ( rk[j >> 1] >> ( ( j & 1 ) * 16 ) ) & 0xffffu;
+        const uint32_t pos = s_lstart[d] + s_whist[warp][d] + rank;
+        sk[pos] = k[j];
+        sv[pos] = v[j];
+      }
+    }
+    __syncthreads();
+    for ( uint32_t i = tid; i < cnt; i += kSortThreads )
+    {
+      const uint64_t key = sk[i];
+      const uint32_t gp = s_gbase[digit( key )] + i;
+      if ( gp < n )
+      {
+        keys_out[gp] = key;
+        vals_out[gp] = sv[i];
+      }
+    }
+    __syncthreads();  // the stage is drained: the next iteration may refill it
+    st ^= 1;
+    tile = next;
   }
 }
 
@@ -237,7 +347,7 @@ cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64
                         uint32_t spin_limit, int stall, cudaStream_t s)
 {
   constexpr int RADIX = 1 << BITS;
-  const size_t smem = static_cast< size_t >( kSortTile ) * ( sizeof( uint64_t ) + sizeof( uint32_t ) + 1 );
+  const size_t smem = static_cast< size_t >( 2 ) * kSortTile * ( sizeof( uint64_t ) + sizeof( uint32_t ) );
   // The attribute is per device: set it once for each device this process launches on.
   static std::atomic< unsigned long long > configured{ 0 };
   int dev = 0;
@@ -252,9 +362,14 @@ cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64
     configured.fetch_or( bit );
   }
   const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
-  k_onesweep< BITS ><<< static_cast< unsigned >( tiles ), kSortThreads, smem, s >>>(
-    keys_in, vals_in, keys_out, vals_out, n, pass, hist + static_cast< size_t >( pass ) * RADIX,
-    status + static_cast< size_t >( pass ) * ( tiles + 1 ) * RADIX, sc, spin_limit, stall );
+  // persistent: two blocks per SM (shared memory for two 48 KB stages each), never more blocks than tiles
+  const uint64_t cap = static_cast< uint64_t >( device_sm_count() ) * 2;
+  const unsigned grid = static_cast< unsigned >( tiles < cap ? tiles : cap );
+  const int use_tma = ( ( reinterpret_cast< uintptr_t >( keys_in ) | reinterpret_cast< uintptr_t >( vals_in ) ) & 15 ) == 0;
+  k_onesweep< BITS ><<< grid, kSortThreads, smem, s >>>( keys_in, vals_in, keys_out, vals_out, n, pass,
+                                                        hist + static_cast< size_t >( pass ) * RADIX,
+                                                        status + static_cast< size_t >( pass ) * ( tiles + 1 ) * RADIX,
+                                                        sc, spin_limit, stall, use_tma );
   return cudaGetLastError();
 }
 
