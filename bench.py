@@ -144,16 +144,18 @@ def peaks():
 #   bounds   read 72 (vertices) + write 24 (centroid, SoA)                                      = 96
 #   keys     read 24 (centroid) + write 8 (key)                                                 = 32
 #   sort     per pass read 12 + write 12 (key + index)                                          = 24 per pass
-#   build    read 72 (vertices, gathered) + 4 (index) + 2 (boundary keys) + write 2 D S (element slabs in rank
-#            order) + 2 D S / 32 (query-group boxes) + (4 D S + 8 child + 8 range + 8 parent) / 8 (internal node
-#            per bucket)                                                                        = 78 + 2DS(1 + 1/32) + (4DS + 24)/8
+#   slabs    read 4 (index) + 72 (vertices, gathered) + write 2 D S (element slabs in rank order) + 2 D S / 8
+#            (leaf-bucket boxes) + 2 D S / 32 (query-group boxes)                               = 76 + 2DS(1 + 1/8 + 1/32)
+#   build    read 2 D S / 8 (bucket boxes) + 2 (boundary keys) + write (4 D S + 8 child + 8 range + 8 parent) / 8
+#            (one internal node per bucket)                                                     = 2 + 2DS/8 + (4DS + 24)/8
 #   traverse read 2 D S / 32 (query-group box) per query; survivors read their slabs and the tree
 LEAF = 8
 
 
 def stage_bytes(D, S, passes):
     return {"bounds": 96, "keys": 32, "sort": 24 * passes,
-            "build": 78 + 2 * D * S * (1 + 1 / 32) + (4 * D * S + 24) / LEAF,
+            "slabs": 76 + 2 * D * S * (1 + 1 / LEAF + 1 / 32),
+            "build": 2 + 2 * D * S / LEAF + (4 * D * S + 24) / LEAF,
             "traverse": 2 * D * S / 32}
 
 
@@ -270,7 +272,7 @@ def run_gpu(args, world, rank, local):
         if st_ms.get(s, 0) > 0:
             elems = prims if s != "traverse" else na
             stage_bw[s] = elems * b / (st_ms[s] * 1e-3) / 1e9
-    dom = max(("bounds", "keys", "sort", "build"), key=lambda s: st_ms[s])
+    dom = max(("bounds", "keys", "sort", "slabs", "build"), key=lambda s: st_ms[s])
     peak, peak_kind = peaks()
     n_launch = max(1, st_launch[dom])
     per_launch_ms = st_ms[dom] / n_launch

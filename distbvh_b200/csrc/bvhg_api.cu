@@ -70,7 +70,7 @@ struct object
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
   dev_buf hist, status;
-  dev_buf elem_box, warp_box, node_box, child, range, parent, exch, queue;
+  dev_buf elem_box, warp_box, bucket_box, node_box, child, range, parent, exch, queue;
   dev_buf scal;  // obj_scalars
   // Each object's build runs on its own stream, forked from and joined back into the context stream with
   // events, so two objects' builds overlap (one's latency-bound tree climb beside the other's streaming kernels).
@@ -292,12 +292,21 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   if ( mode == BVHG_REFIT )
   {
     if ( !o.topo ) return fail( ctx, BVHG_ERR_STATE, "refit without a rebuild of this element count" );
-    stage_scope st( ctx, BVHG_STAGE_BUILD );
     const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
-    if ( m > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( m - 1 ) * sizeof( int ), s ) );
-    BVHG_CUDA( ctx, launch_refit( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.elem_box.p,
-                                  o.warp_box.p, o.node_box.p, o.parent.as< int >(), o.exch.as< int >(), o.sc(), s ) );
-    st.launched();
+    {
+      stage_scope st( ctx, BVHG_STAGE_SLABS );
+      BVHG_CUDA( ctx, launch_slabs( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.elem_box.p,
+                                    o.bucket_box.p, o.warp_box.p, o.sc(), s ) );
+      st.launched();
+    }
+    if ( m > 1 )
+    {
+      stage_scope st( ctx, BVHG_STAGE_BUILD );
+      BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( m - 1 ) * sizeof( int ), s ) );
+      BVHG_CUDA( ctx, launch_refit( K, fp32, n, o.bucket_box.p, o.node_box.p, o.parent.as< int >(),
+                                    o.exch.as< int >(), o.sc(), s ) );
+      st.launched();
+    }
     o.built = true;
     return BVHG_OK;
   }
@@ -319,6 +328,7 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;  // leaf buckets
   BVHG_CUDA( ctx, o.elem_box.reserve( n * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.bucket_box.reserve( m * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.node_box.reserve( ( m - 1 ) * D * 4 * sb + 16 ) );
   BVHG_CUDA( ctx, o.child.reserve( ( m - 1 ) * 8 + 8 ) );
   BVHG_CUDA( ctx, o.range.reserve( ( m - 1 ) * 8 + 8 ) );
@@ -359,11 +369,16 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
     o.sort_result_alt = ( passes & 1 ) ? 1 : 0;
   }
   {
+    stage_scope st( ctx, BVHG_STAGE_SLABS );
+    BVHG_CUDA( ctx, launch_slabs( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.elem_box.p,
+                                  o.bucket_box.p, o.warp_box.p, o.sc(), s ) );
+    st.launched();
+  }
+  if ( m > 1 )
+  {
     stage_scope st( ctx, BVHG_STAGE_BUILD );
-    BVHG_CUDA( ctx, launch_build( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_keys(), o.sorted_vals(),
-                                  o.elem_box.p, o.warp_box.p, o.node_box.p, o.child.as< int2 >(),
-                                  o.range.as< int2 >(), o.parent.as< int >(), o.exch.as< int >(),
-                                  o.queue.as< int4 >(), o.sc(), s ) );
+    BVHG_CUDA( ctx, launch_build( K, fp32, n, o.sorted_keys(), o.bucket_box.p, o.node_box.p, o.child.as< int2 >(),
+                                  o.range.as< int2 >(), o.parent.as< int >(), o.queue.as< int4 >(), o.sc(), s ) );
     st.launched();
   }
   if ( m > 1 )

@@ -9,6 +9,7 @@
 //              keys[r], vals[r] hold the key and original index of rank r (vals = the permutation)
 //   elem_box   n * D * 2 T: slabs of the element of rank r, [r][a][min,max] (leaf tests and queries)
 //   warp_box   ceil(n / 32) * D * 2 T: union of the slabs of ranks [32 w, 32 w + 31] (the query side's cull)
+//   bucket_box m * D * 2 T: union of the slabs of leaf bucket b (ranks [8 b, 8 b + 7]), input of the tree build
 //   node_box   (m - 1) * D * 2 * 2 T: both children's slabs of internal node k, [k][a][child][min,max], so one
 //              32-byte (FP64) or 16-byte (FP32) sector per axis tests both children
 //   child      (m - 1) int2: child index, >= 0 internal node, < 0 bucket with ~child = bucket index
@@ -97,18 +98,23 @@ cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *v
 
 // Element slabs + agglomerative LBVH build over leaf buckets with bottom-up refit (FP64 or FP32 slabs): the
 // block-local phase, which queues unfinished subtrees for launch_climb.
-cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint64_t *keys, const uint32_t *vals, void *elem_box, void *warp_box, void *node_box,
-                         int2 *child, int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc,
+// Element slabs in rank order (elem_box), the union of each leaf bucket (bucket_box, m rows) and of each group of
+// 32 ranks (warp_box); a one-bucket object's root. Marks a failed sort when perm is not a permutation.
+cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
+                         const uint32_t *vals, void *elem_box, void *bucket_box, void *warp_box, obj_scalars *sc,
                          cudaStream_t s);
+
+// Block-local LBVH build over the bucket boxes (nodes closed inside a block of 256 buckets; the rest queued for
+// launch_climb). Nothing to do for one bucket.
+cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, const void *bucket_box, void *node_box,
+                         int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s);
 
 // Global climb of the build (subtrees the block-local phase queued); after launch_build, only when m > 1.
 cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint64_t *keys, void *node_box, int2 *child, int2 *range,
                          int *parent, int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s);
 
-// Refit with the topology of the last build: recompute element slabs, bucket boxes and every internal node.
-cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *elem_box, void *warp_box, void *node_box, const int *parent,
+// Refit with the topology of the last build, after launch_slabs recomputed the bucket boxes: every internal node.
+cudaError_t launch_refit(int K, bool fp32, uint64_t n, const void *bucket_box, void *node_box, const int *parent,
                          int *exch, obj_scalars *sc, cudaStream_t s);
 
 struct tree_view

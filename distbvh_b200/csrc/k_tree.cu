@@ -187,68 +187,100 @@ __device__ __forceinline__ long long bdelta(const uint64_t *__restrict__ keys, i
   return ( static_cast< long long >( delta( keys, kLeafSize * b + kLeafSize - 1 ) ) << 32 ) | static_cast< unsigned >( b );
 }
 
-// Slabs of the elements of leaf bucket b (ranks kLeafSize * b .. + kLeafSize - 1, < n): each element's slabs go to
-// elem_box in rank order, their union to lo/hi. Returns false when the permutation is not one.
+constexpr int kSlabThreads = 128;  // ranks per block of the element slab kernel
+
+// Element slabs in rank order, one thread per rank (the element perm[r] of rank r); then, per block of 128 ranks,
+// the unions of its 16 leaf buckets and its 4 query groups of 32 ranks. The rows are staged in shared memory
+// (padded to C + 1 components against bank conflicts) and written out coalesced: elem_box row r, bucket_box row
+// b and warp_box row g each hold the C = 2 D values (min, max) per slab. A one-bucket object also gets its root
+// box here. A rank whose index is not an element index marks a failed sort.
 template< int K, typename T, int VT >
-__device__ __forceinline__ bool bucket_slabs(const double *__restrict__ verts, uint32_t Vrt, int n, int b, double eps,
-                                             float eps_hi, const uint32_t *__restrict__ vals, T *__restrict__ elem_box,
-                                             T *lo, T *hi)
+__global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( VT == 8 ? 3 : 4 ) ) k_elem_slabs(const double *__restrict__ verts, uint32_t Vrt,
+                                                                  int n, double eps, float eps_hi,
+                                                                  const uint32_t *__restrict__ vals,
+                                                                  T *__restrict__ elem_box, T *__restrict__ bucket_box,
+                                                                  T *__restrict__ warp_box, obj_scalars *sc)
 {
   constexpr int D = K / 2;
+  constexpr int C = 2 * D;
+  constexpr int P = C + 1;
+  constexpr int G = 32 / kLeafSize;  // buckets per query group
   using io = box_io< T >;
-  const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
-#pragma unroll
-  for ( int a = 0; a < D; ++a )
+  __shared__ T s_el[kSlabThreads * P];
+  __shared__ T s_bk[( kSlabThreads / kLeafSize ) * P];
+  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // no valid permutation
+  const int tid = threadIdx.x;
+  const int r0 = static_cast< int >( blockIdx.x ) * kSlabThreads;
+  const int rows = min( kSlabThreads, n - r0 );
+  if ( tid < rows )
   {
-    lo[a] = inf;
-    hi[a] = -inf;
-  }
-  const int r0 = kLeafSize * b;
-  const int r1 = min( r0 + kLeafSize, n );
-  bool ok = true;
-  for ( int r = r0; r < r1; ++r )
-  {
-    const uint32_t e = __ldg( vals + r );
-    if ( e >= static_cast< uint32_t >( n ) )
+    const uint32_t e = __ldg( vals + r0 + tid );
+    T lo[D], hi[D];
+    if ( e < static_cast< uint32_t >( n ) )
     {
-      ok = false;
-      continue;
+      leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
+    } else {
+      atomicCAS( &sc->error, 0, kErrTimeout );
+      const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
+      {
+        lo[a] = inf;
+        hi[a] = -inf;
+      }
     }
-    T el[D], eh[D];
-    leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, el, eh );
 #pragma unroll
     for ( int a = 0; a < D; ++a )
     {
-      io::store2( elem_box + ( static_cast< size_t >( r ) * D + a ) * 2, el[a], eh[a] );
-      lo[a] = io::mn( lo[a], el[a] );
-      hi[a] = io::mx( hi[a], eh[a] );
+      s_el[tid * P + 2 * a] = lo[a];
+      s_el[tid * P + 2 * a + 1] = hi[a];
     }
   }
-  return ok;
-}
-
-// Union boxes of 32 consecutive ranks (kQueryGroup / kLeafSize buckets, adjacent lanes): the traversal culls a
-// warp of 32 queries with one of them.
-template< typename T, int D >
-__device__ __forceinline__ void store_query_group_box(T *warp_box, int b, int m, bool active, const T *lo, const T *hi)
-{
-  using io = box_io< T >;
-  constexpr int G = 32 / kLeafSize;  // buckets per group
-  const T inf = static_cast< T >( __longlong_as_double( 0x7ff0000000000000LL ) );
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for ( int a = 0; a < D; ++a )
+  __syncthreads();
+  T *eb = elem_box + static_cast< size_t >( r0 ) * C;
+  for ( int k = tid; k < rows * C; k += kSlabThreads )
   {
-    T l = active ? lo[a] : inf;
-    T h = active ? hi[a] : -inf;
-#pragma unroll
-    for ( int o = 1; o < G; o <<= 1 )
+    const int q = k / C;
+    eb[k] = s_el[q * P + ( k - q * C )];
+  }
+  // bucket unions (ranks in order, as the serial union of the reference merges them)
+  const int nb = ( rows + kLeafSize - 1 ) / kLeafSize;
+  T *bb = bucket_box + static_cast< size_t >( r0 / kLeafSize ) * C;
+  for ( int k = tid; k < nb * C; k += kSlabThreads )
+  {
+    const int q = k / C, c = k - q * C;
+    const int j1 = min( kLeafSize, rows - q * kLeafSize );
+    T v = s_el[q * kLeafSize * P + c];
+    for ( int j = 1; j < j1; ++j )
     {
-      l = io::mn( l, __shfl_xor_sync( 0xffffffffu, l, o ) );
-      h = io::mx( h, __shfl_xor_sync( 0xffffffffu, h, o ) );
+      const T x = s_el[( q * kLeafSize + j ) * P + c];
+      v = ( c & 1 ) ? io::mx( v, x ) : io::mn( v, x );
     }
-    if ( ( lane & ( G - 1 ) ) == 0 && b < m )
-      io::store2( warp_box + ( static_cast< size_t >( b / G ) * D + a ) * 2, l, h );
+    s_bk[q * P + c] = v;
+    bb[k] = v;
+  }
+  __syncthreads();
+  // query-group unions
+  const int ng = ( nb + G - 1 ) / G;
+  T *wb = warp_box + static_cast< size_t >( r0 / 32 ) * C;
+  for ( int k = tid; k < ng * C; k += kSlabThreads )
+  {
+    const int g = k / C, c = k - g * C;
+    const int j1 = min( G, nb - g * G );
+    T v = s_bk[g * G * P + c];
+    for ( int j = 1; j < j1; ++j )
+    {
+      const T x = s_bk[( g * G + j ) * P + c];
+      v = ( c & 1 ) ? io::mx( v, x ) : io::mn( v, x );
+    }
+    wb[k] = v;
+  }
+  if ( n <= kLeafSize )
+  {
+    // one bucket: it is the tree
+    T *rb = reinterpret_cast< T * >( sc->root_box );
+    if ( tid < C ) rb[tid] = s_bk[tid];
+    if ( tid == 0 ) sc->root = ~0;
   }
 }
 
@@ -256,8 +288,7 @@ __device__ __forceinline__ void store_query_group_box(T *warp_box, int b, int m,
 // nodes it closes is staged in shared memory and written out once at the end, as whole rows of node_box (both
 // children's slabs of consecutive nodes are contiguous), child, range and parent.
 //
-// a. Each thread computes the slabs of its bucket's elements (written to elem_box in rank order), their union
-//    (the bucket box, into the warp's box table in shared memory) and the 32-rank query-group boxes. A table has
+// a. Each warp loads its 32 bucket boxes (k_elem_slabs wrote them) into its box table in shared memory. A table has
 //    64 rows: 32 buckets and 32 internal nodes (node p of the block lives in the table of warp (p - bbase) / 32,
 //    row 32 + (p - bbase) % 32); a row holds the C = 2 D components, padded to C + 1 against bank conflicts.
 // b. Warp rounds (topology in registers): every lane holding an unfinished subtree [l, r] (in buckets) picks its
@@ -269,12 +300,9 @@ __device__ __forceinline__ void store_query_group_box(T *warp_box, int b, int m,
 // d. Subtrees still unfinished publish their box into their parent's slot and are queued for phase 2 as
 //    (parent * 2 + side, l, r, node).
 // e. Coalesced write-out of every node closed in the block.
-template< int K, typename T, int VT >
-__global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double *__restrict__ verts, uint32_t Vrt, int n,
-                                                              double eps, float eps_hi,
-                                                              const uint64_t *__restrict__ keys,
-                                                              const uint32_t *__restrict__ vals,
-                                                              T *__restrict__ elem_box, T *__restrict__ warp_box,
+template< int K, typename T >
+__global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const uint64_t *__restrict__ keys,
+                                                              const T *__restrict__ bucket_box,
                                                               T *__restrict__ node_box, int *__restrict__ child,
                                                               int2 *__restrict__ range, int *__restrict__ parent,
                                                               int4 *__restrict__ queue, obj_scalars *sc)
@@ -303,34 +331,16 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(const double 
   // box table element of ref (table * 64 + row), component c
   auto box = [&](int ref, int c) -> T & { return s_box[ref * ( C + 1 ) + c]; };
   auto node_ref = [&](int p) { const int q = p - bbase; return ( q >> 5 ) * 64 + 32 + ( q & 31 ); };
-  // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word).
-  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // same value for all threads
+  // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word). A
+  // one-bucket object got its root from the slab kernel.
+  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout || m == 1 ) return;  // uniform
   bool active = b < m;
 
-  // a. element slabs, bucket box, query-group boxes
+  // a. the warp's 32 bucket boxes into its box table (coalesced rows)
+  for ( int k = lane; k < 32 * C; k += 32 )
   {
-    T lo[D], hi[D];
-    if ( active && !bucket_slabs< K, T, VT >( verts, Vrt, n, b, eps, eps_hi, vals, elem_box, lo, hi ) )
-      atomicCAS( &sc->error, 0, kErrTimeout );
-    store_query_group_box< T, D >( warp_box, b, m, active, lo, hi );
-    if ( m == 1 )
-    {
-      if ( b == 0 )
-      {
-        sc->root = ~0;
-        store_root( sc, lo, hi );
-      }
-      return;  // m is uniform
-    }
-    if ( active )
-    {
-#pragma unroll
-      for ( int a = 0; a < D; ++a )
-      {
-        box( warp * 64 + lane, 2 * a ) = lo[a];
-        box( warp * 64 + lane, 2 * a + 1 ) = hi[a];
-      }
-    }
+    const int row = k / C;
+    if ( wbase + row < m ) box( warp * 64 + row, k - row * C ) = bucket_box[static_cast< size_t >( wbase ) * C + k];
   }
   const long long dself = ( b + 1 < m ) ? bdelta( keys, b ) : 0ll;
   long long dleft = 0;
@@ -627,28 +637,26 @@ __global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__
   }
 }
 
-// Refit with a fixed topology (one thread per bucket): the elements' slabs and the bucket box again (elements keep
-// their ranks), then the first/second-arrival climb along the stored parent links. exch must hold -1.
-template< int K, typename T, int VT >
-__global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restrict__ verts, uint32_t Vrt, int n,
-                                                         double eps, float eps_hi, const uint32_t *__restrict__ vals,
-                                                         T *__restrict__ elem_box, T *__restrict__ warp_box,
-                                                         T *node_box, const int *__restrict__ parent, int *exch,
+// Refit with a fixed topology (one thread per bucket, after k_elem_slabs recomputed the element, bucket and group
+// boxes; elements keep their ranks): the first/second-arrival climb along the stored parent links. exch must
+// hold -1.
+template< int K, typename T >
+__global__ void __launch_bounds__( kBuildThreads ) k_refit(int n, const T *__restrict__ bucket_box, T *node_box,
+                                                         const int *__restrict__ parent, int *exch,
                                                          obj_scalars *__restrict__ sc)
 {
   constexpr int D = K / 2;
   using io = box_io< T >;
   const int b = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
   const int m = ( n + kLeafSize - 1 ) / kLeafSize;
-  const bool active = b < m;
+  if ( b >= m || m == 1 ) return;  // a one-bucket object's root box came from the slab kernel
+  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
   T lo[D], hi[D];
-  if ( active ) bucket_slabs< K, T, VT >( verts, Vrt, n, b, eps, eps_hi, vals, elem_box, lo, hi );
-  store_query_group_box< T, D >( warp_box, b, m, active, lo, hi );
-  if ( !active ) return;
-  if ( m == 1 )
+#pragma unroll
+  for ( int a = 0; a < D; ++a )
   {
-    store_root( sc, lo, hi );
-    return;
+    lo[a] = bucket_box[( static_cast< size_t >( b ) * D + a ) * 2];
+    hi[a] = bucket_box[( static_cast< size_t >( b ) * D + a ) * 2 + 1];
   }
   const int root = sc->root;
   int slot = b;
@@ -679,21 +687,45 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(const double *__restr
 }
 
 template< int K, typename T, int VT >
-cudaError_t launch_build_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys,
-                           const uint32_t *vals, void *elem_box, void *warp_box, void *node_box, int2 *child,
-                           int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc, cudaStream_t s)
+cudaError_t launch_slabs_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
+                           void *elem_box, void *bucket_box, void *warp_box, obj_scalars *sc, cudaStream_t s)
 {
-  const float eps_hi = f32_up( eps );
+  const unsigned grid = static_cast< unsigned >( ( n + kSlabThreads - 1 ) / kSlabThreads );
+  k_elem_slabs< K, T, VT ><<< grid, kSlabThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, f32_up( eps ),
+                                                           vals, static_cast< T * >( elem_box ),
+                                                           static_cast< T * >( bucket_box ),
+                                                           static_cast< T * >( warp_box ), sc );
+  return cudaGetLastError();
+}
+
+template< int K, typename T >
+cudaError_t slabs_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *eb, void *bb,
+                    void *wb, obj_scalars *sc, cudaStream_t s)
+{
+  switch ( V )
+  {
+    case 3: return launch_slabs_t< K, T, 3 >( verts, V, n, eps, vals, eb, bb, wb, sc, s );
+    case 4: return launch_slabs_t< K, T, 4 >( verts, V, n, eps, vals, eb, bb, wb, sc, s );
+    case 8: return launch_slabs_t< K, T, 8 >( verts, V, n, eps, vals, eb, bb, wb, sc, s );
+    default: return launch_slabs_t< K, T, 0 >( verts, V, n, eps, vals, eb, bb, wb, sc, s );
+  }
+}
+
+template< int K, typename T >
+cudaError_t launch_build_t(uint64_t n, const uint64_t *keys, const void *bucket_box, void *node_box, int2 *child,
+                           int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s)
+{
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
+  if ( m <= 1 ) return cudaSuccess;  // the slab kernel stored a one-bucket object's root
   const unsigned grid = static_cast< unsigned >( ( m + kBuildThreads - 1 ) / kBuildThreads );
   const size_t smem = static_cast< size_t >( 2 * kBuildThreads ) * ( 2 * ( K / 2 ) + 1 ) * sizeof( T );  // [W * 64][C + 1]
-  const cudaError_t e = cudaFuncSetAttribute( k_build_leaf< K, T, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const cudaError_t e = cudaFuncSetAttribute( k_build_leaf< K, T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast< int >( smem ) );
   if ( e != cudaSuccess ) return e;
-  k_build_leaf< K, T, VT ><<< grid, kBuildThreads, smem, s >>>(
-    verts, V, static_cast< int >( n ), eps, eps_hi, keys, vals, static_cast< T * >( elem_box ),
-    static_cast< T * >( warp_box ), static_cast< T * >( node_box ), reinterpret_cast< int * >( child ), range, parent,
-    queue, sc );
+  k_build_leaf< K, T ><<< grid, kBuildThreads, smem, s >>>( static_cast< int >( n ), keys,
+                                                           static_cast< const T * >( bucket_box ),
+                                                           static_cast< T * >( node_box ),
+                                                           reinterpret_cast< int * >( child ), range, parent, queue, sc );
   return cudaGetLastError();
 }
 
@@ -710,45 +742,16 @@ cudaError_t launch_climb_t(uint64_t n, const uint64_t *keys, void *node_box, int
   return cudaGetLastError();
 }
 
-template< int K, typename T, int VT >
-cudaError_t launch_refit_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
-                           void *elem_box, void *warp_box, void *node_box, const int *parent, int *exch,
+template< int K, typename T >
+cudaError_t launch_refit_t(uint64_t n, const void *bucket_box, void *node_box, const int *parent, int *exch,
                            obj_scalars *sc, cudaStream_t s)
 {
-  const float eps_hi = f32_up( eps );
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
+  if ( m <= 1 ) return cudaSuccess;
   const unsigned grid = static_cast< unsigned >( ( m + kBuildThreads - 1 ) / kBuildThreads );
-  k_refit< K, T, VT ><<< grid, kBuildThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, eps_hi, vals,
-                                                       static_cast< T * >( elem_box ), static_cast< T * >( warp_box ),
-                                                       static_cast< T * >( node_box ), parent, exch, sc );
+  k_refit< K, T ><<< grid, kBuildThreads, 0, s >>>( static_cast< int >( n ), static_cast< const T * >( bucket_box ),
+                                                   static_cast< T * >( node_box ), parent, exch, sc );
   return cudaGetLastError();
-}
-
-template< int K, typename T >
-cudaError_t build_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint64_t *keys, const uint32_t *vals,
-                    void *eb, void *wb, void *nb, int2 *child, int2 *range, int *parent, int *exch, int4 *queue,
-                    obj_scalars *sc, cudaStream_t s)
-{
-  switch ( V )
-  {
-    case 3: return launch_build_t< K, T, 3 >( verts, V, n, eps, keys, vals, eb, wb, nb, child, range, parent, exch, queue, sc, s );
-    case 4: return launch_build_t< K, T, 4 >( verts, V, n, eps, keys, vals, eb, wb, nb, child, range, parent, exch, queue, sc, s );
-    case 8: return launch_build_t< K, T, 8 >( verts, V, n, eps, keys, vals, eb, wb, nb, child, range, parent, exch, queue, sc, s );
-    default: return launch_build_t< K, T, 0 >( verts, V, n, eps, keys, vals, eb, wb, nb, child, range, parent, exch, queue, sc, s );
-  }
-}
-
-template< int K, typename T >
-cudaError_t refit_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *eb, void *wb,
-                    void *nb, const int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
-{
-  switch ( V )
-  {
-    case 3: return launch_refit_t< K, T, 3 >( verts, V, n, eps, vals, eb, wb, nb, parent, exch, sc, s );
-    case 4: return launch_refit_t< K, T, 4 >( verts, V, n, eps, vals, eb, wb, nb, parent, exch, sc, s );
-    case 8: return launch_refit_t< K, T, 8 >( verts, V, n, eps, vals, eb, wb, nb, parent, exch, sc, s );
-    default: return launch_refit_t< K, T, 0 >( verts, V, n, eps, vals, eb, wb, nb, parent, exch, sc, s );
-  }
 }
 
 // Original-order slabs (parity probe).
@@ -782,25 +785,35 @@ cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, voi
 
 }  // namespace
 
-cudaError_t launch_build(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint64_t *keys, const uint32_t *vals, void *elem_box, void *warp_box, void *node_box,
-                         int2 *child, int2 *range, int *parent, int *exch, int4 *queue, obj_scalars *sc,
+cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
+                         const uint32_t *vals, void *elem_box, void *bucket_box, void *warp_box, obj_scalars *sc,
                          cudaStream_t s)
 {
-#define BVHG_BUILD_CASE( KK )                                                                                      \
-  case KK:                                                                                                        \
-    return fp32 ? build_v< KK, float >( verts, V, n, eps, keys, vals, elem_box, warp_box, node_box, child, range,  \
-                                        parent, exch, queue, sc, s )                                               \
-                : build_v< KK, double >( verts, V, n, eps, keys, vals, elem_box, warp_box, node_box, child, range, \
-                                         parent, exch, queue, sc, s );
   switch ( K )
   {
-    BVHG_BUILD_CASE( 6 )
-    BVHG_BUILD_CASE( 18 )
-    BVHG_BUILD_CASE( 26 )
+    case 6: return fp32 ? slabs_v< 6, float >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s )
+                        : slabs_v< 6, double >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s );
+    case 18: return fp32 ? slabs_v< 18, float >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s )
+                         : slabs_v< 18, double >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s );
+    case 26: return fp32 ? slabs_v< 26, float >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s )
+                         : slabs_v< 26, double >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s );
     default: return cudaErrorInvalidValue;
   }
-#undef BVHG_BUILD_CASE
+}
+
+cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, const void *bucket_box, void *node_box,
+                         int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s)
+{
+  switch ( K )
+  {
+    case 6: return fp32 ? launch_build_t< 6, float >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s )
+                        : launch_build_t< 6, double >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s );
+    case 18: return fp32 ? launch_build_t< 18, float >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s )
+                         : launch_build_t< 18, double >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s );
+    case 26: return fp32 ? launch_build_t< 26, float >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s )
+                         : launch_build_t< 26, double >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s );
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint64_t *keys, void *node_box, int2 *child, int2 *range,
@@ -818,18 +831,17 @@ cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint64_t *keys, voi
   }
 }
 
-cudaError_t launch_refit(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *elem_box, void *warp_box, void *node_box, const int *parent,
+cudaError_t launch_refit(int K, bool fp32, uint64_t n, const void *bucket_box, void *node_box, const int *parent,
                          int *exch, obj_scalars *sc, cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return fp32 ? refit_v< 6, float >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s )
-                        : refit_v< 6, double >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s );
-    case 18: return fp32 ? refit_v< 18, float >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s )
-                         : refit_v< 18, double >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s );
-    case 26: return fp32 ? refit_v< 26, float >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s )
-                         : refit_v< 26, double >( verts, V, n, eps, vals, elem_box, warp_box, node_box, parent, exch, sc, s );
+    case 6: return fp32 ? launch_refit_t< 6, float >( n, bucket_box, node_box, parent, exch, sc, s )
+                        : launch_refit_t< 6, double >( n, bucket_box, node_box, parent, exch, sc, s );
+    case 18: return fp32 ? launch_refit_t< 18, float >( n, bucket_box, node_box, parent, exch, sc, s )
+                         : launch_refit_t< 18, double >( n, bucket_box, node_box, parent, exch, sc, s );
+    case 26: return fp32 ? launch_refit_t< 26, float >( n, bucket_box, node_box, parent, exch, sc, s )
+                         : launch_refit_t< 26, double >( n, bucket_box, node_box, parent, exch, sc, s );
     default: return cudaErrorInvalidValue;
   }
 }

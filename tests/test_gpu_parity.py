@@ -294,7 +294,7 @@ def test_stage_timing_and_launch_count():
         ctx.build(oa)
         ctx.self_collision(oa)
         ms, launches = ctx.stage_times()
-        assert launches["sort"] == 8 and launches["build"] == 1 and launches["climb"] == 1
+        assert launches["sort"] == 8 and launches["slabs"] == 1 and launches["build"] == 1 and launches["climb"] == 1
         assert launches["traverse"] >= 1
         assert all(v >= 0 for v in ms.values()) and ms["sort"] > 0
         assert ctx.launch_count() >= 12
