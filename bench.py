@@ -144,6 +144,7 @@ def peaks():
 #   bounds   read 72 (vertices) + write 24 (centroid, SoA)                                      = 96
 #   keys     read 24 (centroid) + write 8 (key)                                                 = 32
 #   sort     per pass read 12 + write 12 (key + index)                                          = 24 per pass
+#   fixup    read 12 + write 12 (key + index; neighbours of a run are cache hits)               = 24
 #   slabs    read 4 (index) + 72 (vertices, gathered) + write 2 D S (element slabs in rank order) + 2 D S / 8
 #            (leaf-bucket boxes) + 2 D S / 32 (query-group boxes)                               = 76 + 2DS(1 + 1/8 + 1/32)
 #   build    read 2 D S / 8 (bucket boxes) + 2 (boundary keys) + write (4 D S + 8 child + 8 range + 8 parent) / 8
@@ -153,7 +154,7 @@ LEAF = 8
 
 
 def stage_bytes(D, S, passes):
-    return {"bounds": 96, "keys": 32, "sort": 24 * passes,
+    return {"bounds": 96, "keys": 32, "sort": 24 * passes, "fixup": 24,
             "slabs": 76 + 2 * D * S * (1 + 1 / LEAF + 1 / 32),
             "build": 2 + 2 * D * S / LEAF + (4 * D * S + 24) / LEAF,
             "traverse": 2 * D * S / 32}
@@ -272,7 +273,7 @@ def run_gpu(args, world, rank, local):
         if st_ms.get(s, 0) > 0:
             elems = prims if s != "traverse" else na
             stage_bw[s] = elems * b / (st_ms[s] * 1e-3) / 1e9
-    dom = max(("bounds", "keys", "sort", "slabs", "build"), key=lambda s: st_ms[s])
+    dom = max(("bounds", "keys", "sort", "fixup", "slabs", "build"), key=lambda s: st_ms[s])
     peak, peak_kind = peaks()
     n_launch = max(1, st_launch[dom])
     per_launch_ms = st_ms[dom] / n_launch

@@ -16,7 +16,7 @@ PLAIN_FP64, FILTER_FP32 = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
 REBUILD, REFIT = 0, 1
 FLAG_STAGE_TIMING = 0x1
-STAGES = ("bounds", "keys", "sort", "build", "traverse", "recheck", "output", "climb", "slabs")
+STAGES = ("bounds", "keys", "sort", "build", "traverse", "recheck", "output", "climb", "slabs", "fixup")
 
 # Every entry point declared in include/bvhg.h.
 EXPORTS = (

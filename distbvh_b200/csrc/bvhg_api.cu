@@ -339,7 +339,11 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
     stage_scope st( ctx, BVHG_STAGE_BOUNDS );
     BVHG_CUDA( ctx, cudaMemcpyAsync( o.sc(), ctx->init_template, sizeof( obj_scalars ), cudaMemcpyHostToDevice, s ) );
     BVHG_CUDA( ctx, cudaMemsetAsync( o.hist.p, 0, passes * radix * 4, s ) );
-    BVHG_CUDA( ctx, cudaMemsetAsync( o.status.p, 0, passes * ( tiles + 1 ) * radix * 4, s ) );
+    {
+      const size_t first_words = static_cast< size_t >( sort_first_pass( bits ) ) * ( tiles + 1 ) * radix;
+      BVHG_CUDA( ctx, cudaMemsetAsync( o.status.as< uint32_t >() + first_words, 0,
+                                       ( passes * ( tiles + 1 ) * radix - first_words ) * 4, s ) );
+    }
     if ( m > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( m - 1 ) * 4, s ) );
     BVHG_CUDA( ctx, launch_centroid_bounds( K, o.verts, o.V, n, ctx->cfg.epsilon, o.cx.as< double >(),
                                             o.cy.as< double >(), o.cz.as< double >(), o.sc(), s ) );
@@ -351,12 +355,15 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
                                       o.keys.as< uint64_t >(), o.hist.as< uint32_t >(), s ) );
     st.launched();
   }
+  uint64_t *kin = o.keys.as< uint64_t >(), *kout = o.keys_alt.as< uint64_t >();
+  uint32_t *vin = nullptr, *vout = o.vals_alt.as< uint32_t >();
   {
     stage_scope st( ctx, BVHG_STAGE_SORT );
-    uint64_t *kin = o.keys.as< uint64_t >(), *kout = o.keys_alt.as< uint64_t >();
-    uint32_t *vin = nullptr, *vout = o.vals_alt.as< uint32_t >();
+    // Radix passes over the high key half only; the fix-up then sorts each run of equal high halves by the low
+    // half (runs are a handful of elements for meshes: 2^31 cells of the Morton grid).
     uint32_t *vother = o.vals.as< uint32_t >();
-    for ( int p = 0; p < passes; ++p )
+    const int first = sort_first_pass( bits );
+    for ( int p = first; p < passes; ++p )
     {
       BVHG_CUDA( ctx, launch_onesweep( bits, kin, vin, kout, vout, n, p, o.hist.as< uint32_t >(),
                                        o.status.as< uint32_t >(), o.sc(), ctx->spin_limit, ctx->stall_sort, s ) );
@@ -366,7 +373,13 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
       vin = vout;
       vout = next_out;
     }
-    o.sort_result_alt = ( passes & 1 ) ? 1 : 0;
+  }
+  {
+    // the fix-up reads the last pass's output and writes the other buffers
+    stage_scope st( ctx, BVHG_STAGE_FIXUP );
+    BVHG_CUDA( ctx, launch_sort_fixup( kin, vin, kout, vout, n, o.sc(), s ) );
+    st.launched();
+    o.sort_result_alt = ( kout == o.keys_alt.as< uint64_t >() ) ? 1 : 0;
   }
   {
     stage_scope st( ctx, BVHG_STAGE_SLABS );
@@ -711,10 +724,28 @@ bvhg_status bvhg_get_morton(bvhg_ctx *ctx, int32_t obj, uint64_t *sorted_keys, u
   if ( o.n == 0 ) return BVHG_OK;
   bvhg_status st = check_scalar_errors( ctx, o );
   if ( st != BVHG_OK ) return st;
-  if ( sorted_keys ) BVHG_CUDA( ctx, cudaMemcpy( sorted_keys, o.sorted_keys(), o.n * 8, cudaMemcpyDeviceToHost ) );
-  if ( perm ) BVHG_CUDA( ctx, cudaMemcpy( perm, o.sorted_vals(), o.n * 4, cudaMemcpyDeviceToHost ) );
   obj_scalars h;
   BVHG_CUDA( ctx, cudaMemcpy( &h, o.sc(), sizeof( h ), cudaMemcpyDeviceToHost ) );
+  if ( h.sort_approx )
+  {
+    // A run of equal high key halves was too long for the device fix-up: the build order is valid but not the
+    // stable order. The stable order is the order of (key, element index) pairs.
+    std::vector< std::pair< uint64_t, uint32_t > > kv( o.n );
+    std::vector< uint64_t > k( o.n );
+    std::vector< uint32_t > v( o.n );
+    BVHG_CUDA( ctx, cudaMemcpy( k.data(), o.sorted_keys(), o.n * 8, cudaMemcpyDeviceToHost ) );
+    BVHG_CUDA( ctx, cudaMemcpy( v.data(), o.sorted_vals(), o.n * 4, cudaMemcpyDeviceToHost ) );
+    for ( uint64_t i = 0; i < o.n; ++i ) kv[i] = { k[i], v[i] };
+    std::sort( kv.begin(), kv.end() );
+    for ( uint64_t i = 0; i < o.n; ++i )
+    {
+      if ( sorted_keys ) sorted_keys[i] = kv[i].first;
+      if ( perm ) perm[i] = kv[i].second;
+    }
+  } else {
+    if ( sorted_keys ) BVHG_CUDA( ctx, cudaMemcpy( sorted_keys, o.sorted_keys(), o.n * 8, cudaMemcpyDeviceToHost ) );
+    if ( perm ) BVHG_CUDA( ctx, cudaMemcpy( perm, o.sorted_vals(), o.n * 4, cudaMemcpyDeviceToHost ) );
+  }
   if ( min3 ) std::memcpy( min3, h.min3, sizeof( h.min3 ) );
   if ( inv3 ) std::memcpy( inv3, h.inv3, sizeof( h.inv3 ) );
   return BVHG_OK;

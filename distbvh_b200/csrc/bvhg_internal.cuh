@@ -34,6 +34,7 @@ struct obj_scalars
   int root;                          // root internal node, or ~elem when n == 1
   int error;                         // bvhg_status raised by a kernel (first one wins)
   unsigned int climb_count;          // subtrees queued for the global phase of the tree build
+  unsigned int sort_approx;          // 1: a run of equal high key halves was too long for the low-half fix-up
   alignas( 16 ) unsigned char root_box[26 * 8];  // the root's slabs, D (min, max) pairs of the slab type
   unsigned int sort_tile_counter[64];// tile dispenser per radix pass
 };
@@ -91,6 +92,13 @@ cudaError_t launch_centroid_bounds(int K, const double *verts, uint32_t V, uint6
 
 cudaError_t launch_keys_hist(int bits, const double *cx, const double *cy, const double *cz, uint64_t n,
                              obj_scalars *sc, uint64_t *keys, uint32_t *hist, cudaStream_t s);
+
+// Stable sort of each run of equal high key halves by the low half (in -> out), after the passes over bits 32..62.
+cudaError_t launch_sort_fixup(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
+                              uint32_t *vals_out, uint64_t n, obj_scalars *sc, cudaStream_t s);
+
+// Passes of the sort that build() runs: those whose digit lies in the high key half (the fix-up sorts the rest).
+inline int sort_first_pass(int bits) { return 32 / bits; }
 
 cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,

@@ -373,7 +373,71 @@ cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64
   return cudaGetLastError();
 }
 
+// Low-half fix-up after the radix passes over the high key half (bits 32..62). Those passes leave the keys stably
+// ordered by their high 32 bits: every run of equal high halves is in original-index order. Placing each element
+// of a run at the run's start plus its rank by (full key, position) -- a stable sort of the run by the low half --
+// then gives the stable order of the full keys. One thread per element, out of place (in -> out), so that no
+// thread reads what another writes. Runs are found by scanning neighbours (cache hits: a warp reads contiguous
+// keys). A run longer than kFixRun keeps its order and is flagged in sc->sort_approx (still a valid build order;
+// exact probes sort such runs again on the host).
+constexpr int kFixRun = 32;
+
+__global__ void __launch_bounds__( 256 ) k_sort_fixup(const uint64_t *__restrict__ keys_in,
+                                                      const uint32_t *__restrict__ vals_in,
+                                                      uint64_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+                                                      uint32_t n, obj_scalars *sc)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ( i >= n ) return;
+  const uint64_t ki = keys_in[i];
+  const uint32_t hi = static_cast< uint32_t >( ki >> 32 );
+  uint32_t s = i, e = i;
+  bool limit = false;
+  while ( s > 0 && static_cast< uint32_t >( __ldg( keys_in + s - 1 ) >> 32 ) == hi )
+  {
+    --s;
+    if ( i - s >= kFixRun )
+    {
+      limit = true;
+      break;
+    }
+  }
+  while ( !limit && e + 1 < n && static_cast< uint32_t >( __ldg( keys_in + e + 1 ) >> 32 ) == hi )
+  {
+    ++e;
+    if ( e - i >= kFixRun )
+    {
+      limit = true;
+      break;
+    }
+  }
+  uint32_t pos = i;
+  if ( limit || e - s + 1 > kFixRun )
+  {
+    atomicOr( &sc->sort_approx, 1u );
+  } else if ( e > s ) {
+    uint32_t rank = 0;
+    for ( uint32_t j = s; j <= e; ++j )
+    {
+      const uint64_t kj = __ldg( keys_in + j );
+      rank += ( kj < ki || ( kj == ki && j < i ) ) ? 1u : 0u;
+    }
+    pos = s + rank;
+  }
+  keys_out[pos] = ki;
+  vals_out[pos] = vals_in[i];
+}
+
 }  // namespace
+
+cudaError_t launch_sort_fixup(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
+                              uint32_t *vals_out, uint64_t n, obj_scalars *sc, cudaStream_t s)
+{
+  if ( n == 0 ) return cudaSuccess;
+  k_sort_fixup<<< static_cast< unsigned >( ( n + 255 ) / 256 ), 256, 0, s >>>( keys_in, vals_in, keys_out, vals_out,
+                                                                             static_cast< uint32_t >( n ), sc );
+  return cudaGetLastError();
+}
 
 cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,

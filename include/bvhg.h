@@ -101,14 +101,15 @@ enum
 {
   BVHG_STAGE_BOUNDS = 0,     /* centroids + Morton bounds */
   BVHG_STAGE_KEYS = 1,       /* Morton keys + digit histograms */
-  BVHG_STAGE_SORT = 2,       /* all radix passes */
+  BVHG_STAGE_SORT = 2,       /* radix passes over the high key half */
   BVHG_STAGE_BUILD = 3,      /* block-local LBVH build and node boxes over the buckets (or the refit climb) */
   BVHG_STAGE_TRAVERSE = 4,   /* tree traversal (candidate pairs) */
   BVHG_STAGE_RECHECK = 5,    /* FP64 recheck of FP32 candidates */
   BVHG_STAGE_OUTPUT = 6,     /* gid mapping + output copy */
   BVHG_STAGE_CLIMB = 7,      /* global climb of the LBVH build (subtrees left open by the block-local phase) */
   BVHG_STAGE_SLABS = 8,      /* element slabs in Morton rank order, leaf-bucket and query-group boxes */
-  BVHG_NUM_STAGES = 9
+  BVHG_STAGE_FIXUP = 9,      /* stable order of each run of equal high key halves by the low half */
+  BVHG_NUM_STAGES = 10
 };
 
 BVHG_API void bvhg_config_default(bvhg_config *cfg);

@@ -85,6 +85,37 @@ def test_many_tiles_sort():
         check_stages(ctx, oa, a, 18, 0.0)
 
 
+def clustered_soup(counts, seed):
+    """Tiny triangles in clusters of the given sizes, each inside one cell of the top 31 Morton bits (10 bits of
+    x, 10 of y, 11 of z: the clusters sit at cell centres of a 1024 x 1024 x 2048 grid over the unit cube, 2e-4
+    wide), plus two corner elements that fix the Morton bounds to the unit cube. Members of a cluster share the
+    high key half and differ in the low."""
+    rng = np.random.default_rng(seed)
+    parts = [np.array([[[0, 0, 0], [1e-3, 0, 0], [0, 1e-3, 0]]]),
+             np.array([[[1, 1, 1], [1 - 1e-3, 1, 1], [1, 1 - 1e-3, 1]]])]
+    for j, c in enumerate(counts):
+        centre = (np.array([307, 511 - 40 * j, 2 * (129 + 17 * j)]) + 0.5) / np.array([1024.0, 1024.0, 2048.0])
+        pts = centre + rng.uniform(-1e-4, 1e-4, (c, 1, 3)) + rng.uniform(-2e-6, 2e-6, (c, 3, 3))
+        parts.append(pts)
+    xyz = np.concatenate(parts).astype(np.float64)
+    return np.ascontiguousarray(xyz[rng.permutation(xyz.shape[0])])
+
+
+@pytest.mark.parametrize("counts", [(2, 5, 31, 32), (33, 3), (500, 40, 7)])
+def test_runs_of_equal_high_key_halves(counts):
+    """The build sorts by the high key half and fixes each run of equal high halves by the low half: short runs
+    on the device, runs beyond its limit through the exact host order of the probe. Either way the probe returns
+    the stable order and the pair sets are exact."""
+    a = clustered_soup(counts, seed=sum(counts))
+    b = clustered_soup(counts[::-1], seed=7 + sum(counts))
+    with bvhg.Context(k=18) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        check_stages(ctx, oa, a, 18, 0.0)
+        check_stages(ctx, ob, b, 18, 0.0)
+        assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b, 18))
+        assert np.array_equal(orc.canonical(ctx.self_collision(oa)), orc.self_pair_set(a, 18))
+
+
 def test_two_plates_config():
     a, b = meshes.two_plates()
     eps = meshes.TWO_PLATES_EPSILON
@@ -294,7 +325,8 @@ def test_stage_timing_and_launch_count():
         ctx.build(oa)
         ctx.self_collision(oa)
         ms, launches = ctx.stage_times()
-        assert launches["sort"] == 8 and launches["slabs"] == 1 and launches["build"] == 1 and launches["climb"] == 1
+        # four radix passes over the high key half, then the low-half fix-up
+        assert launches["sort"] == 4 and launches["fixup"] == 1 and launches["slabs"] == 1 and launches["build"] == 1 and launches["climb"] == 1
         assert launches["traverse"] >= 1
         assert all(v >= 0 for v in ms.values()) and ms["sort"] > 0
         assert ctx.launch_count() >= 12
