@@ -330,3 +330,31 @@ def test_stage_timing_and_launch_count():
         assert launches["traverse"] >= 1
         assert all(v >= 0 for v in ms.values()) and ms["sort"] > 0
         assert ctx.launch_count() >= 12
+
+
+GOLDEN = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "ref_vectors.npz"))
+
+
+@pytest.mark.parametrize("case", [str(c) for c in GOLDEN["cases"]])
+@pytest.mark.parametrize("k", [6, 18, 26])
+def test_gpu_matches_reference_vectors(case, k):
+    """The CUDA path against vectors computed by the reference's own code (tests/golden/make_golden.py)."""
+    g = lambda key: GOLDEN[f"{case}/{key}"]  # noqa: E731
+    a, b, eps = g("a"), g("b"), float(g("eps"))
+    with bvhg.Context(k=k, epsilon=eps) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        for side, o, x in (("a", oa, a), ("b", ob, b)):
+            n = x.shape[0]
+            assert np.array_equal(u64(ctx.kdops(o, n)), u64(g(f"{side}/kdops{k}")))
+            assert np.array_equal(u64(ctx.centroids(o, n)), u64(g(f"{side}/centroids")))
+            keys, perm, mn, inv = ctx.morton(o, n)
+            assert np.array_equal(u64(mn), u64(g(f"{side}/min3"))) and np.array_equal(u64(inv), u64(g(f"{side}/inv3")))
+            want = g(f"{side}/keys")
+            assert np.array_equal(perm, np.argsort(want, kind="stable")) and np.array_equal(keys, want[perm])
+        got = orc.canonical(ctx.broadphase(oa, ob))
+        self_got = orc.canonical(ctx.self_collision(oa))
+        if k == 18:
+            assert np.array_equal(got, orc.canonical(g("pairs18")))
+        else:
+            assert got.shape[0] == int(g(f"tree_count{k}"))
+            assert np.array_equal(self_got, orc.canonical(np.sort(g(f"self{k}"), axis=1)))
