@@ -2,8 +2,9 @@
 """Benchmark: build + broadphase Mprims/s of the per-rank element broadphase on B200.
 
 Workload (one step): an icosphere of 5,242,880 triangles (level 9, radius 0.5) pressed 0.01 into a plate of
-4,194,304 triangles (2048 x 1024 quads), 18-DOP, epsilon 0, inter-object pairs: element slabs, centroids and
-Morton bounds, Morton keys, 8-bit-digit radix sort, LBVH build + refit of both objects, traversal, exact pair set.
+4,194,304 triangles (2048 x 1024 quads), 18-DOP, epsilon 0, inter-object pairs: centroids and Morton bounds,
+Morton keys, stable radix sort (8-bit digits over the high key half + low-half fix-up), element slabs, LBVH build
+with node k-DOPs of both objects, traversal, exact pair set.
 Synthetic seeded geometry (the reference's sphere/plate deck is not available); inputs 680 MB, larger than L2.
 
   value  device-resident vertices -> device-resident pair set, FP64 plain form, CUDA events on the library's
@@ -11,7 +12,7 @@ Synthetic seeded geometry (the reference's sphere/plate deck is not available); 
   e2e    the same step through the C ABI with pinned HOST buffers: H2D of both vertex arrays and D2H of the
          pair list inside the timed region.
 
-`--impl reference` times the reference's algorithms on the host cores instead (see cpu_reference()).
+`--impl reference` times the reference's algorithms on the host cores instead (see run_reference()).
 Under torchrun every rank runs its own copy of the scene (independent objects, no collective on the data path:
 weak scaling); timing is max over ranks.
 """

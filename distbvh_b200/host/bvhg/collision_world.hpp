@@ -1,0 +1,457 @@
+// collision_world.hpp — vt-free, single-rank host mirror of distBVH's collision_world / collision_object API over
+// the C ABI of libbvhg.so (include/bvhg.h). Header-only C++17; link with -lbvhg.
+//
+// It keeps the reference's L5 signatures (src/bvh/collision_world.hpp:54-114, src/bvh/collision_object.hpp:55-283):
+//
+//   bvhg::collision_world world( od_factor );
+//   auto &a = world.create_collision_object();
+//   a.set_entity_data( elements, bvhg::split_algorithm::clustering );  // span / vector of the caller's element type
+//   a.init_broadphase();
+//   world.set_narrowphase_functor< Element >( functor );                 // narrowphase_result_pair( bc_a, bc_b )
+//   world.start_iteration(); a.broadphase( b ); world.finish_iteration();
+//   a.for_each_result< R >( []( const R & ) { ... } );
+//
+// Differences, each forced by the single-rank, element-exact design:
+//   - The element type supplies vertices instead of a k-DOP: `e.vertices()` (or a free get_entity_vertices(e))
+//     returning a contiguous range of 3-vectors indexable as v[0..2], and `e.global_id()` (or
+//     get_entity_global_id(e)). The library computes the k-DOP exactly as kdop_base::from_vertices
+//     (src/bvh/kdop.hpp:238-264) with world_config::k (26 by default: the reference's bphase_kdop).
+//   - Patches: an object's elements are split into od_factor patches of consecutive Morton ranks (the reference's
+//     clustering splits the same order at its largest key jumps, src/bvh/split/cluster.hpp:89-179). The functor
+//     is called once for every patch pair that holds at least one overlapping element pair (the reference calls
+//     it for every pair of overlapping patch k-DOPs, a superset), with both patches' elements as spans in rank
+//     order and, in addition, the exact element pairs of that patch pair (broadphase_collision::candidates,
+//     indices into the two spans). A functor that only reports overlapping elements gives the same results.
+//   - The element bytes handed to the functor are copies made at init_broadphase (the reference ships copies to
+//     the narrowphase rank too); the caller's array is read only during set_entity_data.
+//   - Errors throw bvhg::error (the reference asserts and terminates).
+#ifndef BVHG_HOST_COLLISION_WORLD_HPP
+#define BVHG_HOST_COLLISION_WORLD_HPP
+
+#include "../../../include/bvhg.h"
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+namespace bvhg
+{
+class error : public std::runtime_error
+{
+public:
+  error(bvhg_status s, const std::string &what) : std::runtime_error( what ), status( s ) {}
+  bvhg_status status;
+};
+
+// Same enumerators as src/bvh/types.hpp:52-57; all three order patches by Morton rank here.
+enum class split_algorithm
+{
+  geom_axis,
+  ml_geom_axis,
+  clustering
+};
+
+struct world_config
+{
+  int k = 26;                                  // 6, 18 or 26
+  bvhg_precision precision = BVHG_PLAIN_FP64;  // or BVHG_FILTER_FP32 (same pair set)
+  double epsilon = 0.0;                        // slab inflation
+  int device = 0;
+  void *stream = nullptr;                      // cudaStream_t; NULL = one the library owns
+};
+
+template< typename T >
+class span
+{
+public:
+  span() = default;
+  span(T *p, std::size_t n) : m_p( p ), m_n( n ) {}
+  template< typename C >
+  span(C &c) : m_p( c.data() ), m_n( c.size() )
+  {}
+  T *data() const { return m_p; }
+  std::size_t size() const { return m_n; }
+  T &operator[](std::size_t i) const { return m_p[i]; }
+  T *begin() const { return m_p; }
+  T *end() const { return m_p + m_n; }
+
+private:
+  T *m_p = nullptr;
+  std::size_t m_n = 0;
+};
+
+class collision_object;
+
+// Patch metadata (src/bvh/patch.hpp:55-123, without its k-DOP and centroid).
+struct patch_meta
+{
+  std::size_t gid;
+  std::size_t size;
+  std::size_t global_id() const { return gid; }
+};
+
+// src/bvh/collision_query.hpp:50-64, plus the exact element pairs of the patch pair.
+template< typename T >
+struct broadphase_collision
+{
+  collision_object &object;
+  patch_meta meta;
+  std::size_t patch_id;
+  span< const T > elements;
+  span< const std::pair< uint32_t, uint32_t > > candidates;  // (index in this span, index in the other span)
+};
+
+// src/bvh/collision_query.hpp:66-128: a byte buffer of fixed-stride records.
+class narrowphase_result
+{
+public:
+  narrowphase_result() = default;
+  explicit narrowphase_result(std::size_t stride) : m_stride( stride ) {}
+  void *allocate(std::size_t n)
+  {
+    m_n += n;
+    const std::size_t at = m_data.size();
+    m_data.resize( at + n * m_stride, 0 );
+    return m_data.data() + at;
+  }
+  void append_data(const void *p, std::size_t n)
+  {
+    std::memcpy( allocate( n ), p, n * m_stride );
+  }
+  void *at(std::size_t i) { return m_data.data() + i * m_stride; }
+  const void *at(std::size_t i) const { return m_data.data() + i * m_stride; }
+  std::size_t stride() const noexcept { return m_stride; }
+  std::size_t size() const noexcept { return m_n; }
+
+private:
+  std::vector< unsigned char > m_data;
+  std::size_t m_stride = 0;
+  std::size_t m_n = 0;
+};
+
+template< typename T >
+class typed_narrowphase_result : public narrowphase_result
+{
+public:
+  typed_narrowphase_result() : narrowphase_result( sizeof( T ) ) {}
+  template< typename... Args >
+  T &emplace_back(Args &&...args)
+  {
+    return *( new ( allocate( 1 ) ) T( std::forward< Args >( args )... ) );
+  }
+  T &operator[](std::size_t i) { return *static_cast< T * >( at( i ) ); }
+};
+
+struct narrowphase_result_pair
+{
+  narrowphase_result a;
+  narrowphase_result b;
+};
+
+namespace detail
+{
+inline void check(bvhg_ctx *ctx, bvhg_status s, const char *what)
+{
+  if ( s != BVHG_OK )
+    throw error( s, std::string( what ) + ": " + bvhg_status_string( s ) + ( ctx ? std::string( " (" ) + bvhg_last_error( ctx ) + ")" : "" ) );
+}
+
+template< typename E >
+auto vertices_of(const E &e, int) -> decltype( get_entity_vertices( e ) )
+{
+  return get_entity_vertices( e );
+}
+template< typename E >
+auto vertices_of(const E &e, long) -> decltype( e.vertices() )
+{
+  return e.vertices();
+}
+template< typename E >
+auto global_id_of(const E &e, int) -> decltype( get_entity_global_id( e ) )
+{
+  return get_entity_global_id( e );
+}
+template< typename E >
+auto global_id_of(const E &e, long) -> decltype( e.global_id() )
+{
+  return e.global_id();
+}
+
+// Type-erased element storage of one object (the functor's spans point into it).
+struct element_store
+{
+  std::vector< unsigned char > bytes;  // elements in Morton rank order
+  std::size_t size = 0;
+  std::size_t elem_size = 0;
+  const void *type = nullptr;  // identity of T
+};
+
+template< typename T >
+const void *type_id()
+{
+  static const char id = 0;
+  return &id;
+}
+}  // namespace detail
+
+class collision_world;
+
+class collision_object
+{
+public:
+  collision_object(const collision_object &) = delete;
+  collision_object &operator=(const collision_object &) = delete;
+
+  // collision_object::set_entity_data (src/bvh/collision_object.hpp:69-84). Reads the elements now: vertices and
+  // global ids go to the library, the element values are kept for the narrowphase functor.
+  template< typename T >
+  void set_entity_data(span< const T > data, split_algorithm = split_algorithm::clustering)
+  {
+    // element bytes are copied and handed to the functor as span<const T>, as the reference ships them
+    static_assert( std::is_trivially_copyable< T >::value, "element types must be trivially copyable" );
+    const std::size_t n = data.size();
+    std::vector< double > xyz;
+    std::vector< uint64_t > gid( n );
+    uint32_t V = 0;
+    for ( std::size_t i = 0; i < n; ++i )
+    {
+      const auto &verts = detail::vertices_of( data[i], 0 );
+      const uint32_t vi = static_cast< uint32_t >( std::end( verts ) - std::begin( verts ) );
+      if ( i == 0 )
+      {
+        V = vi;
+        xyz.reserve( n * V * 3 );
+      }
+      if ( vi != V ) throw error( BVHG_ERR_ARG, "set_entity_data: every element needs the same vertex count" );
+      for ( const auto &v : verts )
+        for ( int c = 0; c < 3; ++c ) xyz.push_back( static_cast< double >( v[c] ) );
+      gid[i] = static_cast< uint64_t >( detail::global_id_of( data[i], 0 ) );
+    }
+    m_gid = gid;
+    m_n = n;
+    detail::check( ctx(), bvhg_set_elements( ctx(), m_obj, n ? xyz.data() : nullptr, n ? V : 3, nullptr, n, BVHG_MEM_HOST ),
+                   "set_entity_data" );
+    m_elems.size = n;
+    m_elems.elem_size = sizeof( T );
+    m_elems.type = detail::type_id< T >();
+    m_src = std::vector< unsigned char >( reinterpret_cast< const unsigned char * >( data.data() ),
+                                          reinterpret_cast< const unsigned char * >( data.data() + n ) );
+    m_built = false;
+  }
+  template< typename T >
+  void set_entity_data(const std::vector< T > &data, split_algorithm alg = split_algorithm::clustering)
+  {
+    set_entity_data( span< const T >( data.data(), data.size() ), alg );
+  }
+
+  // collision_object::init_broadphase (src/bvh/collision_object.cpp:148): bounds, Morton keys, sort, tree.
+  void init_broadphase();
+
+  // collision_object::broadphase (src/bvh/collision_object.cpp:248-299): the exact element pairs with `other`,
+  // then the narrowphase functor for every patch pair holding one; results go to both objects.
+  void broadphase(collision_object &other);
+
+  // collision_object::for_each_result (src/bvh/collision_object.hpp:178-187).
+  template< typename R, typename F >
+  void for_each_result(F &&f) const
+  {
+    for ( const auto &r : m_results )
+      for ( std::size_t i = 0; i < r.size(); ++i ) f( *static_cast< const R * >( r.at( i ) ) );
+  }
+
+  // The exact element pairs (global ids) of the last broadphase with `other`.
+  const std::vector< std::pair< uint64_t, uint64_t > > &last_pairs() const { return m_last_pairs; }
+
+  std::size_t id() const noexcept { return m_id; }
+  int overdecomposition_factor() const noexcept;
+  std::size_t num_patches() const noexcept;
+
+  ~collision_object()
+  {
+    if ( ctx() ) bvhg_object_destroy( ctx(), m_obj );
+  }
+
+private:
+  friend class collision_world;
+  collision_object(collision_world &w, std::size_t id);
+  bvhg_ctx *ctx() const;
+
+  std::size_t patch_of_rank(std::size_t r) const
+  {
+    const std::size_t p = num_patches();
+    return p <= 1 ? 0 : ( r * p ) / m_n;
+  }
+  std::size_t patch_begin(std::size_t p) const { return ( p * m_n + num_patches() - 1 ) / num_patches(); }
+
+  collision_world &m_world;
+  std::size_t m_id;
+  int32_t m_obj = -1;
+  std::size_t m_n = 0;
+  bool m_built = false;
+  std::vector< uint64_t > m_gid;
+  std::vector< unsigned char > m_src;  // the caller's elements, original order
+  detail::element_store m_elems;       // rank order (after init_broadphase)
+  std::vector< uint32_t > m_rank;      // rank of element i
+  std::vector< narrowphase_result > m_results;
+  std::vector< std::pair< uint64_t, uint64_t > > m_last_pairs;
+};
+
+class collision_world
+{
+public:
+  template< typename T >
+  using narrowphase_functor =
+    std::function< narrowphase_result_pair( const broadphase_collision< T > &, const broadphase_collision< T > & ) >;
+
+  // collision_world( od_factor, world_config ) (src/bvh/collision_world.cpp:45-74); od_factor is a power of two.
+  explicit collision_world(std::size_t od_factor, const world_config &cfg = {}) : m_od( od_factor ), m_cfg( cfg )
+  {
+    if ( od_factor == 0 || ( od_factor & ( od_factor - 1 ) ) ) throw error( BVHG_ERR_ARG, "od_factor must be a power of two" );
+    bvhg_config c;
+    bvhg_config_default( &c );
+    c.k = cfg.k;
+    c.precision = cfg.precision;
+    c.epsilon = cfg.epsilon;
+    c.device = cfg.device;
+    c.stream = cfg.stream;
+    bvhg_ctx *ctx = nullptr;
+    detail::check( nullptr, bvhg_create( &ctx, &c ), "collision_world" );
+    m_ctx.reset( ctx );
+  }
+  collision_world(const collision_world &) = delete;
+  collision_world &operator=(const collision_world &) = delete;
+  ~collision_world()
+  {
+    m_objects.clear();  // objects release their library handles before the context goes
+  }
+
+  collision_object &create_collision_object()
+  {
+    m_objects.emplace_back( new collision_object( *this, m_objects.size() ) );
+    return *m_objects.back();
+  }
+  std::size_t num_collision_objects() const noexcept { return m_objects.size(); }
+  std::size_t overdecomposition_factor() const noexcept { return m_od; }
+
+  // collision_world::set_narrowphase_functor<T> (src/bvh/collision_world.hpp:58-94).
+  template< typename T >
+  void set_narrowphase_functor(narrowphase_functor< T > fun)
+  {
+    m_functor_type = detail::type_id< T >();
+    m_functor = [fun](collision_object &oa, const patch_meta &ma, const void *ea, std::size_t na, collision_object &ob,
+                      const patch_meta &mb, const void *eb, std::size_t nb,
+                      span< const std::pair< uint32_t, uint32_t > > cand) {
+      broadphase_collision< T > a{ oa, ma, ma.gid, span< const T >( static_cast< const T * >( ea ), na ), cand };
+      broadphase_collision< T > b{ ob, mb, mb.gid, span< const T >( static_cast< const T * >( eb ), nb ), cand };
+      return fun( a, b );
+    };
+  }
+
+  // Iteration bracketing (src/bvh/collision_world.cpp:108-133): results of the previous iteration are dropped.
+  void start_iteration()
+  {
+    for ( auto &o : m_objects ) o->m_results.clear();
+  }
+  void finish_iteration() { detail::check( ctx(), bvhg_synchronize( ctx() ), "finish_iteration" ); }
+
+  bvhg_ctx *ctx() const { return m_ctx.get(); }
+  const world_config &config() const { return m_cfg; }
+
+private:
+  friend class collision_object;
+  struct ctx_deleter
+  {
+    void operator()(bvhg_ctx *c) const { bvhg_destroy( c ); }
+  };
+  std::size_t m_od;
+  world_config m_cfg;
+  std::unique_ptr< bvhg_ctx, ctx_deleter > m_ctx;
+  std::vector< std::unique_ptr< collision_object > > m_objects;
+  const void *m_functor_type = nullptr;
+  std::function< narrowphase_result_pair( collision_object &, const patch_meta &, const void *, std::size_t,
+                                          collision_object &, const patch_meta &, const void *, std::size_t,
+                                          span< const std::pair< uint32_t, uint32_t > > ) >
+    m_functor;
+};
+
+inline collision_object::collision_object(collision_world &w, std::size_t id) : m_world( w ), m_id( id )
+{
+  detail::check( ctx(), bvhg_object_create( ctx(), &m_obj ), "create_collision_object" );
+}
+
+inline bvhg_ctx *collision_object::ctx() const { return m_world.ctx(); }
+inline int collision_object::overdecomposition_factor() const noexcept { return static_cast< int >( m_world.m_od ); }
+inline std::size_t collision_object::num_patches() const noexcept
+{
+  return m_n == 0 ? 0 : ( m_world.m_od < m_n ? m_world.m_od : m_n );
+}
+
+inline void collision_object::init_broadphase()
+{
+  detail::check( ctx(), bvhg_build( ctx(), m_obj, BVHG_REBUILD ), "init_broadphase" );
+  std::vector< uint32_t > perm( m_n );
+  if ( m_n ) detail::check( ctx(), bvhg_get_morton( ctx(), m_obj, nullptr, perm.data(), nullptr, nullptr ), "init_broadphase" );
+  m_rank.assign( m_n, 0 );
+  m_elems.bytes.assign( m_n * m_elems.elem_size, 0 );
+  for ( std::size_t r = 0; r < m_n; ++r )
+  {
+    m_rank[perm[r]] = static_cast< uint32_t >( r );
+    std::memcpy( m_elems.bytes.data() + r * m_elems.elem_size, m_src.data() + perm[r] * m_elems.elem_size,
+                 m_elems.elem_size );
+  }
+  m_built = true;
+}
+
+inline void collision_object::broadphase(collision_object &other)
+{
+  if ( !m_built || !other.m_built ) throw error( BVHG_ERR_STATE, "broadphase before init_broadphase" );
+  // element pairs as local indices (the objects were given no library gids)
+  std::vector< uint64_t > buf( 2 * 4096 );
+  uint64_t count = 0;
+  bvhg_status s = bvhg_broadphase( ctx(), m_obj, other.m_obj, buf.data(), buf.size() / 2, &count, BVHG_MEM_HOST );
+  if ( s == BVHG_ERR_OVERFLOW )
+  {
+    buf.resize( 2 * count );
+    s = bvhg_broadphase( ctx(), m_obj, other.m_obj, buf.data(), count, &count, BVHG_MEM_HOST );
+  }
+  detail::check( ctx(), s, "broadphase" );
+  m_last_pairs.resize( count );
+  // group by patch pair; indices within the patches' rank-ordered spans
+  std::map< std::pair< std::size_t, std::size_t >, std::vector< std::pair< uint32_t, uint32_t > > > groups;
+  for ( uint64_t p = 0; p < count; ++p )
+  {
+    const std::size_t i = buf[2 * p], j = buf[2 * p + 1];
+    m_last_pairs[p] = { m_gid[i], other.m_gid[j] };
+    const std::size_t ra = m_rank[i], rb = other.m_rank[j];
+    const std::size_t pa = patch_of_rank( ra ), pb = other.patch_of_rank( rb );
+    groups[{ pa, pb }].emplace_back( static_cast< uint32_t >( ra - patch_begin( pa ) ),
+                                     static_cast< uint32_t >( rb - other.patch_begin( pb ) ) );
+  }
+  if ( !m_world.m_functor ) return;
+  if ( m_world.m_functor_type != m_elems.type || m_world.m_functor_type != other.m_elems.type )
+    throw error( BVHG_ERR_ARG, "narrowphase functor element type differs from the objects' element type" );
+  for ( auto &g : groups )
+  {
+    const std::size_t pa = g.first.first, pb = g.first.second;
+    const std::size_t a0 = patch_begin( pa ), a1 = patch_begin( pa + 1 );
+    const std::size_t b0 = other.patch_begin( pb ), b1 = other.patch_begin( pb + 1 );
+    const patch_meta ma{ m_id * m_world.m_od + pa, a1 - a0 }, mb{ other.m_id * m_world.m_od + pb, b1 - b0 };
+    narrowphase_result_pair res = m_world.m_functor(
+      *this, ma, m_elems.bytes.data() + a0 * m_elems.elem_size, a1 - a0, other, mb,
+      other.m_elems.bytes.data() + b0 * other.m_elems.elem_size, b1 - b0,
+      span< const std::pair< uint32_t, uint32_t > >( g.second.data(), g.second.size() ) );
+    if ( res.a.size() ) m_results.push_back( std::move( res.a ) );
+    if ( res.b.size() ) other.m_results.push_back( std::move( res.b ) );
+  }
+}
+}  // namespace bvhg
+
+#endif  // BVHG_HOST_COLLISION_WORLD_HPP

@@ -1,0 +1,94 @@
+// Drives the C++ host mirror of collision_world / collision_object (distbvh_b200/host/bvhg/collision_world.hpp)
+// the way the reference's collision_object test drives its API (tests/collision_object_test.cpp:395-430): two
+// objects, a narrowphase functor that records (patch a, element a, patch b, element b) for every candidate, the
+// results read back with for_each_result. Reads two element files (n, then n * 9 doubles of triangle vertices)
+// and prints "pairs <count>" followed by the recorded element gid pairs, one per line.
+#include "bvhg/collision_world.hpp"
+
+#include <algorithm>
+#include <array>
+#include <cstdio>
+#include <vector>
+
+namespace
+{
+struct tri_element
+{
+  std::array< std::array< double, 3 >, 3 > v;
+  std::size_t gid;
+  const std::array< std::array< double, 3 >, 3 > &vertices() const { return v; }
+  std::size_t global_id() const { return gid; }
+};
+
+struct detailed_result
+{
+  std::size_t patch_a, elem_a, patch_b, elem_b;
+};
+
+std::vector< tri_element > read_elements(const char *path, std::size_t gid_base)
+{
+  std::FILE *f = std::fopen( path, "rb" );
+  if ( !f ) throw std::runtime_error( "cannot open input" );
+  uint64_t n = 0;
+  if ( std::fread( &n, 8, 1, f ) != 1 ) throw std::runtime_error( "bad input" );
+  std::vector< double > xyz( n * 9 );
+  if ( std::fread( xyz.data(), 8, xyz.size(), f ) != xyz.size() ) throw std::runtime_error( "bad input" );
+  std::fclose( f );
+  std::vector< tri_element > el( n );
+  for ( uint64_t i = 0; i < n; ++i )
+  {
+    for ( int v = 0; v < 3; ++v )
+      for ( int c = 0; c < 3; ++c ) el[i].v[v][c] = xyz[i * 9 + v * 3 + c];
+    el[i].gid = gid_base + i;
+  }
+  return el;
+}
+}  // namespace
+
+int main(int argc, char **argv)
+{
+  if ( argc < 5 ) return 2;
+  const std::size_t od = static_cast< std::size_t >( std::atoi( argv[3] ) );
+  bvhg::world_config cfg;
+  cfg.k = std::atoi( argv[4] );
+  auto ea = read_elements( argv[1], 0 );
+  auto eb = read_elements( argv[2], 1000000 );
+
+  bvhg::collision_world world( od, cfg );
+  auto &obj = world.create_collision_object();
+  auto &obj2 = world.create_collision_object();
+  obj.set_entity_data( ea, bvhg::split_algorithm::clustering );
+  obj.init_broadphase();
+  obj2.set_entity_data( eb, bvhg::split_algorithm::clustering );
+  obj2.init_broadphase();
+
+  std::size_t calls = 0;
+  world.set_narrowphase_functor< tri_element >(
+    [&](const bvhg::broadphase_collision< tri_element > &a, const bvhg::broadphase_collision< tri_element > &b) {
+      ++calls;
+      bvhg::narrowphase_result_pair res;
+      res.a = bvhg::narrowphase_result( sizeof( detailed_result ) );
+      res.b = bvhg::narrowphase_result( sizeof( detailed_result ) );
+      auto &ra = static_cast< bvhg::typed_narrowphase_result< detailed_result > & >( res.a );
+      if ( a.object.id() != 0 || b.object.id() != 1 ) throw std::runtime_error( "object ids" );
+      for ( const auto &c : a.candidates )
+        ra.emplace_back( detailed_result{ a.meta.global_id(), a.elements[c.first].global_id(), b.meta.global_id(),
+                                          b.elements[c.second].global_id() } );
+      return res;
+    } );
+
+  world.start_iteration();
+  obj.broadphase( obj2 );
+  world.finish_iteration();
+
+  std::vector< std::pair< std::size_t, std::size_t > > got;
+  obj.for_each_result< detailed_result >( [&](const detailed_result &r) {
+    if ( r.patch_a / od != 0 || r.patch_b / od != 1 ) throw std::runtime_error( "patch ids" );
+    got.emplace_back( r.elem_a, r.elem_b );
+  } );
+  std::sort( got.begin(), got.end() );
+  if ( got.size() != obj.last_pairs().size() ) return 3;
+  std::printf( "pairs %zu calls %zu\n", got.size(), calls );
+  for ( const auto &p : got ) std::printf( "%zu %zu\n", p.first, p.second );
+  return 0;
+}
