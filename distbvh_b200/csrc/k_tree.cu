@@ -284,24 +284,22 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
   }
 }
 
-// Phase 1 (one thread per leaf bucket b, blocks of 256 consecutive buckets). Everything a block decides about the
-// nodes it closes is staged in shared memory and written out once at the end, as whole rows of node_box (both
-// children's slabs of consecutive nodes are contiguous), child, range and parent.
+// Phase 1 (one thread per leaf bucket b, blocks of 256 consecutive buckets).
 //
-// a. Each warp loads its 32 bucket boxes (k_elem_slabs wrote them) into its box table in shared memory. A table has
-//    64 rows: 32 buckets and 32 internal nodes (node p of the block lives in the table of warp (p - bbase) / 32,
-//    row 32 + (p - bbase) % 32); a row holds the C = 2 D components, padded to C + 1 against bank conflicts.
+// a. The block loads its 256 bucket boxes (k_elem_slabs wrote them) into a shared box table, one row per bucket
+//    (C = 2 D components, padded to C + 1 against bank conflicts). A subtree's box lives in the row of its first
+//    bucket: merging two subtrees writes the parent's node_box row (both children's slabs, with the lanes of a
+//    warp acting as slab components) straight to global memory and leaves the union in the left child's row.
 // b. Warp rounds (topology in registers): every lane holding an unfinished subtree [l, r] (in buckets) picks its
 //    parent from the dissimilarities just outside the range; two lanes meeting on one parent are its children.
-//    The parent's box is formed with the lanes acting as slab components (one min or max per lane).
 // c. Block rounds: the warps' remaining subtrees meet through shared tables indexed by the first and the last
 //    bucket of each subtree (a left child with parent r looks for a subtree starting at r + 1 that targets the
 //    same parent as right child; a right child with parent l - 1 for one ending at l - 1).
 // d. Subtrees still unfinished publish their box into their parent's slot and are queued for phase 2 as
 //    (parent * 2 + side, l, r, node).
-// e. Coalesced write-out of every node closed in the block.
+// e. Coalesced write-out of the topology of every node closed in the block (child, range, parent).
 template< int K, typename T >
-__global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const uint64_t *__restrict__ keys,
+__global__ void __launch_bounds__( kBuildThreads, 4 ) k_build_leaf(int n, const uint64_t *__restrict__ keys,
                                                               const T *__restrict__ bucket_box,
                                                               T *__restrict__ node_box, int *__restrict__ child,
                                                               int2 *__restrict__ range, int *__restrict__ parent,
@@ -312,9 +310,8 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
   constexpr int W = kBuildThreads / 32;
   using io = box_io< T >;
   extern __shared__ unsigned char s_raw[];
-  T *s_box = reinterpret_cast< T * >( s_raw );  // [W * 64][C + 1]
+  T *s_box = reinterpret_cast< T * >( s_raw );  // [kBuildThreads][C + 1]
   __shared__ int2 s_child[kBuildThreads];       // closed node p - bbase: global child encodings
-  __shared__ int2 s_cref[kBuildThreads];        // closed node p - bbase: box table refs of its children
   __shared__ int2 s_rng[kBuildThreads];         // closed node p - bbase: bucket range (x < 0: not closed here)
   __shared__ int s_pnode[kBuildThreads];        // parent entry of node p - bbase, -1 when not closed here
   __shared__ int s_pleaf[kBuildThreads];        // parent entry of bucket bbase + k
@@ -322,25 +319,39 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
   __shared__ int s_par[kBuildThreads], s_r[kBuildThreads], s_ref[kBuildThreads], s_gn[kBuildThreads];
   __shared__ long long s_delta[kBuildThreads + 1];  // dissimilarity of buckets (bbase - 1 + k, bbase + k)
   __shared__ int4 s_pairs[kBuildThreads / 2];
-  __shared__ int s_npairs, s_root_tid;
+  __shared__ int s_npairs, s_root_ref;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int b = static_cast< int >( blockIdx.x * blockDim.x ) + tid;
   const int wbase = b - lane, bbase = b - tid;
   const int m = ( n + kLeafSize - 1 ) / kLeafSize;  // buckets
-  // box table element of ref (table * 64 + row), component c
   auto box = [&](int ref, int c) -> T & { return s_box[ref * ( C + 1 ) + c]; };
-  auto node_ref = [&](int p) { const int q = p - bbase; return ( q >> 5 ) * 64 + 32 + ( q & 31 ); };
+  // Merge rows rl (left child) and rr (right child) of node p: the node's row of both children's slabs to global
+  // memory, their union into row rl. Called by a whole warp; lanes < C each handle one component.
+  auto merge = [&](int p, int rl, int rr) {
+    if ( lane < C )
+    {
+      const T x = box( rl, lane ), y = box( rr, lane );
+      T *row = node_box + static_cast< size_t >( p ) * D * 4 + ( lane >> 1 ) * 4 + ( lane & 1 );
+      row[0] = x;
+      row[2] = y;
+      box( rl, lane ) = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
+    }
+  };
   // A failed sort leaves no valid permutation: build nothing (the host reports the object's error word). A
   // one-bucket object got its root from the slab kernel.
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout || m == 1 ) return;  // uniform
   bool active = b < m;
 
-  // a. the warp's 32 bucket boxes into its box table (coalesced rows)
-  for ( int k = lane; k < 32 * C; k += 32 )
+  // a. the block's bucket boxes into the table (coalesced rows)
   {
-    const int row = k / C;
-    if ( wbase + row < m ) box( warp * 64 + row, k - row * C ) = bucket_box[static_cast< size_t >( wbase ) * C + k];
+    const int rows = min( kBuildThreads, m - bbase );
+    const T *src = bucket_box + static_cast< size_t >( bbase ) * C;
+    for ( int k = tid; k < rows * C; k += kBuildThreads )
+    {
+      const int row = k / C;
+      box( row, k - row * C ) = src[k];
+    }
   }
   const long long dself = ( b + 1 < m ) ? bdelta( keys, b ) : 0ll;
   long long dleft = 0;
@@ -355,15 +366,15 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
   if ( tid == 0 )
   {
     s_npairs = 0;
-    s_root_tid = -1;
+    s_root_ref = -1;
     s_delta[0] = ( bbase >= 1 && bbase < m ) ? bdelta( keys, bbase - 1 ) : 0ll;
   }
   __syncthreads();  // the returns above are uniform over the grid
 
   int l = b, r = b;
-  int gnode = ~b;             // child encoding of the subtree this lane holds (bucket: ~bucket)
-  int ref = warp * 64 + lane; // its box in the tables
-  int selfp = -1 - tid;       // its parent entry: bucket (-1 - k) or closed node (p - bbase)
+  int gnode = ~b;       // child encoding of the subtree this lane holds (bucket: ~bucket)
+  int ref = tid;        // its box row in the table (the row of its first bucket)
+  int selfp = -1 - tid; // its parent entry: bucket (-1 - k) or closed node (p - bbase)
   int par = 0, side = 0;
   auto set_parent = [&](int entry) {
     if ( selfp < 0 ) s_pleaf[-1 - selfp] = entry;
@@ -397,21 +408,13 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
     {
       const int q = par - bbase;
       s_child[q] = make_int2( gnode, sgnode );
-      s_cref[q] = make_int2( ref, sref );
       s_rng[q] = make_int2( l, sr );
     }
-    // merged boxes, lanes as slab components
     for ( unsigned mm = lefts; mm; mm &= mm - 1 )
     {
       const int L = __ffs( mm ) - 1;
-      const int p = __shfl_sync( 0xffffffffu, par, L );
-      const int rl = __shfl_sync( 0xffffffffu, ref, L );
-      const int rr = __shfl_sync( 0xffffffffu, sref, L );
-      if ( lane < C )
-      {
-        const T x = box( rl, lane ), y = box( rr, lane );
-        box( node_ref( p ), lane ) = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
-      }
+      merge( __shfl_sync( 0xffffffffu, par, L ), __shfl_sync( 0xffffffffu, ref, L ),
+             __shfl_sync( 0xffffffffu, sref, L ) );
     }
     __syncwarp();
     if ( paired )
@@ -420,12 +423,11 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
       {
         r = sr;
         gnode = par;
-        ref = node_ref( par );
         selfp = par - bbase;
         if ( l == 0 && r == m - 1 )
         {
           sc->root = par;
-          s_root_tid = tid;
+          s_root_ref = ref;
           active = false;
         }
       } else {
@@ -474,22 +476,12 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
     const int any = __syncthreads_or( paired );
     if ( !any ) break;
     const int np = s_npairs;
-    // closed nodes' boxes, lanes as slab components (warp w takes pairs w, w + W, ...)
+    // closed nodes (warp w takes pairs w, w + W, ...)
     for ( int k = warp; k < np; k += W )
     {
       const int4 pr = s_pairs[k];
-      const int rl = s_ref[pr.x], rr = s_ref[pr.y];
-      if ( lane < C )
-      {
-        const T x = box( rl, lane ), y = box( rr, lane );
-        box( node_ref( pr.z ), lane ) = ( lane & 1 ) ? io::mx( x, y ) : io::mn( x, y );
-      }
-      if ( lane == 0 )
-      {
-        const int q = pr.z - bbase;
-        s_child[q] = make_int2( s_gn[pr.x], s_gn[pr.y] );
-        s_cref[q] = make_int2( rl, rr );
-      }
+      merge( pr.z, s_ref[pr.x], s_ref[pr.y] );
+      if ( lane == 0 ) s_child[pr.z - bbase] = make_int2( s_gn[pr.x], s_gn[pr.y] );
     }
     const int r2 = ( paired && side == 0 ) ? s_r[partner] : r;
     __syncthreads();
@@ -505,12 +497,11 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
         r = r2;
         s_rng[par - bbase] = make_int2( l, r );
         gnode = par;
-        ref = node_ref( par );
         selfp = par - bbase;
         if ( l == 0 && r == m - 1 )
         {
           sc->root = par;
-          s_root_tid = tid;
+          s_root_ref = ref;
           active = false;
         } else {
           bool left_child;
@@ -528,8 +519,7 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
     __syncthreads();
   }
   // the root's box, when the whole tree closed inside this block
-  if ( s_root_tid >= 0 && lane < C && warp == ( s_root_tid >> 5 ) )
-    reinterpret_cast< T * >( sc->root_box )[lane] = box( node_ref( sc->root ), lane );
+  if ( s_root_ref >= 0 && warp == 0 && lane < C ) reinterpret_cast< T * >( sc->root_box )[lane] = box( s_root_ref, lane );
 
   // d. unfinished subtrees: publish their box into the parent's slot and queue them for phase 2
   const unsigned waiting = __ballot_sync( 0xffffffffu, active );
@@ -555,19 +545,8 @@ __global__ void __launch_bounds__( kBuildThreads, 2 ) k_build_leaf(int n, const 
     }
   }
 
-  // e. coalesced write-out of the nodes closed in this block: node_box rows (16-byte pairs), child, range, parent
+  // e. topology of the nodes closed in this block (their node_box rows were written at merge time)
   const int nclosed = min( kBuildThreads, m - 1 - bbase );  // internal nodes bbase .. bbase + nclosed - 1
-  for ( int k = tid; k < nclosed * C; k += kBuildThreads )
-  {
-    // the row of node q = k / C holds C (min, max) pairs in the order (axis, side); pair t = k % C
-    const int q = k / C, t = k % C;
-    if ( s_rng[q].x < 0 ) continue;
-    const int2 cr = s_cref[q];
-    const int a = t >> 1, sd = t & 1;
-    const int rf = sd ? cr.y : cr.x;
-    io::store2( node_box + ( static_cast< size_t >( bbase + q ) * D + a ) * 4 + sd * 2, box( rf, 2 * a ),
-                box( rf, 2 * a + 1 ) );
-  }
   if ( tid < nclosed && s_rng[tid].x >= 0 )
   {
     reinterpret_cast< int2 * >( child )[bbase + tid] = s_child[tid];
@@ -718,7 +697,7 @@ cudaError_t launch_build_t(uint64_t n, const uint64_t *keys, const void *bucket_
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
   if ( m <= 1 ) return cudaSuccess;  // the slab kernel stored a one-bucket object's root
   const unsigned grid = static_cast< unsigned >( ( m + kBuildThreads - 1 ) / kBuildThreads );
-  const size_t smem = static_cast< size_t >( 2 * kBuildThreads ) * ( 2 * ( K / 2 ) + 1 ) * sizeof( T );  // [W * 64][C + 1]
+  const size_t smem = static_cast< size_t >( kBuildThreads ) * ( 2 * ( K / 2 ) + 1 ) * sizeof( T );  // [rows][C + 1]
   const cudaError_t e = cudaFuncSetAttribute( k_build_leaf< K, T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast< int >( smem ) );
   if ( e != cudaSuccess ) return e;
