@@ -46,6 +46,9 @@ def parse():
     p.add_argument("--ny", type=int, default=1024)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", default="sphere_plate", choices=["sphere_plate", "tet_lattice"],
+                   help="tet_lattice: the precision-form case (26-DOP, FP32 filter vs FP64 plain) instead")
+    p.add_argument("--lattice", type=int, default=256, help="tet_lattice cells per axis (256 = 16,777,216 tets)")
     return p.parse_args()
 
 
@@ -314,6 +317,90 @@ def run_gpu(args, world, rank, local):
     return result, sphere, plate
 
 
+def run_precision(args, world, rank, local):
+    """Precision-form case: one tetrahedron per cell of a jittered lattice^3 (vertex jitter +-0.3 cell, scale
+    LogNormal(0, 0.4)), split as a checkerboard into objects A ((i+j+k) even) and B (odd), 26-DOP, inter-object
+    pairs. FP64 plain and FP32 filter + FP64 recheck, device-resident; the two pair sets compared on the device;
+    the FP32 slab enclosure error against the FP64 slabs over all of object A."""
+    import torch
+    import distbvh_b200 as bvhg
+    from distbvh_b200 import meshes
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    m = args.lattice
+    xyz = meshes.tet_lattice(m)
+    even = meshes.checkerboard(m)
+    a_np, b_np = np.ascontiguousarray(xyz[even]), np.ascontiguousarray(xyz[~even])
+    del xyz
+    d_a, d_b = torch.from_numpy(a_np).to(dev), torch.from_numpy(b_np).to(dev)
+    prims = a_np.shape[0] + b_np.shape[0]
+    stream = torch.cuda.Stream(device=dev)
+    k = 26
+
+    def run(precision):
+        ctx = bvhg.Context(k=k, precision=precision, device=local, stream=stream.cuda_stream)
+        oa, ob = ctx.object(), ctx.object()
+
+        def step(cap, out):
+            ctx.set_elements(oa, d_a, mem=bvhg.MEM_DEVICE)
+            ctx.set_elements(ob, d_b, mem=bvhg.MEM_DEVICE)
+            ctx.build(oa)
+            ctx.build(ob)
+            return ctx.broadphase_raw(oa, ob, out.data_ptr() if out is not None else None, cap, bvhg.MEM_DEVICE)
+
+        st, cnt = step(0, None)  # count only
+        out = torch.empty((max(cnt, 1), 2), dtype=torch.int64, device=dev)
+        for _ in range(args.warmup):
+            st, cnt = step(out.shape[0], out)
+            assert st == 0, st
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            st, cnt = step(out.shape[0], out)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+        cand = ctx.last_candidates() if precision == bvhg.FILTER_FP32 else cnt
+        return ctx, oa, ms, cnt, cand, out[:cnt]
+
+    ctx64, oa64, ms64, n64, _, p64 = run(bvhg.PLAIN_FP64)
+    ctx32, oa32, ms32, n32, cand32, p32 = run(bvhg.FILTER_FP32)
+    key64 = torch.sort(p64[:, 0] * (1 << 32) + p64[:, 1])[0]
+    key32 = torch.sort(p32[:, 0] * (1 << 32) + p32[:, 1])[0]
+    same = n64 == n32 and bool(torch.equal(key64, key32))
+    # FP32 enclosure error over object A: lo32 <= lo64 and hi64 <= hi32 on every slab
+    na = a_np.shape[0]
+    s64 = ctx64.kdops(oa64, na)
+    s32 = ctx32.kdops(oa32, na).astype(np.float64)
+    err_lo, err_hi = s64[:, :, 0] - s32[:, :, 0], s32[:, :, 1] - s64[:, :, 1]
+    width = s64[:, :, 1] - s64[:, :, 0]
+    err = np.concatenate([err_lo.ravel(), err_hi.ravel()])
+    rel = np.concatenate([(err_lo / width).ravel(), (err_hi / width).ravel()])
+    bound = {"elements": int(na), "slabs_per_element": k // 2, "violations": int((err < 0).sum()),
+             "max_abs": float(err.max()), "mean_abs": float(err.mean()),
+             "max_rel_width": float(rel.max()), "mean_rel_width": float(rel.mean())}
+    del s64, s32, err_lo, err_hi, width, err, rel
+    ctx64.close()
+    ctx32.close()
+    return {
+        "metric": METRIC, "value": prims * world / (ms32 * 1e-3) / 1e6, "unit": "Mprims/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded tet lattice)",
+        "config": {"workload": f"tet_lattice: {m}^3 jittered cells, one tet each ({prims} tets), checkerboard "
+                               f"objects A/B, 26-DOP", "k": k, "epsilon": 0.0, "elements": prims,
+                   "l2": "inputs larger than L2"},
+        "form": "FP32 filter + FP64 recheck (value); FP64 plain below",
+        "fp64_plain": {"ms_per_step": ms64, "value": prims * world / (ms64 * 1e-3) / 1e6, "pairs": int(n64)},
+        "filter_fp32": {"ms_per_step": ms32, "pairs": int(n32), "candidates": int(cand32), "same_pair_set": same,
+                        "speedup_vs_fp64": ms64 / ms32,
+                        "false_positive_rate": (cand32 - n32) / cand32 if cand32 else 0.0},
+        "fp32_bound_error": bound,
+    }
+
+
 def cpu_baseline_sample(sphere_level=8, nx=1024, ny=512, threads=0):
     """The reference's algorithms on all host cores over a quarter-size sample of the same scene."""
     from oracle import oracle as orc
@@ -368,6 +455,14 @@ def main():
         out = run_reference(args, world, rank)
         if out is not None:
             print(json.dumps(out))
+        return
+    if args.workload == "tet_lattice":
+        result = run_precision(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(result))
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     result, _, _ = run_gpu(args, world, rank, local)
     if rank == 0:

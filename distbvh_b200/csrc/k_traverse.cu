@@ -49,13 +49,30 @@ struct slab_pair< float >
   }
 };
 
-__device__ __forceinline__ void emit(uint32_t a, uint32_t b, uint2 *pairs, uint64_t cap, pair_scalars *ps)
+// Slots for k outputs of each calling lane, one atomic per group of converged lanes: the lanes' exclusive prefix of
+// k is formed from one ballot per bit of k (k < 64), the lowest lane reserves the group's total.
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned k, unsigned long long *counter)
 {
-  const unsigned long long p = atomicAdd( &ps->count, 1ull );
-  if ( p < cap ) pairs[p] = make_uint2( a, b );
+  const unsigned active = __activemask();
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = ( 1u << lane ) - 1u;
+  unsigned pre = 0, tot = 0;
+#pragma unroll
+  for ( int bit = 0; bit < 6; ++bit )
+  {
+    const unsigned bal = __ballot_sync( active, ( k >> bit ) & 1u );
+    pre += static_cast< unsigned >( __popc( bal & lt ) ) << bit;
+    tot += static_cast< unsigned >( __popc( bal ) ) << bit;
+  }
+  const int leader = __ffs( active ) - 1;
+  unsigned long long base = 0;
+  if ( static_cast< int >( lane ) == leader && tot ) base = atomicAdd( counter, static_cast< unsigned long long >( tot ) );
+  base = __shfl_sync( active, base, leader );
+  return base + pre;
 }
 
-// The elements of target bucket bb against the query slabs (ranks > skip only, for self-collision).
+// The elements of target bucket bb against the query slabs (ranks > skip only, for self-collision). The hits are
+// collected first and stored through one warp-aggregated reservation; pairs beyond capacity are counted only.
 template< int D, typename T >
 __device__ __forceinline__ void test_bucket(const T *qlo, const T *qhi, uint32_t qe, int bb, int nt, int skip,
                                             const T *__restrict__ telem, const uint32_t *__restrict__ tperm,
@@ -63,6 +80,7 @@ __device__ __forceinline__ void test_bucket(const T *qlo, const T *qhi, uint32_t
 {
   const int r0 = max( kLeafSize * bb, skip + 1 );
   const int r1 = min( kLeafSize * bb + kLeafSize, nt );
+  unsigned hits = 0;
   for ( int r = r0; r < r1; ++r )
   {
     const T *eb = telem + static_cast< size_t >( r ) * D * 2;
@@ -73,8 +91,11 @@ __device__ __forceinline__ void test_bucket(const T *qlo, const T *qhi, uint32_t
       if ( !o ) break;
       o = qlo[a] < __ldg( eb + 2 * a + 1 ) && __ldg( eb + 2 * a ) < qhi[a];
     }
-    if ( o ) emit( qe, __ldg( tperm + r ), pairs, cap, ps );
+    if ( o ) hits |= 1u << ( r - r0 );
   }
+  unsigned long long pos = warp_reserve( static_cast< unsigned >( __popc( hits ) ), &ps->count );
+  for ( ; hits; hits &= hits - 1, ++pos )
+    if ( pos < cap ) pairs[pos] = make_uint2( qe, __ldg( tperm + r0 + __ffs( hits ) - 1 ) );
 }
 
 template< int K, typename T >
@@ -261,11 +282,8 @@ __global__ void __launch_bounds__( 256 ) k_recheck(const double *__restrict__ va
         ok = alo < bhi && blo < ahi;
       }
     }
-    if ( ok )
-    {
-      const unsigned long long o = atomicAdd( &ps->count2, 1ull );
-      if ( o < cap ) out[o] = c;
-    }
+    const unsigned long long o = warp_reserve( ok ? 1u : 0u, &ps->count2 );
+    if ( ok && o < cap ) out[o] = c;
   }
 }
 

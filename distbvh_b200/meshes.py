@@ -138,6 +138,12 @@ def tet_lattice(m, seed=3, jitter=0.3, sigma=0.4):
     return c + (t - c) * s
 
 
+def checkerboard(m):
+    """Object membership of the tet_lattice cells: True for (i + j + k) even (object A), False for odd (B)."""
+    idx = np.arange(m ** 3, dtype=np.int64)
+    return ((idx % m + (idx // m) % m + idx // (m * m)) & 1) == 0
+
+
 def random_soup(n, V=3, seed=0, box=1.0, size=0.05, stream=0):
     """n random elements of V vertices: centre U(0, box)^3, each vertex within +-size of the centre."""
     c = uniform(seed, 3 * stream + 1, 3 * n).reshape(n, 1, 3) * box

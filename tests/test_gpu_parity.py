@@ -358,3 +358,23 @@ def test_gpu_matches_reference_vectors(case, k):
         else:
             assert got.shape[0] == int(g(f"tree_count{k}"))
             assert np.array_equal(self_got, orc.canonical(np.sort(g(f"self{k}"), axis=1)))
+
+
+def test_precision_form_on_the_tet_lattice():
+    """The precision-form case at small size: a jittered 20^3 tet lattice, checkerboard objects, 26-DOP. FP64
+    plain and FP32 filter + recheck both give the oracle's pair set; FP32 slabs enclose the FP64 slabs."""
+    m = 20
+    xyz = meshes.tet_lattice(m)
+    even = meshes.checkerboard(m)
+    a, b = np.ascontiguousarray(xyz[even]), np.ascontiguousarray(xyz[~even])
+    want = orc.pair_set(a, b, 26)
+    assert want.shape[0] > a.shape[0]  # dense contact: every tet overlaps several neighbours
+    with bvhg.Context(k=26) as c64, bvhg.Context(k=26, precision=bvhg.FILTER_FP32) as c32:
+        a64, b64 = build_pair(c64, a, b)
+        a32, b32 = build_pair(c32, a, b)
+        assert np.array_equal(orc.canonical(c64.broadphase(a64, b64)), want)
+        assert np.array_equal(orc.canonical(c32.broadphase(a32, b32)), want)
+        assert c32.last_candidates() >= want.shape[0]
+        s64 = c64.kdops(a64, a.shape[0])
+        s32 = c32.kdops(a32, a.shape[0]).astype(np.float64)
+        assert (s32[:, :, 0] <= s64[:, :, 0]).all() and (s64[:, :, 1] <= s32[:, :, 1]).all()
