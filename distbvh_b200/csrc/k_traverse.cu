@@ -98,6 +98,11 @@ __device__ __forceinline__ void test_bucket(const T *qlo, const T *qhi, uint32_t
     if ( pos < cap ) pairs[pos] = make_uint2( qe, __ldg( tperm + r0 + __ffs( hits ) - 1 ) );
 }
 
+// One warp per group of 32 query ranks (a packet), lane = query element. The warp walks the target tree once for
+// its packet: every lane tests its own element's slabs against both children of the current node (the node row is
+// read once for the warp, a broadcast), and a child is entered with the mask of the lanes that overlap it (a lane
+// that misses a node misses all of its descendants). Stack entries are (node, lane mask), in shared memory. At a
+// leaf bucket the lanes of the mask test their element against the bucket's elements.
 template< int K, typename T >
 __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict__ qwarp,
                                                            const T *__restrict__ qelem,
@@ -113,15 +118,18 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
 {
   constexpr int D = K / 2;
   constexpr int D0 = D < 4 ? D : 4;
+  constexpr int WPB = kTravThreads / 32;
+  __shared__ int2 s_stack[WPB][kStack];  // (node, lane mask)
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31u;
+  int2 *stack = s_stack[threadIdx.x >> 5];
   // No tree exists after a failed sort of either object.
   if ( *reinterpret_cast< const volatile int * >( &tsc->error ) == kErrTimeout ||
        *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
     return;
-  if ( ( i & ~31u ) >= nq ) return;  // warps entirely past the last rank have no group box
+  if ( ( i & ~31u ) >= nq ) return;  // warps entirely past the last rank have no group box (uniform per warp)
   const T *rb = reinterpret_cast< const T * >( tsc->root_box );
-  // 1. The union box of this warp's 32 query ranks against the target's root box, first four slabs first: a warp
-  //    of queries far from the other object stops after one broadcast load.
+  // 1. The packet's union box against the target's root box, first four slabs first (uniform per warp).
   {
     const T *wb = qwarp + static_cast< size_t >( i >> 5 ) * D * 2;
     bool o = true;
@@ -132,77 +140,95 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
     for ( int a = D0; a < D; ++a ) o = o && ( __ldg( wb + 2 * a ) < rb[2 * a + 1] && rb[2 * a] < __ldg( wb + 2 * a + 1 ) );
     if ( !o ) return;
   }
-  if ( i >= nq ) return;
-  // 2. The query's own slabs against the root box.
+  // 2. Each lane's own slabs against the root box.
+  const bool valid = i < nq;
   T qlo[D], qhi[D];
+  bool in_root = valid;
   {
-    const T *qs = qelem + static_cast< size_t >( i ) * D * 2;
-    bool o = true;
+    const T *qs = qelem + static_cast< size_t >( valid ? i : 0 ) * D * 2;
 #pragma unroll
     for ( int a = 0; a < D; ++a )
     {
-      qlo[a] = __ldg( qs + 2 * a );
-      qhi[a] = __ldg( qs + 2 * a + 1 );
-      o = o && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
+      qlo[a] = valid ? __ldg( qs + 2 * a ) : T( 0 );
+      qhi[a] = valid ? __ldg( qs + 2 * a + 1 ) : T( 0 );
+      in_root = in_root && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
     }
-    if ( !o ) return;
   }
-  const uint32_t qe = __ldg( qperm + i );
+  unsigned mask = __ballot_sync( 0xffffffffu, in_root );
+  if ( !mask ) return;
+  const uint32_t qe = valid ? __ldg( qperm + i ) : 0u;
   const int skip = self ? static_cast< int >( i ) : -1;  // self-collision: only ranks above the query's
   const int root = tsc->root;
   if ( root < 0 )
   {
-    test_bucket< D >( qlo, qhi, qe, ~root, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
+    if ( in_root ) test_bucket< D >( qlo, qhi, qe, ~root, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
     return;
   }
-  int stack[kStack];
   int sp = 0;
   int node = root;
   while ( true )
   {
+    const bool me = ( mask >> lane ) & 1u;
     const int2 c = __ldg( child + node );
     const T *nb = nbox + static_cast< size_t >( node ) * D * 4;
-    bool o0 = true, o1 = true;
+    bool o0 = me, o1 = me;
     if ( self )
     {
       // left child covers buckets [l, node], right child [node + 1, r]; skip subtrees whose last rank <= i
-      o0 = kLeafSize * node + kLeafSize - 1 > static_cast< int >( i );
-      o1 = min( kLeafSize * __ldg( &range[node].y ) + kLeafSize - 1, static_cast< int >( nt ) - 1 ) > static_cast< int >( i );
+      o0 = o0 && kLeafSize * node + kLeafSize - 1 > static_cast< int >( i );
+      o1 = o1 && min( kLeafSize * __ldg( &range[node].y ) + kLeafSize - 1, static_cast< int >( nt ) - 1 ) > static_cast< int >( i );
     }
 #pragma unroll
     for ( int a = 0; a < D; ++a )
     {
-      if ( !( o0 || o1 ) ) break;
-      const slab_pair< T > s = slab_pair< T >::load( nb + a * 4 );
-      o0 = o0 && ( qlo[a] < s.max0 && s.min0 < qhi[a] );
-      o1 = o1 && ( qlo[a] < s.max1 && s.min1 < qhi[a] );
+      if ( !__any_sync( 0xffffffffu, o0 || o1 ) ) break;
+      const slab_pair< T > sl = slab_pair< T >::load( nb + a * 4 );
+      o0 = o0 && ( qlo[a] < sl.max0 && sl.min0 < qhi[a] );
+      o1 = o1 && ( qlo[a] < sl.max1 && sl.min1 < qhi[a] );
     }
+    const unsigned m0 = __ballot_sync( 0xffffffffu, o0 );
+    const unsigned m1 = __ballot_sync( 0xffffffffu, o1 );
     int next = -1;
-    if ( o0 )
+    unsigned nmask = 0;
+    if ( m0 )
     {
-      if ( c.x < 0 ) test_bucket< D >( qlo, qhi, qe, ~c.x, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
-      else next = c.x;
-    }
-    if ( o1 )
-    {
-      if ( c.y < 0 ) test_bucket< D >( qlo, qhi, qe, ~c.y, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
-      else if ( next < 0 ) next = c.y;
-      else
+      if ( c.x < 0 )
       {
+        if ( o0 ) test_bucket< D >( qlo, qhi, qe, ~c.x, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
+      } else {
+        next = c.x;
+        nmask = m0;
+      }
+    }
+    if ( m1 )
+    {
+      if ( c.y < 0 )
+      {
+        if ( o1 ) test_bucket< D >( qlo, qhi, qe, ~c.y, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
+      } else if ( next < 0 ) {
+        next = c.y;
+        nmask = m1;
+      } else {
         if ( sp == kStack )
         {
-          atomicCAS( &ps->error, 0, kErrOverflowStack );
+          if ( lane == 0 ) atomicCAS( &ps->error, 0, kErrOverflowStack );
           return;
         }
-        stack[sp++] = c.y;
+        if ( lane == 0 ) stack[sp] = make_int2( c.y, static_cast< int >( m1 ) );
+        ++sp;
       }
     }
     if ( next < 0 )
     {
       if ( sp == 0 ) break;
-      next = stack[--sp];
+      __syncwarp();
+      const int2 e = stack[--sp];
+      next = e.x;
+      nmask = static_cast< unsigned >( e.y );
     }
+    __syncwarp();
     node = next;
+    mask = nmask;
   }
 }
 
