@@ -79,8 +79,8 @@ __host__ __device__ inline double ord_decode(unsigned long long e)
 
 // Radix sort geometry: 63 significant key bits (morton64 never sets bit 63, hash.hpp:100-103).
 constexpr int kKeyBits = 63;
-constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
+constexpr int kSortThreads = 512;
+constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;
 inline int sort_passes(int bits) { return ( kKeyBits + bits - 1 ) / bits; }
 

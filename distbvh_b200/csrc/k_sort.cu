@@ -25,7 +25,7 @@ constexpr uint32_t kValueMask = ( 1u << 30 ) - 1;
 constexpr int kWarps = kSortThreads / 32;
 constexpr int kLookback = 8;  // predecessor status words fetched per look-back step
 
-// Exclusive scan of one value per thread over a 256-thread block.
+// Exclusive scan of one value per thread over the block.
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s_warp)
 {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
   constexpr uint32_t MASK = RADIX - 1;
   extern __shared__ __align__( 128 ) unsigned char s_raw[];  // 2 stages of [kSortTile keys][kSortTile indices]
   __shared__ __align__( 8 ) uint64_t s_mbar[2];
-  __shared__ uint32_t s_whist[kWarps][RADIX];
+  __shared__ uint32_t s_whist[kWarps / 2][RADIX];  // warp 2p: low 16 bits, warp 2p + 1: high 16 bits
   __shared__ uint32_t s_gbase[RADIX];
   __shared__ uint32_t s_lstart[RADIX];
   __shared__ uint32_t s_scan[kWarps];
@@ -133,6 +133,7 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
     s_next = static_cast< int >( atomicAdd( &sc->sort_tile_counter[pass], 1u ) );
     s_err = 0;
   }
+  for ( int q = tid; q < ( kWarps / 2 ) * RADIX; q += kSortThreads ) ( &s_whist[0][0] )[q] = 0;
   __syncthreads();
   uint32_t tile = static_cast< uint32_t >( s_next );
   // a tile goes through the bulk copy when it is full and the arrays are 16-byte aligned
@@ -198,8 +199,8 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
         v[j] = valid ? ( vals_in ? vals_in[tile_base + li] : tile_base + li ) : 0u;
       }
     }
-    for ( int q = lane; q < RADIX; q += 32 ) s_whist[warp][q] = 0;
-    __syncwarp();
+    const int wrow = warp >> 1, wsh = ( warp & 1 ) * 16;  // s_whist is zero here (cleared before the first tile
+                                                         // and during the previous tile's write-out)
 #pragma unroll
     for ( int j = 0; j < kSortItems; ++j )
     {
@@ -208,7 +209,8 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
       const unsigned peers = __match_any_sync( 0xffffffffu, d );
       const int leader = __ffs( peers ) - 1;
       uint32_t base = 0;
-      if ( valid && lane == leader ) base = atomicAdd( &s_whist[warp][d], static_cast< uint32_t >( __popc( peers ) ) );
+      if ( valid && lane == leader )
+        base = ( atomicAdd( &s_whist[wrow][d], static_cast< uint32_t >( __popc( peers ) ) << wsh ) >> wsh ) & 0xffffu;
       base = __shfl_sync( 0xffffffffu, base, leader );
       const uint32_t rank = base + static_cast< uint32_t >( __popc( peers & lt_mask ) );
       if ( j & 1 ) rk[j >> 1] |= rank << 16;
@@ -221,11 +223,13 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
     if ( tid < RADIX )
     {
 #pragma unroll
-      for ( int w = 0; w < kWarps; ++w )
+      for ( int w = 0; w < kWarps / 2; ++w )
       {
         const uint32_t c = s_whist[w][tid];
-        s_whist[w][tid] = total;
-        total += c;
+        const uint32_t lo = total;
+        total += c & 0xffffu;
+        s_whist[w][tid] = lo | ( total << 16 );
+        total += c >> 16;
       }
       reinterpret_cast< volatile uint32_t * >( status )[static_cast< size_t >( tile ) * RADIX + tid] =
         ( tile == 0 ? kFlagPrefix : kFlagAggregate ) | total;
@@ -319,12 +323,14 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
       {
         const uint32_t d = digit( k[j] );
         const uint32_t rank = ( rk[j >> 1] >> ( ( j & 1 ) * 16 ) ) & 0xffffu;
-        const uint32_t pos = s_lstart[d] + s_whist[warp][d] + rank;
+        const uint32_t pos = s_lstart[d] + ( ( s_whist[wrow][d] >> wsh ) & 0xffffu ) + rank;
         sk[pos] = k[j];
         sv[pos] = v[j];
       }
     }
     __syncthreads();
+    // the warp histograms were last read by the reorder above: clear them for the next tile
+    for ( int q = tid; q < ( kWarps / 2 ) * RADIX; q += kSortThreads ) ( &s_whist[0][0] )[q] = 0;
     for ( uint32_t i = tid; i < cnt; i += kSortThreads )
     {
       const uint64_t key = sk[i];
