@@ -25,6 +25,7 @@ EXPORTS = (
     "bvhg_get_kdops", "bvhg_get_kdops_f32", "bvhg_get_centroids", "bvhg_validate_tree", "bvhg_last_candidates",
     "bvhg_get_stage_times", "bvhg_launch_count", "bvhg_set_spin_limit", "bvhg_test_stall_sort", "bvhg_debug_normal",
     "bvhg_synchronize", "bvhg_last_error", "bvhg_status_string", "bvhg_radix_sort_noalloc",
+    "bvhg_batch_broadphase", "bvhg_batch_autotune",
 )
 
 
@@ -77,6 +78,8 @@ def _load():
         "bvhg_last_error": (ctypes.c_char_p, [P]),
         "bvhg_status_string": (ctypes.c_char_p, [I32]),
         "bvhg_radix_sort_noalloc": (I32, [P, P, P, U64, P]),
+        "bvhg_batch_broadphase": (I32, [P, U32, P, P, I32, P, U64, P, P, I32]),
+        "bvhg_batch_autotune": (I32, [P, U32, P, P, I32, ctypes.POINTER(U32), ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -206,6 +209,36 @@ class Context:
             raise BvhgError(st, f"overflow: {cnt.value} pairs")
         self._check(st)
         return out[: cnt.value]
+
+    def batch_broadphase(self, scenes, mode=0, capacity=None):
+        """scenes: list of (obj_a, obj_b) (equal ids: self-collision). Returns a list of (m_s, 2) uint64 arrays."""
+        a = np.ascontiguousarray([x[0] for x in scenes], dtype=np.int32)
+        b = np.ascontiguousarray([x[1] for x in scenes], dtype=np.int32)
+        n = len(scenes)
+        counts = np.zeros(n, dtype=np.uint64)
+        offsets = np.zeros(n, dtype=np.uint64)
+        if capacity is None:
+            st = lib.bvhg_batch_broadphase(self._h, n, a.ctypes.data, b.ctypes.data, mode, None, 0,
+                                           counts.ctypes.data, offsets.ctypes.data, MEM_HOST)
+            if st not in (0, ERR_OVERFLOW):
+                self._check(st)
+            capacity = int(counts.sum())
+        out = np.empty((max(capacity, 1), 2), dtype=np.uint64)
+        self._check(lib.bvhg_batch_broadphase(self._h, n, a.ctypes.data, b.ctypes.data, mode, out.ctypes.data,
+                                              capacity, counts.ctypes.data, offsets.ctypes.data, MEM_HOST))
+        return [out[int(o):int(o) + int(c)] for o, c in zip(offsets, counts)]
+
+    def batch_broadphase_raw(self, a_ptr, b_ptr, n, mode, out_ptr, capacity, counts_ptr, mem):
+        return lib.bvhg_batch_broadphase(self._h, n, a_ptr, b_ptr, mode, out_ptr, capacity, counts_ptr, None, mem)
+
+    def batch_autotune(self, scenes, mode=0):
+        a = np.ascontiguousarray([x[0] for x in scenes], dtype=np.int32)
+        b = np.ascontiguousarray([x[1] for x in scenes], dtype=np.int32)
+        lanes = ctypes.c_uint32()
+        ms = ctypes.c_double()
+        self._check(lib.bvhg_batch_autotune(self._h, len(scenes), a.ctypes.data, b.ctypes.data, mode,
+                                            ctypes.byref(lanes), ctypes.byref(ms)))
+        return lanes.value, ms.value
 
     def morton(self, obj, n):
         keys = np.empty(n, dtype=np.uint64)

@@ -88,6 +88,42 @@ struct object
   const uint32_t *sorted_vals() const { return sort_result_alt ? vals_alt.as< uint32_t >() : vals.as< uint32_t >(); }
 };
 
+// Batching form: every object and scene of a batch as one CUDA graph (builds and traversals spread over lanes of
+// concurrent streams, no host round trip between scenes), captured once per batch layout and replayed.
+struct batch_state
+{
+  std::vector< uint64_t > key;  // layout the graph was captured for
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int lanes = 16;  // concurrent streams (bvhg_batch_autotune picks it)
+  std::vector< cudaStream_t > lane;
+  std::vector< cudaEvent_t > obj_done, lane_done;
+  cudaEvent_t fork = nullptr;
+  dev_buf cand, exact, out, ps, err_src, err_words;
+  std::vector< uint64_t > cap, off;  // per scene: pair capacity and offset into cand / exact / out
+  pair_scalars *host_ps = nullptr;
+  int *host_err = nullptr;
+  size_t host_scenes = 0, host_objs = 0;
+  void drop_graph()
+  {
+    if ( exec ) cudaGraphExecDestroy( exec );
+    if ( graph ) cudaGraphDestroy( graph );
+    exec = nullptr;
+    graph = nullptr;
+    key.clear();
+  }
+  ~batch_state()
+  {
+    drop_graph();
+    for ( auto st : lane ) cudaStreamDestroy( st );
+    for ( auto e : obj_done ) cudaEventDestroy( e );
+    for ( auto e : lane_done ) cudaEventDestroy( e );
+    if ( fork ) cudaEventDestroy( fork );
+    if ( host_ps ) cudaFreeHost( host_ps );
+    if ( host_err ) cudaFreeHost( host_err );
+  }
+};
+
 struct timed_stage
 {
   int stage;
@@ -119,6 +155,7 @@ struct bvhg_ctx
   double stage_ms[BVHG_NUM_STAGES] = {};
   uint64_t stage_launches[BVHG_NUM_STAGES] = {};
   uint64_t launches = 0;
+  std::unique_ptr< batch_state > batch;
 };
 
 namespace {
@@ -251,6 +288,40 @@ bvhg_status check_scalar_errors(bvhg_ctx *ctx, const object &o)
 
 bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s);
 
+// Device buffers of an object's rebuild for its present element count (no allocation when they suffice).
+bvhg_status reserve_object(bvhg_ctx *ctx, object &o)
+{
+  const uint64_t n = o.n;
+  const int D = ctx->cfg.k / 2;
+  const size_t sb = slab_bytes( ctx );
+  const int bits = ctx->cfg.sort_digit_bits;
+  const int passes = sort_passes( bits );
+  const uint64_t radix = 1ull << bits;
+  const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
+  BVHG_CUDA( ctx, o.scal.reserve( sizeof( obj_scalars ) ) );
+  BVHG_CUDA( ctx, o.cx.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.cy.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.cz.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.keys.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.keys_alt.reserve( n * 8 ) );
+  BVHG_CUDA( ctx, o.vals.reserve( n * 4 ) );
+  BVHG_CUDA( ctx, o.vals_alt.reserve( n * 4 ) );
+  BVHG_CUDA( ctx, o.hist.reserve( passes * radix * 4 ) );
+  BVHG_CUDA( ctx, o.status.reserve( passes * ( tiles + 1 ) * radix * 4 ) );
+  const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;  // leaf buckets
+  BVHG_CUDA( ctx, o.elem_box.reserve( n * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.bucket_box.reserve( m * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.node_box.reserve( ( m - 1 ) * D * 4 * sb + 16 ) );
+  BVHG_CUDA( ctx, o.child.reserve( ( m - 1 ) * 8 + 8 ) );
+  BVHG_CUDA( ctx, o.range.reserve( ( m - 1 ) * 8 + 8 ) );
+  BVHG_CUDA( ctx, o.parent.reserve( ( 2 * m ) * 4 ) );
+  BVHG_CUDA( ctx, o.exch.reserve( m * 4 ) );
+  BVHG_CUDA( ctx, o.queue.reserve( m * 16 ) );
+  return BVHG_OK;
+}
+
+
 bvhg_status do_build(bvhg_ctx *ctx, object &o, int mode)
 {
   const uint64_t n = o.n;
@@ -314,27 +385,11 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   const int passes = sort_passes( bits );
   const uint64_t radix = 1ull << bits;
   const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
-  // capacity
-  BVHG_CUDA( ctx, o.scal.reserve( sizeof( obj_scalars ) ) );
-  BVHG_CUDA( ctx, o.cx.reserve( n * 8 ) );
-  BVHG_CUDA( ctx, o.cy.reserve( n * 8 ) );
-  BVHG_CUDA( ctx, o.cz.reserve( n * 8 ) );
-  BVHG_CUDA( ctx, o.keys.reserve( n * 8 ) );
-  BVHG_CUDA( ctx, o.keys_alt.reserve( n * 8 ) );
-  BVHG_CUDA( ctx, o.vals.reserve( n * 4 ) );
-  BVHG_CUDA( ctx, o.vals_alt.reserve( n * 4 ) );
-  BVHG_CUDA( ctx, o.hist.reserve( passes * radix * 4 ) );
-  BVHG_CUDA( ctx, o.status.reserve( passes * ( tiles + 1 ) * radix * 4 ) );
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;  // leaf buckets
-  BVHG_CUDA( ctx, o.elem_box.reserve( n * D * 2 * sb ) );
-  BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
-  BVHG_CUDA( ctx, o.bucket_box.reserve( m * D * 2 * sb ) );
-  BVHG_CUDA( ctx, o.node_box.reserve( ( m - 1 ) * D * 4 * sb + 16 ) );
-  BVHG_CUDA( ctx, o.child.reserve( ( m - 1 ) * 8 + 8 ) );
-  BVHG_CUDA( ctx, o.range.reserve( ( m - 1 ) * 8 + 8 ) );
-  BVHG_CUDA( ctx, o.parent.reserve( ( 2 * m ) * 4 ) );
-  BVHG_CUDA( ctx, o.exch.reserve( m * 4 ) );
-  BVHG_CUDA( ctx, o.queue.reserve( m * 16 ) );
+  {
+    const bvhg_status rs = reserve_object( ctx, o );
+    if ( rs != BVHG_OK ) return rs;
+  }
   {
     stage_scope st( ctx, BVHG_STAGE_BOUNDS );
     BVHG_CUDA( ctx, cudaMemcpyAsync( o.sc(), ctx->init_template, sizeof( obj_scalars ), cudaMemcpyHostToDevice, s ) );
@@ -516,6 +571,244 @@ bvhg_status emit_pairs(bvhg_ctx *ctx, const object &a, const object &b, bool sel
   return BVHG_OK;
 }
 
+
+// ---- batching form ---------------------------------------------------------------------------------------------
+
+struct batch_args
+{
+  uint32_t nscenes;
+  const int32_t *a, *b;
+  int mode;
+};
+
+// Captures the graph of one batch: all unique objects' builds, then every scene's traversal (+ recheck) and gid
+// mapping into its own slot of the batch buffers, then the gather of the objects' error words.
+bvhg_status capture_batch(bvhg_ctx *ctx, batch_state &B, const batch_args &x, const std::vector< int32_t > &uniq,
+                          const std::vector< int > &slot)
+{
+  const int K = ctx->cfg.k;
+  const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
+  const int L = B.lanes;
+  while ( static_cast< int >( B.lane.size() ) < L )
+  {
+    cudaStream_t st = nullptr;
+    BVHG_CUDA( ctx, cudaStreamCreateWithFlags( &st, cudaStreamNonBlocking ) );
+    B.lane.push_back( st );
+    cudaEvent_t e = nullptr;
+    BVHG_CUDA( ctx, cudaEventCreateWithFlags( &e, cudaEventDisableTiming ) );
+    B.lane_done.push_back( e );
+  }
+  while ( B.obj_done.size() < uniq.size() )
+  {
+    cudaEvent_t e = nullptr;
+    BVHG_CUDA( ctx, cudaEventCreateWithFlags( &e, cudaEventDisableTiming ) );
+    B.obj_done.push_back( e );
+  }
+  if ( !B.fork ) BVHG_CUDA( ctx, cudaEventCreateWithFlags( &B.fork, cudaEventDisableTiming ) );
+  B.drop_graph();
+  const uint32_t flags = ctx->cfg.flags;
+  ctx->cfg.flags &= ~BVHG_FLAG_STAGE_TIMING;  // no timing events inside a graph
+  cudaStream_t s = ctx->stream;
+  BVHG_CUDA( ctx, cudaStreamBeginCapture( s, cudaStreamCaptureModeRelaxed ) );
+  auto body = [&]() -> bvhg_status {
+    pair_scalars *ps = B.ps.as< pair_scalars >();
+    BVHG_CUDA( ctx, cudaMemsetAsync( ps, 0, x.nscenes * sizeof( pair_scalars ), s ) );
+    BVHG_CUDA( ctx, cudaEventRecord( B.fork, s ) );
+    for ( int l = 0; l < L; ++l ) BVHG_CUDA( ctx, cudaStreamWaitEvent( B.lane[l], B.fork, 0 ) );
+    for ( size_t i = 0; i < uniq.size(); ++i )
+    {
+      object &o = *ctx->objs[uniq[i]];
+      cudaStream_t ls = B.lane[i % L];
+      if ( o.n > 0 )
+      {
+        const bvhg_status st = do_build_on( ctx, o, x.mode, ls );
+        if ( st != BVHG_OK ) return st;
+      } else {
+        o.built = true;
+      }
+      BVHG_CUDA( ctx, cudaEventRecord( B.obj_done[i], ls ) );
+    }
+    for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
+    {
+      cudaStream_t ls = B.lane[sc % L];
+      object &oa = *ctx->objs[x.a[sc]];
+      object &ob = *ctx->objs[x.b[sc]];
+      BVHG_CUDA( ctx, cudaStreamWaitEvent( ls, B.obj_done[slot[x.a[sc]]], 0 ) );
+      BVHG_CUDA( ctx, cudaStreamWaitEvent( ls, B.obj_done[slot[x.b[sc]]], 0 ) );
+      const bool self = x.a[sc] == x.b[sc];
+      if ( oa.n == 0 || ob.n == 0 || ( self && oa.n < 2 ) ) continue;
+      uint2 *cand = B.cand.as< uint2 >() + B.off[sc];
+      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( oa ), view_of( ob ), self, cand, B.cap[sc], ps + sc, ls ) );
+      const uint2 *fin = cand;
+      const unsigned long long *cnt = &ps[sc].count;
+      if ( fp32 )
+      {
+        uint2 *ex = B.exact.as< uint2 >() + B.off[sc];
+        BVHG_CUDA( ctx, launch_recheck( K, oa.verts, oa.V, ob.verts, ob.V, ctx->cfg.epsilon, cand, B.cap[sc], ex,
+                                        B.cap[sc], ps + sc, ls ) );
+        fin = ex;
+        cnt = &ps[sc].count2;
+      }
+      BVHG_CUDA( ctx, launch_gid_pairs_dev( fin, cnt, B.cap[sc], oa.gid, ob.gid, self,
+                                            B.out.as< uint64_t >() + 2 * B.off[sc], ls ) );
+      ctx->launches += fp32 ? 3 : 2;
+    }
+    for ( int l = 0; l < L; ++l )
+    {
+      BVHG_CUDA( ctx, cudaEventRecord( B.lane_done[l], B.lane[l] ) );
+      BVHG_CUDA( ctx, cudaStreamWaitEvent( s, B.lane_done[l], 0 ) );
+    }
+    BVHG_CUDA( ctx, launch_gather_words( B.err_src.as< const int *const >(), static_cast< int >( uniq.size() ),
+                                         B.err_words.as< int >(), s ) );
+    return BVHG_OK;
+  };
+  const bvhg_status st = body();
+  ctx->cfg.flags = flags;
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture( s, &g );
+  if ( st != BVHG_OK )
+  {
+    if ( g ) cudaGraphDestroy( g );
+    return st;
+  }
+  if ( ce != cudaSuccess ) return cuda_fail( ctx, ce, "cudaStreamEndCapture" );
+  B.graph = g;
+  BVHG_CUDA( ctx, cudaGraphInstantiate( &B.exec, B.graph, 0 ) );
+  return BVHG_OK;
+}
+
+// Runs a batch: returns the per-scene exact counts in `counts` (host) and leaves scene sc's pairs in
+// B.out[2 * B.off[sc] ...]. Grows per-scene capacities and recaptures until every scene fits.
+bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
+{
+  if ( !ctx->batch ) ctx->batch = std::make_unique< batch_state >();
+  batch_state &B = *ctx->batch;
+  const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
+  // unique objects in first-use order
+  std::vector< int32_t > uniq;
+  std::vector< int > slot( ctx->objs.size(), -1 );
+  for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
+    for ( int32_t o : { x.a[sc], x.b[sc] } )
+    {
+      if ( !valid_obj( ctx, o ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object in batch" );
+      object &ob = *ctx->objs[o];
+      if ( !ob.has_data ) return fail( ctx, BVHG_ERR_STATE, "batch object without element data" );
+      if ( x.mode == BVHG_REFIT && ob.n > 0 && !ob.topo ) return fail( ctx, BVHG_ERR_STATE, "refit without a rebuild" );
+      if ( slot[o] < 0 )
+      {
+        slot[o] = static_cast< int >( uniq.size() );
+        uniq.push_back( o );
+      }
+    }
+  for ( int32_t o : uniq )
+  {
+    object &ob = *ctx->objs[o];
+    join_object( ctx, ob );
+    if ( ob.n > 0 && x.mode == BVHG_REBUILD )
+    {
+      const bvhg_status rs = reserve_object( ctx, ob );
+      if ( rs != BVHG_OK ) return rs;
+    }
+  }
+  // per-scene capacities: the last run's if the batch has the same scenes, else an estimate
+  const bool same_scenes = B.cap.size() == x.nscenes && B.key.size() > 3 && B.key[1] == x.nscenes;
+  if ( !same_scenes )
+  {
+    B.cap.assign( x.nscenes, 0 );
+    for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
+      B.cap[sc] = 1024 + 2 * ( ctx->objs[x.a[sc]]->n + ctx->objs[x.b[sc]]->n );
+  }
+  for ( int attempt = 0; attempt < 4; ++attempt )
+  {
+    B.off.assign( x.nscenes, 0 );
+    uint64_t total = 0;
+    for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
+    {
+      B.off[sc] = total;
+      total += B.cap[sc];
+    }
+    BVHG_CUDA( ctx, B.cand.reserve( total * sizeof( uint2 ) ) );
+    if ( fp32 ) BVHG_CUDA( ctx, B.exact.reserve( total * sizeof( uint2 ) ) );
+    BVHG_CUDA( ctx, B.out.reserve( total * 16 ) );
+    BVHG_CUDA( ctx, B.ps.reserve( x.nscenes * sizeof( pair_scalars ) ) );
+    BVHG_CUDA( ctx, B.err_words.reserve( uniq.size() * sizeof( int ) ) );
+    BVHG_CUDA( ctx, B.err_src.reserve( uniq.size() * sizeof( void * ) ) );
+    if ( B.host_scenes < x.nscenes )
+    {
+      if ( B.host_ps ) cudaFreeHost( B.host_ps );
+      B.host_ps = nullptr;
+      BVHG_CUDA( ctx, cudaMallocHost( reinterpret_cast< void ** >( &B.host_ps ), x.nscenes * sizeof( pair_scalars ) ) );
+      B.host_scenes = x.nscenes;
+    }
+    if ( B.host_objs < uniq.size() )
+    {
+      if ( B.host_err ) cudaFreeHost( B.host_err );
+      B.host_err = nullptr;
+      BVHG_CUDA( ctx, cudaMallocHost( reinterpret_cast< void ** >( &B.host_err ), uniq.size() * sizeof( int ) ) );
+      B.host_objs = uniq.size();
+    }
+    // graph identity: everything a replay would read from the captured parameters
+    std::vector< uint64_t > key{ static_cast< uint64_t >( x.mode ), x.nscenes, static_cast< uint64_t >( B.lanes ),
+                                 reinterpret_cast< uint64_t >( B.cand.p ), reinterpret_cast< uint64_t >( B.out.p ),
+                                 reinterpret_cast< uint64_t >( B.exact.p ), reinterpret_cast< uint64_t >( B.ps.p ) };
+    for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
+    {
+      key.push_back( static_cast< uint64_t >( x.a[sc] ) );
+      key.push_back( static_cast< uint64_t >( x.b[sc] ) );
+      key.push_back( B.cap[sc] );
+    }
+    std::vector< const int * > srcs;
+    for ( int32_t o : uniq )
+    {
+      const object &ob = *ctx->objs[o];
+      for ( uint64_t v : { ob.n, static_cast< uint64_t >( ob.V ), reinterpret_cast< uint64_t >( ob.verts ),
+                           reinterpret_cast< uint64_t >( ob.gid ), reinterpret_cast< uint64_t >( ob.scal.p ),
+                           reinterpret_cast< uint64_t >( ob.keys.p ), reinterpret_cast< uint64_t >( ob.elem_box.p ),
+                           reinterpret_cast< uint64_t >( ob.node_box.p ) } )
+        key.push_back( v );
+      srcs.push_back( &ob.sc()->error );
+    }
+    if ( key != B.key || !B.exec )
+    {
+      BVHG_CUDA( ctx, cudaMemcpy( B.err_src.p, srcs.data(), srcs.size() * sizeof( void * ), cudaMemcpyHostToDevice ) );
+      const bvhg_status st = capture_batch( ctx, B, x, uniq, slot );
+      if ( st != BVHG_OK ) return st;
+      B.key = key;
+    } else {
+      // a replay rebuilds the same objects: their host-side state is what the capture left
+      for ( int32_t o : uniq ) ctx->objs[o]->built = true;
+    }
+    BVHG_CUDA( ctx, cudaGraphLaunch( B.exec, ctx->stream ) );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( B.host_ps, B.ps.p, x.nscenes * sizeof( pair_scalars ), cudaMemcpyDeviceToHost,
+                                     ctx->stream ) );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( B.host_err, B.err_words.p, uniq.size() * sizeof( int ), cudaMemcpyDeviceToHost,
+                                     ctx->stream ) );
+    BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+    for ( size_t i = 0; i < uniq.size(); ++i )
+    {
+      const bvhg_status st = object_error( ctx, B.host_err[i] );
+      if ( st != BVHG_OK ) return st;
+    }
+    bool grown = false;
+    uint64_t cand_total = 0;
+    for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
+    {
+      const pair_scalars &h = B.host_ps[sc];
+      if ( h.error ) return fail( ctx, BVHG_ERR_CUDA, "traversal stack overflow in batch scene " + std::to_string( sc ) );
+      const uint64_t need = fp32 ? std::max( h.count, h.count2 ) : h.count;
+      cand_total += h.count;
+      counts[sc] = fp32 ? h.count2 : h.count;
+      if ( need > B.cap[sc] )
+      {
+        B.cap[sc] = need + need / 4 + 64;
+        grown = true;
+      }
+    }
+    ctx->last_candidates = cand_total;
+    if ( !grown ) return BVHG_OK;
+  }
+  return fail( ctx, BVHG_ERR_CUDA, "batch pair capacities did not converge" );
+}
 }  // namespace
 
 extern "C" {
@@ -687,6 +980,88 @@ bvhg_status bvhg_broadphase(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, uint64_
   bvhg_status st = find_pairs( ctx, a, b, false, &lp, &np );
   if ( st != BVHG_OK ) return st;
   return emit_pairs( ctx, a, b, false, lp, np, pairs, capacity, count, mem );
+}
+
+bvhg_status bvhg_batch_broadphase(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a, const int32_t *obj_b,
+                                  int32_t mode, uint64_t *pairs, uint64_t capacity, uint64_t *counts,
+                                  uint64_t *offsets, int32_t mem)
+{
+  if ( !ctx ) return BVHG_ERR_ARG;
+  if ( nscenes > 0 && ( !obj_a || !obj_b || !counts ) ) return fail( ctx, BVHG_ERR_ARG, "null scene arrays" );
+  if ( mode != BVHG_REBUILD && mode != BVHG_REFIT ) return fail( ctx, BVHG_ERR_ARG, "bad build mode" );
+  if ( mem != BVHG_MEM_HOST && mem != BVHG_MEM_DEVICE ) return fail( ctx, BVHG_ERR_ARG, "bad memory kind" );
+  if ( capacity > 0 && !pairs ) return fail( ctx, BVHG_ERR_ARG, "null pair buffer" );
+  if ( nscenes == 0 ) return BVHG_OK;
+  cudaSetDevice( ctx->cfg.device );
+  const batch_args x{ nscenes, obj_a, obj_b, mode };
+  bvhg_status st = run_batch( ctx, x, counts );
+  if ( st != BVHG_OK ) return st;
+  // compact the scenes' pairs into the caller's buffer in scene order
+  uint64_t total = 0;
+  for ( uint32_t sc = 0; sc < nscenes; ++sc )
+  {
+    if ( offsets ) offsets[sc] = total;
+    total += counts[sc];
+  }
+  if ( total > capacity ) return fail( ctx, BVHG_ERR_OVERFLOW, "pair buffer too small: " + std::to_string( total ) + " pairs" );
+  batch_state &B = *ctx->batch;
+  uint64_t at = 0;
+  for ( uint32_t sc = 0; sc < nscenes; ++sc )
+  {
+    if ( counts[sc] )
+      BVHG_CUDA( ctx, cudaMemcpyAsync( pairs + 2 * at, B.out.as< uint64_t >() + 2 * B.off[sc], counts[sc] * 16,
+                                       mem == BVHG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                       ctx->stream ) );
+    at += counts[sc];
+  }
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a, const int32_t *obj_b,
+                                int32_t mode, uint32_t *lanes, double *ms)
+{
+  if ( !ctx ) return BVHG_ERR_ARG;
+  if ( nscenes == 0 || !obj_a || !obj_b ) return fail( ctx, BVHG_ERR_ARG, "empty batch" );
+  if ( mode != BVHG_REBUILD && mode != BVHG_REFIT ) return fail( ctx, BVHG_ERR_ARG, "bad build mode" );
+  cudaSetDevice( ctx->cfg.device );
+  if ( !ctx->batch ) ctx->batch = std::make_unique< batch_state >();
+  const batch_args x{ nscenes, obj_a, obj_b, mode };
+  std::vector< uint64_t > counts( nscenes );
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  BVHG_CUDA( ctx, cudaEventCreate( &e0 ) );
+  BVHG_CUDA( ctx, cudaEventCreate( &e1 ) );
+  int best = ctx->batch->lanes;
+  float best_ms = 0.f;
+  bvhg_status st = BVHG_OK;
+  for ( int L : { 1, 4, 8, 16, 32, 64 } )
+  {
+    ctx->batch->lanes = L;
+    st = run_batch( ctx, x, counts.data() );  // captures this lane count's graph and settles the capacities
+    if ( st != BVHG_OK ) break;
+    float t = 0.f;
+    cudaEventRecord( e0, ctx->stream );
+    for ( int r = 0; r < 3; ++r ) cudaGraphLaunch( ctx->batch->exec, ctx->stream );
+    cudaEventRecord( e1, ctx->stream );
+    if ( cudaEventSynchronize( e1 ) != cudaSuccess || cudaEventElapsedTime( &t, e0, e1 ) != cudaSuccess )
+    {
+      st = fail( ctx, BVHG_ERR_CUDA, "autotune timing" );
+      break;
+    }
+    t /= 3.f;
+    if ( best_ms == 0.f || t < best_ms )
+    {
+      best_ms = t;
+      best = L;
+    }
+  }
+  cudaEventDestroy( e0 );
+  cudaEventDestroy( e1 );
+  ctx->batch->lanes = best;
+  ctx->batch->drop_graph();
+  if ( lanes ) *lanes = static_cast< uint32_t >( best );
+  if ( ms ) *ms = best_ms;
+  return st;
 }
 
 bvhg_status bvhg_self_collision(bvhg_ctx *ctx, int32_t obj, uint64_t *pairs, uint64_t capacity, uint64_t *count,

@@ -149,6 +149,14 @@ cudaError_t launch_recheck(int K, const double *verts_a, uint32_t Va, const doub
 
 // Writes pairs as global ids: out[2p] = gid_a[a] (or a), out[2p + 1] = gid_b[b] (or b); normalize orders each
 // pair by local index first (self-collision).
+// Global-id mapping with the pair count read on the device (at most cap); for graph-captured batches.
+cudaError_t launch_gid_pairs_dev(const uint2 *pairs, const unsigned long long *count, uint64_t cap,
+                                 const uint64_t *gid_a, const uint64_t *gid_b, bool normalize, uint64_t *out,
+                                 cudaStream_t s);
+
+// dst[i] = *src[i] for i < n (src: device array of device pointers).
+cudaError_t launch_gather_words(const int *const *src, int n, int *dst, cudaStream_t s);
+
 cudaError_t launch_gid_pairs(const uint2 *pairs, uint64_t count, const uint64_t *gid_a, const uint64_t *gid_b,
                              bool normalize, uint64_t *out, cudaStream_t s);
 

@@ -339,7 +339,50 @@ __global__ void k_gid_pairs(const uint2 *__restrict__ pairs, uint64_t count, con
   }
 }
 
+// k_gid_pairs with the count read on the device (at most cap): for launches whose count is unknown when they are
+// enqueued (batched scenes in a CUDA graph).
+__global__ void k_gid_pairs_dev(const uint2 *__restrict__ pairs, const unsigned long long *count, uint64_t cap,
+                                const uint64_t *__restrict__ gid_a, const uint64_t *__restrict__ gid_b, int normalize,
+                                uint64_t *__restrict__ out)
+{
+  const uint64_t n = min( static_cast< uint64_t >( *reinterpret_cast< const volatile unsigned long long * >( count ) ), cap );
+  for ( uint64_t p = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; p < n;
+        p += static_cast< uint64_t >( gridDim.x ) * blockDim.x )
+  {
+    uint2 c = pairs[p];
+    if ( normalize && c.x > c.y ) c = make_uint2( c.y, c.x );
+    const uint64_t a = gid_a ? __ldg( gid_a + c.x ) : c.x;
+    const uint64_t b = gid_b ? __ldg( gid_b + c.y ) : c.y;
+    reinterpret_cast< ulonglong2 * >( out )[p] = make_ulonglong2( a, b );
+  }
+}
+
+// dst[i] = *src[i]: the error words of many objects in one copy.
+__global__ void k_gather_words(const int *const *__restrict__ src, int n, int *__restrict__ dst)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if ( i < n ) dst[i] = *reinterpret_cast< const volatile int * >( src[i] );
+}
+
 }  // namespace
+
+cudaError_t launch_gid_pairs_dev(const uint2 *pairs, const unsigned long long *count, uint64_t cap,
+                                 const uint64_t *gid_a, const uint64_t *gid_b, bool normalize, uint64_t *out,
+                                 cudaStream_t s)
+{
+  if ( cap == 0 ) return cudaSuccess;
+  const uint64_t blocks = ( cap + 255 ) / 256;
+  const unsigned grid = static_cast< unsigned >( blocks < 148 * 4 ? blocks : 148 * 4 );
+  k_gid_pairs_dev<<< grid, 256, 0, s >>>( pairs, count, cap, gid_a, gid_b, normalize ? 1 : 0, out );
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_words(const int *const *src, int n, int *dst, cudaStream_t s)
+{
+  if ( n == 0 ) return cudaSuccess;
+  k_gather_words<<< ( n + 255 ) / 256, 256, 0, s >>>( src, n, dst );
+  return cudaGetLastError();
+}
 
 cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, uint2 *pairs, uint64_t cap,
                             pair_scalars *ps, cudaStream_t s)

@@ -137,6 +137,25 @@ BVHG_API bvhg_status bvhg_broadphase(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b
 BVHG_API bvhg_status bvhg_self_collision(bvhg_ctx *ctx, int32_t obj, uint64_t *pairs, uint64_t capacity, uint64_t *count,
                                 int32_t mem);
 
+/* Batching form (no single counterpart in the reference: it runs many broadphase(other) calls of
+ * src/bvh/collision_object.cpp:248 at once). Scene s pairs objects obj_a[s] and obj_b[s] (obj_a[s] == obj_b[s]: that
+ * object's self-collision); objects already hold their elements (bvhg_set_elements) and may appear in several
+ * scenes. Every object in the batch is built once (mode: BVHG_REBUILD, or BVHG_REFIT after a rebuild) and every
+ * scene traversed, as one CUDA graph: builds and scenes spread over concurrent streams, no host round trip between
+ * them. The graph is captured on the first call for a batch layout (objects, element counts, vertex pointers,
+ * per-scene capacities) and replayed while the layout stays the same, so a time-stepped loop that updates
+ * coordinates in place replays it. counts[s] (host, required) receives scene s's exact pair count; the pairs go
+ * to `pairs` (mem) scene after scene, (gid_a, gid_b) like bvhg_broadphase, scene s starting at pair offsets[s]
+ * (offsets may be NULL). BVHG_ERR_OVERFLOW when the total exceeds capacity (counts are then still valid). */
+BVHG_API bvhg_status bvhg_batch_broadphase(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a,
+                                          const int32_t *obj_b, int32_t mode, uint64_t *pairs, uint64_t capacity,
+                                          uint64_t *counts, uint64_t *offsets, int32_t mem);
+/* Autotuner of the batching form: times the batch's graph with 1, 4, 8, 16, 32 and 64 concurrent streams and keeps
+ * the fastest for later bvhg_batch_broadphase calls on this context. lanes and ms (may be NULL) receive the choice
+ * and its time per batch. */
+BVHG_API bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a, const int32_t *obj_b,
+                                        int32_t mode, uint32_t *lanes, double *ms);
+
 /* Parity probes (host buffers). sorted_keys[r] and perm[r] (original index of rank r) may be NULL; min3/inv3 are
  * the Morton bounds (3 doubles each, may be NULL). */
 BVHG_API bvhg_status bvhg_get_morton(bvhg_ctx *ctx, int32_t obj, uint64_t *sorted_keys, uint32_t *perm, double *min3,

@@ -1,0 +1,88 @@
+"""Batching form: many independent scenes as one CUDA graph (bvhg_batch_broadphase), against the oracle.
+
+Scenes of uneven sizes (including an empty object and a self-collision scene) must each give the exact pair set
+of the single-scene path; replays of the captured graph after coordinates change in place must too (REBUILD and
+REFIT); the autotuner must pick one of its lane counts and leave the context usable.
+"""
+import numpy as np
+import pytest
+
+import distbvh_b200 as bvhg
+from distbvh_b200 import meshes
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def make_scenes(seed, nscenes, k):
+    rng = np.random.default_rng(seed)
+    bodies = []
+    for s in range(nscenes):
+        n_a, n_b = (int(x) for x in np.exp(rng.uniform(np.log(50), np.log(4000), 2)))
+        size = 0.6 * (n_a + n_b) ** (-1.0 / 3.0)
+        a = meshes.random_soup(n_a, 3, seed=seed * 1000 + 2 * s, size=size)
+        b = meshes.random_soup(n_b, 3, seed=seed * 1000 + 2 * s + 1, size=size, stream=1)
+        bodies.append((a, b))
+    return bodies
+
+
+@pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
+def test_batch_matches_single_scenes(precision):
+    bodies = make_scenes(5, 12, 18)
+    with bvhg.Context(k=18, precision=precision) as ctx:
+        objs = []
+        for a, b in bodies:
+            oa, ob = ctx.object(), ctx.object()
+            ctx.set_elements(oa, a)
+            ctx.set_elements(ob, b)
+            objs.append((oa, ob))
+        empty = ctx.object()
+        ctx.set_elements(empty, np.zeros((0, 3, 3)))
+        scenes = objs + [(objs[0][0], objs[0][0]), (empty, objs[1][1])]
+        for rep in range(2):  # capture, then replay
+            got = ctx.batch_broadphase(scenes)
+            for s, (a, b) in enumerate(bodies):
+                assert np.array_equal(orc.canonical(got[s]), orc.pair_set(a, b, 18)), (rep, s)
+            assert np.array_equal(orc.canonical(got[len(bodies)]), orc.self_pair_set(bodies[0][0], 18))
+            assert got[len(bodies) + 1].shape[0] == 0
+        # the objects are built: single-scene calls agree
+        assert np.array_equal(orc.canonical(ctx.broadphase(*objs[3])), orc.pair_set(*bodies[3], 18))
+
+
+def test_batch_replay_after_motion_rebuild_and_refit():
+    bodies = make_scenes(9, 8, 18)
+    dev = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in bodies]
+    with bvhg.Context(k=18) as ctx:
+        objs = []
+        for da, db in dev:
+            oa, ob = ctx.object(), ctx.object()
+            ctx.set_elements(oa, da)
+            ctx.set_elements(ob, db)
+            objs.append((oa, ob))
+        ctx.batch_broadphase(objs, mode=bvhg.REBUILD)
+        for step, mode in enumerate((bvhg.REFIT, bvhg.REBUILD, bvhg.REFIT)):
+            shift = torch.tensor([0.003 * (step + 1), -0.002, 0.001], dtype=torch.float64, device="cuda")
+            for (da, db) in dev:
+                db += shift  # in place: the borrowed device pointers stay the same, the graph replays
+            torch.cuda.synchronize()
+            got = ctx.batch_broadphase(objs, mode=mode)
+            for s, (da, db) in enumerate(dev):
+                want = orc.pair_set(da.cpu().numpy(), db.cpu().numpy(), 18)
+                assert np.array_equal(orc.canonical(got[s]), want), (step, s)
+
+
+def test_batch_autotune_picks_a_lane_count():
+    bodies = make_scenes(13, 24, 18)
+    with bvhg.Context(k=18) as ctx:
+        objs = []
+        for a, b in bodies:
+            oa, ob = ctx.object(), ctx.object()
+            ctx.set_elements(oa, a)
+            ctx.set_elements(ob, b)
+            objs.append((oa, ob))
+        lanes, ms = ctx.batch_autotune(objs)
+        assert lanes in (1, 4, 8, 16, 32, 64) and ms > 0
+        got = ctx.batch_broadphase(objs)
+        for s, (a, b) in enumerate(bodies):
+            assert np.array_equal(orc.canonical(got[s]), orc.pair_set(a, b, 18))
