@@ -28,6 +28,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# The batching form runs its scenes as parallel branches of one CUDA graph: let the device take up to 32 of them at a
+# time (the default is 8 hardware work queues). Must be set before the process creates its CUDA context.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "build+broadphase Mprims/s, FP32-filter vs FP64 plain on B200, same exact pair set"
 K = 18
@@ -46,8 +49,9 @@ def parse():
     p.add_argument("--ny", type=int, default=1024)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="sphere_plate", choices=["sphere_plate", "tet_lattice"],
-                   help="tet_lattice: the precision-form case (26-DOP, FP32 filter vs FP64 plain) instead")
+    p.add_argument("--workload", default="sphere_plate", choices=["sphere_plate", "tet_lattice", "batch", "timestep"],
+                   help="tet_lattice: the precision-form case (26-DOP, FP32 filter vs FP64 plain); batch: 512 "
+                        "two-body scenes in one graph; timestep: 32 tumbling tori, refit vs rebuild")
     p.add_argument("--lattice", type=int, default=256, help="tet_lattice cells per axis (256 = 16,777,216 tets)")
     return p.parse_args()
 
@@ -401,6 +405,171 @@ def run_precision(args, world, rank, local):
     }
 
 
+def run_batch_form(args, world, rank, local):
+    """Batching form: 512 two-body scenes (per-scene counts LogUniform[1k, 200k], about 20M triangles), FP64,
+    18-DOP, every build and scene traversal as one replayed CUDA graph with the autotuned lane count; pairs stay on
+    the device. Parity: every scene's batch pair set against the single-scene path on a sample of scenes."""
+    import torch
+    import distbvh_b200 as bvhg
+    from distbvh_b200 import meshes
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    scenes = meshes.batch_scenes(512)
+    prims = sum(a.shape[0] + b.shape[0] for a, b in scenes)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = bvhg.Context(k=K, device=local, stream=stream.cuda_stream)
+    tensors, objs = [], []
+    for a, b in scenes:
+        da, db = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+        oa, ob = ctx.object(), ctx.object()
+        ctx.set_elements(oa, da, mem=bvhg.MEM_DEVICE)
+        ctx.set_elements(ob, db, mem=bvhg.MEM_DEVICE)
+        tensors += [da, db]
+        objs.append((oa, ob))
+    lanes, tune_ms = ctx.batch_autotune(objs)
+    ia = np.ascontiguousarray([o[0] for o in objs], dtype=np.int32)
+    ib = np.ascontiguousarray([o[1] for o in objs], dtype=np.int32)
+    counts = np.zeros(len(objs), dtype=np.uint64)
+    st = ctx.batch_broadphase_raw(ia.ctypes.data, ib.ctypes.data, len(objs), bvhg.REBUILD, None, 0,
+                                  counts.ctypes.data, bvhg.MEM_DEVICE)
+    total = int(counts.sum())
+    out = torch.empty((max(total, 1), 2), dtype=torch.int64, device=dev)
+
+    def step():
+        st = ctx.batch_broadphase_raw(ia.ctypes.data, ib.ctypes.data, len(objs), bvhg.REBUILD, out.data_ptr(),
+                                      out.shape[0], counts.ctypes.data, bvhg.MEM_DEVICE)
+        assert st == 0, st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+    # parity sample: the batch's pairs of a scene = the single-scene path's
+    offs = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int64)
+    got = out[:total].cpu().numpy()
+    checked, same = 0, True
+    for sidx in np.linspace(0, len(objs) - 1, 12).astype(int):
+        single = np.asarray(ctx.broadphase(*objs[sidx]), dtype=np.int64)
+        mine = got[offs[sidx]:offs[sidx] + int(counts[sidx])]
+        same = same and np.array_equal(np.unique(single, axis=0), np.unique(mine, axis=0))
+        checked += 1
+    ctx.close()
+    return {
+        "metric": METRIC, "value": prims * world / (ms * 1e-3) / 1e6, "unit": "Mprims/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded two-body scenes)",
+        "config": {"workload": f"batch: 512 two-body scenes, per-scene elements LogUniform[1k, 200k] ({prims} tris),"
+                               " 18-DOP, one CUDA graph", "k": K, "elements": prims, "pairs": total,
+                   "lanes": lanes, "autotune_ms": tune_ms},
+        "parity": {"scenes_checked_against_single_scene_path": checked, "same_pair_sets": bool(same)},
+    }
+
+
+def run_timestep(args, world, rank, local):
+    """Time-stepped contact: 32 tori of 262,144 triangles tumbling with seeded linear and angular velocities over
+    64 steps (dt: at most half a mean edge of vertex motion per step), all 496 body pairs batched, FP32 filter +
+    FP64 recheck. Refit every step vs rebuild every step vs rebuild every 8 steps; the pair sets of the refit run
+    are compared with the rebuild run's every step."""
+    import torch
+    import distbvh_b200 as bvhg
+    from distbvh_b200 import meshes
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nb, steps = 32, 64
+    base = torch.from_numpy(meshes.torus(512, 256)).to(dev)
+    rng = np.random.default_rng(21)
+    centers = np.array([[1.2 * (i % 4), 1.2 * ((i // 4) % 4), 0.9 * (i // 16)] for i in range(nb)], dtype=np.float64)
+    v = rng.uniform(-1.0, 1.0, (nb, 3))
+    w = rng.uniform(-1.0, 1.0, (nb, 3))
+    edge = 0.00666
+    dt = 0.5 * edge / float(np.max(np.linalg.norm(v, axis=1) + np.linalg.norm(w, axis=1) * 0.65))
+
+    def rot(axis_angle):
+        th = np.linalg.norm(axis_angle)
+        if th == 0:
+            return np.eye(3)
+        k = axis_angle / th
+        Kx = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+        return np.eye(3) + np.sin(th) * Kx + (1 - np.cos(th)) * Kx @ Kx
+
+    init_R = [rot(rng.uniform(-np.pi, np.pi, 3)) for _ in range(nb)]
+
+    def pose(t):
+        """Vertices of every body at step t (rigid motion about its own centre)."""
+        out = []
+        for i in range(nb):
+            R = torch.from_numpy(rot(w[i] * dt * t) @ init_R[i]).to(dev)
+            c = torch.from_numpy(centers[i] + v[i] * dt * t).to(dev)
+            out.append(base @ R.T + c)
+        return out
+
+    scenes = [(i, j) for i in range(nb) for j in range(i + 1, nb)]
+    stream = torch.cuda.Stream(device=dev)
+
+    def run(policy):
+        ctx = bvhg.Context(k=K, precision=bvhg.FILTER_FP32, device=local, stream=stream.cuda_stream)
+        bodies = pose(0)
+        objs = [ctx.object() for _ in range(nb)]
+        for o, x in zip(objs, bodies):
+            ctx.set_elements(o, x, mem=bvhg.MEM_DEVICE)
+        sc = [(objs[i], objs[j]) for i, j in scenes]
+        ia = np.ascontiguousarray([a for a, _ in sc], dtype=np.int32)
+        ib = np.ascontiguousarray([b for _, b in sc], dtype=np.int32)
+        counts = np.zeros(len(sc), dtype=np.uint64)
+        cap = 1 << 22
+        out = torch.empty((cap, 2), dtype=torch.int64, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        total_ms, sets = 0.0, []
+        for t in range(steps):
+            if t:
+                new = pose(t)
+                for x, y in zip(bodies, new):
+                    x.copy_(y)  # in place: the graph's borrowed pointers stay valid
+            torch.cuda.synchronize(dev)
+            mode = bvhg.REBUILD if policy(t) else bvhg.REFIT
+            e0.record(stream)
+            st = ctx.batch_broadphase_raw(ia.ctypes.data, ib.ctypes.data, len(sc), mode, out.data_ptr(), cap,
+                                          counts.ctypes.data, bvhg.MEM_DEVICE)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            assert st == 0, st
+            if t >= 2:  # the first two steps capture the REBUILD and REFIT graphs
+                total_ms += e0.elapsed_time(e1)
+            n = int(counts.sum())
+            keys = torch.sort(out[:n, 0] * (1 << 32) + out[:n, 1])[0]
+            sets.append((counts.copy(), keys))
+        ctx.close()
+        return total_ms / (steps - 2), sets
+
+    ms_refit, sets_refit = run(lambda t: t == 0)
+    ms_rebuild, sets_rebuild = run(lambda t: True)
+    ms_r8, sets_r8 = run(lambda t: t % 8 == 0)
+    same = all(np.array_equal(a[0], b[0]) and bool(torch.equal(a[1], b[1])) and
+               np.array_equal(a[0], c[0]) and bool(torch.equal(a[1], c[1]))
+               for a, b, c in zip(sets_refit, sets_rebuild, sets_r8))
+    prims = nb * base.shape[0]
+    pairs_per_step = [int(c.sum()) for c, _ in sets_rebuild]
+    return {
+        "metric": METRIC, "value": prims * world / (ms_refit * 1e-3) / 1e6, "unit": "Mprims/s", "n_gpus": world,
+        "steps": steps, "warmup": 2, "ms_per_step": ms_refit, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded tumbling tori)",
+        "config": {"workload": f"timestep: {nb} tori x {base.shape[0]} tris, {len(scenes)} body pairs batched, "
+                               f"{steps} steps, FP32 filter + FP64 recheck", "k": K, "elements": prims,
+                   "dt": dt, "pairs_min_max": [min(pairs_per_step), max(pairs_per_step)]},
+        "refit_every_step_ms": ms_refit, "rebuild_every_step_ms": ms_rebuild, "rebuild_every_8_ms": ms_r8,
+        "same_pair_sets_every_step": bool(same),
+    }
+
+
 def cpu_baseline_sample(sphere_level=8, nx=1024, ny=512, threads=0):
     """The reference's algorithms on all host cores over a quarter-size sample of the same scene."""
     from oracle import oracle as orc
@@ -456,8 +625,9 @@ def main():
         if out is not None:
             print(json.dumps(out))
         return
-    if args.workload == "tet_lattice":
-        result = run_precision(args, world, rank, local)
+    if args.workload != "sphere_plate":
+        fn = {"tet_lattice": run_precision, "batch": run_batch_form, "timestep": run_timestep}[args.workload]
+        result = fn(args, world, rank, local)
         if rank == 0:
             print(json.dumps(result))
         if world > 1:

@@ -90,9 +90,18 @@ struct object
 
 // Batching form: every object and scene of a batch as one CUDA graph (builds and traversals spread over lanes of
 // concurrent streams, no host round trip between scenes), captured once per batch layout and replayed.
-struct batch_state
+struct batch_graph
 {
   std::vector< uint64_t > key;  // layout the graph was captured for
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+struct batch_state
+{
+  // The last few captured layouts (a time-stepped loop alternates REBUILD and REFIT graphs of the same bodies).
+  std::vector< batch_graph > graphs;
+  std::vector< uint64_t > key;  // layout of the graph in use
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int lanes = 16;  // concurrent streams (bvhg_batch_autotune picks it)
@@ -104,10 +113,38 @@ struct batch_state
   pair_scalars *host_ps = nullptr;
   int *host_err = nullptr;
   size_t host_scenes = 0, host_objs = 0;
+  // Makes the cached graph of `k` current; false when none matches.
+  bool select(const std::vector< uint64_t > &k)
+  {
+    for ( auto &g : graphs )
+      if ( g.key == k )
+      {
+        key = g.key;
+        graph = g.graph;
+        exec = g.exec;
+        return true;
+      }
+    return false;
+  }
+  // Caches the graph just captured (graph, exec, key), dropping the oldest beyond four.
+  void keep()
+  {
+    if ( graphs.size() >= 4 )
+    {
+      cudaGraphExecDestroy( graphs.front().exec );
+      cudaGraphDestroy( graphs.front().graph );
+      graphs.erase( graphs.begin() );
+    }
+    graphs.push_back( { key, graph, exec } );
+  }
   void drop_graph()
   {
-    if ( exec ) cudaGraphExecDestroy( exec );
-    if ( graph ) cudaGraphDestroy( graph );
+    for ( auto &g : graphs )
+    {
+      cudaGraphExecDestroy( g.exec );
+      cudaGraphDestroy( g.graph );
+    }
+    graphs.clear();
     exec = nullptr;
     graph = nullptr;
     key.clear();
@@ -392,14 +429,15 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   }
   {
     stage_scope st( ctx, BVHG_STAGE_BOUNDS );
-    BVHG_CUDA( ctx, cudaMemcpyAsync( o.sc(), ctx->init_template, sizeof( obj_scalars ), cudaMemcpyHostToDevice, s ) );
-    BVHG_CUDA( ctx, cudaMemsetAsync( o.hist.p, 0, passes * radix * 4, s ) );
     {
+      // one launch resets the scalars, histograms, the look-back words of the passes that run and the exchange
       const size_t first_words = static_cast< size_t >( sort_first_pass( bits ) ) * ( tiles + 1 ) * radix;
-      BVHG_CUDA( ctx, cudaMemsetAsync( o.status.as< uint32_t >() + first_words, 0,
-                                       ( passes * ( tiles + 1 ) * radix - first_words ) * 4, s ) );
+      BVHG_CUDA( ctx, launch_obj_init( o.sc(), o.hist.as< uint32_t >(), passes * radix,
+                                       o.status.as< uint32_t >() + first_words,
+                                       passes * ( tiles + 1 ) * radix - first_words, o.exch.as< int >(),
+                                       m > 1 ? m - 1 : 0, s ) );
+      st.launched();
     }
-    if ( m > 1 ) BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( m - 1 ) * 4, s ) );
     BVHG_CUDA( ctx, launch_centroid_bounds( K, o.verts, o.V, n, ctx->cfg.epsilon, o.cx.as< double >(),
                                             o.cy.as< double >(), o.cz.as< double >(), o.sc(), s ) );
     st.launched();
@@ -605,7 +643,8 @@ bvhg_status capture_batch(bvhg_ctx *ctx, batch_state &B, const batch_args &x, co
     B.obj_done.push_back( e );
   }
   if ( !B.fork ) BVHG_CUDA( ctx, cudaEventCreateWithFlags( &B.fork, cudaEventDisableTiming ) );
-  B.drop_graph();
+  B.graph = nullptr;
+  B.exec = nullptr;
   const uint32_t flags = ctx->cfg.flags;
   ctx->cfg.flags &= ~BVHG_FLAG_STAGE_TIMING;  // no timing events inside a graph
   cudaStream_t s = ctx->stream;
@@ -750,7 +789,9 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
     // graph identity: everything a replay would read from the captured parameters
     std::vector< uint64_t > key{ static_cast< uint64_t >( x.mode ), x.nscenes, static_cast< uint64_t >( B.lanes ),
                                  reinterpret_cast< uint64_t >( B.cand.p ), reinterpret_cast< uint64_t >( B.out.p ),
-                                 reinterpret_cast< uint64_t >( B.exact.p ), reinterpret_cast< uint64_t >( B.ps.p ) };
+                                 reinterpret_cast< uint64_t >( B.exact.p ), reinterpret_cast< uint64_t >( B.ps.p ),
+                                 reinterpret_cast< uint64_t >( B.err_src.p ),
+                                 reinterpret_cast< uint64_t >( B.err_words.p ) };
     for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
     {
       key.push_back( static_cast< uint64_t >( x.a[sc] ) );
@@ -768,12 +809,16 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
         key.push_back( v );
       srcs.push_back( &ob.sc()->error );
     }
-    if ( key != B.key || !B.exec )
+    // the error-word sources of this batch's objects (every cached graph reads them from the same array)
+    BVHG_CUDA( ctx, cudaMemcpyAsync( B.err_src.p, srcs.data(), srcs.size() * sizeof( void * ), cudaMemcpyHostToDevice,
+                                     ctx->stream ) );
+    BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+    if ( !B.select( key ) )
     {
-      BVHG_CUDA( ctx, cudaMemcpy( B.err_src.p, srcs.data(), srcs.size() * sizeof( void * ), cudaMemcpyHostToDevice ) );
       const bvhg_status st = capture_batch( ctx, B, x, uniq, slot );
       if ( st != BVHG_OK ) return st;
       B.key = key;
+      B.keep();
     } else {
       // a replay rebuilds the same objects: their host-side state is what the capture left
       for ( int32_t o : uniq ) ctx->objs[o]->built = true;

@@ -100,6 +100,10 @@ cudaError_t launch_sort_fixup(const uint64_t *keys_in, const uint32_t *vals_in, 
 // Passes of the sort that build() runs: those whose digit lies in the high key half (the fix-up sorts the rest).
 inline int sort_first_pass(int bits) { return 32 / bits; }
 
+// Reset state of a rebuild in one launch (scalars, histograms, look-back words, climb exchange slots).
+cudaError_t launch_obj_init(obj_scalars *sc, uint32_t *hist, uint64_t hist_words, uint32_t *status,
+                            uint64_t status_words, int *exch, uint64_t exch_words, cudaStream_t s);
+
 cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
                             obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s);

@@ -271,6 +271,44 @@ cudaError_t launch_kh_t(const double *cx, const double *cy, const double *cz, ui
 
 int device_sm_count() { return sm_count(); }
 
+namespace {
+
+// The reset state of a rebuild in one launch: the object's scalars (zero, Morton-bound minima at the largest
+// encoding), the digit histograms, the look-back words of the passes that run, the climb's exchange slots (-1).
+__global__ void k_obj_init(obj_scalars *sc, uint32_t *hist, uint64_t hist_words, uint32_t *status,
+                           uint64_t status_words, int *exch, uint64_t exch_words)
+{
+  const uint64_t stride = static_cast< uint64_t >( gridDim.x ) * blockDim.x;
+  const uint64_t t = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
+  constexpr uint64_t sc_words = sizeof( obj_scalars ) / 4;
+  for ( uint64_t i = t; i < sc_words; i += stride ) reinterpret_cast< uint32_t * >( sc )[i] = 0u;
+  for ( uint64_t i = t; i < hist_words; i += stride ) hist[i] = 0u;
+  for ( uint64_t i = t; i < status_words; i += stride ) status[i] = 0u;
+  for ( uint64_t i = t; i < exch_words; i += stride ) exch[i] = -1;
+  // the minima start at the largest encoding (written after the zeroing by the same thread)
+  for ( uint64_t i = t; i < sc_words; i += stride )
+  {
+    const uint64_t byte = i * 4;
+    if ( byte < 3 * sizeof( unsigned long long ) ) reinterpret_cast< uint32_t * >( sc )[i] = 0xffffffffu;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_obj_init(obj_scalars *sc, uint32_t *hist, uint64_t hist_words, uint32_t *status,
+                            uint64_t status_words, int *exch, uint64_t exch_words, cudaStream_t s)
+{
+  uint64_t most = sizeof( obj_scalars ) / 4;
+  if ( hist_words > most ) most = hist_words;
+  if ( status_words > most ) most = status_words;
+  if ( exch_words > most ) most = exch_words;
+  const uint64_t blocks = ( most + 255 ) / 256;
+  const uint64_t cap = static_cast< uint64_t >( sm_count() ) * 4;
+  k_obj_init<<< static_cast< unsigned >( blocks < cap ? blocks : cap ), 256, 0, s >>>( sc, hist, hist_words, status,
+                                                                                     status_words, exch, exch_words );
+  return cudaGetLastError();
+}
+
 cudaError_t launch_centroid_bounds(int K, const double *verts, uint32_t V, uint64_t n, double eps, double *cx,
                                    double *cy, double *cz, obj_scalars *sc, cudaStream_t s)
 {

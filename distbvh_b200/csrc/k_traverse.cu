@@ -17,6 +17,7 @@
 #include "kdop_math.cuh"
 
 namespace bvhg {
+int device_sm_count();
 namespace {
 
 constexpr int kTravThreads = 128;
@@ -98,37 +99,19 @@ __device__ __forceinline__ void test_bucket(const T *qlo, const T *qhi, uint32_t
     if ( pos < cap ) pairs[pos] = make_uint2( qe, __ldg( tperm + r0 + __ffs( hits ) - 1 ) );
 }
 
-// One warp per group of 32 query ranks (a packet), lane = query element. The warp walks the target tree once for
-// its packet: every lane tests its own element's slabs against both children of the current node (the node row is
-// read once for the warp, a broadcast), and a child is entered with the mask of the lanes that overlap it (a lane
-// that misses a node misses all of its descendants). Stack entries are (node, lane mask), in shared memory. At a
-// leaf bucket the lanes of the mask test their element against the bucket's elements.
+// One packet: the union box of ranks pk*32 .. pk*32 + 31 against the target root, then the walk (see k_traverse).
 template< int K, typename T >
-__global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict__ qwarp,
-                                                           const T *__restrict__ qelem,
-                                                           const uint32_t *__restrict__ qperm, uint32_t nq,
-                                                           const int2 *__restrict__ child,
-                                                           const T *__restrict__ nbox,
-                                                           const int2 *__restrict__ range,
-                                                           const T *__restrict__ telem,
-                                                           const uint32_t *__restrict__ tperm,
-                                                           const obj_scalars *__restrict__ tsc, uint32_t nt,
-                                                           const obj_scalars *__restrict__ qsc, int self,
-                                                           uint2 *pairs, uint64_t cap, pair_scalars *ps)
+__device__ __forceinline__ void traverse_packet(const uint32_t i, const unsigned lane, int2 *stack,
+                                                const T *__restrict__ qwarp, const T *__restrict__ qelem,
+                                                const uint32_t *__restrict__ qperm, uint32_t nq,
+                                                const int2 *__restrict__ child, const T *__restrict__ nbox,
+                                                const int2 *__restrict__ range, const T *__restrict__ telem,
+                                                const uint32_t *__restrict__ tperm,
+                                                const obj_scalars *__restrict__ tsc, uint32_t nt, int self,
+                                                uint2 *pairs, uint64_t cap, pair_scalars *ps, const T *rb)
 {
   constexpr int D = K / 2;
   constexpr int D0 = D < 4 ? D : 4;
-  constexpr int WPB = kTravThreads / 32;
-  __shared__ int2 s_stack[WPB][kStack];  // (node, lane mask)
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned lane = threadIdx.x & 31u;
-  int2 *stack = s_stack[threadIdx.x >> 5];
-  // No tree exists after a failed sort of either object.
-  if ( *reinterpret_cast< const volatile int * >( &tsc->error ) == kErrTimeout ||
-       *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
-    return;
-  if ( ( i & ~31u ) >= nq ) return;  // warps entirely past the last rank have no group box (uniform per warp)
-  const T *rb = reinterpret_cast< const T * >( tsc->root_box );
   // 1. The packet's union box against the target's root box, first four slabs first (uniform per warp).
   {
     const T *wb = qwarp + static_cast< size_t >( i >> 5 ) * D * 2;
@@ -232,11 +215,63 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
   }
 }
 
+
+// One warp per group of 32 query ranks (a packet), lane = query element. The warp walks the target tree once for
+// its packet: every lane tests its own element's slabs against both children of the current node (the node row is
+// read once for the warp, a broadcast), and a child is entered with the mask of the lanes that overlap it (a lane
+// that misses a node misses all of its descendants). Stack entries are (node, lane mask), in shared memory. At a
+// leaf bucket the lanes of the mask test their element against the bucket's elements.
+template< int K, typename T >
+__global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict__ qwarp,
+                                                           const T *__restrict__ qelem,
+                                                           const uint32_t *__restrict__ qperm, uint32_t nq,
+                                                           const int2 *__restrict__ child,
+                                                           const T *__restrict__ nbox,
+                                                           const int2 *__restrict__ range,
+                                                           const T *__restrict__ telem,
+                                                           const uint32_t *__restrict__ tperm,
+                                                           const obj_scalars *__restrict__ tsc, uint32_t nt,
+                                                           const obj_scalars *__restrict__ qsc, int self,
+                                                           uint2 *pairs, uint64_t cap, pair_scalars *ps)
+{
+  constexpr int D = K / 2;
+  constexpr int D0 = D < 4 ? D : 4;
+  constexpr int WPB = kTravThreads / 32;
+  __shared__ int2 s_stack[WPB][kStack];  // (node, lane mask)
+  const unsigned lane = threadIdx.x & 31u;
+  int2 *stack = s_stack[threadIdx.x >> 5];
+  // No tree exists after a failed sort of either object.
+  if ( *reinterpret_cast< const volatile int * >( &tsc->error ) == kErrTimeout ||
+       *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
+    return;
+  const T *rb = reinterpret_cast< const T * >( tsc->root_box );
+  // 0. Root against root: objects far apart (most pairs of a batch) end here for the whole grid.
+  {
+    const T *qr = reinterpret_cast< const T * >( qsc->root_box );
+    bool o = true;
+#pragma unroll
+    for ( int a = 0; a < D0; ++a ) o = o && ( qr[2 * a] < rb[2 * a + 1] && rb[2 * a] < qr[2 * a + 1] );
+    if ( !o ) return;
+  }
+  // Packets (warps of 32 query ranks) are taken grid-stride.
+  const uint32_t packets = ( nq + 31 ) / 32;
+  const uint32_t warp_stride = ( gridDim.x * blockDim.x ) >> 5;
+  for ( uint32_t pk = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5; pk < packets; pk += warp_stride )
+  {
+    const uint32_t i = pk * 32 + lane;
+    traverse_packet< K, T >( i, lane, stack, qwarp, qelem, qperm, nq, child, nbox, range, telem, tperm, tsc, nt, self,
+                             pairs, cap, ps, rb );
+  }
+}
+
 template< int K, typename T >
 cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, uint2 *pairs, uint64_t cap, pair_scalars *ps,
                           cudaStream_t s)
 {
-  const unsigned grid = static_cast< unsigned >( ( q.n + kTravThreads - 1 ) / kTravThreads );
+  // one warp per packet (the kernel strides over packets only when the grid is capped by the launch limit)
+  const uint64_t blocks = ( q.n + kTravThreads - 1 ) / kTravThreads;
+  const uint64_t capb = 1ull << 30;
+  const unsigned grid = static_cast< unsigned >( blocks < capb ? blocks : capb );
   k_traverse< K, T ><<< grid, kTravThreads, 0, s >>>(
     static_cast< const T * >( q.warp_box ), static_cast< const T * >( q.elem_box ), q.perm,
     static_cast< uint32_t >( q.n ), t.child, static_cast< const T * >( t.node_box ), t.range,
@@ -317,7 +352,10 @@ template< int K >
 cudaError_t recheck_k(const double *va, uint32_t Va, const double *vb, uint32_t Vb, double eps, const uint2 *cand,
                       uint64_t ncand, uint2 *out, uint64_t cap, pair_scalars *ps, cudaStream_t s)
 {
-  const unsigned grid = 148 * 8;
+  // grid-stride over the candidates (their count is read on the device): at most 4 blocks per SM
+  const uint64_t blocks = ( ncand + 255 ) / 256;
+  const uint64_t capb = static_cast< uint64_t >( device_sm_count() ) * 4;
+  const unsigned grid = static_cast< unsigned >( blocks < capb ? ( blocks ? blocks : 1 ) : capb );
   if ( Va == 3 && Vb == 3 ) k_recheck< K, 3, 3 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
   else if ( Va == 4 && Vb == 4 ) k_recheck< K, 4, 4 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
   else if ( Va == 8 && Vb == 8 ) k_recheck< K, 8, 8 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
@@ -372,7 +410,7 @@ cudaError_t launch_gid_pairs_dev(const uint2 *pairs, const unsigned long long *c
 {
   if ( cap == 0 ) return cudaSuccess;
   const uint64_t blocks = ( cap + 255 ) / 256;
-  const unsigned grid = static_cast< unsigned >( blocks < 148 * 4 ? blocks : 148 * 4 );
+  const unsigned grid = static_cast< unsigned >( blocks < 148 * 2 ? blocks : 148 * 2 );
   k_gid_pairs_dev<<< grid, 256, 0, s >>>( pairs, count, cap, gid_a, gid_b, normalize ? 1 : 0, out );
   return cudaGetLastError();
 }

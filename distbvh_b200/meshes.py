@@ -98,6 +98,21 @@ def icosphere(level, radius=1.0, center=(0.0, 0.0, 0.0)):
     return t * radius + np.asarray(center, dtype=np.float64)
 
 
+def torus(nu, nv, major=0.5, minor=0.15):
+    """Triangulated torus about the z axis: nu x nv quads (2 triangles each), centred at the origin."""
+    u = np.linspace(0.0, 2.0 * np.pi, nu + 1)[:-1]
+    v = np.linspace(0.0, 2.0 * np.pi, nv + 1)[:-1]
+    U, Vv = np.meshgrid(u, v, indexing="ij")
+    P = np.stack([(major + minor * np.cos(Vv)) * np.cos(U), (major + minor * np.cos(Vv)) * np.sin(U),
+                  minor * np.sin(Vv)], axis=-1)
+    P1 = np.roll(P, -1, axis=0)
+    P2 = np.roll(P, -1, axis=1)
+    P3 = np.roll(P1, -1, axis=1)
+    t1 = np.stack([P, P1, P3], axis=2).reshape(-1, 3, 3)
+    t2 = np.stack([P, P3, P2], axis=2).reshape(-1, 3, 3)
+    return np.ascontiguousarray(np.concatenate([t1, t2]))
+
+
 # --- the benchmark configurations ---------------------------------------------------------------------------
 
 TWO_PLATES_EPSILON = 0.005  # plate A is flat at z = 0 and B sits at z >= 0.002: without inflation S is empty
@@ -136,6 +151,24 @@ def tet_lattice(m, seed=3, jitter=0.3, sigma=0.4):
     c = t.mean(axis=1, keepdims=True)
     s = np.exp(sigma * normal(seed, 2, m ** 3))[:, None, None]
     return c + (t - c) * s
+
+
+def batch_scenes(nscenes=512, lo=1000, hi=200000, seed=11):
+    """Two-body scenes for the batching form: per-scene element counts LogUniform[lo, hi] (split between the two
+    bodies), element centroids uniform in the body's unit cube, triangle size 1.5 n^(-1/3), and a random rigid
+    offset of each body (up to half a cube) so that scenes have uneven overlap. Returns [(a, b), ...]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(nscenes):
+        n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        na = max(1, n // 2)
+        nb = max(1, n - na)
+        size = 0.75 * n ** (-1.0 / 3.0)  # vertices within +-size of the centroid: edge about 1.5 n^(-1/3)
+        a = random_soup(na, 3, seed=seed * 100003 + 2 * s, size=size)
+        b = random_soup(nb, 3, seed=seed * 100003 + 2 * s + 1, size=size, stream=1)
+        b = b + rng.uniform(-0.5, 0.5, 3)
+        out.append((a, b))
+    return out
 
 
 def checkerboard(m):
