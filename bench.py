@@ -153,8 +153,9 @@ def peaks():
 #   keys     read 24 (centroid) + write 8 (key)                                                 = 32
 #   sort     per pass read 12 + write 12 (key + index)                                          = 24 per pass
 #   fixup    read 12 + write 12 (key + index; neighbours of a run are cache hits)               = 24
-#   slabs    read 4 (index) + 72 (vertices, gathered) + write 2 D S (element slabs in rank order) + 2 D S / 8
-#            (leaf-bucket boxes) + 2 D S / 32 (query-group boxes)                               = 76 + 2DS(1 + 1/8 + 1/32)
+#   slabs    read 4 (index) + 72 (vertices, gathered) + write 2 D S / 8 (leaf-bucket boxes) + 2 D S / 32
+#            (query-group boxes); element slabs are not stored (the traversal caches the ones it tests)
+#                                                                                               = 76 + 2DS(1/8 + 1/32)
 #   build    read 2 D S / 8 (bucket boxes) + 2 (boundary keys) + write (4 D S + 8 child + 8 range + 8 parent) / 8
 #            (one internal node per bucket)                                                     = 2 + 2DS/8 + (4DS + 24)/8
 #   traverse read 2 D S / 32 (query-group box) per query; survivors read their slabs and the tree
@@ -163,7 +164,7 @@ LEAF = 8
 
 def stage_bytes(D, S, passes):
     return {"bounds": 96, "keys": 32, "sort": 24 * passes, "fixup": 24,
-            "slabs": 76 + 2 * D * S * (1 + 1 / LEAF + 1 / 32),
+            "slabs": 76 + 2 * D * S * (1 / LEAF + 1 / 32),
             "build": 2 + 2 * D * S / LEAF + (4 * D * S + 24) / LEAF,
             "traverse": 2 * D * S / 32}
 

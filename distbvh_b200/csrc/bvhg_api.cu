@@ -66,11 +66,16 @@ struct object
   bool built = false;  // slabs current for the present vertex data
   bool topo = false;   // a rebuild's topology exists for the present n and V (refit allowed)
   int sort_result_alt = 0;  // sorted keys/vals ended in the *_alt buffers
+  // Dense contact (a broadphase of this object found pairs for a sizable fraction of the elements): its next builds
+  // store every element's slabs, which its traversals then only read; in sparse contact they compute the few they
+  // test from the vertices instead of storing all of them.
+  bool store_slabs = false;
+  bool stored = false;  // the last build stored them
   dev_buf verts_own, gid_own;
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
   dev_buf hist, status;
-  dev_buf elem_box, warp_box, bucket_box, node_box, child, range, parent, exch, queue;
+  dev_buf warp_box, bucket_box, node_box, child, range, parent, exch, queue, elem_cache, cache_state;
   dev_buf scal;  // obj_scalars
   // Each object's build runs on its own stream, forked from and joined back into the context stream with
   // events, so two objects' builds overlap (one's latency-bound tree climb beside the other's streaming kernels).
@@ -346,9 +351,10 @@ bvhg_status reserve_object(bvhg_ctx *ctx, object &o)
   BVHG_CUDA( ctx, o.hist.reserve( passes * radix * 4 ) );
   BVHG_CUDA( ctx, o.status.reserve( passes * ( tiles + 1 ) * radix * 4 ) );
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;  // leaf buckets
-  BVHG_CUDA( ctx, o.elem_box.reserve( n * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.bucket_box.reserve( m * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.elem_cache.reserve( n * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.cache_state.reserve( m * 4 ) );
   BVHG_CUDA( ctx, o.node_box.reserve( ( m - 1 ) * D * 4 * sb + 16 ) );
   BVHG_CUDA( ctx, o.child.reserve( ( m - 1 ) * 8 + 8 ) );
   BVHG_CUDA( ctx, o.range.reserve( ( m - 1 ) * 8 + 8 ) );
@@ -403,8 +409,10 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
     const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
     {
       stage_scope st( ctx, BVHG_STAGE_SLABS );
-      BVHG_CUDA( ctx, launch_slabs( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.elem_box.p,
-                                    o.bucket_box.p, o.warp_box.p, o.sc(), s ) );
+      BVHG_CUDA( ctx, launch_slabs( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(),
+                                    o.bucket_box.p, o.warp_box.p, o.store_slabs ? o.elem_cache.p : nullptr,
+                                    o.cache_state.as< unsigned >(), o.sc(), s ) );
+      o.stored = o.store_slabs;
       st.launched();
     }
     if ( m > 1 )
@@ -476,8 +484,10 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   }
   {
     stage_scope st( ctx, BVHG_STAGE_SLABS );
-    BVHG_CUDA( ctx, launch_slabs( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(), o.elem_box.p,
-                                  o.bucket_box.p, o.warp_box.p, o.sc(), s ) );
+    BVHG_CUDA( ctx, launch_slabs( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(),
+                                  o.bucket_box.p, o.warp_box.p, o.store_slabs ? o.elem_cache.p : nullptr,
+                                  o.cache_state.as< unsigned >(), o.sc(), s ) );
+    o.stored = o.store_slabs;
     st.launched();
   }
   if ( m > 1 )
@@ -506,7 +516,11 @@ tree_view view_of(const object &o)
   v.child = o.child.as< int2 >();
   v.range = o.range.as< int2 >();
   v.warp_box = o.warp_box.p;
-  v.elem_box = o.elem_box.p;
+  v.verts = o.verts;
+  v.V = o.V;
+  v.elem_cache = o.elem_cache.p;
+  v.cache_state = o.cache_state.as< unsigned >();
+  v.stored = o.stored;
   v.perm = o.sorted_vals();
   v.n = o.n;
   v.sc = o.sc();
@@ -537,7 +551,7 @@ bvhg_status find_pairs(bvhg_ctx *ctx, object &a, object &b, bool self, const uin
     BVHG_CUDA( ctx, cudaMemsetAsync( ps, 0, sizeof( pair_scalars ), s ) );
     {
       stage_scope st( ctx, BVHG_STAGE_TRAVERSE );
-      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( a ), view_of( b ), self, ctx->pairs.as< uint2 >(),
+      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( a ), view_of( b ), self, ctx->cfg.epsilon, ctx->pairs.as< uint2 >(),
                                        ctx->pair_cap, ps, s ) );
       st.launched();
     }
@@ -582,6 +596,16 @@ bvhg_status find_pairs(bvhg_ctx *ctx, object &a, object &b, bool self, const uin
     return BVHG_OK;
   }
   return fail( ctx, BVHG_ERR_CUDA, "pair buffer did not converge" );
+}
+
+// Contact density decides whether the objects' next builds store their element slabs (see object::store_slabs):
+// candidate pairs for at least 2% of the elements involved.
+void note_density(object &a, object &b, bool self, uint64_t candidates)
+{
+  const uint64_t elems = self ? a.n : a.n + b.n;
+  const bool dense = candidates * 50 >= elems && candidates > 0;
+  a.store_slabs = dense;
+  b.store_slabs = dense;
 }
 
 bvhg_status emit_pairs(bvhg_ctx *ctx, const object &a, const object &b, bool self, const uint2 *pairs, uint64_t np,
@@ -677,7 +701,7 @@ bvhg_status capture_batch(bvhg_ctx *ctx, batch_state &B, const batch_args &x, co
       const bool self = x.a[sc] == x.b[sc];
       if ( oa.n == 0 || ob.n == 0 || ( self && oa.n < 2 ) ) continue;
       uint2 *cand = B.cand.as< uint2 >() + B.off[sc];
-      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( oa ), view_of( ob ), self, cand, B.cap[sc], ps + sc, ls ) );
+      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( oa ), view_of( ob ), self, ctx->cfg.epsilon, cand, B.cap[sc], ps + sc, ls ) );
       const uint2 *fin = cand;
       const unsigned long long *cnt = &ps[sc].count;
       if ( fp32 )
@@ -802,9 +826,10 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
     for ( int32_t o : uniq )
     {
       const object &ob = *ctx->objs[o];
-      for ( uint64_t v : { ob.n, static_cast< uint64_t >( ob.V ), reinterpret_cast< uint64_t >( ob.verts ),
+      for ( uint64_t v : { ob.n, static_cast< uint64_t >( ob.V ), static_cast< uint64_t >( ob.store_slabs ),
+                           reinterpret_cast< uint64_t >( ob.verts ),
                            reinterpret_cast< uint64_t >( ob.gid ), reinterpret_cast< uint64_t >( ob.scal.p ),
-                           reinterpret_cast< uint64_t >( ob.keys.p ), reinterpret_cast< uint64_t >( ob.elem_box.p ),
+                           reinterpret_cast< uint64_t >( ob.keys.p ), reinterpret_cast< uint64_t >( ob.bucket_box.p ),
                            reinterpret_cast< uint64_t >( ob.node_box.p ) } )
         key.push_back( v );
       srcs.push_back( &ob.sc()->error );
@@ -850,7 +875,23 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
       }
     }
     ctx->last_candidates = cand_total;
-    if ( !grown ) return BVHG_OK;
+    if ( !grown )
+    {
+      // contact density per object over its scenes, for the next run's builds
+      std::vector< uint64_t > cand_of( ctx->objs.size(), 0 ), elems_of( ctx->objs.size(), 0 );
+      for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
+      {
+        const uint64_t c = B.host_ps[sc].count;
+        const uint64_t e = ctx->objs[x.a[sc]]->n + ( x.a[sc] == x.b[sc] ? 0 : ctx->objs[x.b[sc]]->n );
+        for ( int32_t o : { x.a[sc], x.b[sc] } )
+        {
+          cand_of[o] += c;
+          elems_of[o] += e;
+        }
+      }
+      for ( int32_t o : uniq ) ctx->objs[o]->store_slabs = cand_of[o] > 0 && cand_of[o] * 50 >= elems_of[o];
+      return BVHG_OK;
+    }
   }
   return fail( ctx, BVHG_ERR_CUDA, "batch pair capacities did not converge" );
 }
@@ -1024,6 +1065,7 @@ bvhg_status bvhg_broadphase(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, uint64_
   uint64_t np = 0;
   bvhg_status st = find_pairs( ctx, a, b, false, &lp, &np );
   if ( st != BVHG_OK ) return st;
+  note_density( a, b, false, ctx->last_candidates );
   return emit_pairs( ctx, a, b, false, lp, np, pairs, capacity, count, mem );
 }
 
@@ -1129,6 +1171,7 @@ bvhg_status bvhg_self_collision(bvhg_ctx *ctx, int32_t obj, uint64_t *pairs, uin
   uint64_t np = 0;
   bvhg_status st = find_pairs( ctx, o, o, true, &lp, &np );
   if ( st != BVHG_OK ) return st;
+  note_density( o, o, true, ctx->last_candidates );
   return emit_pairs( ctx, o, o, true, lp, np, pairs, capacity, count, mem );
 }
 
@@ -1257,21 +1300,23 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
   BVHG_CUDA( ctx, tmp.reserve( n * D * 2 * sb ) );
   BVHG_CUDA( ctx, launch_probe_kdops( ctx->cfg.k, fp32, o.verts, o.V, n, ctx->cfg.epsilon, tmp.p, ctx->stream ) );
   BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
-  std::vector< double > lb, eb, nb, wb, rootb;
+  std::vector< double > lb, nb, wb, bb, rootb;
   BVHG_CUDA( ctx, fetch( tmp.p, n * D * 2, lb ) );
-  BVHG_CUDA( ctx, fetch( o.elem_box.p, n * D * 2, eb ) );
   BVHG_CUDA( ctx, fetch( o.node_box.p, ( m - 1 ) * D * 4, nb ) );
   BVHG_CUDA( ctx, fetch( o.warp_box.p, nw * D * 2, wb ) );
+  BVHG_CUDA( ctx, fetch( o.bucket_box.p, m * D * 2, bb ) );
   obj_scalars h;
   BVHG_CUDA( ctx, cudaMemcpy( &h, o.sc(), sizeof( h ), cudaMemcpyDeviceToHost ) );
   BVHG_CUDA( ctx, fetch( o.sc()->root_box, D * 2, rootb ) );
   std::vector< uint32_t > perm( n );
   BVHG_CUDA( ctx, cudaMemcpy( perm.data(), o.sorted_vals(), n * 4, cudaMemcpyDeviceToHost ) );
-  // rank-order element slabs are the elements' slabs
+  // the elements' slabs in rank order (the build does not store them)
+  std::vector< double > eb( n * D * 2 );
   for ( uint64_t r = 0; r < n; ++r )
-    for ( int k = 0; k < 2 * D; ++k )
-      if ( eb[r * D * 2 + k] != lb[static_cast< size_t >( perm[r] ) * D * 2 + k] )
-        return fail( ctx, BVHG_ERR_STATE, "rank-order element slabs differ from the elements' slabs" );
+  {
+    if ( perm[r] >= n ) return fail( ctx, BVHG_ERR_STATE, "permutation entry out of range" );
+    for ( int k = 0; k < 2 * D; ++k ) eb[r * D * 2 + k] = lb[static_cast< size_t >( perm[r] ) * D * 2 + k];
+  }
   // union of ranks [lo, hi) into out (2 D values)
   auto unite = [&](uint64_t lo, uint64_t hi, std::vector< double > &out) {
     out.assign( 2 * D, 0.0 );
@@ -1295,7 +1340,12 @@ bvhg_status bvhg_validate_tree(bvhg_ctx *ctx, int32_t obj, uint32_t *depth_out)
       if ( wb[w * D * 2 + k] != u[k] ) return fail( ctx, BVHG_ERR_STATE, "query group box is not the union of its ranks" );
   }
   std::vector< std::vector< double > > bucket( m );
-  for ( uint64_t b = 0; b < m; ++b ) unite( kLeafSize * b, std::min< uint64_t >( n, kLeafSize * b + kLeafSize ), bucket[b] );
+  for ( uint64_t b = 0; b < m; ++b )
+  {
+    unite( kLeafSize * b, std::min< uint64_t >( n, kLeafSize * b + kLeafSize ), bucket[b] );
+    for ( int k = 0; k < 2 * D; ++k )
+      if ( bb[b * D * 2 + k] != bucket[b][k] ) return fail( ctx, BVHG_ERR_STATE, "bucket box is not the union of its ranks" );
+  }
   if ( m == 1 )
   {
     if ( h.root != ~0 ) return fail( ctx, BVHG_ERR_STATE, "bad root of a one-bucket tree" );

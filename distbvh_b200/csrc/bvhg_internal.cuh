@@ -7,9 +7,11 @@
 //   cx, cy, cz n doubles each: centroids, structure of arrays (coalesced write in K1, read in K2)
 //   keys/vals  n u64 Morton keys and n u32 element indices, ping-ponged by the radix passes; after the sort
 //              keys[r], vals[r] hold the key and original index of rank r (vals = the permutation)
-//   elem_box   n * D * 2 T: slabs of the element of rank r, [r][a][min,max] (leaf tests and queries)
 //   warp_box   ceil(n / 32) * D * 2 T: union of the slabs of ranks [32 w, 32 w + 31] (the query side's cull)
 //   bucket_box m * D * 2 T: union of the slabs of leaf bucket b (ranks [8 b, 8 b + 7]), input of the tree build
+//   elem_cache n * D * 2 T: element slabs in rank order: written by the slab kernel for objects in dense contact,
+//              else by the first traversal that tests their bucket
+//   cache_state m u32: per bucket 0 empty / 1 being written / 2 ready (the slab kernel resets it)
 //   node_box   (m - 1) * D * 2 * 2 T: both children's slabs of internal node k, [k][a][child][min,max], so one
 //              32-byte (FP64) or 16-byte (FP32) sector per axis tests both children
 //   child      (m - 1) int2: child index, >= 0 internal node, < 0 bucket with ~child = bucket index
@@ -110,11 +112,12 @@ cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *v
 
 // Element slabs + agglomerative LBVH build over leaf buckets with bottom-up refit (FP64 or FP32 slabs): the
 // block-local phase, which queues unfinished subtrees for launch_climb.
-// Element slabs in rank order (elem_box), the union of each leaf bucket (bucket_box, m rows) and of each group of
-// 32 ranks (warp_box); a one-bucket object's root. Marks a failed sort when perm is not a permutation.
+// Element slabs in rank order (stored to elem_rows when given, for objects in dense contact), the union of each leaf
+// bucket (bucket_box, m rows) and of each group of 32 ranks (warp_box); a one-bucket object's root. Marks a failed
+// sort when perm is not a permutation.
 cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *elem_box, void *bucket_box, void *warp_box, obj_scalars *sc,
-                         cudaStream_t s);
+                         const uint32_t *vals, void *bucket_box, void *warp_box, void *elem_rows,
+                         unsigned *cache_state, obj_scalars *sc, cudaStream_t s);
 
 // Block-local LBVH build over the bucket boxes (nodes closed inside a block of 256 buckets; the rest queued for
 // launch_climb). Nothing to do for one bucket.
@@ -135,15 +138,19 @@ struct tree_view
   const int2 *child;
   const int2 *range;
   const void *warp_box;
-  const void *elem_box;
+  const double *verts;  // element vertices, [element][vertex][xyz] (element slabs are recomputed from them)
+  uint32_t V;
+  const void *elem_cache;     // element slabs in rank order, written when a traversal first tests their bucket
+  const unsigned *cache_state;  // per bucket: 0 empty, 1 being written, 2 ready (reset by the slab kernel)
+  bool stored;                  // the slab kernel wrote every element's slabs to elem_cache
   const uint32_t *perm;
   uint64_t n;
   const obj_scalars *sc;
 };
 
 // Queries every leaf of q against tree t; writes (q element, t element) local index pairs.
-cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, uint2 *pairs, uint64_t cap,
-                            pair_scalars *ps, cudaStream_t s);
+cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, double eps, uint2 *pairs,
+                            uint64_t cap, pair_scalars *ps, cudaStream_t s);
 
 // FP64 recheck of FP32 candidates: keeps (a, b) iff the FP64 slabs of a and b overlap, compacted into out.
 // The candidate count is min(ps->count, cand_cap), read on the device.

@@ -142,8 +142,9 @@ __device__ __forceinline__ uint64_t quant21(double c, double mn, double inv)
   return static_cast< uint64_t >( static_cast< long long >( scaled ) ) & 0x1fffffull;
 }
 
-// K2. Morton key of every element, written in original order, plus the digit histogram of every radix pass
-// (warp-aggregated shared-memory counters, one global atomic per nonzero bin per block).
+// K2. Morton key of every element, written in original order, plus the digit histogram of every radix pass that
+// runs, those over the high key half (warp-aggregated shared-memory counters, one global atomic per nonzero bin
+// per block).
 template< int BITS >
 __global__ void __launch_bounds__( kElemThreads ) k_keys_hist(const double *__restrict__ cx,
                                                             const double *__restrict__ cy,
@@ -153,9 +154,11 @@ __global__ void __launch_bounds__( kElemThreads ) k_keys_hist(const double *__re
 {
   constexpr int RADIX = 1 << BITS;
   constexpr int PASSES = ( kKeyBits + BITS - 1 ) / BITS;
-  __shared__ uint32_t s_hist[PASSES * RADIX];
+  constexpr int FIRST = 32 / BITS;  // only the passes over the high key half run (the fix-up sorts the low half)
+  constexpr int NH = PASSES - FIRST;
+  __shared__ uint32_t s_hist[NH * RADIX];
   __shared__ double s_min[3], s_inv[3];
-  for ( int k = threadIdx.x; k < PASSES * RADIX; k += kElemThreads ) s_hist[k] = 0;
+  for ( int k = threadIdx.x; k < NH * RADIX; k += kElemThreads ) s_hist[k] = 0;
   if ( threadIdx.x < 3 )
   {
     const int c = threadIdx.x;
@@ -193,22 +196,22 @@ __global__ void __launch_bounds__( kElemThreads ) k_keys_hist(const double *__re
     }
     const unsigned vmask = __ballot_sync( 0xffffffffu, valid );
 #pragma unroll
-    for ( int p = 0; p < PASSES; ++p )
+    for ( int p = FIRST; p < PASSES; ++p )
     {
       const unsigned d = static_cast< unsigned >( ( key >> ( p * BITS ) ) & ( RADIX - 1 ) );
       // Spatially coherent warps share their high digits: one atomic for a uniform warp, else one per lane.
       const unsigned d0 = __shfl_sync( 0xffffffffu, d, 0 );
       if ( __all_sync( 0xffffffffu, d == d0 || !valid ) && vmask == 0xffffffffu )
       {
-        if ( lane == 0 ) atomicAdd( &s_hist[p * RADIX + d0], 32u );
+        if ( lane == 0 ) atomicAdd( &s_hist[( p - FIRST ) * RADIX + d0], 32u );
       } else if ( valid ) {
-        atomicAdd( &s_hist[p * RADIX + d], 1u );
+        atomicAdd( &s_hist[( p - FIRST ) * RADIX + d], 1u );
       }
     }
   }
   __syncthreads();
-  for ( int k = threadIdx.x; k < PASSES * RADIX; k += kElemThreads )
-    if ( s_hist[k] ) atomicAdd( &hist[k], s_hist[k] );
+  for ( int k = threadIdx.x; k < NH * RADIX; k += kElemThreads )
+    if ( s_hist[k] ) atomicAdd( &hist[FIRST * RADIX + k], s_hist[k] );
 }
 
 int sm_count()

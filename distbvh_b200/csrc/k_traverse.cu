@@ -72,49 +72,129 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned k, unsigned 
   return base + pre;
 }
 
-// The elements of target bucket bb against the query slabs (ranks > skip only, for self-collision). The hits are
-// collected first and stored through one warp-aggregated reservation; pairs beyond capacity are counted only.
-template< int D, typename T >
-__device__ __forceinline__ void test_bucket(const T *qlo, const T *qhi, uint32_t qe, int bb, int nt, int skip,
-                                            const T *__restrict__ telem, const uint32_t *__restrict__ tperm,
-                                            uint2 *pairs, uint64_t cap, pair_scalars *ps)
+// Slabs of element e straight into a shared-memory row (C = 2 D values: min, max per slab), as leaf_slabs computes
+// them (the same FP64 slabs, or the same FP32 enclosures, that k_elem_slabs unites into the bucket boxes).
+template< int K, typename T, int VT >
+__device__ __noinline__ void slabs_to_row(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
+                                             float eps_hi, T *row)
 {
-  const int r0 = max( kLeafSize * bb, skip + 1 );
-  const int r1 = min( kLeafSize * bb + kLeafSize, nt );
-  unsigned hits = 0;
-  for ( int r = r0; r < r1; ++r )
-  {
-    const T *eb = telem + static_cast< size_t >( r ) * D * 2;
-    bool o = true;
+  constexpr int D = K / 2;
+  T lo[D], hi[D];
+  leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
 #pragma unroll
-    for ( int a = 0; a < D; ++a )
-    {
-      if ( !o ) break;
-      o = qlo[a] < __ldg( eb + 2 * a + 1 ) && __ldg( eb + 2 * a ) < qhi[a];
-    }
-    if ( o ) hits |= 1u << ( r - r0 );
+  for ( int a = 0; a < D; ++a )
+  {
+    row[2 * a] = lo[a];
+    row[2 * a + 1] = hi[a];
   }
-  unsigned long long pos = warp_reserve( static_cast< unsigned >( __popc( hits ) ), &ps->count );
-  for ( ; hits; hits &= hits - 1, ++pos )
-    if ( pos < cap ) pairs[pos] = make_uint2( qe, __ldg( tperm + r0 + __ffs( hits ) - 1 ) );
+}
+
+// Everything one query packet needs besides the tree (see k_traverse).
+template< typename T >
+struct trav_args
+{
+  const T *qwarp;
+  const double *qverts;
+  uint32_t qV;
+  const T *qrows;    // query element slabs in rank order (stored variant only)
+  const uint32_t *qperm;
+  uint32_t nq;
+  const int2 *child;
+  const T *nbox;
+  const int2 *range;
+  const double *tverts;
+  uint32_t tV;
+  T *tcache;         // element slabs of the target, in rank order, filled on first use of their bucket
+  unsigned *tstate;  // per target bucket: 0 not cached, 1 being written, 2 ready
+  const uint32_t *tperm;
+  const obj_scalars *tsc;
+  uint32_t nt;
+  int self;
+  double eps;
+  float eps_hi;
+  uint2 *pairs;
+  uint64_t cap;
+  pair_scalars *ps;
+};
+
+// Target leaf bucket bb for the lanes in `mine`: the warp first computes the bucket's element slabs into its cache
+// (lane j: element of rank 8 bb + j), then every lane of the mask tests its query against them (ranks above its own
+// in self-collision). Hits go out through one warp-aggregated reservation. Called by the whole warp.
+template< int K, typename T, int VT, bool LAZY >
+__device__ __forceinline__ void test_bucket(const trav_args< T > &x, const T *qlo, const T *qhi, uint32_t qe, int bb,
+                                            int skip, bool mine, T *cache, unsigned lane)
+{
+  constexpr int D = K / 2;
+  const int t0 = kLeafSize * bb;
+  const int cnt = min( kLeafSize, static_cast< int >( x.nt ) - t0 );
+  // The bucket's element slabs: from the target's cache when the slab kernel or an earlier visit wrote them, else
+  // computed from the vertices (and written to the cache by the one warp that claims the bucket; others never wait
+  // for it). The stored variant has every bucket ready.
+  unsigned state = 2;
+  if constexpr ( LAZY )
+  {
+  if ( lane == 0 )
+  {
+    asm volatile( "ld.acquire.gpu.global.u32 %0, [%1];" : "=r"( state ) : "l"( x.tstate + bb ) : "memory" );
+    if ( state == 0 ) state = atomicCAS( x.tstate + bb, 0u, 1u ) == 0u ? 3u : 1u;  // 3: this warp writes it
+  }
+  state = __shfl_sync( 0xffffffffu, state, 0 );
+  __syncwarp();  // orders the other lanes' cache reads after lane 0's acquire
+  }
+  T *crow = x.tcache + static_cast< size_t >( t0 ) * 2 * D;
+  // ready: test straight against the cached rows (early exit reads few slabs); else compute them into shared memory
+  const T *rows = state == 2 ? crow : cache;
+  if constexpr ( LAZY )
+  {
+  if ( state != 2 && static_cast< int >( lane ) < cnt )
+    slabs_to_row< K, T, VT >( x.tverts, x.tV, __ldg( x.tperm + t0 + lane ), x.eps, x.eps_hi, cache + lane * 2 * D );
+  __syncwarp();
+  if ( state == 3 )
+  {
+    for ( int k = static_cast< int >( lane ); k < cnt * 2 * D; k += 32 ) crow[k] = cache[k];
+    __syncwarp();
+    if ( lane == 0 )
+    {
+      __threadfence();
+      atomicExch( x.tstate + bb, 2u );
+    }
+  }
+  __syncwarp();
+  }
+  if ( mine )
+  {
+    const int r0 = max( t0, skip + 1 );
+    unsigned hits = 0;
+    for ( int r = r0; r < t0 + cnt; ++r )
+    {
+      const T *eb = rows + ( r - t0 ) * 2 * D;
+      bool o = true;
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
+      {
+        if ( !o ) break;
+        if constexpr ( LAZY ) o = qlo[a] < eb[2 * a + 1] && eb[2 * a] < qhi[a];
+        else o = qlo[a] < __ldg( eb + 2 * a + 1 ) && __ldg( eb + 2 * a ) < qhi[a];  // read-only in this variant
+      }
+      if ( o ) hits |= 1u << ( r - t0 );
+    }
+    unsigned long long pos = warp_reserve( static_cast< unsigned >( __popc( hits ) ), &x.ps->count );
+    for ( ; hits; hits &= hits - 1, ++pos )
+      if ( pos < x.cap ) x.pairs[pos] = make_uint2( qe, __ldg( x.tperm + t0 + __ffs( hits ) - 1 ) );
+  }
+  __syncwarp();  // the cache is refilled by the next leaf
 }
 
 // One packet: the union box of ranks pk*32 .. pk*32 + 31 against the target root, then the walk (see k_traverse).
-template< int K, typename T >
-__device__ __forceinline__ void traverse_packet(const uint32_t i, const unsigned lane, int2 *stack,
-                                                const T *__restrict__ qwarp, const T *__restrict__ qelem,
-                                                const uint32_t *__restrict__ qperm, uint32_t nq,
-                                                const int2 *__restrict__ child, const T *__restrict__ nbox,
-                                                const int2 *__restrict__ range, const T *__restrict__ telem,
-                                                const uint32_t *__restrict__ tperm,
-                                                const obj_scalars *__restrict__ tsc, uint32_t nt, int self,
-                                                uint2 *pairs, uint64_t cap, pair_scalars *ps, const T *rb)
+template< int K, typename T, int VT, bool LAZY >
+__device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const uint32_t i, const unsigned lane,
+                                                int2 *stack, T *cache, const T *rb)
 {
   constexpr int D = K / 2;
   constexpr int D0 = D < 4 ? D : 4;
   // 1. The packet's union box against the target's root box, first four slabs first (uniform per warp).
   {
-    const T *wb = qwarp + static_cast< size_t >( i >> 5 ) * D * 2;
+    const T *wb = x.qwarp + static_cast< size_t >( i >> 5 ) * D * 2;
     bool o = true;
 #pragma unroll
     for ( int a = 0; a < D0; ++a ) o = o && ( __ldg( wb + 2 * a ) < rb[2 * a + 1] && rb[2 * a] < __ldg( wb + 2 * a + 1 ) );
@@ -123,28 +203,40 @@ __device__ __forceinline__ void traverse_packet(const uint32_t i, const unsigned
     for ( int a = D0; a < D; ++a ) o = o && ( __ldg( wb + 2 * a ) < rb[2 * a + 1] && rb[2 * a] < __ldg( wb + 2 * a + 1 ) );
     if ( !o ) return;
   }
-  // 2. Each lane's own slabs against the root box.
-  const bool valid = i < nq;
+  // 2. Each lane's own slabs, from its element's vertices, against the root box.
+  const bool valid = i < x.nq;
+  const uint32_t qe = valid ? __ldg( x.qperm + i ) : 0u;
   T qlo[D], qhi[D];
   bool in_root = valid;
+  if constexpr ( LAZY )
   {
-    const T *qs = qelem + static_cast< size_t >( valid ? i : 0 ) * D * 2;
+    if ( valid ) leaf_slabs< K, T, VT >( x.qverts, x.qV, qe, x.eps, x.eps_hi, qlo, qhi );
+  } else {
+    const T *qs = x.qrows + static_cast< size_t >( valid ? i : 0 ) * D * 2;
 #pragma unroll
     for ( int a = 0; a < D; ++a )
     {
-      qlo[a] = valid ? __ldg( qs + 2 * a ) : T( 0 );
-      qhi[a] = valid ? __ldg( qs + 2 * a + 1 ) : T( 0 );
-      in_root = in_root && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
+      qlo[a] = __ldg( qs + 2 * a );
+      qhi[a] = __ldg( qs + 2 * a + 1 );
     }
+  }
+#pragma unroll
+  for ( int a = 0; a < D; ++a )
+  {
+    if ( !valid )
+    {
+      qlo[a] = T( 0 );
+      qhi[a] = T( 0 );
+    }
+    in_root = in_root && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
   }
   unsigned mask = __ballot_sync( 0xffffffffu, in_root );
   if ( !mask ) return;
-  const uint32_t qe = valid ? __ldg( qperm + i ) : 0u;
-  const int skip = self ? static_cast< int >( i ) : -1;  // self-collision: only ranks above the query's
-  const int root = tsc->root;
+  const int skip = x.self ? static_cast< int >( i ) : -1;  // self-collision: only ranks above the query's
+  const int root = x.tsc->root;
   if ( root < 0 )
   {
-    if ( in_root ) test_bucket< D >( qlo, qhi, qe, ~root, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
+    test_bucket< K, T, VT, LAZY >( x, qlo, qhi, qe, ~root, skip, in_root, cache, lane );
     return;
   }
   int sp = 0;
@@ -152,14 +244,15 @@ __device__ __forceinline__ void traverse_packet(const uint32_t i, const unsigned
   while ( true )
   {
     const bool me = ( mask >> lane ) & 1u;
-    const int2 c = __ldg( child + node );
-    const T *nb = nbox + static_cast< size_t >( node ) * D * 4;
+    const int2 c = __ldg( x.child + node );
+    const T *nb = x.nbox + static_cast< size_t >( node ) * D * 4;
     bool o0 = me, o1 = me;
-    if ( self )
+    if ( x.self )
     {
       // left child covers buckets [l, node], right child [node + 1, r]; skip subtrees whose last rank <= i
       o0 = o0 && kLeafSize * node + kLeafSize - 1 > static_cast< int >( i );
-      o1 = o1 && min( kLeafSize * __ldg( &range[node].y ) + kLeafSize - 1, static_cast< int >( nt ) - 1 ) > static_cast< int >( i );
+      o1 = o1 && min( kLeafSize * __ldg( &x.range[node].y ) + kLeafSize - 1, static_cast< int >( x.nt ) - 1 ) >
+                   static_cast< int >( i );
     }
 #pragma unroll
     for ( int a = 0; a < D; ++a )
@@ -175,26 +268,24 @@ __device__ __forceinline__ void traverse_packet(const uint32_t i, const unsigned
     unsigned nmask = 0;
     if ( m0 )
     {
-      if ( c.x < 0 )
+      if ( c.x < 0 ) test_bucket< K, T, VT, LAZY >( x, qlo, qhi, qe, ~c.x, skip, o0, cache, lane );
+      else
       {
-        if ( o0 ) test_bucket< D >( qlo, qhi, qe, ~c.x, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
-      } else {
         next = c.x;
         nmask = m0;
       }
     }
     if ( m1 )
     {
-      if ( c.y < 0 )
+      if ( c.y < 0 ) test_bucket< K, T, VT, LAZY >( x, qlo, qhi, qe, ~c.y, skip, o1, cache, lane );
+      else if ( next < 0 )
       {
-        if ( o1 ) test_bucket< D >( qlo, qhi, qe, ~c.y, static_cast< int >( nt ), skip, telem, tperm, pairs, cap, ps );
-      } else if ( next < 0 ) {
         next = c.y;
         nmask = m1;
       } else {
         if ( sp == kStack )
         {
-          if ( lane == 0 ) atomicCAS( &ps->error, 0, kErrOverflowStack );
+          if ( lane == 0 ) atomicCAS( &x.ps->error, 0, kErrOverflowStack );
           return;
         }
         if ( lane == 0 ) stack[sp] = make_int2( c.y, static_cast< int >( m1 ) );
@@ -215,36 +306,29 @@ __device__ __forceinline__ void traverse_packet(const uint32_t i, const unsigned
   }
 }
 
-
 // One warp per group of 32 query ranks (a packet), lane = query element. The warp walks the target tree once for
-// its packet: every lane tests its own element's slabs against both children of the current node (the node row is
-// read once for the warp, a broadcast), and a child is entered with the mask of the lanes that overlap it (a lane
-// that misses a node misses all of its descendants). Stack entries are (node, lane mask), in shared memory. At a
-// leaf bucket the lanes of the mask test their element against the bucket's elements.
-template< int K, typename T >
-__global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict__ qwarp,
-                                                           const T *__restrict__ qelem,
-                                                           const uint32_t *__restrict__ qperm, uint32_t nq,
-                                                           const int2 *__restrict__ child,
-                                                           const T *__restrict__ nbox,
-                                                           const int2 *__restrict__ range,
-                                                           const T *__restrict__ telem,
-                                                           const uint32_t *__restrict__ tperm,
-                                                           const obj_scalars *__restrict__ tsc, uint32_t nt,
-                                                           const obj_scalars *__restrict__ qsc, int self,
-                                                           uint2 *pairs, uint64_t cap, pair_scalars *ps)
+// its packet: every lane tests its own element's slabs (computed from its vertices) against both children of the
+// current node (the node row is read once for the warp, a broadcast), and a child is entered with the mask of the
+// lanes that overlap it (a lane that misses a node misses all of its descendants). Stack entries are (node, lane
+// mask), in shared memory. At a leaf bucket the warp computes the bucket's element slabs once into a shared cache
+// and the lanes of the mask test their element against them.
+template< int K, typename T, int VT, bool LAZY >
+__global__ void __launch_bounds__( kTravThreads, LAZY ? 2 : 6 ) k_traverse(const trav_args< T > x,
+                                                                         const obj_scalars *__restrict__ qsc)
 {
   constexpr int D = K / 2;
   constexpr int D0 = D < 4 ? D : 4;
   constexpr int WPB = kTravThreads / 32;
-  __shared__ int2 s_stack[WPB][kStack];  // (node, lane mask)
+  __shared__ int2 s_stack[WPB][kStack];                          // (node, lane mask)
+  __shared__ __align__( 16 ) T s_cache[WPB][kLeafSize * 2 * D];  // slabs of the leaf bucket being tested
   const unsigned lane = threadIdx.x & 31u;
   int2 *stack = s_stack[threadIdx.x >> 5];
+  T *cache = s_cache[threadIdx.x >> 5];
   // No tree exists after a failed sort of either object.
-  if ( *reinterpret_cast< const volatile int * >( &tsc->error ) == kErrTimeout ||
+  if ( *reinterpret_cast< const volatile int * >( &x.tsc->error ) == kErrTimeout ||
        *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
     return;
-  const T *rb = reinterpret_cast< const T * >( tsc->root_box );
+  const T *rb = reinterpret_cast< const T * >( x.tsc->root_box );
   // 0. Root against root: objects far apart (most pairs of a batch) end here for the whole grid.
   {
     const T *qr = reinterpret_cast< const T * >( qsc->root_box );
@@ -254,29 +338,57 @@ __global__ void __launch_bounds__( kTravThreads ) k_traverse(const T *__restrict
     if ( !o ) return;
   }
   // Packets (warps of 32 query ranks) are taken grid-stride.
-  const uint32_t packets = ( nq + 31 ) / 32;
+  const uint32_t packets = ( x.nq + 31 ) / 32;
   const uint32_t warp_stride = ( gridDim.x * blockDim.x ) >> 5;
   for ( uint32_t pk = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5; pk < packets; pk += warp_stride )
-  {
-    const uint32_t i = pk * 32 + lane;
-    traverse_packet< K, T >( i, lane, stack, qwarp, qelem, qperm, nq, child, nbox, range, telem, tperm, tsc, nt, self,
-                             pairs, cap, ps, rb );
-  }
+    traverse_packet< K, T, VT, LAZY >( x, pk * 32 + lane, lane, stack, cache, rb );
 }
 
 template< int K, typename T >
-cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, uint2 *pairs, uint64_t cap, pair_scalars *ps,
-                          cudaStream_t s)
+cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, double eps, uint2 *pairs, uint64_t cap,
+                          pair_scalars *ps, cudaStream_t s)
 {
-  // one warp per packet (the kernel strides over packets only when the grid is capped by the launch limit)
+  trav_args< T > x;
+  x.qwarp = static_cast< const T * >( q.warp_box );
+  x.qverts = q.verts;
+  x.qV = q.V;
+  x.qrows = static_cast< const T * >( q.elem_cache );
+  x.qperm = q.perm;
+  x.nq = static_cast< uint32_t >( q.n );
+  x.child = t.child;
+  x.nbox = static_cast< const T * >( t.node_box );
+  x.range = t.range;
+  x.tverts = t.verts;
+  x.tV = t.V;
+  x.tcache = static_cast< T * >( const_cast< void * >( t.elem_cache ) );
+  x.tstate = const_cast< unsigned * >( t.cache_state );
+  x.tperm = t.perm;
+  x.tsc = t.sc;
+  x.nt = static_cast< uint32_t >( t.n );
+  x.self = self ? 1 : 0;
+  x.eps = eps;
+  x.eps_hi = f32_round_up( eps );
+  x.pairs = pairs;
+  x.cap = cap;
+  x.ps = ps;
+  // one warp per packet
   const uint64_t blocks = ( q.n + kTravThreads - 1 ) / kTravThreads;
-  const uint64_t capb = 1ull << 30;
-  const unsigned grid = static_cast< unsigned >( blocks < capb ? blocks : capb );
-  k_traverse< K, T ><<< grid, kTravThreads, 0, s >>>(
-    static_cast< const T * >( q.warp_box ), static_cast< const T * >( q.elem_box ), q.perm,
-    static_cast< uint32_t >( q.n ), t.child, static_cast< const T * >( t.node_box ), t.range,
-    static_cast< const T * >( t.elem_box ), t.perm, t.sc, static_cast< uint32_t >( t.n ), q.sc, self ? 1 : 0, pairs,
-    cap, ps );
+  const unsigned grid = static_cast< unsigned >( blocks < ( 1ull << 30 ) ? blocks : ( 1ull << 30 ) );
+  // both objects' element slabs stored (dense contact): the variant that only reads them; else the one that
+  // computes the slabs it tests from the vertices (unrolled when both objects have the same vertex count)
+  if ( q.stored && t.stored )
+  {
+    k_traverse< K, T, 3, false ><<< grid, kTravThreads, 0, s >>>( x, q.sc );
+    return cudaGetLastError();
+  }
+  const uint32_t V = q.V == t.V ? q.V : 0;
+  switch ( V )
+  {
+    case 3: k_traverse< K, T, 3, true ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+    case 4: k_traverse< K, T, 4, true ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+    case 8: k_traverse< K, T, 8, true ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+    default: k_traverse< K, T, 0, true ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+  }
   return cudaGetLastError();
 }
 
@@ -422,17 +534,17 @@ cudaError_t launch_gather_words(const int *const *src, int n, int *dst, cudaStre
   return cudaGetLastError();
 }
 
-cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, uint2 *pairs, uint64_t cap,
-                            pair_scalars *ps, cudaStream_t s)
+cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, double eps, uint2 *pairs,
+                            uint64_t cap, pair_scalars *ps, cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return fp32 ? launch_trav_t< 6, float >( q, t, self, pairs, cap, ps, s )
-                        : launch_trav_t< 6, double >( q, t, self, pairs, cap, ps, s );
-    case 18: return fp32 ? launch_trav_t< 18, float >( q, t, self, pairs, cap, ps, s )
-                         : launch_trav_t< 18, double >( q, t, self, pairs, cap, ps, s );
-    case 26: return fp32 ? launch_trav_t< 26, float >( q, t, self, pairs, cap, ps, s )
-                         : launch_trav_t< 26, double >( q, t, self, pairs, cap, ps, s );
+    case 6: return fp32 ? launch_trav_t< 6, float >( q, t, self, eps, pairs, cap, ps, s )
+                        : launch_trav_t< 6, double >( q, t, self, eps, pairs, cap, ps, s );
+    case 18: return fp32 ? launch_trav_t< 18, float >( q, t, self, eps, pairs, cap, ps, s )
+                         : launch_trav_t< 18, double >( q, t, self, eps, pairs, cap, ps, s );
+    case 26: return fp32 ? launch_trav_t< 26, float >( q, t, self, eps, pairs, cap, ps, s )
+                         : launch_trav_t< 26, double >( q, t, self, eps, pairs, cap, ps, s );
     default: return cudaErrorInvalidValue;
   }
 }

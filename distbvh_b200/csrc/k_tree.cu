@@ -21,14 +21,6 @@ namespace {
 
 constexpr int kBuildThreads = 256;
 
-// epsilon rounded up to FP32 (host side).
-float f32_up(double x)
-{
-  if ( x == 0.0 ) return 0.f;
-  float f = static_cast< float >( x );
-  if ( static_cast< double >( f ) < x ) f = nextafterf( f, INFINITY );
-  return f;
-}
 
 // Dissimilarity of ranks j and j + 1: 33 + highest differing key bit when the keys differ, else
 // 1 + highest differing bit of the ranks. Larger = more different.
@@ -79,85 +71,6 @@ struct box_io< float >
   __device__ static float mx(float a, float b) { return fmaxf( a, b ); }
 };
 
-// Slabs of element e (gathered vertices) into lo/hi.
-template< int K, typename T, int VT >
-__device__ __forceinline__ void leaf_slabs(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
-                                           float eps_hi, T *lo, T *hi)
-{
-  constexpr int D = K / 2;
-  constexpr int VMAX = VT > 0 ? VT : 32;
-  const int V = VT > 0 ? VT : static_cast< int >( Vrt );
-  double p[VT > 0 ? VT * 3 : 3];
-  const double *src = verts + static_cast< size_t >( e ) * V * 3;
-  if constexpr ( VT > 0 )
-  {
-#pragma unroll
-    for ( int k = 0; k < VT * 3; ++k ) p[k] = __ldg( src + k );
-#pragma unroll
-    for ( int a = 0; a < D; ++a )
-    {
-      if constexpr ( sizeof( T ) == 8 )
-      {
-        double l, h;
-        slab64< K >( p, VT, a, eps, l, h );
-        lo[a] = l;
-        hi[a] = h;
-      } else {
-        float l, h;
-        slab32< K >( p, VT, a, eps_hi, l, h );
-        lo[a] = l;
-        hi[a] = h;
-      }
-    }
-  } else {
-    (void)VMAX;
-    (void)p;
-    // Generic vertex count: one vertex at a time, slab by slab (vertices re-read from L1).
-#pragma unroll
-    for ( int a = 0; a < D; ++a )
-    {
-      if constexpr ( sizeof( T ) == 8 )
-      {
-        double l = 0, h = 0;
-        for ( int v = 0; v < V; ++v )
-        {
-          const double q[3] = { __ldg( src + 3 * v ), __ldg( src + 3 * v + 1 ), __ldg( src + 3 * v + 2 ) };
-          double vl, vh;
-          slab64< K >( q, 1, a, eps, vl, vh );
-          if ( v == 0 )
-          {
-            l = vl;
-            h = vh;
-          } else {
-            l = std_min( l, vl );
-            h = std_max( h, vh );
-          }
-        }
-        lo[a] = l;
-        hi[a] = h;
-      } else {
-        float l = 0, h = 0;
-        for ( int v = 0; v < V; ++v )
-        {
-          const double q[3] = { __ldg( src + 3 * v ), __ldg( src + 3 * v + 1 ), __ldg( src + 3 * v + 2 ) };
-          float vl, vh;
-          slab32< K >( q, 1, a, eps_hi, vl, vh );
-          if ( v == 0 )
-          {
-            l = vl;
-            h = vh;
-          } else {
-            l = fminf( l, vl );
-            h = fmaxf( h, vh );
-          }
-        }
-        lo[a] = l;
-        hi[a] = h;
-      }
-    }
-  }
-}
-
 // The root's slabs, for the traversal's first test.
 template< typename T, size_t D >
 __device__ __forceinline__ void store_root(obj_scalars *sc, const T ( &lo )[D], const T ( &hi )[D])
@@ -189,17 +102,20 @@ __device__ __forceinline__ long long bdelta(const uint64_t *__restrict__ keys, i
 
 constexpr int kSlabThreads = 128;  // ranks per block of the element slab kernel
 
-// Element slabs in rank order, one thread per rank (the element perm[r] of rank r); then, per block of 128 ranks,
-// the unions of its 16 leaf buckets and its 4 query groups of 32 ranks. The rows are staged in shared memory
-// (padded to C + 1 components against bank conflicts) and written out coalesced: elem_box row r, bucket_box row
-// b and warp_box row g each hold the C = 2 D values (min, max) per slab. A one-bucket object also gets its root
-// box here. A rank whose index is not an element index marks a failed sort.
+// Element slabs in rank order, one thread per rank (the element perm[r] of rank r), staged in shared memory (padded
+// to C + 1 components against bank conflicts); per block of 128 ranks, the unions of its 16 leaf buckets and its 4
+// query groups of 32 ranks are written out coalesced: bucket_box row b and warp_box row g each hold the C = 2 D
+// values (min, max) per slab. The element slabs themselves go to elem_rows (row r: rank r) only when given (objects
+// in dense contact, whose traversals test most buckets); otherwise the traversal computes the few it tests from the
+// vertices and caches them. cache_state marks each bucket's rows ready (2) or not (0). A one-bucket object also gets
+// its root box here. A rank whose index is not an element index marks a failed sort.
 template< int K, typename T, int VT >
 __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( VT == 8 ? 3 : 4 ) ) k_elem_slabs(const double *__restrict__ verts, uint32_t Vrt,
                                                                   int n, double eps, float eps_hi,
                                                                   const uint32_t *__restrict__ vals,
-                                                                  T *__restrict__ elem_box, T *__restrict__ bucket_box,
-                                                                  T *__restrict__ warp_box, obj_scalars *sc)
+                                                                  T *__restrict__ bucket_box, T *__restrict__ warp_box,
+                                                                  T *__restrict__ elem_rows,
+                                                                  unsigned *__restrict__ cache_state, obj_scalars *sc)
 {
   constexpr int D = K / 2;
   constexpr int C = 2 * D;
@@ -212,6 +128,8 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
   const int tid = threadIdx.x;
   const int r0 = static_cast< int >( blockIdx.x ) * kSlabThreads;
   const int rows = min( kSlabThreads, n - r0 );
+  // the traversal's element-slab cache of these buckets: written here (ready), or stale from here on
+  if ( tid < ( rows + kLeafSize - 1 ) / kLeafSize ) cache_state[r0 / kLeafSize + tid] = elem_rows ? 2u : 0u;
   if ( tid < rows )
   {
     const uint32_t e = __ldg( vals + r0 + tid );
@@ -237,11 +155,14 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
     }
   }
   __syncthreads();
-  T *eb = elem_box + static_cast< size_t >( r0 ) * C;
-  for ( int k = tid; k < rows * C; k += kSlabThreads )
+  if ( elem_rows )
   {
-    const int q = k / C;
-    eb[k] = s_el[q * P + ( k - q * C )];
+    T *eb = elem_rows + static_cast< size_t >( r0 ) * C;
+    for ( int k = tid; k < rows * C; k += kSlabThreads )
+    {
+      const int q = k / C;
+      eb[k] = s_el[q * P + ( k - q * C )];
+    }
   }
   // bucket unions (ranks in order, as the serial union of the reference merges them)
   const int nb = ( rows + kLeafSize - 1 ) / kLeafSize;
@@ -667,26 +588,27 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(int n, const T *__res
 
 template< int K, typename T, int VT >
 cudaError_t launch_slabs_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
-                           void *elem_box, void *bucket_box, void *warp_box, obj_scalars *sc, cudaStream_t s)
+                           void *bucket_box, void *warp_box, void *elem_rows, unsigned *cache_state, obj_scalars *sc,
+                           cudaStream_t s)
 {
   const unsigned grid = static_cast< unsigned >( ( n + kSlabThreads - 1 ) / kSlabThreads );
-  k_elem_slabs< K, T, VT ><<< grid, kSlabThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, f32_up( eps ),
-                                                           vals, static_cast< T * >( elem_box ),
-                                                           static_cast< T * >( bucket_box ),
-                                                           static_cast< T * >( warp_box ), sc );
+  k_elem_slabs< K, T, VT ><<< grid, kSlabThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, f32_round_up( eps ),
+                                                           vals, static_cast< T * >( bucket_box ),
+                                                           static_cast< T * >( warp_box ),
+                                                           static_cast< T * >( elem_rows ), cache_state, sc );
   return cudaGetLastError();
 }
 
 template< int K, typename T >
-cudaError_t slabs_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *eb, void *bb,
-                    void *wb, obj_scalars *sc, cudaStream_t s)
+cudaError_t slabs_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *bb, void *wb,
+                    void *er, unsigned *cs, obj_scalars *sc, cudaStream_t s)
 {
   switch ( V )
   {
-    case 3: return launch_slabs_t< K, T, 3 >( verts, V, n, eps, vals, eb, bb, wb, sc, s );
-    case 4: return launch_slabs_t< K, T, 4 >( verts, V, n, eps, vals, eb, bb, wb, sc, s );
-    case 8: return launch_slabs_t< K, T, 8 >( verts, V, n, eps, vals, eb, bb, wb, sc, s );
-    default: return launch_slabs_t< K, T, 0 >( verts, V, n, eps, vals, eb, bb, wb, sc, s );
+    case 3: return launch_slabs_t< K, T, 3 >( verts, V, n, eps, vals, bb, wb, er, cs, sc, s );
+    case 4: return launch_slabs_t< K, T, 4 >( verts, V, n, eps, vals, bb, wb, er, cs, sc, s );
+    case 8: return launch_slabs_t< K, T, 8 >( verts, V, n, eps, vals, bb, wb, er, cs, sc, s );
+    default: return launch_slabs_t< K, T, 0 >( verts, V, n, eps, vals, bb, wb, er, cs, sc, s );
   }
 }
 
@@ -753,7 +675,7 @@ __global__ void k_probe_kdops(const double *__restrict__ verts, uint32_t Vrt, ui
 template< int K, typename T >
 cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, void *out, cudaStream_t s)
 {
-  const float eps_hi = f32_up( eps );
+  const float eps_hi = f32_round_up( eps );
   const unsigned grid = static_cast< unsigned >( ( n + 255 ) / 256 );
   if ( V == 3 ) k_probe_kdops< K, T, 3 ><<< grid, 256, 0, s >>>( verts, V, n, eps, eps_hi, static_cast< T * >( out ) );
   else if ( V == 4 ) k_probe_kdops< K, T, 4 ><<< grid, 256, 0, s >>>( verts, V, n, eps, eps_hi, static_cast< T * >( out ) );
@@ -765,17 +687,17 @@ cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, voi
 }  // namespace
 
 cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *elem_box, void *bucket_box, void *warp_box, obj_scalars *sc,
-                         cudaStream_t s)
+                         const uint32_t *vals, void *bucket_box, void *warp_box, void *elem_rows,
+                         unsigned *cache_state, obj_scalars *sc, cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return fp32 ? slabs_v< 6, float >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s )
-                        : slabs_v< 6, double >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s );
-    case 18: return fp32 ? slabs_v< 18, float >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s )
-                         : slabs_v< 18, double >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s );
-    case 26: return fp32 ? slabs_v< 26, float >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s )
-                         : slabs_v< 26, double >( verts, V, n, eps, vals, elem_box, bucket_box, warp_box, sc, s );
+    case 6: return fp32 ? slabs_v< 6, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s )
+                        : slabs_v< 6, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s );
+    case 18: return fp32 ? slabs_v< 18, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s )
+                         : slabs_v< 18, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s );
+    case 26: return fp32 ? slabs_v< 26, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s )
+                         : slabs_v< 26, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s );
     default: return cudaErrorInvalidValue;
   }
 }

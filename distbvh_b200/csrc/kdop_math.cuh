@@ -11,10 +11,20 @@
 // a32.min <= a64.min < b64.max <= b32.max, so the FP32 candidate set is a superset of the FP64 pair set.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace bvhg {
+
+// epsilon rounded up to FP32 (host side): the FP32 enclosure's inflation.
+inline float f32_round_up(double x)
+{
+  if ( x == 0.0 ) return 0.f;
+  float f = static_cast< float >( x );
+  if ( static_cast< double >( f ) < x ) f = nextafterf( f, INFINITY );
+  return f;
+}
 
 constexpr double kOverRoot2 = 0.7071067811865475;  // dop_18::over_root_2, dop_26::one_over_root_2 (kdop.hpp:608,659)
 constexpr double kOverRoot3 = 0.5773502691896258;  // dop_26::one_over_root_3 (kdop.hpp:660)
@@ -184,6 +194,85 @@ __device__ __forceinline__ void slab32(const double *p, int V, int a, float eps_
     }
     lo = fminf( lo, slo );
     hi = fmaxf( hi, shi );
+  }
+}
+
+// Slabs of element e (gathered vertices) into lo/hi.
+template< int K, typename T, int VT >
+__device__ __forceinline__ void leaf_slabs(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
+                                           float eps_hi, T *lo, T *hi)
+{
+  constexpr int D = K / 2;
+  constexpr int VMAX = VT > 0 ? VT : 32;
+  const int V = VT > 0 ? VT : static_cast< int >( Vrt );
+  double p[VT > 0 ? VT * 3 : 3];
+  const double *src = verts + static_cast< size_t >( e ) * V * 3;
+  if constexpr ( VT > 0 )
+  {
+#pragma unroll
+    for ( int k = 0; k < VT * 3; ++k ) p[k] = __ldg( src + k );
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      if constexpr ( sizeof( T ) == 8 )
+      {
+        double l, h;
+        slab64< K >( p, VT, a, eps, l, h );
+        lo[a] = l;
+        hi[a] = h;
+      } else {
+        float l, h;
+        slab32< K >( p, VT, a, eps_hi, l, h );
+        lo[a] = l;
+        hi[a] = h;
+      }
+    }
+  } else {
+    (void)VMAX;
+    (void)p;
+    // Generic vertex count: one vertex at a time, slab by slab (vertices re-read from L1).
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      if constexpr ( sizeof( T ) == 8 )
+      {
+        double l = 0, h = 0;
+        for ( int v = 0; v < V; ++v )
+        {
+          const double q[3] = { __ldg( src + 3 * v ), __ldg( src + 3 * v + 1 ), __ldg( src + 3 * v + 2 ) };
+          double vl, vh;
+          slab64< K >( q, 1, a, eps, vl, vh );
+          if ( v == 0 )
+          {
+            l = vl;
+            h = vh;
+          } else {
+            l = std_min( l, vl );
+            h = std_max( h, vh );
+          }
+        }
+        lo[a] = l;
+        hi[a] = h;
+      } else {
+        float l = 0, h = 0;
+        for ( int v = 0; v < V; ++v )
+        {
+          const double q[3] = { __ldg( src + 3 * v ), __ldg( src + 3 * v + 1 ), __ldg( src + 3 * v + 2 ) };
+          float vl, vh;
+          slab32< K >( q, 1, a, eps_hi, vl, vh );
+          if ( v == 0 )
+          {
+            l = vl;
+            h = vh;
+          } else {
+            l = fminf( l, vl );
+            h = fmaxf( h, vh );
+          }
+        }
+        lo[a] = l;
+        hi[a] = h;
+      }
+    }
   }
 }
 

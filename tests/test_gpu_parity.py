@@ -378,3 +378,24 @@ def test_precision_form_on_the_tet_lattice():
         s64 = c64.kdops(a64, a.shape[0])
         s32 = c32.kdops(a32, a.shape[0]).astype(np.float64)
         assert (s32[:, :, 0] <= s64[:, :, 0]).all() and (s64[:, :, 1] <= s32[:, :, 1]).all()
+
+
+@pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
+def test_stored_and_computed_element_slabs_agree(precision):
+    """Traversals compute the element slabs they test from the vertices (sparse contact) or read the ones the build
+    stored (dense contact, decided from the previous broadphase's candidate count): both give the exact set."""
+    m = 14
+    xyz = meshes.tet_lattice(m)
+    even = meshes.checkerboard(m)
+    a, b = np.ascontiguousarray(xyz[even]), np.ascontiguousarray(xyz[~even])
+    want = orc.pair_set(a, b, 26)
+    want_self = orc.self_pair_set(a, 26)
+    with bvhg.Context(k=26, precision=precision) as ctx:
+        for step in range(3):  # first build: computed; later builds: stored (the contact is dense)
+            oa, ob = (build_pair(ctx, a, b) if step == 0 else (oa, ob))
+            if step:
+                ctx.build(oa)
+                ctx.build(ob)
+            assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), want), step
+            assert np.array_equal(orc.canonical(ctx.self_collision(oa)), want_self), step
+            ctx.validate_tree(oa)
