@@ -72,20 +72,45 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned k, unsigned 
   return base + pre;
 }
 
-// Slabs of element e straight into a shared-memory row (C = 2 D values: min, max per slab), as leaf_slabs computes
-// them (the same FP64 slabs, or the same FP32 enclosures, that k_elem_slabs unites into the bucket boxes).
+// Slabs of element e straight into a shared-memory row (C = 2 D values: min, max per slab), slab by slab so that
+// only the vertices stay in registers: the same FP64 slabs, or the same FP32 enclosures, that k_elem_slabs unites
+// into the bucket boxes.
 template< int K, typename T, int VT >
-__device__ __noinline__ void slabs_to_row(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
+__device__ __forceinline__ void slabs_to_row(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
                                              float eps_hi, T *row)
 {
   constexpr int D = K / 2;
-  T lo[D], hi[D];
-  leaf_slabs< K, T, VT >( verts, Vrt, e, eps, eps_hi, lo, hi );
-#pragma unroll
-  for ( int a = 0; a < D; ++a )
+  if constexpr ( VT > 0 )
   {
-    row[2 * a] = lo[a];
-    row[2 * a + 1] = hi[a];
+    double p[VT * 3];
+    const double *src = verts + static_cast< size_t >( e ) * VT * 3;
+#pragma unroll
+    for ( int k = 0; k < VT * 3; ++k ) p[k] = __ldg( src + k );
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      if constexpr ( sizeof( T ) == 8 )
+      {
+        double l, h;
+        slab64< K >( p, VT, a, eps, l, h );
+        row[2 * a] = l;
+        row[2 * a + 1] = h;
+      } else {
+        float l, h;
+        slab32< K >( p, VT, a, eps_hi, l, h );
+        row[2 * a] = l;
+        row[2 * a + 1] = h;
+      }
+    }
+  } else {
+    T lo[D], hi[D];
+    leaf_slabs< K, T, 0 >( verts, Vrt, e, eps, eps_hi, lo, hi );
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      row[2 * a] = lo[a];
+      row[2 * a + 1] = hi[a];
+    }
   }
 }
 
@@ -313,7 +338,7 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
 // mask), in shared memory. At a leaf bucket the warp computes the bucket's element slabs once into a shared cache
 // and the lanes of the mask test their element against them.
 template< int K, typename T, int VT, bool LAZY >
-__global__ void __launch_bounds__( kTravThreads, LAZY ? 2 : 6 ) k_traverse(const trav_args< T > x,
+__global__ void __launch_bounds__( kTravThreads, LAZY ? 4 : 6 ) k_traverse(const trav_args< T > x,
                                                                          const obj_scalars *__restrict__ qsc)
 {
   constexpr int D = K / 2;
