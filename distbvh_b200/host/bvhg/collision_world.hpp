@@ -16,12 +16,13 @@
 //     returning a contiguous range of 3-vectors indexable as v[0..2], and `e.global_id()` (or
 //     get_entity_global_id(e)). The library computes the k-DOP exactly as kdop_base::from_vertices
 //     (src/bvh/kdop.hpp:238-264) with world_config::k (26 by default: the reference's bphase_kdop).
-//   - Patches: an object's elements are split into od_factor patches of consecutive Morton ranks (the reference's
-//     clustering splits the same order at its largest key jumps, src/bvh/split/cluster.hpp:89-179). The functor
-//     is called once for every patch pair that holds at least one overlapping element pair (the reference calls
-//     it for every pair of overlapping patch k-DOPs, a superset), with both patches' elements as spans in rank
-//     order and, in addition, the exact element pairs of that patch pair (broadphase_collision::candidates,
-//     indices into the two spans). A functor that only reports overlapping elements gives the same results.
+//   - Patches: an object's elements are split into od_factor patches exactly as the reference's Morton clustering
+//     splits them (morton_cluster, src/bvh/split/cluster.hpp:89-179; every split algorithm uses it here). The
+//     functor is called once for every patch pair that holds at least one overlapping element pair (the reference
+//     calls it for every pair of overlapping patch k-DOPs, a superset), with both patches' elements as spans in
+//     the reference's order and, in addition, the exact element pairs of that patch pair
+//     (broadphase_collision::candidates, indices into the two spans). A functor that only reports overlapping
+//     elements gives the same results.
 //   - The element bytes handed to the functor are copies made at init_broadphase (the reference ships copies to
 //     the narrowphase rank too); the caller's array is read only during set_entity_data.
 //   - Errors throw bvhg::error (the reference asserts and terminates).
@@ -30,6 +31,7 @@
 
 #include "../../../include/bvhg.h"
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -200,6 +202,46 @@ const void *type_id()
   static const char id = 0;
   return &id;
 }
+// The reference's Morton clustering (src/bvh/split/cluster.hpp:89-179) from the library's sorted 63-bit keys and
+// permutation (order[r] = element of rank r): the 32-bit Morton hash of an element is its 63-bit key shifted right
+// by 33 (quantize32 keeps the top 10 of the 21 bits per axis); the order becomes the stable one of the hashes
+// (equal hashes in element order); the split depth of neighbours i, i + 1 is 31 - floor(log2(h_i ^ h_{i+1})) (all
+// ones for equal hashes); the P - 1 smallest depths (ties: the lower position) are the splits; and patch k spans
+// positions [split[k - 1], split[k]) of that order, as set_entity_data_impl cuts it
+// (src/bvh/collision_object.cpp:125-133). Returns the P + 1 patch boundaries.
+inline std::vector< std::size_t > morton_cluster(const std::vector< uint64_t > &keys, std::vector< uint32_t > &order,
+                                                 std::size_t P)
+{
+  const std::size_t n = keys.size();
+  for ( std::size_t r = 0; r < n; )
+  {
+    std::size_t e = r + 1;
+    while ( e < n && ( keys[e] >> 33 ) == ( keys[r] >> 33 ) ) ++e;
+    std::sort( order.begin() + r, order.begin() + e );
+    r = e;
+  }
+  const std::size_t nsplit = P - 1;
+  std::vector< std::size_t > split( nsplit, n > 0 ? n - 1 : 0 );
+  if ( n > 1 && nsplit > 0 )
+  {
+    std::vector< std::pair< uint32_t, uint32_t > > d( n - 1 );
+    for ( std::size_t i = 0; i + 1 < n; ++i )
+    {
+      const uint32_t mask = static_cast< uint32_t >( ( keys[i] >> 33 ) ^ ( keys[i + 1] >> 33 ) );
+      d[i] = { mask ? static_cast< uint32_t >( __builtin_clz( mask ) ) : 0xffffffffu, static_cast< uint32_t >( i ) };
+    }
+    const std::size_t take = std::min( nsplit, n - 1 );
+    std::nth_element( d.begin(), d.begin() + ( take - 1 ), d.end() );
+    std::vector< std::size_t > chosen;
+    for ( std::size_t k = 0; k < take; ++k ) chosen.push_back( d[k].second );
+    std::sort( chosen.begin(), chosen.end() );
+    for ( std::size_t k = 0; k < take; ++k ) split[k] = chosen[k];
+  }
+  std::vector< std::size_t > pbeg( P + 1, 0 );
+  for ( std::size_t k = 1; k < P; ++k ) pbeg[k] = split[k - 1];
+  pbeg[P] = n;
+  return pbeg;
+}
 }  // namespace detail
 
 class collision_world;
@@ -270,6 +312,17 @@ public:
   // The exact element pairs (global ids) of the last broadphase with `other`.
   const std::vector< std::pair< uint64_t, uint64_t > > &last_pairs() const { return m_last_pairs; }
 
+  // Global ids of each patch's elements, in the patch order (after init_broadphase).
+  std::vector< std::vector< uint64_t > > patch_global_ids() const
+  {
+    std::vector< std::vector< uint64_t > > out( num_patches() );
+    std::vector< uint32_t > order( m_n );
+    for ( std::size_t i = 0; i < m_n; ++i ) order[m_rank[i]] = static_cast< uint32_t >( i );
+    for ( std::size_t p = 0; p < out.size(); ++p )
+      for ( std::size_t r = m_pbeg[p]; r < m_pbeg[p + 1]; ++r ) out[p].push_back( m_gid[order[r]] );
+    return out;
+  }
+
   std::size_t id() const noexcept { return m_id; }
   int overdecomposition_factor() const noexcept;
   std::size_t num_patches() const noexcept;
@@ -284,12 +337,12 @@ private:
   collision_object(collision_world &w, std::size_t id);
   bvhg_ctx *ctx() const;
 
+  // the patch holding position r of the patch order, and where patch p starts (m_pbeg has od_factor + 1 entries)
   std::size_t patch_of_rank(std::size_t r) const
   {
-    const std::size_t p = num_patches();
-    return p <= 1 ? 0 : ( r * p ) / m_n;
+    return static_cast< std::size_t >( std::upper_bound( m_pbeg.begin(), m_pbeg.end(), r ) - m_pbeg.begin() ) - 1;
   }
-  std::size_t patch_begin(std::size_t p) const { return ( p * m_n + num_patches() - 1 ) / num_patches(); }
+  std::size_t patch_begin(std::size_t p) const { return m_pbeg[p]; }
 
   collision_world &m_world;
   std::size_t m_id;
@@ -298,8 +351,9 @@ private:
   bool m_built = false;
   std::vector< uint64_t > m_gid;
   std::vector< unsigned char > m_src;  // the caller's elements, original order
-  detail::element_store m_elems;       // rank order (after init_broadphase)
-  std::vector< uint32_t > m_rank;      // rank of element i
+  detail::element_store m_elems;       // patch order (after init_broadphase)
+  std::vector< uint32_t > m_rank;      // position of element i in the patch order
+  std::vector< std::size_t > m_pbeg;   // patch p = positions [m_pbeg[p], m_pbeg[p + 1])
   std::vector< narrowphase_result > m_results;
   std::vector< std::pair< uint64_t, uint64_t > > m_last_pairs;
 };
@@ -389,22 +443,22 @@ inline collision_object::collision_object(collision_world &w, std::size_t id) : 
 
 inline bvhg_ctx *collision_object::ctx() const { return m_world.ctx(); }
 inline int collision_object::overdecomposition_factor() const noexcept { return static_cast< int >( m_world.m_od ); }
-inline std::size_t collision_object::num_patches() const noexcept
-{
-  return m_n == 0 ? 0 : ( m_world.m_od < m_n ? m_world.m_od : m_n );
-}
+inline std::size_t collision_object::num_patches() const noexcept { return m_world.m_od; }
 
 inline void collision_object::init_broadphase()
 {
   detail::check( ctx(), bvhg_build( ctx(), m_obj, BVHG_REBUILD ), "init_broadphase" );
-  std::vector< uint32_t > perm( m_n );
-  if ( m_n ) detail::check( ctx(), bvhg_get_morton( ctx(), m_obj, nullptr, perm.data(), nullptr, nullptr ), "init_broadphase" );
+  std::vector< uint32_t > order( m_n );
+  std::vector< uint64_t > keys( m_n );
+  if ( m_n )
+    detail::check( ctx(), bvhg_get_morton( ctx(), m_obj, keys.data(), order.data(), nullptr, nullptr ), "init_broadphase" );
+  m_pbeg = detail::morton_cluster( keys, order, m_world.m_od );
   m_rank.assign( m_n, 0 );
   m_elems.bytes.assign( m_n * m_elems.elem_size, 0 );
   for ( std::size_t r = 0; r < m_n; ++r )
   {
-    m_rank[perm[r]] = static_cast< uint32_t >( r );
-    std::memcpy( m_elems.bytes.data() + r * m_elems.elem_size, m_src.data() + perm[r] * m_elems.elem_size,
+    m_rank[order[r]] = static_cast< uint32_t >( r );
+    std::memcpy( m_elems.bytes.data() + r * m_elems.elem_size, m_src.data() + order[r] * m_elems.elem_size,
                  m_elems.elem_size );
   }
   m_built = true;

@@ -35,6 +35,8 @@ class Ref:
             f.restype = _U
         L.ref_self_pairs.argtypes = [_P, _U, _I, _D, _P, _U]
         L.ref_self_pairs.restype = _U
+        L.ref_radix_sort_u64.argtypes = [_P, _U, _P, _P]
+        L.ref_cluster.argtypes = [_P, _U, _I, _U, _P, _P]
         self.lib = L
         self.tree_k = L.ref_tree_k()
         assert self.tree_k == tree_k
@@ -84,3 +86,20 @@ class Ref:
         b = np.ascontiguousarray(b, dtype=np.float64)
         return self._pairs(self.lib.ref_brute_pairs18, a.ctypes.data, a.shape[0], b.ctypes.data, b.shape[0],
                            a.shape[1], eps, cap=cap)
+
+    def radix_sort_u64(self, keys):
+        """The reference's stable 1-bit radix sort: (sorted keys, permutation)."""
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        out = np.zeros_like(keys)
+        perm = np.zeros(keys.shape[0], dtype=np.uint64)
+        self.lib.ref_radix_sort_u64(keys.ctypes.data, keys.shape[0], out.ctypes.data, perm.ctypes.data)
+        return out, perm
+
+    def cluster(self, xyz, clusters):
+        """morton_cluster: (element order, clusters - 1 split positions)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        order = np.zeros(xyz.shape[0], dtype=np.uint64)
+        splits = np.zeros(max(clusters - 1, 0), dtype=np.uint64)
+        self.lib.ref_cluster(xyz.ctypes.data, xyz.shape[0], xyz.shape[1], clusters, order.ctypes.data,
+                             splits.ctypes.data)
+        return order, splits

@@ -12,7 +12,9 @@
 #include <bvh/hash.hpp>
 #include <bvh/kdop.hpp>
 #include <bvh/snapshot.hpp>
+#include <bvh/split/cluster.hpp>
 #include <bvh/tree_build.hpp>
+#include <bvh/util/sort.hpp>
 
 #include <cstdint>
 #include <vector>
@@ -195,5 +197,40 @@ uint64_t ref_brute_pairs18(const double *xa, uint64_t na, const double *xb, uint
         ++cnt;
       }
   return cnt;
+}
+
+// The reference's stable 1-bit radix sort (src/bvh/util/sort.hpp:75-144) of n 64-bit keys with their indices.
+void ref_radix_sort_u64(const uint64_t *keys, uint64_t n, uint64_t *sorted, uint64_t *perm)
+{
+  bvh::radix_sorter< uint64_t, std::size_t > sorter( n );
+  bvh::view< uint64_t * > h( "keys", n );
+  bvh::view< std::size_t * > idx( "indices", n );
+  for ( uint64_t i = 0; i < n; ++i )
+  {
+    h( i ) = keys[i];
+    idx( i ) = i;
+  }
+  sorter( h, idx );
+  for ( uint64_t i = 0; i < n; ++i )
+  {
+    sorted[i] = h( i );
+    perm[i] = idx( i );
+  }
+}
+
+// Morton clustering of the elements into `clusters` patches (morton_cluster, src/bvh/split/cluster.hpp:89-179, as
+// set_entity_data_clustering uses it, src/bvh/collision_object.hpp:89-131): order[r] = element of rank r, splits
+// (clusters - 1 values) = the patch boundaries in that order (patch k = ranks [splits[k-1], splits[k])).
+void ref_cluster(const double *xyz, uint64_t n, int V, uint64_t clusters, uint64_t *order, uint64_t *splits)
+{
+  auto el = make_elements( xyz, n, V, 0.0 );
+  bvh::morton_cluster mc( n );
+  bvh::view< const ref_element * > ev( el.data(), n );
+  bvh::view< std::size_t * > idx( "indices", n );
+  for ( uint64_t i = 0; i < n; ++i ) idx( i ) = i;
+  bvh::view< std::size_t * > sp( "splits", clusters > 0 ? clusters - 1 : 0 );
+  mc( ev, idx, sp );
+  for ( uint64_t i = 0; i < n; ++i ) order[i] = idx( i );
+  for ( uint64_t k = 0; k + 1 < clusters; ++k ) splits[k] = sp( k );
 }
 }

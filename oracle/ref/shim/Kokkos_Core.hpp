@@ -108,6 +108,38 @@ std::enable_if_t< !std::is_arithmetic_v< B > > deep_copy(const A &dst, const B &
   for ( std::size_t i = 0; i < dst.size(); ++i ) dst( i ) = src( i );
 }
 
+template< class... >
+struct RangePolicy
+{
+  std::size_t b, e;
+  RangePolicy(std::size_t b_, std::size_t e_) : b( b_ ), e( e_ ) {}
+};
+
+template< class F, class... P >
+void parallel_for(const RangePolicy< P... > &p, const F &f)
+{
+  for ( std::size_t i = p.b; i < p.e; ++i ) f( static_cast< int >( i ) );
+}
+
+namespace detail
+{
+template< class M >
+struct scan_value;
+template< class C, class R, class A0, class A1, class A2 >
+struct scan_value< R ( C::* )( A0, A1, A2 ) const >
+{
+  using type = std::remove_cv_t< std::remove_reference_t< A1 > >;
+};
+}  // namespace detail
+
+// One host thread: the scan functor sees every index once, in order, with final = true.
+template< class F >
+void parallel_scan(std::size_t n, const F &f)
+{
+  typename detail::scan_value< decltype( &F::operator() ) >::type acc{};
+  for ( std::size_t i = 0; i < n; ++i ) f( static_cast< int >( i ), acc, true );
+}
+
 template< class F >
 void parallel_for(std::size_t n, const F &f)
 {

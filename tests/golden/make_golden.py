@@ -2,6 +2,9 @@
 reference's headers through oracle/_ref (build it first with oracle/ref_build.sh; the reference sources are
 needed only here, not by the tests that read the fixture).
 
+Also the reference's Morton clustering of a 700-triangle soup into 1, 8 and 64 patches and its 1-bit radix sort of
+3000 keys with duplicates.
+
 Cases: seeded element soups of triangles, tetrahedra and hexahedra (two objects each) and two small plates in
 the shape of the reference's two-plate contact case, each with inflation 0 and 0.003 (plates: 0.005). Stored per
 case and object: vertices; k-DOP slabs for K = 6, 18, 26 (kdop_base::from_vertices; 18 through dop_18's
@@ -69,6 +72,17 @@ def main():
             out[f"{name}/self{tk}"] = r.self_pairs(a, eps)[1]
         out[f"{name}/pairs18"] = r26.brute_pairs18(a, b, eps)[1]
     out["cases"] = np.array(names)
+    # Morton clustering into patches (morton_cluster) for the collision_world mirror, and the 1-bit radix sort
+    cl = meshes.random_soup(700, 3, seed=4242, size=0.03)
+    out["cluster/xyz"] = cl
+    for od in (1, 8, 64):
+        order, splits = r26.cluster(cl, od)
+        out[f"cluster/od{od}/order"], out[f"cluster/od{od}/splits"] = order, splits
+    rng = np.random.default_rng(99)
+    keys = rng.integers(0, 1 << 63, 3000, dtype=np.uint64)
+    keys[::7] = keys[3]  # duplicates
+    out["radix/keys"] = keys
+    out["radix/sorted"], out["radix/perm"] = r26.radix_sort_u64(keys)
     path = os.path.join(ROOT, "tests", "golden", "ref_vectors.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes,", len(names), "cases")

@@ -254,3 +254,11 @@ def test_oracle_matches_reference_vectors(case):
         # one tree: its ids are right (either order within a pair), the whole set must match
         assert np.array_equal(orc.self_pair_set(a, k, eps), orc.canonical(np.sort(g(f"self{k}"), axis=1)))
     assert np.array_equal(orc.pair_set(a, b, 18, eps), orc.canonical(g("pairs18")))
+
+
+def test_stable_sort_matches_the_reference_radix_sorter():
+    """radix_sorter (src/bvh/util/sort.hpp:75-144) run by the reference's own code on 3000 keys with duplicates."""
+    keys = GOLDEN["radix/keys"]
+    perm = orc.stable_perm(keys)
+    assert np.array_equal(perm.astype(np.uint64), GOLDEN["radix/perm"])
+    assert np.array_equal(keys[perm], GOLDEN["radix/sorted"])

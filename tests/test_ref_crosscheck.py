@@ -64,3 +64,12 @@ def test_morton64_known_answers(refs):
     rng = np.random.default_rng(3)
     for x, y, z in rng.integers(0, 1 << 21, (200, 3)):
         assert r.morton64(int(x), int(y), int(z)) == int(orc.morton64(int(x), int(y), int(z)))
+
+
+def test_radix_sorter_and_cluster(refs):
+    rng = np.random.default_rng(17)
+    keys = rng.integers(0, 1 << 63, 5000, dtype=np.uint64)
+    keys[::5] = keys[11]
+    s, p = refs[26].radix_sort_u64(keys)
+    assert np.array_equal(p.astype(np.int64), orc.stable_perm(keys).astype(np.int64))
+    assert np.array_equal(s, np.sort(keys, kind="stable"))
