@@ -207,9 +207,10 @@ def run_gpu(args, world, rank, local):
         return cnt
 
     def step_host(ctx, oa, ob):
+        # each object's build is issued right after its upload: A's build runs while B's vertices cross PCIe
         ctx.set_elements(oa, h_a.numpy(), mem=bvhg.MEM_HOST)
-        ctx.set_elements(ob, h_b.numpy(), mem=bvhg.MEM_HOST)
         ctx.build(oa)
+        ctx.set_elements(ob, h_b.numpy(), mem=bvhg.MEM_HOST)
         ctx.build(ob)
         st, cnt = ctx.broadphase_raw(oa, ob, h_out.data_ptr(), cap, bvhg.MEM_HOST)
         if st != 0:
@@ -580,10 +581,24 @@ def cpu_baseline_sample(sphere_level=8, nx=1024, ny=512, threads=0):
     cnt, stages = orc.pipeline(s, p, K, EPS, threads)
     dt = time.perf_counter() - t
     n = s.shape[0] + p.shape[0]
-    return {"value": n / dt / 1e6, "unit": "Mprims/s", "cores": orc.max_threads() if threads == 0 else threads,
-            "kind": "port", "sample": f"icosphere L{sphere_level} + plate {nx}x{ny} quads ({n} tris, same scene "
-            f"at 1/4 size), 18-DOP, one pass", "seconds": dt, "pairs": int(cnt),
-            "stages_s": stages}
+    out = {"value": n / dt / 1e6, "unit": "Mprims/s", "cores": orc.max_threads() if threads == 0 else threads,
+           "kind": "port", "sample": f"icosphere L{sphere_level} + plate {nx}x{ny} quads ({n} tris, same scene "
+           f"at 1/4 size), 18-DOP, one pass", "seconds": dt, "pairs": int(cnt),
+           "stages_s": stages}
+    # The reference's own serial element path (its headers, built into oracle/_ref when the sources were present):
+    # from_vertices, top-down tree of dop_26 snapshots, potential_collision_set; 26-DOP, its only tree form.
+    from oracle import ref
+    if ref.available():
+        s6, p6 = meshes.sphere_plate(6, 256, 128)
+        r = ref.Ref(26)
+        t = time.perf_counter()
+        rc, _ = r.tree_pairs(s6, p6, EPS, cap=0)
+        dt6 = time.perf_counter() - t
+        n6 = s6.shape[0] + p6.shape[0]
+        out["reference_code"] = {"value": n6 / dt6 / 1e6, "unit": "Mprims/s", "cores": 1, "k": 26,
+                                 "sample": f"icosphere L6 + plate 256x128 quads ({n6} tris), the reference's serial "
+                                           "top-down dop_26 path", "seconds": dt6, "pairs": rc}
+    return out
 
 
 def run_reference(args, world, rank):
