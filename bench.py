@@ -207,10 +207,9 @@ def run_gpu(args, world, rank, local):
         return cnt
 
     def step_host(ctx, oa, ob):
-        # each object's build is issued right after its upload: A's build runs while B's vertices cross PCIe
         ctx.set_elements(oa, h_a.numpy(), mem=bvhg.MEM_HOST)
-        ctx.build(oa)
         ctx.set_elements(ob, h_b.numpy(), mem=bvhg.MEM_HOST)
+        ctx.build(oa)
         ctx.build(ob)
         st, cnt = ctx.broadphase_raw(oa, ob, h_out.data_ptr(), cap, bvhg.MEM_HOST)
         if st != 0:
