@@ -119,7 +119,7 @@ cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint
                          const uint32_t *vals, void *bucket_box, void *warp_box, void *elem_rows,
                          unsigned *cache_state, obj_scalars *sc, cudaStream_t s);
 
-// Block-local LBVH build over the bucket boxes (nodes closed inside a block of 256 buckets; the rest queued for
+// Block-local LBVH build over the bucket boxes (nodes closed inside a block of 128 buckets; the rest queued for
 // launch_climb). Nothing to do for one bucket.
 cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, const void *bucket_box, void *node_box,
                          int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s);

@@ -8,7 +8,7 @@
 // the radix tree of the bucket-boundary keys, built bottom-up agglomeratively (Apetrei): a subtree [l, r] joins
 // the neighbour across its more similar boundary.
 //
-// No thread ever waits. Nodes whose two children close inside a block of 256 buckets are merged in shared memory
+// No thread ever waits. Nodes whose two children close inside a block of 128 buckets are merged in shared memory
 // (warp rounds, then block rounds) and written out coalesced; the rest use a global exchange slot per node: the
 // first arrival's slab stores are ordered before its acq_rel atomic exchange, and the second arrival reads them
 // through L2 after its own.
@@ -19,7 +19,7 @@ namespace bvhg {
 
 namespace {
 
-constexpr int kBuildThreads = 256;
+constexpr int kBuildThreads = 128;
 
 
 // Dissimilarity of ranks j and j + 1: 33 + highest differing key bit when the keys differ, else
@@ -205,9 +205,9 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
   }
 }
 
-// Phase 1 (one thread per leaf bucket b, blocks of 256 consecutive buckets).
+// Phase 1 (one thread per leaf bucket b, blocks of 128 consecutive buckets).
 //
-// a. The block loads its 256 bucket boxes (k_elem_slabs wrote them) into a shared box table, one row per bucket
+// a. The block loads its 128 bucket boxes (k_elem_slabs wrote them) into a shared box table, one row per bucket
 //    (C = 2 D components, padded to C + 1 against bank conflicts). A subtree's box lives in the row of its first
 //    bucket: merging two subtrees writes the parent's node_box row (both children's slabs, with the lanes of a
 //    warp acting as slab components) straight to global memory and leaves the union in the left child's row.
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
 //    (parent * 2 + side, l, r, node).
 // e. Coalesced write-out of the topology of every node closed in the block (child, range, parent).
 template< int K, typename T >
-__global__ void __launch_bounds__( kBuildThreads, 4 ) k_build_leaf(int n, const uint64_t *__restrict__ keys,
+__global__ void __launch_bounds__( kBuildThreads, 8 ) k_build_leaf(int n, const uint64_t *__restrict__ keys,
                                                               const T *__restrict__ bucket_box,
                                                               T *__restrict__ node_box, int *__restrict__ child,
                                                               int2 *__restrict__ range, int *__restrict__ parent,
