@@ -399,3 +399,25 @@ def test_stored_and_computed_element_slabs_agree(precision):
             assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), want), step
             assert np.array_equal(orc.canonical(ctx.self_collision(oa)), want_self), step
             ctx.validate_tree(oa)
+
+
+@pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
+def test_objects_with_different_vertex_counts(precision):
+    """A triangle object against a tetrahedron object and a hexahedron object (the traversal's generic vertex
+    path), sparse and dense, both orders."""
+    tri = meshes.random_soup(3000, 3, seed=301, size=0.03)
+    tet = meshes.random_soup(2500, 4, seed=302, size=0.03, stream=1)
+    hexa = meshes.random_soup(800, 8, seed=303, size=0.06, stream=2)
+    with bvhg.Context(k=18, precision=precision) as ctx:
+        objs = {}
+        for name, x in (("tri", tri), ("tet", tet), ("hex", hexa)):
+            objs[name] = ctx.object()
+            ctx.set_elements(objs[name], x)
+            ctx.build(objs[name])
+        for rep in range(2):  # the second round runs after the density decision of the first
+            for a, b in (("tri", "tet"), ("tet", "tri"), ("tri", "hex"), ("hex", "tet")):
+                xa, xb = {"tri": tri, "tet": tet, "hex": hexa}[a], {"tri": tri, "tet": tet, "hex": hexa}[b]
+                got = orc.canonical(ctx.broadphase(objs[a], objs[b]))
+                assert np.array_equal(got, orc.pair_set(xa, xb, 18)), (rep, a, b)
+            for name in objs:
+                ctx.build(objs[name])
