@@ -75,7 +75,7 @@ struct object
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
   dev_buf hist, status;
-  dev_buf warp_box, bucket_box, node_box, child, range, parent, exch, queue, elem_cache, cache_state;
+  dev_buf warp_box, bucket_box, node_box, child, range, parent, exch, queue, elem_cache;
   dev_buf scal;  // obj_scalars
   // Each object's build runs on its own stream, forked from and joined back into the context stream with
   // events, so two objects' builds overlap (one's latency-bound tree climb beside the other's streaming kernels).
@@ -354,7 +354,6 @@ bvhg_status reserve_object(bvhg_ctx *ctx, object &o)
   BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.bucket_box.reserve( m * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.elem_cache.reserve( n * D * 2 * sb ) );
-  BVHG_CUDA( ctx, o.cache_state.reserve( m * 4 ) );
   BVHG_CUDA( ctx, o.node_box.reserve( ( m - 1 ) * D * 4 * sb + 16 ) );
   BVHG_CUDA( ctx, o.child.reserve( ( m - 1 ) * 8 + 8 ) );
   BVHG_CUDA( ctx, o.range.reserve( ( m - 1 ) * 8 + 8 ) );
@@ -411,7 +410,7 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
       stage_scope st( ctx, BVHG_STAGE_SLABS );
       BVHG_CUDA( ctx, launch_slabs( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(),
                                     o.bucket_box.p, o.warp_box.p, o.store_slabs ? o.elem_cache.p : nullptr,
-                                    o.cache_state.as< unsigned >(), o.sc(), s ) );
+                                    o.sc(), s ) );
       o.stored = o.store_slabs;
       st.launched();
     }
@@ -486,7 +485,7 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
     stage_scope st( ctx, BVHG_STAGE_SLABS );
     BVHG_CUDA( ctx, launch_slabs( K, fp32, o.verts, o.V, n, ctx->cfg.epsilon, o.sorted_vals(),
                                   o.bucket_box.p, o.warp_box.p, o.store_slabs ? o.elem_cache.p : nullptr,
-                                  o.cache_state.as< unsigned >(), o.sc(), s ) );
+                                  o.sc(), s ) );
     o.stored = o.store_slabs;
     st.launched();
   }
@@ -519,7 +518,6 @@ tree_view view_of(const object &o)
   v.verts = o.verts;
   v.V = o.V;
   v.elem_cache = o.elem_cache.p;
-  v.cache_state = o.cache_state.as< unsigned >();
   v.stored = o.stored;
   v.perm = o.sorted_vals();
   v.n = o.n;

@@ -9,9 +9,8 @@
 //              keys[r], vals[r] hold the key and original index of rank r (vals = the permutation)
 //   warp_box   ceil(n / 32) * D * 2 T: union of the slabs of ranks [32 w, 32 w + 31] (the query side's cull)
 //   bucket_box m * D * 2 T: union of the slabs of leaf bucket b (ranks [8 b, 8 b + 7]), input of the tree build
-//   elem_cache n * D * 2 T: element slabs in rank order: written by the slab kernel for objects in dense contact,
-//              else by the first traversal that tests their bucket
-//   cache_state m u32: per bucket 0 empty / 1 being written / 2 ready (the slab kernel resets it)
+//   elem_cache n * D * 2 T: element slabs in rank order, written by the slab kernel for objects in dense contact
+//              only (sparse traversals compute the few they test from the vertices)
 //   node_box   (m - 1) * D * 2 * 2 T: both children's slabs of internal node k, [k][a][child][min,max], so one
 //              32-byte (FP64) or 16-byte (FP32) sector per axis tests both children
 //   child      (m - 1) int2: child index, >= 0 internal node, < 0 bucket with ~child = bucket index
@@ -117,7 +116,7 @@ cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *v
 // sort when perm is not a permutation.
 cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
                          const uint32_t *vals, void *bucket_box, void *warp_box, void *elem_rows,
-                         unsigned *cache_state, obj_scalars *sc, cudaStream_t s);
+                         obj_scalars *sc, cudaStream_t s);
 
 // Block-local LBVH build over the bucket boxes (nodes closed inside a block of 128 buckets; the rest queued for
 // launch_climb). Nothing to do for one bucket.
@@ -140,9 +139,8 @@ struct tree_view
   const void *warp_box;
   const double *verts;  // element vertices, [element][vertex][xyz] (element slabs are recomputed from them)
   uint32_t V;
-  const void *elem_cache;     // element slabs in rank order, written when a traversal first tests their bucket
-  const unsigned *cache_state;  // per bucket: 0 empty, 1 being written, 2 ready (reset by the slab kernel)
-  bool stored;                  // the slab kernel wrote every element's slabs to elem_cache
+  const void *elem_cache;  // element slabs in rank order (valid when stored)
+  bool stored;             // the slab kernel wrote every element's slabs to elem_cache
   const uint32_t *perm;
   uint64_t n;
   const obj_scalars *sc;

@@ -129,8 +129,7 @@ struct trav_args
   const int2 *range;
   const double *tverts;
   uint32_t tV;
-  T *tcache;         // element slabs of the target, in rank order, filled on first use of their bucket
-  unsigned *tstate;  // per target bucket: 0 not cached, 1 being written, 2 ready
+  const T *tcache;   // element slabs of the target in rank order (stored variant only)
   const uint32_t *tperm;
   const obj_scalars *tsc;
   uint32_t nt;
@@ -143,7 +142,7 @@ struct trav_args
 };
 
 // Target leaf bucket bb for the lanes in `mine`: the warp first computes the bucket's element slabs into its cache
-// (lane j: element of rank 8 bb + j), then every lane of the mask tests its query against them (ranks above its own
+// (lane j: element of rank 8 bb + j; the stored variant reads the stored rows instead), then every lane of the mask tests its query against them (ranks above its own
 // in self-collision). Hits go out through one warp-aggregated reservation. Called by the whole warp.
 template< int K, typename T, int VT, bool LAZY >
 __device__ __forceinline__ void test_bucket(const trav_args< T > &x, const T *qlo, const T *qhi, uint32_t qe, int bb,
@@ -152,39 +151,15 @@ __device__ __forceinline__ void test_bucket(const trav_args< T > &x, const T *ql
   constexpr int D = K / 2;
   const int t0 = kLeafSize * bb;
   const int cnt = min( kLeafSize, static_cast< int >( x.nt ) - t0 );
-  // The bucket's element slabs: from the target's cache when the slab kernel or an earlier visit wrote them, else
-  // computed from the vertices (and written to the cache by the one warp that claims the bucket; others never wait
-  // for it). The stored variant has every bucket ready.
-  unsigned state = 2;
+  // The bucket's element slabs: the stored rows (dense contact), or computed from the vertices into the warp's
+  // shared-memory cache by lanes 0..7 (sparse contact: a bucket is tested by few packets, so nothing is kept).
+  const T *rows = x.tcache + static_cast< size_t >( t0 ) * 2 * D;
   if constexpr ( LAZY )
   {
-  if ( lane == 0 )
-  {
-    asm volatile( "ld.acquire.gpu.global.u32 %0, [%1];" : "=r"( state ) : "l"( x.tstate + bb ) : "memory" );
-    if ( state == 0 ) state = atomicCAS( x.tstate + bb, 0u, 1u ) == 0u ? 3u : 1u;  // 3: this warp writes it
-  }
-  state = __shfl_sync( 0xffffffffu, state, 0 );
-  __syncwarp();  // orders the other lanes' cache reads after lane 0's acquire
-  }
-  T *crow = x.tcache + static_cast< size_t >( t0 ) * 2 * D;
-  // ready: test straight against the cached rows (early exit reads few slabs); else compute them into shared memory
-  const T *rows = state == 2 ? crow : cache;
-  if constexpr ( LAZY )
-  {
-  if ( state != 2 && static_cast< int >( lane ) < cnt )
-    slabs_to_row< K, T, VT >( x.tverts, x.tV, __ldg( x.tperm + t0 + lane ), x.eps, x.eps_hi, cache + lane * 2 * D );
-  __syncwarp();
-  if ( state == 3 )
-  {
-    for ( int k = static_cast< int >( lane ); k < cnt * 2 * D; k += 32 ) crow[k] = cache[k];
+    if ( static_cast< int >( lane ) < cnt )
+      slabs_to_row< K, T, VT >( x.tverts, x.tV, __ldg( x.tperm + t0 + lane ), x.eps, x.eps_hi, cache + lane * 2 * D );
     __syncwarp();
-    if ( lane == 0 )
-    {
-      __threadfence();
-      atomicExch( x.tstate + bb, 2u );
-    }
-  }
-  __syncwarp();
+    rows = cache;
   }
   if ( mine )
   {
@@ -199,7 +174,7 @@ __device__ __forceinline__ void test_bucket(const trav_args< T > &x, const T *ql
       {
         if ( !o ) break;
         if constexpr ( LAZY ) o = qlo[a] < eb[2 * a + 1] && eb[2 * a] < qhi[a];
-        else o = qlo[a] < __ldg( eb + 2 * a + 1 ) && __ldg( eb + 2 * a ) < qhi[a];  // read-only in this variant
+        else o = qlo[a] < __ldg( eb + 2 * a + 1 ) && __ldg( eb + 2 * a ) < qhi[a];
       }
       if ( o ) hits |= 1u << ( r - t0 );
     }
@@ -335,8 +310,8 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
 // its packet: every lane tests its own element's slabs (computed from its vertices) against both children of the
 // current node (the node row is read once for the warp, a broadcast), and a child is entered with the mask of the
 // lanes that overlap it (a lane that misses a node misses all of its descendants). Stack entries are (node, lane
-// mask), in shared memory. At a leaf bucket the warp computes the bucket's element slabs once into a shared cache
-// and the lanes of the mask test their element against them.
+// mask), in shared memory. At a leaf bucket the lanes of the mask test their element against the bucket's element
+// slabs: the stored rows (dense contact) or, computed once by the warp from the vertices, a shared cache.
 template< int K, typename T, int VT, bool LAZY >
 __global__ void __launch_bounds__( kTravThreads, LAZY ? 4 : 6 ) k_traverse(const trav_args< T > x,
                                                                          const obj_scalars *__restrict__ qsc)
@@ -385,8 +360,7 @@ cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, double eps, uint2
   x.range = t.range;
   x.tverts = t.verts;
   x.tV = t.V;
-  x.tcache = static_cast< T * >( const_cast< void * >( t.elem_cache ) );
-  x.tstate = const_cast< unsigned * >( t.cache_state );
+  x.tcache = static_cast< const T * >( t.elem_cache );
   x.tperm = t.perm;
   x.tsc = t.sc;
   x.nt = static_cast< uint32_t >( t.n );

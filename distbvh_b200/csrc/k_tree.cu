@@ -107,15 +107,13 @@ constexpr int kSlabThreads = 128;  // ranks per block of the element slab kernel
 // query groups of 32 ranks are written out coalesced: bucket_box row b and warp_box row g each hold the C = 2 D
 // values (min, max) per slab. The element slabs themselves go to elem_rows (row r: rank r) only when given (objects
 // in dense contact, whose traversals test most buckets); otherwise the traversal computes the few it tests from the
-// vertices and caches them. cache_state marks each bucket's rows ready (2) or not (0). A one-bucket object also gets
-// its root box here. A rank whose index is not an element index marks a failed sort.
+// vertices. A one-bucket object also gets its root box here. A rank whose index is not an element index marks a failed sort.
 template< int K, typename T, int VT >
 __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( VT == 8 ? 3 : 4 ) ) k_elem_slabs(const double *__restrict__ verts, uint32_t Vrt,
                                                                   int n, double eps, float eps_hi,
                                                                   const uint32_t *__restrict__ vals,
                                                                   T *__restrict__ bucket_box, T *__restrict__ warp_box,
-                                                                  T *__restrict__ elem_rows,
-                                                                  unsigned *__restrict__ cache_state, obj_scalars *sc)
+                                                                  T *__restrict__ elem_rows, obj_scalars *sc)
 {
   constexpr int D = K / 2;
   constexpr int C = 2 * D;
@@ -128,8 +126,6 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
   const int tid = threadIdx.x;
   const int r0 = static_cast< int >( blockIdx.x ) * kSlabThreads;
   const int rows = min( kSlabThreads, n - r0 );
-  // the traversal's element-slab cache of these buckets: written here (ready), or stale from here on
-  if ( tid < ( rows + kLeafSize - 1 ) / kLeafSize ) cache_state[r0 / kLeafSize + tid] = elem_rows ? 2u : 0u;
   if ( tid < rows )
   {
     const uint32_t e = __ldg( vals + r0 + tid );
@@ -588,27 +584,26 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(int n, const T *__res
 
 template< int K, typename T, int VT >
 cudaError_t launch_slabs_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
-                           void *bucket_box, void *warp_box, void *elem_rows, unsigned *cache_state, obj_scalars *sc,
-                           cudaStream_t s)
+                           void *bucket_box, void *warp_box, void *elem_rows, obj_scalars *sc, cudaStream_t s)
 {
   const unsigned grid = static_cast< unsigned >( ( n + kSlabThreads - 1 ) / kSlabThreads );
   k_elem_slabs< K, T, VT ><<< grid, kSlabThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, f32_round_up( eps ),
                                                            vals, static_cast< T * >( bucket_box ),
                                                            static_cast< T * >( warp_box ),
-                                                           static_cast< T * >( elem_rows ), cache_state, sc );
+                                                           static_cast< T * >( elem_rows ), sc );
   return cudaGetLastError();
 }
 
 template< int K, typename T >
 cudaError_t slabs_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *bb, void *wb,
-                    void *er, unsigned *cs, obj_scalars *sc, cudaStream_t s)
+                    void *er, obj_scalars *sc, cudaStream_t s)
 {
   switch ( V )
   {
-    case 3: return launch_slabs_t< K, T, 3 >( verts, V, n, eps, vals, bb, wb, er, cs, sc, s );
-    case 4: return launch_slabs_t< K, T, 4 >( verts, V, n, eps, vals, bb, wb, er, cs, sc, s );
-    case 8: return launch_slabs_t< K, T, 8 >( verts, V, n, eps, vals, bb, wb, er, cs, sc, s );
-    default: return launch_slabs_t< K, T, 0 >( verts, V, n, eps, vals, bb, wb, er, cs, sc, s );
+    case 3: return launch_slabs_t< K, T, 3 >( verts, V, n, eps, vals, bb, wb, er, sc, s );
+    case 4: return launch_slabs_t< K, T, 4 >( verts, V, n, eps, vals, bb, wb, er, sc, s );
+    case 8: return launch_slabs_t< K, T, 8 >( verts, V, n, eps, vals, bb, wb, er, sc, s );
+    default: return launch_slabs_t< K, T, 0 >( verts, V, n, eps, vals, bb, wb, er, sc, s );
   }
 }
 
@@ -688,16 +683,16 @@ cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, voi
 
 cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
                          const uint32_t *vals, void *bucket_box, void *warp_box, void *elem_rows,
-                         unsigned *cache_state, obj_scalars *sc, cudaStream_t s)
+                         obj_scalars *sc, cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return fp32 ? slabs_v< 6, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s )
-                        : slabs_v< 6, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s );
-    case 18: return fp32 ? slabs_v< 18, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s )
-                         : slabs_v< 18, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s );
-    case 26: return fp32 ? slabs_v< 26, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s )
-                         : slabs_v< 26, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, cache_state, sc, s );
+    case 6: return fp32 ? slabs_v< 6, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s )
+                        : slabs_v< 6, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s );
+    case 18: return fp32 ? slabs_v< 18, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s )
+                         : slabs_v< 18, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s );
+    case 26: return fp32 ? slabs_v< 26, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s )
+                         : slabs_v< 26, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s );
     default: return cudaErrorInvalidValue;
   }
 }
