@@ -79,14 +79,18 @@ struct object
   dev_buf scal;  // obj_scalars
   // Each object's build runs on its own stream, forked from and joined back into the context stream with
   // events, so two objects' builds overlap (one's latency-bound tree climb beside the other's streaming kernels).
-  cudaStream_t st = nullptr;
+  // The largest object builds on a high-priority stream: its chain is the longest, and the others' kernels fill
+  // the SMs its latency-bound phases leave idle.
+  cudaStream_t st = nullptr, st_hi = nullptr;
   cudaEvent_t done = nullptr;
   bool pending = false;
   ~object()
   {
     if ( st ) cudaStreamSynchronize( st );
+    if ( st_hi ) cudaStreamSynchronize( st_hi );
     if ( done ) cudaEventDestroy( done );
     if ( st ) cudaStreamDestroy( st );
+    if ( st_hi ) cudaStreamDestroy( st_hi );
   }
   obj_scalars *sc() const { return scal.as< obj_scalars >(); }
   const uint64_t *sorted_keys() const { return sort_result_alt ? keys_alt.as< uint64_t >() : keys.as< uint64_t >(); }
@@ -285,13 +289,22 @@ cudaError_t fork_object(bvhg_ctx *ctx, object &o, cudaStream_t *out)
     *out = ctx->stream;
     return cudaSuccess;
   }
+  bool largest = true;
+  for ( const auto &p : ctx->objs )
+    if ( p && p.get() != &o && p->n > o.n ) largest = false;
   cudaError_t e = cudaSuccess;
-  if ( !o.st ) e = cudaStreamCreateWithFlags( &o.st, cudaStreamNonBlocking );
+  cudaStream_t *sp = largest ? &o.st_hi : &o.st;
+  if ( !*sp )
+  {
+    int least = 0, greatest = 0;
+    e = cudaDeviceGetStreamPriorityRange( &least, &greatest );
+    if ( e == cudaSuccess ) e = cudaStreamCreateWithPriority( sp, cudaStreamNonBlocking, largest ? greatest : least );
+  }
   if ( e == cudaSuccess && !o.done ) e = cudaEventCreateWithFlags( &o.done, cudaEventDisableTiming );
   if ( e == cudaSuccess && !ctx->fork_evt ) e = cudaEventCreateWithFlags( &ctx->fork_evt, cudaEventDisableTiming );
   if ( e == cudaSuccess ) e = cudaEventRecord( ctx->fork_evt, ctx->stream );
-  if ( e == cudaSuccess ) e = cudaStreamWaitEvent( o.st, ctx->fork_evt, 0 );
-  *out = o.st;
+  if ( e == cudaSuccess ) e = cudaStreamWaitEvent( *sp, ctx->fork_evt, 0 );
+  *out = *sp;
   return e;
 }
 
