@@ -75,7 +75,7 @@ struct object
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
   dev_buf hist, status;
-  dev_buf warp_box, bucket_box, node_box, child, range, parent, exch, queue, elem_cache;
+  dev_buf warp_box, bucket_box, node_box, child, range, parent, exch, bdel, queue, elem_cache;
   dev_buf scal;  // obj_scalars
   // Each object's build runs on its own stream, forked from and joined back into the context stream with
   // events, so two objects' builds overlap (one's latency-bound tree climb beside the other's streaming kernels).
@@ -372,6 +372,7 @@ bvhg_status reserve_object(bvhg_ctx *ctx, object &o)
   BVHG_CUDA( ctx, o.range.reserve( ( m - 1 ) * 8 + 8 ) );
   BVHG_CUDA( ctx, o.parent.reserve( ( 2 * m ) * 4 ) );
   BVHG_CUDA( ctx, o.exch.reserve( m * 4 ) );
+  BVHG_CUDA( ctx, o.bdel.reserve( m ) );
   BVHG_CUDA( ctx, o.queue.reserve( m * 16 ) );
   return BVHG_OK;
 }
@@ -505,15 +506,17 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   if ( m > 1 )
   {
     stage_scope st( ctx, BVHG_STAGE_BUILD );
-    BVHG_CUDA( ctx, launch_build( K, fp32, n, o.sorted_keys(), o.bucket_box.p, o.node_box.p, o.child.as< int2 >(),
-                                  o.range.as< int2 >(), o.parent.as< int >(), o.queue.as< int4 >(), o.sc(), s ) );
+    BVHG_CUDA( ctx, launch_build( K, fp32, n, o.sorted_keys(), o.bdel.as< uint8_t >(), o.bucket_box.p, o.node_box.p,
+                                  o.child.as< int2 >(), o.range.as< int2 >(), o.parent.as< int >(),
+                                  o.queue.as< int4 >(), o.sc(), s ) );
     st.launched();
   }
   if ( m > 1 )
   {
     stage_scope st( ctx, BVHG_STAGE_CLIMB );
-    BVHG_CUDA( ctx, launch_climb( K, fp32, n, o.sorted_keys(), o.node_box.p, o.child.as< int2 >(), o.range.as< int2 >(),
-                                  o.parent.as< int >(), o.exch.as< int >(), o.queue.as< int4 >(), o.sc(), s ) );
+    BVHG_CUDA( ctx, launch_climb( K, fp32, n, o.bdel.as< uint8_t >(), o.node_box.p, o.child.as< int2 >(),
+                                  o.range.as< int2 >(), o.parent.as< int >(), o.exch.as< int >(),
+                                  o.queue.as< int4 >(), o.sc(), s ) );
     st.launched();
   }
   o.built = true;

@@ -17,6 +17,7 @@
 //   range      (m - 1) int2: [first bucket, last bucket] covered by the node (self-collision pruning)
 //   parent     m + (m - 1) int32: parent * 2 + side of every bucket and internal node (refit)
 //   exch       m - 1 int32: the agglomerative build's exchange slot per internal node (-1 = empty)
+//   bdel       m - 1 u8: dissimilarity of every bucket boundary (written by the block-local build for the climb)
 //   queue      m int4: subtrees the block-local build phases leave to the global phase
 #pragma once
 
@@ -120,11 +121,13 @@ cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint
 
 // Block-local LBVH build over the bucket boxes (nodes closed inside a block of 128 buckets; the rest queued for
 // launch_climb). Nothing to do for one bucket.
-cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, const void *bucket_box, void *node_box,
-                         int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s);
+// bdel (m - 1 bytes) receives the dissimilarity of every bucket boundary for the climb.
+cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, uint8_t *bdel, const void *bucket_box,
+                         void *node_box, int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc,
+                         cudaStream_t s);
 
 // Global climb of the build (subtrees the block-local phase queued); after launch_build, only when m > 1.
-cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint64_t *keys, void *node_box, int2 *child, int2 *range,
+cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint8_t *bdel, void *node_box, int2 *child, int2 *range,
                          int *parent, int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s);
 
 // Refit with the topology of the last build, after launch_slabs recomputed the bucket boxes: every internal node.

@@ -40,6 +40,14 @@ __device__ __forceinline__ int atomic_exch_acq_rel(int *p, int v)
   return old;
 }
 
+// Load with acquire semantics at GPU scope (later loads are ordered after it).
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+  int v;
+  asm volatile( "ld.acquire.gpu.global.b32 %0, [%1];" : "=r"( v ) : "l"( p ) : "memory" );
+  return v;
+}
+
 template< typename T >
 struct box_io;
 
@@ -98,6 +106,13 @@ __device__ __forceinline__ int delta_of(uint64_t a, uint64_t b, int j)
 __device__ __forceinline__ long long bdelta(const uint64_t *__restrict__ keys, int b)
 {
   return ( static_cast< long long >( delta( keys, kLeafSize * b + kLeafSize - 1 ) ) << 32 ) | static_cast< unsigned >( b );
+}
+
+// The same value from the per-boundary byte the block-local build stored (bdel[b] = the element dissimilarity
+// across boundary b): the climb reads one byte of a small, cache-resident array instead of two keys.
+__device__ __forceinline__ long long cdelta(const uint8_t *__restrict__ bdel, int b)
+{
+  return ( static_cast< long long >( __ldg( bdel + b ) ) << 32 ) | static_cast< unsigned >( b );
 }
 
 constexpr int kSlabThreads = 128;  // ranks per block of the element slab kernel
@@ -217,6 +232,7 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
 // e. Coalesced write-out of the topology of every node closed in the block (child, range, parent).
 template< int K, typename T >
 __global__ void __launch_bounds__( kBuildThreads, 8 ) k_build_leaf(int n, const uint64_t *__restrict__ keys,
+                                                              uint8_t *__restrict__ bdel,
                                                               const T *__restrict__ bucket_box,
                                                               T *__restrict__ node_box, int *__restrict__ child,
                                                               int2 *__restrict__ range, int *__restrict__ parent,
@@ -271,6 +287,7 @@ __global__ void __launch_bounds__( kBuildThreads, 8 ) k_build_leaf(int n, const 
     }
   }
   const long long dself = ( b + 1 < m ) ? bdelta( keys, b ) : 0ll;
+  if ( b + 1 < m ) bdel[b] = static_cast< uint8_t >( dself >> 32 );  // for the climb: one byte per boundary
   long long dleft = 0;
   if ( lane == 0 && wbase >= 1 && wbase < m ) dleft = bdelta( keys, wbase - 1 );
   dleft = __shfl_sync( 0xffffffffu, dleft, 0 );
@@ -474,11 +491,11 @@ __global__ void __launch_bounds__( kBuildThreads, 8 ) k_build_leaf(int n, const 
 }
 
 // Phase 2 (dense, one thread per queued subtree): the agglomerative climb with a global exchange slot per node.
-// The first arrival at a node leaves; the second merges and climbs on. The exchange is an acq_rel atomic:
-// it orders the first arrival's slab stores before it and the second arrival's slab loads (through L2) after
-// it. Slabs written by phase 1 are visible here (kernel boundary).
+// The first arrival at a node leaves; the second merges and climbs on. The first arrival publishes through an
+// acq_rel atomic exchange that orders its slab stores before it; the second arrival's slab loads (through L2)
+// are ordered after its acquire load or exchange. Slabs written by phase 1 are visible here (kernel boundary).
 template< int K, typename T >
-__global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__restrict__ keys, T *node_box,
+__global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint8_t *__restrict__ bdel, T *node_box,
                                                      int *child, int2 *__restrict__ range, int *__restrict__ parent,
                                                      int *exch, const int4 *__restrict__ queue, obj_scalars *sc)
 {
@@ -497,8 +514,15 @@ __global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__
     for ( int a = 0; a < D; ++a ) io::load2_cg( pb + a * 4 + side * 2, lo[a], hi[a] );
     while ( true )
     {
-      const int other = atomic_exch_acq_rel( exch + par, side == 0 ? l : r );
-      if ( other < 0 ) break;  // first arrival: the sibling's thread finishes this node
+      // A sibling that already arrived is seen with one acquire load (its slab stores were released by its
+      // exchange); only when the slot looks empty does this thread publish through the exchange itself, whose
+      // release also covers its own slab stores. A late second arrival thus waits for no store of its own.
+      int other = ld_acquire( exch + par );
+      if ( other < 0 )
+      {
+        other = atomic_exch_acq_rel( exch + par, side == 0 ? l : r );
+        if ( other < 0 ) break;  // first arrival: the sibling's thread finishes this node
+      }
       if ( side == 0 ) r = other;
       else l = other;
 #pragma unroll
@@ -521,7 +545,7 @@ __global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint64_t *__
       bool left_child;
       if ( l == 0 ) left_child = true;
       else if ( r == m - 1 ) left_child = false;
-      else left_child = bdelta( keys, r ) < bdelta( keys, l - 1 );
+      else left_child = cdelta( bdel, r ) < cdelta( bdel, l - 1 );
       par = left_child ? r : l - 1;
       side = left_child ? 0 : 1;
       pb = node_box + static_cast< size_t >( par ) * D * 4;
@@ -608,8 +632,8 @@ cudaError_t slabs_v(const double *verts, uint32_t V, uint64_t n, double eps, con
 }
 
 template< int K, typename T >
-cudaError_t launch_build_t(uint64_t n, const uint64_t *keys, const void *bucket_box, void *node_box, int2 *child,
-                           int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s)
+cudaError_t launch_build_t(uint64_t n, const uint64_t *keys, uint8_t *bdel, const void *bucket_box, void *node_box,
+                           int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
   if ( m <= 1 ) return cudaSuccess;  // the slab kernel stored a one-bucket object's root
@@ -618,7 +642,7 @@ cudaError_t launch_build_t(uint64_t n, const uint64_t *keys, const void *bucket_
   const cudaError_t e = cudaFuncSetAttribute( k_build_leaf< K, T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast< int >( smem ) );
   if ( e != cudaSuccess ) return e;
-  k_build_leaf< K, T ><<< grid, kBuildThreads, smem, s >>>( static_cast< int >( n ), keys,
+  k_build_leaf< K, T ><<< grid, kBuildThreads, smem, s >>>( static_cast< int >( n ), keys, bdel,
                                                            static_cast< const T * >( bucket_box ),
                                                            static_cast< T * >( node_box ),
                                                            reinterpret_cast< int * >( child ), range, parent, queue, sc );
@@ -626,14 +650,14 @@ cudaError_t launch_build_t(uint64_t n, const uint64_t *keys, const void *bucket_
 }
 
 template< int K, typename T >
-cudaError_t launch_climb_t(uint64_t n, const uint64_t *keys, void *node_box, int2 *child, int2 *range, int *parent,
+cudaError_t launch_climb_t(uint64_t n, const uint8_t *bdel, void *node_box, int2 *child, int2 *range, int *parent,
                            int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
   // The queue length is known only on the device: a grid-stride grid sized for the usual fraction.
   const uint64_t want = ( m / 8 + 127 ) / 128;
   const unsigned cgrid = static_cast< unsigned >( want < 148 * 16 ? ( want ? want : 1 ) : 148 * 16 );
-  k_build_climb< K, T ><<< cgrid, 128, 0, s >>>( static_cast< int >( n ), keys, static_cast< T * >( node_box ),
+  k_build_climb< K, T ><<< cgrid, 128, 0, s >>>( static_cast< int >( n ), bdel, static_cast< T * >( node_box ),
                                                 reinterpret_cast< int * >( child ), range, parent, exch, queue, sc );
   return cudaGetLastError();
 }
@@ -697,32 +721,33 @@ cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint
   }
 }
 
-cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, const void *bucket_box, void *node_box,
-                         int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s)
+cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, uint8_t *bdel, const void *bucket_box,
+                         void *node_box, int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc,
+                         cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return fp32 ? launch_build_t< 6, float >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s )
-                        : launch_build_t< 6, double >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s );
-    case 18: return fp32 ? launch_build_t< 18, float >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s )
-                         : launch_build_t< 18, double >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s );
-    case 26: return fp32 ? launch_build_t< 26, float >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s )
-                         : launch_build_t< 26, double >( n, keys, bucket_box, node_box, child, range, parent, queue, sc, s );
+    case 6: return fp32 ? launch_build_t< 6, float >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s )
+                        : launch_build_t< 6, double >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s );
+    case 18: return fp32 ? launch_build_t< 18, float >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s )
+                         : launch_build_t< 18, double >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s );
+    case 26: return fp32 ? launch_build_t< 26, float >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s )
+                         : launch_build_t< 26, double >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s );
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint64_t *keys, void *node_box, int2 *child, int2 *range,
+cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint8_t *bdel, void *node_box, int2 *child, int2 *range,
                          int *parent, int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return fp32 ? launch_climb_t< 6, float >( n, keys, node_box, child, range, parent, exch, queue, sc, s )
-                        : launch_climb_t< 6, double >( n, keys, node_box, child, range, parent, exch, queue, sc, s );
-    case 18: return fp32 ? launch_climb_t< 18, float >( n, keys, node_box, child, range, parent, exch, queue, sc, s )
-                         : launch_climb_t< 18, double >( n, keys, node_box, child, range, parent, exch, queue, sc, s );
-    case 26: return fp32 ? launch_climb_t< 26, float >( n, keys, node_box, child, range, parent, exch, queue, sc, s )
-                         : launch_climb_t< 26, double >( n, keys, node_box, child, range, parent, exch, queue, sc, s );
+    case 6: return fp32 ? launch_climb_t< 6, float >( n, bdel, node_box, child, range, parent, exch, queue, sc, s )
+                        : launch_climb_t< 6, double >( n, bdel, node_box, child, range, parent, exch, queue, sc, s );
+    case 18: return fp32 ? launch_climb_t< 18, float >( n, bdel, node_box, child, range, parent, exch, queue, sc, s )
+                         : launch_climb_t< 18, double >( n, bdel, node_box, child, range, parent, exch, queue, sc, s );
+    case 26: return fp32 ? launch_climb_t< 26, float >( n, bdel, node_box, child, range, parent, exch, queue, sc, s )
+                         : launch_climb_t< 26, double >( n, bdel, node_box, child, range, parent, exch, queue, sc, s );
     default: return cudaErrorInvalidValue;
   }
 }
