@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbvhg.so")
 SOURCES = ["bvhg_api.cu", "k_element.cu", "k_sort.cu", "k_tree.cu", "k_traverse.cu", "k_noalloc.cu"]
-HEADERS = ["bvhg_internal.cuh", "kdop_math.cuh", os.path.join("..", "..", "include", "bvhg.h")]
+HEADERS = ["bvhg_internal.cuh", "kdop_math.cuh", "bulk_copy.cuh", os.path.join("..", "..", "include", "bvhg.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

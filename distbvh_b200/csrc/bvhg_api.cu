@@ -460,7 +460,7 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
       st.launched();
     }
     BVHG_CUDA( ctx, launch_centroid_bounds( K, o.verts, o.V, n, ctx->cfg.epsilon, o.cx.as< double >(),
-                                            o.cy.as< double >(), o.cz.as< double >(), o.sc(), s ) );
+                                            o.cy.as< double >(), o.cz.as< double >(), o.sc(), ctx->spin_limit, s ) );
     st.launched();
   }
   {

@@ -90,7 +90,7 @@ inline int sort_passes(int bits) { return ( kKeyBits + bits - 1 ) / bits; }
 // All return cudaGetLastError() of the launch.
 
 cudaError_t launch_centroid_bounds(int K, const double *verts, uint32_t V, uint64_t n, double eps, double *cx,
-                                   double *cy, double *cz, obj_scalars *sc, cudaStream_t s);
+                                   double *cy, double *cz, obj_scalars *sc, uint32_t spin_limit, cudaStream_t s);
 
 cudaError_t launch_keys_hist(int bits, const double *cx, const double *cy, const double *cz, uint64_t n,
                              obj_scalars *sc, uint64_t *keys, uint32_t *hist, cudaStream_t s);

@@ -6,6 +6,7 @@
 // its vertices, accumulated from zero and divided by the vertex count (tests/TestCommon.hpp:62-65).
 // K2 follows morton_impl (contact_entity.hpp:104-118) with quantize64 (hash.hpp:177-198) and morton64
 // (hash.hpp:72-103): q = u64(((c - min) * inv) * 2^21) & 0x1fffff per axis; key = z<<2 | y<<1 | x interleave.
+#include "bulk_copy.cuh"
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
 
@@ -60,6 +61,36 @@ __device__ __forceinline__ void reduce_bounds(double mn[3], double mx[3], bool b
   if ( threadIdx.x == 0 && s_bad ) atomicCAS( &sc->error, 0, kErrArg );
 }
 
+// One element (its V vertices at p, in shared memory): centroid to cx/cy/cz[i], cardinal slabs into the running
+// min/max, non-finite coordinates into bad.
+template< int K >
+__device__ __forceinline__ void element_centroid_bounds(const double *p, int V, double eps, uint64_t i,
+                                                        double *__restrict__ cx, double *__restrict__ cy,
+                                                        double *__restrict__ cz, double mn[3], double mx[3], bool &bad)
+{
+  double sx = 0.0, sy = 0.0, sz = 0.0;
+  for ( int v = 0; v < V; ++v )
+  {
+    const double x = p[3 * v], y = p[3 * v + 1], z = p[3 * v + 2];
+    bad |= !( isfinite( x ) && isfinite( y ) && isfinite( z ) );
+    sx = __dadd_rn( sx, x );
+    sy = __dadd_rn( sy, y );
+    sz = __dadd_rn( sz, z );
+  }
+  const double dv = static_cast< double >( V );
+  cx[i] = __ddiv_rn( sx, dv );
+  cy[i] = __ddiv_rn( sy, dv );
+  cz[i] = __ddiv_rn( sz, dv );
+#pragma unroll
+  for ( int a = 0; a < 3; ++a )
+  {
+    double lo, hi;
+    slab64< K >( p, V, a, eps, lo, hi );
+    mn[a] = ( lo < mn[a] ) ? lo : mn[a];
+    mx[a] = ( hi > mx[a] ) ? hi : mx[a];
+  }
+}
+
 // K1. Each block stages a tile of 256 elements (256 * V * 24 bytes, contiguous) into shared memory with
 // coalesced 16-byte loads, then each thread reduces its own element. Grid-stride over tiles.
 template< int K, int VT >
@@ -94,30 +125,92 @@ __global__ void __launch_bounds__( kElemThreads ) k_centroid_bounds(const double
     }
     __syncthreads();
     if ( static_cast< int >( threadIdx.x ) < cnt )
+      element_centroid_bounds< K >( s_v + threadIdx.x * per, V, eps, t0 + threadIdx.x, cx, cy, cz, mn, mx, bad );
+  }
+  reduce_bounds( mn, mx, bad, sc );
+}
+
+// K1 for a fixed vertex count, persistent and double-buffered: block b takes tiles b, b + G, b + 2G, ... (G = the
+// grid); while it reduces one tile from shared memory, the bulk copy (TMA) of its next tile streams into the other
+// stage. Full tiles (256 elements, 256 * VT * 24 bytes, 16-byte aligned) go through the bulk copy; the last,
+// partial tile through plain loads. Every wait on a copy is bounded: past spin_limit polls the block raises the
+// object's error word, waits (bounded) for its copies in flight and stops.
+template< int K, int VT >
+__global__ void __launch_bounds__( kElemThreads, VT == 8 ? 2 : 4 ) k_centroid_bounds_tma(const double *__restrict__ verts, uint64_t n,
+                                                                      double eps, double *__restrict__ cx,
+                                                                      double *__restrict__ cy, double *__restrict__ cz,
+                                                                      obj_scalars *__restrict__ sc, uint32_t spin_limit)
+{
+  constexpr int per = VT * 3;
+  constexpr uint32_t kTileD = kElemThreads * per;  // doubles per tile
+  extern __shared__ __align__( 128 ) double s_stage[];  // 2 stages of kTileD doubles
+  __shared__ __align__( 8 ) uint64_t s_mbar[2];
+  const double inf = __longlong_as_double( 0x7ff0000000000000LL );
+  double mn[3] = { inf, inf, inf };
+  double mx[3] = { -inf, -inf, -inf };
+  bool bad = false;
+  const uint64_t tiles = ( n + kElemThreads - 1 ) / kElemThreads;
+  const uint64_t full = n / kElemThreads;  // tiles that are bulk-copied
+  const uint64_t G = gridDim.x;
+  const int tid = threadIdx.x;
+  auto issue = [&](uint64_t t, int st) {
+    mbar_expect_tx( &s_mbar[st], kTileD * 8 );
+    bulk_load( s_stage + st * kTileD, verts + t * kTileD, kTileD * 8, &s_mbar[st] );
+  };
+  uint32_t pend = 0;  // thread 0: bit s set while stage s has a copy in flight
+  if ( tid == 0 )
+  {
+    mbar_init( &s_mbar[0], 1 );
+    mbar_init( &s_mbar[1], 1 );
+    mbar_init_fence();
+    if ( blockIdx.x < full )
     {
-      const double *p = s_v + threadIdx.x * per;
-      double sx = 0.0, sy = 0.0, sz = 0.0;
-      for ( int v = 0; v < V; ++v )
+      issue( blockIdx.x, 0 );
+      pend |= 1u;
+    }
+    if ( blockIdx.x + G < full )
+    {
+      issue( blockIdx.x + G, 1 );
+      pend |= 2u;
+    }
+  }
+  __syncthreads();
+  uint32_t phases = 0;  // bit s: parity of stage s's next completion
+  int st = 0;
+  for ( uint64_t t = blockIdx.x; t < tiles; t += G, st ^= 1 )
+  {
+    double *sv = s_stage + st * kTileD;
+    const int cnt = static_cast< int >( min( static_cast< uint64_t >( kElemThreads ), n - t * kElemThreads ) );
+    if ( t < full )
+    {
+      const uint32_t ph = ( phases >> st ) & 1u;
+      const bool ok = mbar_wait_bounded( &s_mbar[st], ph, spin_limit );
+      phases ^= 1u << st;
+      if ( tid == 0 && ok ) pend &= ~( 1u << st );
+      if ( __syncthreads_or( !ok ) )
       {
-        const double x = p[3 * v], y = p[3 * v + 1], z = p[3 * v + 2];
-        bad |= !( isfinite( x ) && isfinite( y ) && isfinite( z ) );
-        sx = __dadd_rn( sx, x );
-        sy = __dadd_rn( sy, y );
-        sz = __dadd_rn( sz, z );
+        if ( tid == 0 )
+        {
+          atomicCAS( &sc->error, 0, kErrTimeout );
+          // the shared memory stays allocated until the copies in flight have landed (or the wait gives up)
+          for ( int s2 = 0; s2 < 2; ++s2 )
+            if ( pend & ( 1u << s2 ) )
+              mbar_wait_bounded( &s_mbar[s2], ( ( phases >> s2 ) & 1u ) ^ ( s2 == st ? 1u : 0u ), spin_limit );
+        }
+        return;
       }
-      const double dv = static_cast< double >( V );
-      const uint64_t i = t0 + threadIdx.x;
-      cx[i] = __ddiv_rn( sx, dv );
-      cy[i] = __ddiv_rn( sy, dv );
-      cz[i] = __ddiv_rn( sz, dv );
-#pragma unroll
-      for ( int a = 0; a < 3; ++a )
-      {
-        double lo, hi;
-        slab64< K >( p, V, a, eps, lo, hi );
-        mn[a] = ( lo < mn[a] ) ? lo : mn[a];
-        mx[a] = ( hi > mx[a] ) ? hi : mx[a];
-      }
+    } else {
+      const double *src = verts + t * kTileD;
+      for ( int k = tid; k < cnt * per; k += kElemThreads ) sv[k] = __ldcs( src + k );
+      __syncthreads();
+    }
+    if ( tid < cnt ) element_centroid_bounds< K >( sv + tid * per, VT, eps, t * kElemThreads + tid, cx, cy, cz, mn, mx, bad );
+    __syncthreads();  // the stage was read by every thread: it may be refilled
+    if ( tid == 0 && t + 2 * G < full )
+    {
+      fence_proxy_async_smem();
+      issue( t + 2 * G, st );
+      pend |= 1u << st;
     }
   }
   reduce_bounds( mn, mx, bad, sc );
@@ -229,8 +322,36 @@ int sm_count()
 
 template< int K, int VT >
 cudaError_t launch_cb_t(const double *verts, uint32_t V, uint64_t n, double eps, double *cx, double *cy, double *cz,
-                        obj_scalars *sc, cudaStream_t s)
+                        obj_scalars *sc, uint32_t spin_limit, cudaStream_t s)
 {
+  if constexpr ( VT > 0 )
+  {
+    if ( ( reinterpret_cast< uintptr_t >( verts ) & 15 ) == 0 )
+    {
+      const size_t smem2 = static_cast< size_t >( 2 ) * kElemThreads * VT * 3 * sizeof( double );
+      // per device: the shared-memory opt-in and the resident blocks per SM of the persistent grid
+      static int per_sm[64] = {};
+      int dev = 0;
+      cudaError_t e = cudaGetDevice( &dev );
+      if ( e != cudaSuccess ) return e;
+      if ( dev < 0 || dev >= 64 ) return cudaErrorInvalidDevice;
+      if ( !per_sm[dev] )
+      {
+        e = cudaFuncSetAttribute( k_centroid_bounds_tma< K, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast< int >( smem2 ) );
+        if ( e != cudaSuccess ) return e;
+        int b = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &b, k_centroid_bounds_tma< K, VT >, kElemThreads, smem2 );
+        if ( e != cudaSuccess ) return e;
+        per_sm[dev] = b > 0 ? b : 1;
+      }
+      const uint64_t tiles = ( n + kElemThreads - 1 ) / kElemThreads;
+      const uint64_t cap = static_cast< uint64_t >( sm_count() ) * per_sm[dev];
+      const unsigned grid = static_cast< unsigned >( tiles < cap ? ( tiles ? tiles : 1 ) : cap );
+      k_centroid_bounds_tma< K, VT ><<< grid, kElemThreads, smem2, s >>>( verts, n, eps, cx, cy, cz, sc, spin_limit );
+      return cudaGetLastError();
+    }
+  }
   const size_t smem = static_cast< size_t >( kElemThreads ) * V * 3 * sizeof( double );
   // Static shared memory counts against the same 48 KB default: opt in whenever the tile is large.
   if ( smem >= 40 * 1024 )
@@ -248,14 +369,14 @@ cudaError_t launch_cb_t(const double *verts, uint32_t V, uint64_t n, double eps,
 
 template< int K >
 cudaError_t launch_cb_k(const double *verts, uint32_t V, uint64_t n, double eps, double *cx, double *cy, double *cz,
-                        obj_scalars *sc, cudaStream_t s)
+                        obj_scalars *sc, uint32_t spin_limit, cudaStream_t s)
 {
   switch ( V )
   {
-    case 3: return launch_cb_t< K, 3 >( verts, V, n, eps, cx, cy, cz, sc, s );
-    case 4: return launch_cb_t< K, 4 >( verts, V, n, eps, cx, cy, cz, sc, s );
-    case 8: return launch_cb_t< K, 8 >( verts, V, n, eps, cx, cy, cz, sc, s );
-    default: return launch_cb_t< K, 0 >( verts, V, n, eps, cx, cy, cz, sc, s );
+    case 3: return launch_cb_t< K, 3 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
+    case 4: return launch_cb_t< K, 4 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
+    case 8: return launch_cb_t< K, 8 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
+    default: return launch_cb_t< K, 0 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
   }
 }
 
@@ -313,13 +434,13 @@ cudaError_t launch_obj_init(obj_scalars *sc, uint32_t *hist, uint64_t hist_words
 }
 
 cudaError_t launch_centroid_bounds(int K, const double *verts, uint32_t V, uint64_t n, double eps, double *cx,
-                                   double *cy, double *cz, obj_scalars *sc, cudaStream_t s)
+                                   double *cy, double *cz, obj_scalars *sc, uint32_t spin_limit, cudaStream_t s)
 {
   switch ( K )
   {
-    case 6: return launch_cb_k< 6 >( verts, V, n, eps, cx, cy, cz, sc, s );
-    case 18: return launch_cb_k< 18 >( verts, V, n, eps, cx, cy, cz, sc, s );
-    case 26: return launch_cb_k< 26 >( verts, V, n, eps, cx, cy, cz, sc, s );
+    case 6: return launch_cb_k< 6 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
+    case 18: return launch_cb_k< 18 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
+    case 26: return launch_cb_k< 26 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
     default: return cudaErrorInvalidValue;
   }
 }

@@ -11,6 +11,7 @@
 // look-back over the preceding tiles' status words, reorders the tile in shared memory and writes contiguous
 // digit runs. Every look-back wait is bounded: past spin_limit polls the block records BVHG_ERR_TIMEOUT and
 // goes on with a garbage offset (the host reports the error; no thread waits forever).
+#include "bulk_copy.cuh"
 #include "bvhg_internal.cuh"
 
 #include <atomic>
@@ -44,43 +45,6 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s
     if ( k < w ) wpre += s_warp[k];
   __syncthreads();
   return wpre + inc - x;
-}
-
-// Shared-memory address of a pointer into shared memory (PTX operand form).
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-  return static_cast< uint32_t >( __cvta_generic_to_shared( p ) );
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-  asm volatile( "mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"( smem_addr( bar ) ), "r"( count ) : "memory" );
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-  asm volatile( "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"( smem_addr( bar ) ), "r"( bytes )
-                : "memory" );
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase)
-{
-  uint32_t ok;
-  asm volatile( "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-                : "=r"( ok )
-                : "r"( smem_addr( bar ) ), "r"( phase )
-                : "memory" );
-  return ok != 0;
-}
-
-// One-dimensional bulk copy global -> shared (TMA), completing on an mbarrier. Both addresses 16-byte aligned,
-// size a multiple of 16.
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-  asm volatile( "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                  smem_addr( dst ) ),
-                "l"( src ), "r"( bytes ), "r"( smem_addr( bar ) )
-                : "memory" );
 }
 
 // Persistent radix pass. A block keeps taking tiles from the pass's tile counter; while it ranks, resolves and
@@ -129,7 +93,7 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
   {
     mbar_init( &s_mbar[0], 1 );
     mbar_init( &s_mbar[1], 1 );
-    asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+    mbar_init_fence();
     s_next = static_cast< int >( atomicAdd( &sc->sort_tile_counter[pass], 1u ) );
     s_err = 0;
   }
@@ -312,7 +276,7 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
     // the other stage was drained by the previous iteration's write-out (barrier below): refill it
     if ( tid == 0 && next < tiles && tma_tile( next ) )
     {
-      asm volatile( "fence.proxy.async.shared::cta;" ::: "memory" );
+      fence_proxy_async_smem();
       issue( next, st ^ 1 );
     }
     // reorder the tile into its own stage buffer (its data now lives in registers)
