@@ -16,6 +16,7 @@ namespace bvhg {
 namespace {
 
 constexpr int kElemThreads = 256;
+constexpr int kKeyUnroll = 4;  // elements per thread per step of the key kernel
 
 // Exact min/max block reduction of 6 doubles, then one order-preserving 64-bit atomic per value.
 __device__ __forceinline__ void reduce_bounds(double mn[3], double mx[3], bool bad, obj_scalars *sc)
@@ -271,34 +272,50 @@ __global__ void __launch_bounds__( kElemThreads ) k_keys_hist(const double *__re
   const double m0 = s_min[0], m1 = s_min[1], m2 = s_min[2];
   const double i0 = s_inv[0], i1 = s_inv[1], i2 = s_inv[2];
   const unsigned lane = threadIdx.x & 31;
-  const uint64_t stride = static_cast< uint64_t >( gridDim.x ) * kElemThreads;
-  const uint64_t base = static_cast< uint64_t >( blockIdx.x ) * kElemThreads;
+  // Each warp takes runs of kKeyUnroll * 32 consecutive elements (element w0 + 32 u + lane in step u): the loads of
+  // all steps are issued before the first key is formed, which keeps kKeyUnroll loads per thread in flight.
+  constexpr int U = kKeyUnroll;
+  const uint64_t stride = static_cast< uint64_t >( gridDim.x ) * kElemThreads * U;
+  const uint64_t base = static_cast< uint64_t >( blockIdx.x ) * kElemThreads * U;
   // Every warp runs the same number of iterations so that the warp-wide match below sees all 32 lanes.
-  for ( uint64_t w0 = base + ( threadIdx.x & ~31u ); w0 < n; w0 += stride )
+  for ( uint64_t w0 = base + ( threadIdx.x & ~31u ) * U; w0 < n; w0 += stride )
   {
-    const uint64_t i = w0 + lane;
-    const bool valid = i < n;
-    uint64_t key = 0;
-    if ( valid )
-    {
-      const uint64_t qx = quant21( cx[i], m0, i0 );
-      const uint64_t qy = quant21( cy[i], m1, i1 );
-      const uint64_t qz = quant21( cz[i], m2, i2 );
-      key = ( expand64( qz ) << 2 ) | ( expand64( qy ) << 1 ) | expand64( qx );
-      keys[i] = key;
-    }
-    const unsigned vmask = __ballot_sync( 0xffffffffu, valid );
+    double vx[U], vy[U], vz[U];
 #pragma unroll
-    for ( int p = FIRST; p < PASSES; ++p )
+    for ( int u = 0; u < U; ++u )
     {
-      const unsigned d = static_cast< unsigned >( ( key >> ( p * BITS ) ) & ( RADIX - 1 ) );
-      // Spatially coherent warps share their high digits: one atomic for a uniform warp, else one per lane.
-      const unsigned d0 = __shfl_sync( 0xffffffffu, d, 0 );
-      if ( __all_sync( 0xffffffffu, d == d0 || !valid ) && vmask == 0xffffffffu )
+      const uint64_t i = w0 + 32 * u + lane;
+      vx[u] = i < n ? cx[i] : 0.0;
+      vy[u] = i < n ? cy[i] : 0.0;
+      vz[u] = i < n ? cz[i] : 0.0;
+    }
+#pragma unroll
+    for ( int u = 0; u < U; ++u )
+    {
+      const uint64_t i = w0 + 32 * u + lane;
+      const bool valid = i < n;
+      uint64_t key = 0;
+      if ( valid )
       {
-        if ( lane == 0 ) atomicAdd( &s_hist[( p - FIRST ) * RADIX + d0], 32u );
-      } else if ( valid ) {
-        atomicAdd( &s_hist[( p - FIRST ) * RADIX + d], 1u );
+        const uint64_t qx = quant21( vx[u], m0, i0 );
+        const uint64_t qy = quant21( vy[u], m1, i1 );
+        const uint64_t qz = quant21( vz[u], m2, i2 );
+        key = ( expand64( qz ) << 2 ) | ( expand64( qy ) << 1 ) | expand64( qx );
+        keys[i] = key;
+      }
+      const unsigned vmask = __ballot_sync( 0xffffffffu, valid );
+#pragma unroll
+      for ( int p = FIRST; p < PASSES; ++p )
+      {
+        const unsigned d = static_cast< unsigned >( ( key >> ( p * BITS ) ) & ( RADIX - 1 ) );
+        // Spatially coherent warps share their high digits: one atomic for a uniform warp, else one per lane.
+        const unsigned d0 = __shfl_sync( 0xffffffffu, d, 0 );
+        if ( __all_sync( 0xffffffffu, d == d0 || !valid ) && vmask == 0xffffffffu )
+        {
+          if ( lane == 0 ) atomicAdd( &s_hist[( p - FIRST ) * RADIX + d0], 32u );
+        } else if ( valid ) {
+          atomicAdd( &s_hist[( p - FIRST ) * RADIX + d], 1u );
+        }
       }
     }
   }
@@ -384,7 +401,7 @@ template< int BITS >
 cudaError_t launch_kh_t(const double *cx, const double *cy, const double *cz, uint64_t n, obj_scalars *sc,
                         uint64_t *keys, uint32_t *hist, cudaStream_t s)
 {
-  const uint64_t blocks = ( n + kElemThreads - 1 ) / kElemThreads;
+  const uint64_t blocks = ( n + kElemThreads * kKeyUnroll - 1 ) / ( kElemThreads * kKeyUnroll );
   const uint64_t cap = static_cast< uint64_t >( sm_count() ) * 8;
   const unsigned grid = static_cast< unsigned >( blocks < cap ? ( blocks ? blocks : 1 ) : cap );
   k_keys_hist< BITS ><<< grid, kElemThreads, 0, s >>>( cx, cy, cz, n, sc, keys, hist );
