@@ -421,3 +421,22 @@ def test_objects_with_different_vertex_counts(precision):
                 assert np.array_equal(got, orc.pair_set(xa, xb, 18)), (rep, a, b)
             for name in objs:
                 ctx.build(objs[name])
+
+
+@pytest.mark.parametrize("k", [6, 18, 26])
+@pytest.mark.parametrize("V", [3, 4, 8])
+@pytest.mark.parametrize("eps", [0.0, -0.0, 0.25])
+def test_signed_zeros_and_exact_cancellations(k, V, eps):
+    """Coordinates from {+-0, +-0.25, +-1}: many projections cancel exactly or add signed zeros, which is where
+    the kernels' shortcuts for the normal components 0 and +-1 must still give the bits of
+    ((v0 * n0) + (v1 * n1)) + (v2 * n2) - eps / + eps. Slabs, centroids, bounds, keys and pairs, bit for bit."""
+    rng = np.random.default_rng(1000 + 10 * k + V)
+    values = np.array([-0.0, 0.0, 0.25, -0.25, 1.0, -1.0])
+    a = values[rng.integers(0, len(values), size=(1500, V, 3))]
+    b = values[rng.integers(0, len(values), size=(1200, V, 3))]
+    assert np.signbit(a).any() and (a == 0).any()
+    with bvhg.Context(k=k, epsilon=eps) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        check_stages(ctx, oa, a, k, eps)
+        check_stages(ctx, ob, b, k, eps)
+        assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b, k, eps))
