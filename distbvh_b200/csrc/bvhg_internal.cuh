@@ -47,7 +47,7 @@ struct pair_scalars
   unsigned long long count;   // pairs found (may exceed capacity)
   unsigned long long count2;  // pairs surviving the FP64 recheck
   int error;
-  int pad;
+  unsigned packet_next;       // the traversal's dispenser of packet chunks
 };
 
 constexpr int kLeafSize = 8;  // elements per tree leaf (consecutive Morton ranks)

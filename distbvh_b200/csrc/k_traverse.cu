@@ -50,6 +50,15 @@ struct slab_pair< float >
   }
 };
 
+// Axes of a node row loaded together in the walk (a chunk of loads in flight per round trip; bounded by registers).
+template< int K, typename T >
+constexpr int kNodeChunk = ( K / 2 ) <= 4 ? K / 2 : ( sizeof( T ) == 4 ? ( K / 2 + 1 ) / 2 : 3 );
+
+// Resident blocks per SM of the walk: 4 for the variants that compute slabs (128 registers), 6 for the one that
+// reads stored slabs.
+template< int K, typename T, bool LAZY >
+constexpr int kTravBlocksPerSM = LAZY ? 4 : 6;
+
 // Slots for k outputs of each calling lane, one atomic per group of converged lanes: the lanes' exclusive prefix of
 // k is formed from one ballot per bit of k (k < 64), the lowest lane reserves the group's total.
 __device__ __forceinline__ unsigned long long warp_reserve(unsigned k, unsigned long long *counter)
@@ -254,13 +263,23 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
       o1 = o1 && min( kLeafSize * __ldg( &x.range[node].y ) + kLeafSize - 1, static_cast< int >( x.nt ) - 1 ) >
                    static_cast< int >( i );
     }
+    // The node row's slabs in chunks of kNodeChunk axes: a chunk's loads (one sector per axis) are all in flight
+    // before its tests, and the warp stops between chunks once no lane overlaps either child.
 #pragma unroll
-    for ( int a = 0; a < D; ++a )
+    for ( int a0 = 0; a0 < D; a0 += kNodeChunk< K, T > )
     {
-      if ( !__any_sync( 0xffffffffu, o0 || o1 ) ) break;
-      const slab_pair< T > sl = slab_pair< T >::load( nb + a * 4 );
-      o0 = o0 && ( qlo[a] < sl.max0 && sl.min0 < qhi[a] );
-      o1 = o1 && ( qlo[a] < sl.max1 && sl.min1 < qhi[a] );
+      if ( a0 > 0 && !__any_sync( 0xffffffffu, o0 || o1 ) ) break;
+      slab_pair< T > sl[kNodeChunk< K, T >];
+#pragma unroll
+      for ( int j = 0; j < kNodeChunk< K, T >; ++j )
+        if ( a0 + j < D ) sl[j] = slab_pair< T >::load( nb + ( a0 + j ) * 4 );
+#pragma unroll
+      for ( int j = 0; j < kNodeChunk< K, T >; ++j )
+      {
+        if ( a0 + j >= D ) break;
+        o0 = o0 && ( qlo[a0 + j] < sl[j].max0 && sl[j].min0 < qhi[a0 + j] );
+        o1 = o1 && ( qlo[a0 + j] < sl[j].max1 && sl[j].min1 < qhi[a0 + j] );
+      }
     }
     const unsigned m0 = __ballot_sync( 0xffffffffu, o0 );
     const unsigned m1 = __ballot_sync( 0xffffffffu, o1 );
@@ -313,7 +332,7 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
 // mask), in shared memory. At a leaf bucket the lanes of the mask test their element against the bucket's element
 // slabs: the stored rows (dense contact) or, computed once by the warp from the vertices, a shared cache.
 template< int K, typename T, int VT, bool LAZY >
-__global__ void __launch_bounds__( kTravThreads, LAZY ? 4 : 6 ) k_traverse(const trav_args< T > x,
+__global__ void __launch_bounds__( kTravThreads, kTravBlocksPerSM< K, T, LAZY > ) k_traverse(const trav_args< T > x,
                                                                          const obj_scalars *__restrict__ qsc)
 {
   constexpr int D = K / 2;
@@ -337,11 +356,41 @@ __global__ void __launch_bounds__( kTravThreads, LAZY ? 4 : 6 ) k_traverse(const
     for ( int a = 0; a < D0; ++a ) o = o && ( qr[2 * a] < rb[2 * a + 1] && rb[2 * a] < qr[2 * a + 1] );
     if ( !o ) return;
   }
-  // Packets (warps of 32 query ranks) are taken grid-stride.
   const uint32_t packets = ( x.nq + 31 ) / 32;
-  const uint32_t warp_stride = ( gridDim.x * blockDim.x ) >> 5;
-  for ( uint32_t pk = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5; pk < packets; pk += warp_stride )
-    traverse_packet< K, T, VT, LAZY >( x, pk * 32 + lane, lane, stack, cache, rb );
+  if constexpr ( !LAZY )
+  {
+    // Dense contact (stored slabs): one packet per warp, the hardware balances the walks.
+    const uint32_t pk = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+    if ( pk < packets ) traverse_packet< K, T, VT, LAZY >( x, pk * 32 + lane, lane, stack, cache, rb );
+    return;
+  }
+  // Sparse contact: packets (32 query ranks) in a persistent grid. A warp takes chunks from the pair counters'
+  // packet dispenser; chunk c holds the packets c, c + C, c + 2C, ... (C chunks), so a contact region (consecutive
+  // Morton ranks) is spread over many chunks. Lane j tests the union box of the chunk's packet j against the target
+  // root (one load per lane for the packets far from the target), then the warp walks the survivors one after the
+  // other.
+  const uint32_t chunks = ( packets + 31 ) / 32;
+  while ( true )
+  {
+    uint32_t c = 0;
+    if ( lane == 0 ) c = atomicAdd( &x.ps->packet_next, 1u );
+    c = __shfl_sync( 0xffffffffu, c, 0 );
+    if ( c >= chunks ) break;
+    const uint64_t pk = c + static_cast< uint64_t >( lane ) * chunks;
+    bool o = false;
+    if ( pk < packets )
+    {
+      const T *wb = x.qwarp + pk * D * 2;
+      o = true;
+#pragma unroll
+      for ( int a = 0; a < D; ++a ) o = o && ( __ldg( wb + 2 * a ) < rb[2 * a + 1] && rb[2 * a] < __ldg( wb + 2 * a + 1 ) );
+    }
+    for ( unsigned m = __ballot_sync( 0xffffffffu, o ); m; m &= m - 1 )
+    {
+      const uint32_t p = c + static_cast< uint32_t >( __ffs( m ) - 1 ) * chunks;
+      traverse_packet< K, T, VT, LAZY >( x, p * 32 + lane, lane, stack, cache, rb );
+    }
+  }
 }
 
 template< int K, typename T >
@@ -370,9 +419,15 @@ cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, double eps, uint2
   x.pairs = pairs;
   x.cap = cap;
   x.ps = ps;
-  // one warp per packet
-  const uint64_t blocks = ( q.n + kTravThreads - 1 ) / kTravThreads;
-  const unsigned grid = static_cast< unsigned >( blocks < ( 1ull << 30 ) ? blocks : ( 1ull << 30 ) );
+  // Dense contact: one warp per packet. Sparse: a persistent grid of at most the resident blocks (4 per SM), one
+  // warp per chunk of 32 packets at most.
+  constexpr uint64_t kWarps = kTravThreads / 32;
+  const uint64_t packets = ( q.n + 31 ) / 32;
+  const uint64_t chunks = ( packets + 31 ) / 32;
+  const uint64_t resident = static_cast< uint64_t >( device_sm_count() ) * kTravBlocksPerSM< K, T, true >;
+  uint64_t blocks = ( q.stored && t.stored ) ? ( packets + kWarps - 1 ) / kWarps : ( chunks + kWarps - 1 ) / kWarps;
+  if ( !( q.stored && t.stored ) && blocks > resident ) blocks = resident;
+  const unsigned grid = static_cast< unsigned >( blocks < ( 1ull << 30 ) ? ( blocks ? blocks : 1 ) : ( 1ull << 30 ) );
   // both objects' element slabs stored (dense contact): the variant that only reads them; else the one that
   // computes the slabs it tests from the vertices (unrolled when both objects have the same vertex count)
   if ( q.stored && t.stored )
