@@ -52,7 +52,7 @@ struct slab_pair< float >
 
 // Axes of a node row loaded together in the walk (a chunk of loads in flight per round trip; bounded by registers).
 template< int K, typename T >
-constexpr int kNodeChunk = ( K / 2 ) <= 4 ? K / 2 : ( sizeof( T ) == 4 ? ( K / 2 + 1 ) / 2 : 3 );
+constexpr int kNodeChunk = ( K / 2 ) <= 4 ? K / 2 : ( sizeof( T ) == 4 ? ( K / 2 + 1 ) / 2 : 5 );
 
 // Resident blocks per SM of the walk: 4 for the variants that compute slabs (128 registers), 6 for the one that
 // reads stored slabs.
