@@ -25,7 +25,7 @@ EXPORTS = (
     "bvhg_get_kdops", "bvhg_get_kdops_f32", "bvhg_get_centroids", "bvhg_validate_tree", "bvhg_last_candidates",
     "bvhg_get_stage_times", "bvhg_launch_count", "bvhg_set_spin_limit", "bvhg_test_stall_sort", "bvhg_debug_normal",
     "bvhg_synchronize", "bvhg_last_error", "bvhg_status_string", "bvhg_radix_sort_noalloc",
-    "bvhg_batch_broadphase", "bvhg_batch_autotune",
+    "bvhg_batch_broadphase", "bvhg_batch_autotune", "bvhg_sort_and_sweep",
 )
 
 
@@ -80,6 +80,7 @@ def _load():
         "bvhg_radix_sort_noalloc": (I32, [P, P, P, U64, P]),
         "bvhg_batch_broadphase": (I32, [P, U32, P, P, I32, P, U64, P, P, I32]),
         "bvhg_batch_autotune": (I32, [P, U32, P, P, I32, ctypes.POINTER(U32), ctypes.POINTER(ctypes.c_double)]),
+        "bvhg_sort_and_sweep": (I32, [P, I32, I32, I32, P, U64, ctypes.POINTER(U64), ctypes.POINTER(I32), I32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -192,6 +193,24 @@ class Context:
             raise BvhgError(st, f"overflow: {cnt.value} pairs")
         self._check(st)
         return out[: cnt.value]
+
+    def sort_and_sweep(self, a, b, axis=-1):
+        """Sort-and-sweep pairs (gid in a, gid in b) as an (m, 2) uint64 array, and the axis swept."""
+        cnt = ctypes.c_uint64()
+        used = ctypes.c_int32()
+        st = lib.bvhg_sort_and_sweep(self._h, a, b, axis, None, 0, ctypes.byref(cnt), ctypes.byref(used), MEM_HOST)
+        if st not in (OK, ERR_OVERFLOW):
+            self._check(st)
+        out = np.empty((max(cnt.value, 1), 2), dtype=np.uint64)
+        self._check(lib.bvhg_sort_and_sweep(self._h, a, b, axis, out.ctypes.data, cnt.value, ctypes.byref(cnt),
+                                            ctypes.byref(used), MEM_HOST))
+        return out[: cnt.value], used.value
+
+    def sort_and_sweep_raw(self, a, b, axis, out_ptr, capacity, mem):
+        cnt = ctypes.c_uint64()
+        used = ctypes.c_int32()
+        st = lib.bvhg_sort_and_sweep(self._h, a, b, axis, out_ptr, capacity, ctypes.byref(cnt), ctypes.byref(used), mem)
+        return st, cnt.value, used.value
 
     def broadphase_raw(self, a, b, out_ptr, capacity, mem):
         cnt = ctypes.c_uint64()

@@ -188,6 +188,8 @@ struct bvhg_ctx
   std::vector< std::unique_ptr< object > > objs;
   cudaEvent_t fork_evt = nullptr;
   std::string err;
+  // sort-and-sweep scratch
+  dev_buf sw_keys, sw_vals, sw_rows, sw_hist, sw_status, sw_sc, sw_params, sw_partial;
   // pairs
   dev_buf pairs, pairs2, pairs_out, pscal;
   uint64_t pair_cap = 0, pair2_cap = 0;
@@ -1187,6 +1189,112 @@ bvhg_status bvhg_self_collision(bvhg_ctx *ctx, int32_t obj, uint64_t *pairs, uin
   if ( st != BVHG_OK ) return st;
   note_density( o, o, true, ctx->last_candidates );
   return emit_pairs( ctx, o, o, true, lp, np, pairs, capacity, count, mem );
+}
+
+bvhg_status bvhg_sort_and_sweep(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, int32_t axis, uint64_t *pairs,
+                                uint64_t capacity, uint64_t *count, int32_t *axis_used, int32_t mem)
+{
+  if ( !valid_obj( ctx, obj_a ) || !valid_obj( ctx, obj_b ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  if ( obj_a == obj_b ) return fail( ctx, BVHG_ERR_ARG, "sort-and-sweep needs two objects (bvhg_self_collision for one)" );
+  if ( !count ) return fail( ctx, BVHG_ERR_ARG, "null count" );
+  if ( capacity > 0 && !pairs ) return fail( ctx, BVHG_ERR_ARG, "null pair buffer" );
+  if ( axis < -1 || axis > 2 ) return fail( ctx, BVHG_ERR_ARG, "axis must be -1, 0, 1 or 2" );
+  if ( mem != BVHG_MEM_HOST && mem != BVHG_MEM_DEVICE ) return fail( ctx, BVHG_ERR_ARG, "bad memory kind" );
+  object &a = *ctx->objs[obj_a];
+  object &b = *ctx->objs[obj_b];
+  if ( !a.built || !b.built ) return fail( ctx, BVHG_ERR_STATE, "sort-and-sweep before build" );
+  cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, a );
+  join_object( ctx, b );
+  *count = 0;
+  if ( axis_used ) *axis_used = axis < 0 ? 0 : axis;
+  if ( a.n == 0 || b.n == 0 ) return BVHG_OK;
+  const int K = ctx->cfg.k;
+  const uint64_t nb = b.n;
+  const uint64_t nb4 = ( nb + 3 ) & ~3ull;  // second halves of the ping-pong buffers start 16-byte aligned
+  const uint64_t tiles = ( nb + kSortTile - 1 ) / kSortTile;
+  const uint64_t status_words = 4 * ( tiles + 1 ) * 256;
+  cudaStream_t s = ctx->stream;
+  BVHG_CUDA( ctx, ctx->sw_keys.reserve( 2 * nb4 * 8 ) );
+  BVHG_CUDA( ctx, ctx->sw_vals.reserve( 2 * nb4 * 4 ) );
+  BVHG_CUDA( ctx, ctx->sw_rows.reserve( nb * K * 8 ) );
+  BVHG_CUDA( ctx, ctx->sw_hist.reserve( 4 * 256 * 4 ) );
+  BVHG_CUDA( ctx, ctx->sw_status.reserve( status_words * 4 ) );
+  BVHG_CUDA( ctx, ctx->sw_sc.reserve( sizeof( obj_scalars ) ) );
+  BVHG_CUDA( ctx, ctx->sw_params.reserve( sweep_params_bytes() ) );
+  BVHG_CUDA( ctx, ctx->sw_partial.reserve( sweep_partial_bytes() ) );
+  BVHG_CUDA( ctx, ctx->pscal.reserve( sizeof( pair_scalars ) ) );
+  if ( ctx->pair_cap == 0 )
+  {
+    ctx->pair_cap = 1u << 20;
+    BVHG_CUDA( ctx, ctx->pairs.reserve( ctx->pair_cap * sizeof( uint2 ) ) );
+  }
+  uint64_t *k0 = ctx->sw_keys.as< uint64_t >(), *k1 = k0 + nb4;
+  uint32_t *v0 = ctx->sw_vals.as< uint32_t >(), *v1 = v0 + nb4;
+  obj_scalars *ssc = ctx->sw_sc.as< obj_scalars >();
+  pair_scalars *ps = ctx->pscal.as< pair_scalars >();
+  sweep_launch x{};
+  x.K = K;
+  x.averts = a.verts;
+  x.bverts = b.verts;
+  x.aV = a.V;
+  x.bV = b.V;
+  x.na = a.n;
+  x.nb = nb;
+  x.eps = ctx->cfg.epsilon;
+  x.acx = a.cx.as< double >();
+  x.acy = a.cy.as< double >();
+  x.acz = a.cz.as< double >();
+  x.bcx = b.cx.as< double >();
+  x.bcy = b.cy.as< double >();
+  x.bcz = b.cz.as< double >();
+  x.asc = a.sc();
+  x.bsc = b.sc();
+  x.partial = ctx->sw_partial.as< double >();
+  x.params = ctx->sw_params.p;
+  x.rows = ctx->sw_rows.as< double >();
+  x.keys = k0;
+  x.hist = ctx->sw_hist.as< uint32_t >();
+  x.skeys = k0;  // four passes: k0 -> k1 -> k0 -> k1 -> k0
+  x.svals = v0;
+  x.sc = ssc;
+  x.ps = ps;
+  x.s = s;
+  for ( int attempt = 0; attempt < 3; ++attempt )
+  {
+    x.pairs = ctx->pairs.as< uint2 >();
+    x.cap = ctx->pair_cap;
+    BVHG_CUDA( ctx, cudaMemsetAsync( ssc, 0, sizeof( obj_scalars ), s ) );
+    BVHG_CUDA( ctx, cudaMemsetAsync( x.hist, 0, 4 * 256 * 4, s ) );
+    BVHG_CUDA( ctx, cudaMemsetAsync( ctx->sw_status.p, 0, status_words * 4, s ) );
+    BVHG_CUDA( ctx, cudaMemsetAsync( ps, 0, sizeof( pair_scalars ), s ) );
+    BVHG_CUDA( ctx, launch_sweep_setup( x, axis ) );
+    BVHG_CUDA( ctx, launch_sweep_keys( x ) );
+    for ( int pass = 0; pass < 4; ++pass )
+    {
+      const bool even = ( pass & 1 ) == 0;
+      BVHG_CUDA( ctx, launch_onesweep( 8, even ? k0 : k1, pass == 0 ? nullptr : ( even ? v0 : v1 ), even ? k1 : k0,
+                                       even ? v1 : v0, nb, pass, x.hist, ctx->sw_status.as< uint32_t >(), ssc,
+                                       ctx->spin_limit, 0, s ) );
+    }
+    BVHG_CUDA( ctx, launch_sweep( x ) );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( ctx->host_ps, ps, sizeof( pair_scalars ), cudaMemcpyDeviceToHost, s ) );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( ctx->host_err, &ssc->error, sizeof( int ), cudaMemcpyDeviceToHost, s ) );
+    BVHG_CUDA( ctx, cudaMemcpyAsync( ctx->host_err + 1, x.params, sizeof( int ), cudaMemcpyDeviceToHost, s ) );
+    BVHG_CUDA( ctx, cudaStreamSynchronize( s ) );
+    const bvhg_status st = object_error( ctx, ctx->host_err[0] );
+    if ( st != BVHG_OK ) return st;
+    if ( axis_used ) *axis_used = ctx->host_err[1];
+    const uint64_t np = ctx->host_ps->count;
+    if ( np > ctx->pair_cap )
+    {
+      ctx->pair_cap = np + np / 8;
+      BVHG_CUDA( ctx, ctx->pairs.reserve( ctx->pair_cap * sizeof( uint2 ) ) );
+      continue;
+    }
+    return emit_pairs( ctx, a, b, false, ctx->pairs.as< uint2 >(), np, pairs, capacity, count, mem );
+  }
+  return fail( ctx, BVHG_ERR_CUDA, "pair buffer did not converge" );
 }
 
 bvhg_status bvhg_get_morton(bvhg_ctx *ctx, int32_t obj, uint64_t *sorted_keys, uint32_t *perm, double *min3,

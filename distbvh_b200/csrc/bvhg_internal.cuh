@@ -106,6 +106,39 @@ inline int sort_first_pass(int bits) { return 32 / bits; }
 cudaError_t launch_obj_init(obj_scalars *sc, uint32_t *hist, uint64_t hist_words, uint32_t *status,
                             uint64_t status_words, int *exch, uint64_t exch_words, cudaStream_t s);
 
+// Sort-and-sweep between two objects (k_sweep.cu): the arguments of its three phases.
+struct sweep_launch
+{
+  int K;
+  const double *averts, *bverts;
+  uint32_t aV, bV;
+  uint64_t na, nb;
+  double eps;
+  const double *acx, *acy, *acz, *bcx, *bcy, *bcz;  // centroids (axis choice)
+  const obj_scalars *asc, *bsc;                     // K1 bounds of both objects (global range)
+  double *partial;                                  // sweep_partial_bytes()
+  void *params;                                     // sweep_params_bytes()
+  double *rows;                                     // nb * K doubles: B's element slabs, original order
+  uint64_t *keys;                                   // nb: B's u32 keys, original order
+  uint32_t *hist;                                   // 4 * 256: byte histograms of the keys
+  const uint64_t *skeys;                            // sorted keys
+  const uint32_t *svals;                            // B's element indices in key order
+  const obj_scalars *sc;                            // scalars of the keys' sort (error word)
+  uint2 *pairs;
+  uint64_t cap;
+  pair_scalars *ps;
+  cudaStream_t s;
+};
+size_t sweep_params_bytes();
+size_t sweep_partial_bytes();
+int sweep_axis_read(const void *params_host_copy);
+// The axis (axis < 0: the one of largest centroid variance) and its scale factor, from the objects' bounds.
+cudaError_t launch_sweep_setup(const sweep_launch &x, int axis);
+// B's slab rows, keys, byte histograms and the key window width.
+cudaError_t launch_sweep_keys(const sweep_launch &x);
+// A's sweeps over the sorted keys; pairs (index into A, index into B) counted in ps->count.
+cudaError_t launch_sweep(const sweep_launch &x);
+
 cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
                             obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s);

@@ -15,6 +15,8 @@
  *   bvhg_broadphase     <- collision_object::broadphase(collision_object&) (src/bvh/collision_object.cpp:248) at
  *                          element granularity, i.e. potential_collision_set (src/bvh/collision_query.hpp:370-379).
  *   bvhg_self_collision <- self_collision_set (src/bvh/collision_query.hpp:331-368).
+ *   bvhg_sort_and_sweep <- sort_and_sweep_local with max_variant_axis (src/bvh/narrowphase/kokkos.hpp:125-248),
+ *                          the two objects as the two patches.
  *   bvhg_get_morton     <- the Morton keys and permutation of morton_cluster (src/bvh/split/cluster.hpp:89-179) /
  *                          morton (src/bvh/contact_entity.hpp:175-191); a parity probe.
  *   bvhg_get_kdops      <- entity_snapshot::kdop() (src/bvh/snapshot.hpp:68-125); a parity probe.
@@ -136,6 +138,17 @@ BVHG_API bvhg_status bvhg_broadphase(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b
 /* Intra-object pairs with pairs[2p] < pairs[2p + 1] in local index order, reported as gids. */
 BVHG_API bvhg_status bvhg_self_collision(bvhg_ctx *ctx, int32_t obj, uint64_t *pairs, uint64_t capacity, uint64_t *count,
                                 int32_t mem);
+
+/* Sort-and-sweep between two built objects (sort_and_sweep_local, src/bvh/narrowphase/kokkos.hpp:164-248): B's
+ * slab minima on one cardinal axis become u32 keys over the union of both objects' extents there, a stable sort
+ * orders them, and every element of A sweeps B in key order, emitting the elements that overlap it strictly on
+ * every slab. axis = 0, 1 or 2, or -1 for the axis of largest centroid variance over both objects
+ * (max_variant_axis, kokkos.hpp:125-160); *axis_used (may be NULL) receives the axis swept. The pair set is the
+ * exact S(A, B), the same as bvhg_broadphase's, for any axis (pairs as there: gid in obj_a, gid in obj_b); its
+ * cost grows with the elements of B whose extents on the axis meet each element of A, so it suits patch-sized
+ * objects. FP64 slabs in both precision forms. obj_a != obj_b. Blocks until the count is known. */
+BVHG_API bvhg_status bvhg_sort_and_sweep(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, int32_t axis, uint64_t *pairs,
+                                         uint64_t capacity, uint64_t *count, int32_t *axis_used, int32_t mem);
 
 /* Batching form (no single counterpart in the reference: it runs many broadphase(other) calls of
  * src/bvh/collision_object.cpp:248 at once). Scene s pairs objects obj_a[s] and obj_b[s] (obj_a[s] == obj_b[s]: that

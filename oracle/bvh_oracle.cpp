@@ -594,6 +594,98 @@ std::int64_t orc_self_pairs_tree(const double *s, const double *c, std::uint64_t
   return sink.cnt;
 }
 
+// max_variant_axis (src/bvh/narrowphase/kokkos.hpp:125-160): the cardinal axis of largest variance of the
+// centroids of A and B together, var = sum(c^2) - sum(c)^2 / N, sums in element order (A then B); ties keep the
+// lower axis (0, then 1 only when strictly larger, then 2 only when strictly larger than the kept one).
+int orc_max_variant_axis(const double *ca, std::uint64_t na, const double *cb, std::uint64_t nb)
+{
+  double s[3] = { 0, 0, 0 }, s2[3] = { 0, 0, 0 };
+  for ( std::uint64_t i = 0; i < na + nb; ++i )
+  {
+    const double *c = i < na ? ca + 3 * i : cb + 3 * ( i - na );
+    for ( int k = 0; k < 3; ++k )
+    {
+      s[k] += c[k];
+      s2[k] += c[k] * c[k];
+    }
+  }
+  double var[3];
+  for ( int k = 0; k < 3; ++k ) var[k] = s2[k] - s[k] * s[k] / static_cast< double >( na + nb );
+  int axis = 0;
+  if ( var[1] > var[0] ) axis = 1;
+  if ( var[2] > var[axis] ) axis = 2;
+  return axis;
+}
+
+// sort_and_sweep_local (src/bvh/narrowphase/kokkos.hpp:164-248) with A and B as the two patches:
+// - the global range on the axis is the union of both sets' slab extents there (the patches' k-DOPs);
+// - B's slab minima become u32 keys, (min - global_min) * (UINT32_MAX / (global_max - global_min)), converted as
+//   x86-64 gcc converts a double to u32 (truncation of the signed 64-bit value, NaN -> 0);
+// - a stable sort of (key, index) (the reference's radix_sorter);
+// - for every element of A, B in key order: skip while the scaled B maximum is below A's minimum key, stop at the
+//   first B key above A's maximum key, emit the pairs that overlap strictly on every slab.
+// Pairs are (index into A, index into B). Returns the pair count.
+namespace {
+inline std::uint32_t to_u32(double x)
+{
+  if ( std::isnan( x ) || !( x < 9223372036854775808.0 ) || x < -9223372036854775808.0 ) return 0u;
+  return static_cast< std::uint32_t >( static_cast< std::uint64_t >( static_cast< std::int64_t >( x ) ) );
+}
+}  // namespace
+
+std::int64_t orc_sort_and_sweep(const double *sa, std::uint64_t na, const double *sb, std::uint64_t nb, int K,
+                                int axis, std::uint32_t *out, std::uint64_t cap)
+{
+  const int D = K / 2;
+  if ( na == 0 || nb == 0 ) return 0;
+  double gmin = std::numeric_limits< double >::infinity(), gmax = -gmin;
+  for ( std::uint64_t i = 0; i < na; ++i )
+  {
+    gmin = std::min( gmin, sa[i * 2 * D + 2 * axis] );
+    gmax = std::max( gmax, sa[i * 2 * D + 2 * axis + 1] );
+  }
+  for ( std::uint64_t j = 0; j < nb; ++j )
+  {
+    gmin = std::min( gmin, sb[j * 2 * D + 2 * axis] );
+    gmax = std::max( gmax, sb[j * 2 * D + 2 * axis + 1] );
+  }
+  const double fac = static_cast< double >( std::numeric_limits< std::uint32_t >::max() ) / ( gmax - gmin );
+  std::vector< std::uint32_t > key( nb );
+  std::vector< std::uint32_t > idx( nb );
+  for ( std::uint64_t j = 0; j < nb; ++j )
+  {
+    key[j] = to_u32( ( sb[j * 2 * D + 2 * axis] - gmin ) * fac );
+    idx[j] = static_cast< std::uint32_t >( j );
+  }
+  std::stable_sort( idx.begin(), idx.end(), [&](std::uint32_t x, std::uint32_t y) { return key[x] < key[y]; } );
+  std::int64_t cnt = 0;
+  for ( std::uint64_t i = 0; i < na; ++i )
+  {
+    const double *ak = sa + i * 2 * D;
+    const std::uint32_t amin = to_u32( ( ak[2 * axis] - gmin ) * fac );
+    const std::uint32_t amax = to_u32( ( ak[2 * axis + 1] - gmin ) * fac );
+    for ( std::uint64_t r = 0; r < nb; ++r )
+    {
+      const std::uint32_t j = idx[r];
+      const double *bk = sb + static_cast< std::uint64_t >( j ) * 2 * D;
+      const std::uint32_t bmin = key[j];
+      const double bmax = ( bk[2 * axis + 1] - gmin ) * fac;
+      if ( bmax < amin ) continue;
+      if ( bmin > amax ) break;
+      if ( overlap( ak, bk, D ) )
+      {
+        if ( static_cast< std::uint64_t >( cnt ) < cap )
+        {
+          out[2 * cnt] = static_cast< std::uint32_t >( i );
+          out[2 * cnt + 1] = j;
+        }
+        ++cnt;
+      }
+    }
+  }
+  return cnt;
+}
+
 // Node count of the top-down tree (TreeTest.cpp:49-90 checks 2n - 1 for one element per leaf).
 std::int64_t orc_tree_node_count(const double *s, const double *c, std::uint64_t n, int K)
 {

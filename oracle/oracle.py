@@ -46,6 +46,8 @@ def _load():
         "orc_pairs_tree": (I64, [P, P, U64, P, P, U64, I32, P, U64]),
         "orc_self_pairs_tree": (I64, [P, P, U64, I32, P, U64]),
         "orc_tree_node_count": (I64, [P, P, U64, I32]),
+        "orc_max_variant_axis": (I32, [P, U64, P, U64]),
+        "orc_sort_and_sweep": (I64, [P, U64, P, U64, I32, I32, P, U64]),
         "orc_pipeline": (I64, [P, U64, P, U64, U32, I32, D, I32, P]),
         "orc_max_threads": (I32, []),
     }
@@ -163,6 +165,21 @@ def _pairs_call(fn, args, cap_hint):
         if cnt <= cap:
             return out[:cnt]
         cap = cnt
+
+
+def max_variant_axis(ca, cb):
+    """The sweep axis of sort-and-sweep: the cardinal axis of largest centroid variance over A and B."""
+    ca = _c(ca, np.float64)
+    cb = _c(cb, np.float64)
+    return int(lib.orc_max_variant_axis(ca.ctypes.data, ca.shape[0], cb.ctypes.data, cb.shape[0]))
+
+
+def sort_and_sweep(sa, sb, k, axis):
+    """Pairs (index into A, index into B) of the reference's sort-and-sweep over two element slab sets."""
+    sa = _c(sa, np.float64)
+    sb = _c(sb, np.float64)
+    return _pairs_call(lib.orc_sort_and_sweep, (sa.ctypes.data, sa.shape[0], sb.ctypes.data, sb.shape[0], k, axis),
+                       4 * (sa.shape[0] + sb.shape[0]))
 
 
 def pairs_brute(sa, sb, k):
