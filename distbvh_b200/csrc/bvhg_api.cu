@@ -189,7 +189,7 @@ struct bvhg_ctx
   cudaEvent_t fork_evt = nullptr;
   std::string err;
   // sort-and-sweep scratch
-  dev_buf sw_keys, sw_vals, sw_rows, sw_hist, sw_status, sw_sc, sw_params, sw_partial;
+  dev_buf sw_keys, sw_vals, sw_rows, sw_srows, sw_sbmax, sw_hist, sw_status, sw_sc, sw_params, sw_partial;
   // pairs
   dev_buf pairs, pairs2, pairs_out, pscal;
   uint64_t pair_cap = 0, pair2_cap = 0;
@@ -1218,6 +1218,8 @@ bvhg_status bvhg_sort_and_sweep(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, int
   BVHG_CUDA( ctx, ctx->sw_keys.reserve( 2 * nb4 * 8 ) );
   BVHG_CUDA( ctx, ctx->sw_vals.reserve( 2 * nb4 * 4 ) );
   BVHG_CUDA( ctx, ctx->sw_rows.reserve( nb * K * 8 ) );
+  BVHG_CUDA( ctx, ctx->sw_srows.reserve( nb * K * 8 ) );
+  BVHG_CUDA( ctx, ctx->sw_sbmax.reserve( nb * 8 ) );
   BVHG_CUDA( ctx, ctx->sw_hist.reserve( 4 * 256 * 4 ) );
   BVHG_CUDA( ctx, ctx->sw_status.reserve( status_words * 4 ) );
   BVHG_CUDA( ctx, ctx->sw_sc.reserve( sizeof( obj_scalars ) ) );
@@ -1257,6 +1259,9 @@ bvhg_status bvhg_sort_and_sweep(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, int
   x.hist = ctx->sw_hist.as< uint32_t >();
   x.skeys = k0;  // four passes: k0 -> k1 -> k0 -> k1 -> k0
   x.svals = v0;
+  x.srows = ctx->sw_srows.as< double >();
+  x.sbmax = ctx->sw_sbmax.as< double >();
+  x.aperm = a.sorted_vals();
   x.sc = ssc;
   x.ps = ps;
   x.s = s;

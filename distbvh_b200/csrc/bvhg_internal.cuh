@@ -123,6 +123,9 @@ struct sweep_launch
   uint32_t *hist;                                   // 4 * 256: byte histograms of the keys
   const uint64_t *skeys;                            // sorted keys
   const uint32_t *svals;                            // B's element indices in key order
+  double *srows;                                    // nb * K doubles: B's slab rows in key order
+  double *sbmax;                                    // nb: B's scaled maxima on the axis in key order
+  const uint32_t *aperm;                            // A's elements in Morton order (its build's permutation)
   const obj_scalars *sc;                            // scalars of the keys' sort (error word)
   uint2 *pairs;
   uint64_t cap;

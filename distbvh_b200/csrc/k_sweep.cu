@@ -163,6 +163,27 @@ __global__ void __launch_bounds__( kSweepThreads ) k_sweep_keys(const double *__
   }
 }
 
+// B in key order: its slab rows and its scaled maxima on the axis (the sweeps read both sequentially).
+template< int K >
+__global__ void __launch_bounds__( kSweepThreads ) k_sweep_gather(const double *__restrict__ rows,
+                                                                  const uint32_t *__restrict__ svals, uint64_t n,
+                                                                  const sweep_params *__restrict__ pp,
+                                                                  double *__restrict__ srows,
+                                                                  double *__restrict__ sbmax)
+{
+  constexpr int C = K;  // 2 D values per row
+  const sweep_params p = *pp;
+  for ( uint64_t k = static_cast< uint64_t >( blockIdx.x ) * kSweepThreads + threadIdx.x; k < n * C;
+        k += static_cast< uint64_t >( gridDim.x ) * kSweepThreads )
+  {
+    const uint64_t j = k / C;
+    const int c = static_cast< int >( k - j * C );
+    const double v = __ldg( rows + static_cast< uint64_t >( __ldg( svals + j ) ) * C + c );
+    srows[k] = v;
+    if ( c == 2 * p.axis + 1 ) sbmax[j] = scaled( v, p );
+  }
+}
+
 // First index in [0, n) whose key is >= v (lower) or > v (upper).
 __device__ __forceinline__ uint64_t key_bound(const uint64_t *__restrict__ keys, uint64_t n, uint64_t v, bool upper)
 {
@@ -181,19 +202,23 @@ __device__ __forceinline__ uint64_t key_bound(const uint64_t *__restrict__ keys,
 template< int K, int VT >
 __global__ void __launch_bounds__( kSweepThreads ) k_sweep(const double *__restrict__ verts, uint32_t Vrt, uint64_t na,
                                                            double eps, const sweep_params *__restrict__ pp,
+                                                           const uint32_t *__restrict__ aperm,
                                                            const uint64_t *__restrict__ skeys,
                                                            const uint32_t *__restrict__ svals,
-                                                           const double *__restrict__ rows, uint64_t nb,
+                                                           const double *__restrict__ srows,
+                                                           const double *__restrict__ sbmax, uint64_t nb,
                                                            const obj_scalars *__restrict__ ssc, uint2 *__restrict__ pairs,
                                                            uint64_t cap, pair_scalars *__restrict__ ps)
 {
   constexpr int D = K / 2;
   if ( *reinterpret_cast< const volatile int * >( &ssc->error ) == kErrTimeout ) return;  // keys not sorted
-  const uint64_t i = static_cast< uint64_t >( blockIdx.x ) * kSweepThreads + threadIdx.x;
-  if ( i >= na ) return;
+  const uint64_t t = static_cast< uint64_t >( blockIdx.x ) * kSweepThreads + threadIdx.x;
+  if ( t >= na ) return;
+  // A in its Morton order: the lanes of a warp are neighbours in space and sweep nearly the same key window
+  const uint32_t i = __ldg( aperm + t );
   const sweep_params p = *pp;
   double lo[D], hi[D];
-  leaf_slabs< K, double, VT >( verts, Vrt, static_cast< uint32_t >( i ), eps, 0.f, lo, hi );
+  leaf_slabs< K, double, VT >( verts, Vrt, i, eps, 0.f, lo, hi );
   const double mn = p.axis == 0 ? lo[0] : ( p.axis == 1 ? lo[1] : lo[2] );
   const double mx = p.axis == 0 ? hi[0] : ( p.axis == 1 ? hi[1] : hi[2] );
   const uint32_t amin = key32( scaled( mn, p ) );
@@ -206,10 +231,8 @@ __global__ void __launch_bounds__( kSweepThreads ) k_sweep(const double *__restr
   const double amin_d = static_cast< double >( amin );
   for ( uint64_t j = j0; j < j1; ++j )
   {
-    const uint32_t ib = __ldg( svals + j );
-    const double *row = rows + static_cast< uint64_t >( ib ) * 2 * D;
-    const double bmax = p.axis == 0 ? __ldg( row + 1 ) : ( p.axis == 1 ? __ldg( row + 3 ) : __ldg( row + 5 ) );
-    if ( scaled( bmax, p ) < amin_d ) continue;
+    if ( __ldg( sbmax + j ) < amin_d ) continue;
+    const double *row = srows + j * 2 * D;
     bool o = true;
 #pragma unroll
     for ( int a = 0; a < D; ++a )
@@ -220,7 +243,7 @@ __global__ void __launch_bounds__( kSweepThreads ) k_sweep(const double *__restr
     if ( o )
     {
       const unsigned long long pos = atomicAdd( &ps->count, 1ull );
-      if ( pos < cap ) pairs[pos] = make_uint2( static_cast< uint32_t >( i ), ib );
+      if ( pos < cap ) pairs[pos] = make_uint2( i, __ldg( svals + j ) );
     }
   }
 }
@@ -236,8 +259,12 @@ void sweep_kernels(const sweep_launch &x, cudaError_t &e, bool keys_phase)
                                                              static_cast< sweep_params * >( x.params ) );
   } else {
     const unsigned grid = static_cast< unsigned >( ( x.na + kSweepThreads - 1 ) / kSweepThreads );
-    k_sweep< K, VT ><<< grid, kSweepThreads, 0, x.s >>>( x.averts, x.aV, x.na, x.eps, pp, x.skeys, x.svals, x.rows,
-                                                        x.nb, x.sc, x.pairs, x.cap, x.ps );
+    const unsigned ggrid = static_cast< unsigned >( device_sm_count() ) * 8;
+    k_sweep_gather< K ><<< ggrid, kSweepThreads, 0, x.s >>>( x.rows, x.svals, x.nb, pp, x.srows, x.sbmax );
+    e = cudaGetLastError();
+    if ( e != cudaSuccess ) return;
+    k_sweep< K, VT ><<< grid, kSweepThreads, 0, x.s >>>( x.averts, x.aV, x.na, x.eps, pp, x.aperm, x.skeys, x.svals,
+                                                        x.srows, x.sbmax, x.nb, x.sc, x.pairs, x.cap, x.ps );
   }
   e = cudaGetLastError();
 }
