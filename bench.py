@@ -209,9 +209,10 @@ def run_gpu(args, world, rank, local):
         return cnt
 
     def step_host(ctx, oa, ob):
+        # the sphere's build runs on its own stream while the plate's vertices cross PCIe on the context stream
         ctx.set_elements(oa, h_a.numpy(), mem=bvhg.MEM_HOST)
-        ctx.set_elements(ob, h_b.numpy(), mem=bvhg.MEM_HOST)
         ctx.build(oa)
+        ctx.set_elements(ob, h_b.numpy(), mem=bvhg.MEM_HOST)
         ctx.build(ob)
         st, cnt = ctx.broadphase_raw(oa, ob, h_out.data_ptr(), cap, bvhg.MEM_HOST)
         if st != 0:
