@@ -164,6 +164,13 @@ def peaks():
 LEAF = 8
 
 
+# Refit (k_refit, one thread per bucket climbing the stored parent links): read the bucket box 2 D S + parent 4;
+# per internal node (one per bucket) write both children's sides 4 D S, read the sibling's side 2 D S, exchange and
+# parent words 8; per element (buckets of 8):                                                  = (8DS + 12) / 8
+def refit_bytes(D, S):
+    return (8 * D * S + 12) / LEAF
+
+
 def stage_bytes(D, S, passes):
     return {"bounds": 96, "keys": 32, "sort": 24 * passes, "fixup": 24,
             "slabs": 76 + 2 * D * S * (1 / LEAF + 1 / 32),
@@ -278,6 +285,12 @@ def run_gpu(args, world, rank, local):
     st_ms, st_launch = ctxt.stage_times()
     st_ms = {k: v / reps for k, v in st_ms.items()}
     st_launch = {k: v // reps for k, v in st_launch.items()}
+    # refit (same topology, vertices re-read): element slabs, then the bottom-up refit of every internal node
+    for _ in range(reps):
+        ctxt.build(at, bvhg.REFIT)
+        ctxt.build(bt, bvhg.REFIT)
+    rf_ms, _ = ctxt.stage_times()
+    rf_ms = {k: v / reps for k, v in rf_ms.items() if v > 0}
     passes = st_launch["sort"] // 2
     per_elem = stage_bytes(K // 2, 8, passes)
     stage_bw = {}
@@ -314,6 +327,9 @@ def run_gpu(args, world, rank, local):
                         "speedup_vs_fp64": ms64 / ms32,
                         "false_positive_rate": (cand32 - pairs32) / cand32 if cand32 else 0.0},
         "stages_ms": st_ms, "stage_gbs": stage_bw,
+        "refit": {"ms": sum(rf_ms.values()), "stages_ms": rf_ms,
+                  "slabs_gbs": prims * per_elem["slabs"] / (rf_ms.get("slabs", float("inf")) * 1e-3) / 1e9,
+                  "refit_gbs": prims * refit_bytes(K // 2, 8) / (rf_ms.get("build", float("inf")) * 1e-3) / 1e9},
         "roofline": roofline,
         "gpu_launches": int(launches),
         "e2e": e2e,

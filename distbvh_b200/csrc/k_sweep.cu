@@ -198,7 +198,9 @@ __device__ __forceinline__ uint64_t key_bound(const uint64_t *__restrict__ keys,
   return lo;
 }
 
-// A: one thread per element, its sweep over B's sorted keys.
+// A: one warp per element (A in its Morton order, warps grid-stride over it). All lanes form the element's slabs
+// and window (the same values; the loads are broadcasts), then scan the window 32 keys at a time: lane l tests
+// key j0 + l + 32 k, so every load of the scaled maxima and of the rows is coalesced across the warp.
 template< int K, int VT >
 __global__ void __launch_bounds__( kSweepThreads ) k_sweep(const double *__restrict__ verts, uint32_t Vrt, uint64_t na,
                                                            double eps, const sweep_params *__restrict__ pp,
@@ -212,38 +214,40 @@ __global__ void __launch_bounds__( kSweepThreads ) k_sweep(const double *__restr
 {
   constexpr int D = K / 2;
   if ( *reinterpret_cast< const volatile int * >( &ssc->error ) == kErrTimeout ) return;  // keys not sorted
-  const uint64_t t = static_cast< uint64_t >( blockIdx.x ) * kSweepThreads + threadIdx.x;
-  if ( t >= na ) return;
-  // A in its Morton order: the lanes of a warp are neighbours in space and sweep nearly the same key window
-  const uint32_t i = __ldg( aperm + t );
   const sweep_params p = *pp;
-  double lo[D], hi[D];
-  leaf_slabs< K, double, VT >( verts, Vrt, i, eps, 0.f, lo, hi );
-  const double mn = p.axis == 0 ? lo[0] : ( p.axis == 1 ? lo[1] : lo[2] );
-  const double mx = p.axis == 0 ? hi[0] : ( p.axis == 1 ? hi[1] : hi[2] );
-  const uint32_t amin = key32( scaled( mn, p ) );
-  const uint32_t amax = key32( scaled( mx, p ) );
   const double W = ord_decode( p.wmax_enc );
   const uint64_t wq = W < 8589934592.0 ? static_cast< uint64_t >( ceil( W ) ) : 8589934592ull;  // >= every key span
-  const uint64_t start = amin > wq ? amin - wq : 0;
-  const uint64_t j0 = key_bound( skeys, nb, start, false );
-  const uint64_t j1 = key_bound( skeys, nb, amax, true );
-  const double amin_d = static_cast< double >( amin );
-  for ( uint64_t j = j0; j < j1; ++j )
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t nwarps = static_cast< uint64_t >( gridDim.x ) * ( kSweepThreads / 32 );
+  for ( uint64_t t = ( static_cast< uint64_t >( blockIdx.x ) * kSweepThreads + threadIdx.x ) >> 5; t < na; t += nwarps )
   {
-    if ( __ldg( sbmax + j ) < amin_d ) continue;
-    const double *row = srows + j * 2 * D;
-    bool o = true;
+    const uint32_t i = __ldg( aperm + t );
+    double lo[D], hi[D];
+    leaf_slabs< K, double, VT >( verts, Vrt, i, eps, 0.f, lo, hi );
+    const double mn = p.axis == 0 ? lo[0] : ( p.axis == 1 ? lo[1] : lo[2] );
+    const double mx = p.axis == 0 ? hi[0] : ( p.axis == 1 ? hi[1] : hi[2] );
+    const uint32_t amin = key32( scaled( mn, p ) );
+    const uint32_t amax = key32( scaled( mx, p ) );
+    const uint64_t start = amin > wq ? amin - wq : 0;
+    const uint64_t j0 = key_bound( skeys, nb, start, false );
+    const uint64_t j1 = key_bound( skeys, nb, amax, true );
+    const double amin_d = static_cast< double >( amin );
+    for ( uint64_t j = j0 + lane; j < j1; j += 32 )
+    {
+      if ( __ldg( sbmax + j ) < amin_d ) continue;
+      const double *row = srows + j * 2 * D;
+      bool o = true;
 #pragma unroll
-    for ( int a = 0; a < D; ++a )
-    {
-      if ( !o ) break;
-      o = lo[a] < __ldg( row + 2 * a + 1 ) && __ldg( row + 2 * a ) < hi[a];
-    }
-    if ( o )
-    {
-      const unsigned long long pos = atomicAdd( &ps->count, 1ull );
-      if ( pos < cap ) pairs[pos] = make_uint2( i, __ldg( svals + j ) );
+      for ( int a = 0; a < D; ++a )
+      {
+        if ( !o ) break;
+        o = lo[a] < __ldg( row + 2 * a + 1 ) && __ldg( row + 2 * a ) < hi[a];
+      }
+      if ( o )
+      {
+        const unsigned long long pos = atomicAdd( &ps->count, 1ull );
+        if ( pos < cap ) pairs[pos] = make_uint2( i, __ldg( svals + j ) );
+      }
     }
   }
 }
@@ -258,7 +262,10 @@ void sweep_kernels(const sweep_launch &x, cudaError_t &e, bool keys_phase)
     k_sweep_keys< K, VT ><<< grid, kSweepThreads, 0, x.s >>>( x.bverts, x.bV, x.nb, x.eps, pp, x.rows, x.keys, x.hist,
                                                              static_cast< sweep_params * >( x.params ) );
   } else {
-    const unsigned grid = static_cast< unsigned >( ( x.na + kSweepThreads - 1 ) / kSweepThreads );
+    // warps grid-stride over A: at most 16 resident blocks' worth per SM, never more warps than elements
+    const uint64_t want = ( x.na + kSweepThreads / 32 - 1 ) / ( kSweepThreads / 32 );
+    const uint64_t cap = static_cast< uint64_t >( device_sm_count() ) * 16;
+    const unsigned grid = static_cast< unsigned >( want < cap ? want : cap );
     const unsigned ggrid = static_cast< unsigned >( device_sm_count() ) * 8;
     k_sweep_gather< K ><<< ggrid, kSweepThreads, 0, x.s >>>( x.rows, x.svals, x.nb, pp, x.srows, x.sbmax );
     e = cudaGetLastError();
