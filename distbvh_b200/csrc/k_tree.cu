@@ -579,16 +579,22 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(int n, const T *__res
     hi[a] = bucket_box[( static_cast< size_t >( b ) * D + a ) * 2 + 1];
   }
   const int root = sc->root;
-  int slot = b;
+  int ps = __ldg( parent + b );
   while ( true )
   {
-    const int ps = __ldg( parent + slot );
     const int par = ps >> 1, side = ps & 1;
+    // the next level's parent link is read before this level's exchange (it does not depend on it)
+    const int next = par == root ? 0 : __ldg( parent + m + par );
     T *pb = node_box + static_cast< size_t >( par ) * D * 4;
 #pragma unroll
     for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
-    const int other = atomic_exch_acq_rel( exch + par, 1 );
-    if ( other < 0 ) return;
+    // a sibling that already arrived is seen with one acquire load (see k_build_climb)
+    int other = ld_acquire( exch + par );
+    if ( other < 0 )
+    {
+      other = atomic_exch_acq_rel( exch + par, 1 );
+      if ( other < 0 ) return;
+    }
 #pragma unroll
     for ( int a = 0; a < D; ++a )
     {
@@ -602,7 +608,7 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(int n, const T *__res
       store_root( sc, lo, hi );
       return;
     }
-    slot = m + par;
+    ps = next;
   }
 }
 
