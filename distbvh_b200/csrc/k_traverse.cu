@@ -2,17 +2,19 @@
 //
 // The reference finds pairs with a 4-way simultaneous recursion over two trees (get_overlapping_indices,
 // src/bvh/collision_query.hpp:293-329) or a per-entity descent (query_tree, collision_query.hpp:166-213), both
-// pruning on the strict all-slab overlap (kdop.hpp:120-125, 538-549). Here each thread takes one leaf of the query
-// object, in Morton order so that a warp's queries are spatially coherent, and descends the other object's tree
-// with an explicit stack: both children of a node are tested from one 32-byte (FP64) / 16-byte (FP32) sector per
-// slab, with early exit on the first separating slab. At a leaf bucket the query is tested against each of the
-// bucket's elements. Overlaps are emitted as (query element, tree element) local indices through a global atomic
-// counter; pairs beyond capacity are counted but not stored, so the host can grow the buffer and retry.
+// pruning on the strict all-slab overlap (kdop.hpp:120-125, 538-549). Here a warp walks the other object's tree
+// for a packet of 32 consecutive query ranks (Morton order: spatially coherent), one query per lane, with a stack
+// of (node, lane mask) entries: both children of a node are tested from one row holding their slabs (one 32-byte
+// FP64 / 16-byte FP32 sector per slab, loaded a chunk of slabs at a time), and a child is entered with the mask of
+// the lanes that overlap it. At a leaf bucket each lane of the mask tests its query against the bucket's
+// elements. Overlaps are emitted as (query element, tree element) local indices through one warp-aggregated
+// reservation per bucket visit; pairs beyond capacity are counted but not stored, so the host can grow the buffer
+// and retry. In sparse contact the grid is persistent and culls 32 packets per warp step against the target root
+// before walking the survivors; in dense contact it is one warp per packet.
 //
-// Self-collision (self_collision_set, collision_query.hpp:331-368): the query leaf of rank i only visits
-// subtrees holding ranks > i (internal node k splits its bucket range [l, r] into [l, k] and [k + 1, r]) and
-// tests only bucket elements of rank > i, so every unordered pair is found once and no element is paired with
-// itself.
+// Self-collision (self_collision_set, collision_query.hpp:331-368): the query of rank i only visits subtrees
+// holding ranks > i (internal node k splits its bucket range [l, r] into [l, k] and [k + 1, r]) and tests only
+// bucket elements of rank > i, so every unordered pair is found once and no element is paired with itself.
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
 

@@ -10,8 +10,8 @@
 //
 // No thread ever waits. Nodes whose two children close inside a block of 128 buckets are merged in shared memory
 // (warp rounds, then block rounds) and written out coalesced; the rest use a global exchange slot per node: the
-// first arrival's slab stores are ordered before its acq_rel atomic exchange, and the second arrival reads them
-// through L2 after its own.
+// first arrival's slab stores are ordered before its acq_rel atomic exchange, and the second arrival, which sees
+// the slot taken with an acquire load (or learns it from its own exchange), reads them through L2 after it.
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
 
