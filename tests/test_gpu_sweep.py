@@ -119,3 +119,20 @@ def test_device_output_overflow_and_errors():
         # the context is still usable after the error returns
         got, _ = ctx.sort_and_sweep(oa, ob, 0)
         assert np.array_equal(orc.canonical(got), want)
+
+
+@pytest.mark.parametrize("k", [6, 18, 26])
+def test_reference_known_answers(k):
+    """tests/KokkosTest.cpp:37-140: max_variant_axis picks the grid's long axis; sort_and_sweep_local of a
+    12-element grid against one element finds 12 pairs in both roles."""
+    from tests.grids import element_grid
+    b, gb = element_grid(1, 1, 1, 0)
+    with bvhg.Context(k=k) as ctx:
+        for dims, axis in (((12, 1, 1), 0), ((1, 12, 1), 1), ((1, 1, 12), 2)):
+            a, ga = element_grid(*dims, 0)
+            oa, ob = build_pair(ctx, a, b, ga, gb)
+            got, used = ctx.sort_and_sweep(oa, ob, -1)
+            assert used == axis
+            assert got.shape[0] == 12 and set(got[:, 1].tolist()) == {0} and sorted(got[:, 0].tolist()) == list(range(12))
+            got, _ = ctx.sort_and_sweep(ob, oa, 0)
+            assert got.shape[0] == 12 and set(got[:, 0].tolist()) == {0}

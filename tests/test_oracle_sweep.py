@@ -36,3 +36,30 @@ def test_max_variant_axis_picks_the_long_direction():
         ca = rng.random((500, 3)) * scale
         cb = rng.random((400, 3)) * scale
         assert orc.max_variant_axis(ca, cb) == axis
+
+
+# Known answers of the reference's own tests (tests/KokkosTest.cpp:37-140): the axis of a 12-element grid along x,
+# y or z against one element, and 12 pairs from sort_and_sweep_local in both roles.
+def _grids():
+    from tests.grids import element_grid
+    return element_grid
+
+
+@pytest.mark.parametrize("dims,axis", [((12, 1, 1), 0), ((1, 12, 1), 1), ((1, 1, 12), 2)])
+def test_reference_max_variant_axis_cases(dims, axis):
+    element_grid = _grids()
+    a, _ = element_grid(*dims)
+    b, _ = element_grid(1, 1, 1)
+    assert orc.max_variant_axis(orc.centroids(a), orc.centroids(b)) == axis
+
+
+@pytest.mark.parametrize("k", [6, 18, 26])
+def test_reference_sort_and_sweep_cases(k):
+    element_grid = _grids()
+    a, _ = element_grid(12, 1, 1)
+    b, _ = element_grid(1, 1, 1)
+    sa, sb = orc.kdops(a, k), orc.kdops(b, k)
+    p = orc.sort_and_sweep(sa, sb, k, 0)
+    assert p.shape[0] == 12 and set(p[:, 1].tolist()) == {0} and sorted(p[:, 0].tolist()) == list(range(12))
+    q = orc.sort_and_sweep(sb, sa, k, 0)  # "x-axis flipped"
+    assert q.shape[0] == 12 and set(q[:, 0].tolist()) == {0}
