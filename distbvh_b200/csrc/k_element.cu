@@ -137,7 +137,7 @@ __global__ void __launch_bounds__( kElemThreads ) k_centroid_bounds(const double
 // partial tile through plain loads. Every wait on a copy is bounded: past spin_limit polls the block raises the
 // object's error word, waits (bounded) for its copies in flight and stops.
 template< int K, int VT >
-__global__ void __launch_bounds__( kElemThreads, VT == 8 ? 2 : 4 ) k_centroid_bounds_tma(const double *__restrict__ verts, uint64_t n,
+__global__ void __launch_bounds__( kElemThreads, VT == 8 ? 2 : 3 ) k_centroid_bounds_tma(const double *__restrict__ verts, uint64_t n,
                                                                       double eps, double *__restrict__ cx,
                                                                       double *__restrict__ cy, double *__restrict__ cz,
                                                                       obj_scalars *__restrict__ sc, uint32_t spin_limit)
