@@ -65,6 +65,7 @@ struct object
   bool has_data = false;
   bool built = false;  // slabs current for the present vertex data
   bool topo = false;   // a rebuild's topology exists for the present n and V (refit allowed)
+  bool fresh = false;  // a rebuild ran since the last set_elements: bounds and centroids match the vertices
   int sort_result_alt = 0;  // sorted keys/vals ended in the *_alt buffers
   // Dense contact (a broadphase of this object found pairs for a sizable fraction of the elements): its next builds
   // store every element's slabs, which its traversals then only read; in sparse contact they compute the few they
@@ -389,6 +390,7 @@ bvhg_status do_build(bvhg_ctx *ctx, object &o, int mode)
   if ( n == 0 )
   {
     o.built = true;
+    o.fresh = true;
     return BVHG_OK;
   }
   cudaStream_t s = nullptr;
@@ -439,6 +441,7 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
       st.launched();
     }
     o.built = true;
+    o.fresh = false;  // a refit keeps the last rebuild's bounds and centroids
     return BVHG_OK;
   }
   const int bits = ctx->cfg.sort_digit_bits;
@@ -523,6 +526,7 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
   }
   o.built = true;
   o.topo = true;
+  o.fresh = true;
   return BVHG_OK;
 }
 
@@ -1021,6 +1025,7 @@ bvhg_status bvhg_set_elements(bvhg_ctx *ctx, int32_t obj, const double *xyz, uin
   o.n = n;
   o.V = V;
   o.built = false;
+  o.fresh = false;
   o.has_data = true;
   if ( n == 0 )
   {
@@ -1203,6 +1208,8 @@ bvhg_status bvhg_sort_and_sweep(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, int
   object &a = *ctx->objs[obj_a];
   object &b = *ctx->objs[obj_b];
   if ( !a.built || !b.built ) return fail( ctx, BVHG_ERR_STATE, "sort-and-sweep before build" );
+  // the global range and the axis come from the objects' bounds and centroids, which only a rebuild computes
+  if ( !a.fresh || !b.fresh ) return fail( ctx, BVHG_ERR_STATE, "sort-and-sweep needs a rebuild (not a refit) since set_elements" );
   cudaSetDevice( ctx->cfg.device );
   join_object( ctx, a );
   join_object( ctx, b );

@@ -146,7 +146,9 @@ BVHG_API bvhg_status bvhg_self_collision(bvhg_ctx *ctx, int32_t obj, uint64_t *p
  * (max_variant_axis, kokkos.hpp:125-160); *axis_used (may be NULL) receives the axis swept. The pair set is the
  * exact S(A, B), the same as bvhg_broadphase's, for any axis (pairs as there: gid in obj_a, gid in obj_b); its
  * cost grows with the elements of B whose extents on the axis meet each element of A, so it suits patch-sized
- * objects. FP64 slabs in both precision forms. obj_a != obj_b. Blocks until the count is known. */
+ * objects. FP64 slabs in both precision forms. obj_a != obj_b. Both objects must have been rebuilt (BVHG_REBUILD)
+ * since their last bvhg_set_elements: the range and the axis come from a rebuild's bounds and centroids, which a
+ * refit does not recompute (BVHG_ERR_STATE otherwise). Blocks until the count is known. */
 BVHG_API bvhg_status bvhg_sort_and_sweep(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, int32_t axis, uint64_t *pairs,
                                          uint64_t capacity, uint64_t *count, int32_t *axis_used, int32_t mem);
 

@@ -119,6 +119,12 @@ def test_device_output_overflow_and_errors():
         # the context is still usable after the error returns
         got, _ = ctx.sort_and_sweep(oa, ob, 0)
         assert np.array_equal(orc.canonical(got), want)
+        # a refit keeps the last rebuild's bounds and centroids: the sweep needs a rebuild first
+        ctx.build(ob, bvhg.REFIT)
+        assert ctx.sort_and_sweep_raw(oa, ob, -1, None, 0, bvhg.MEM_HOST)[0] == bvhg._abi.ERR_STATE
+        ctx.build(ob)
+        got, _ = ctx.sort_and_sweep(oa, ob, -1)
+        assert np.array_equal(orc.canonical(got), want)
 
 
 @pytest.mark.parametrize("k", [6, 18, 26])
