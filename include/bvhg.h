@@ -172,7 +172,9 @@ BVHG_API bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const 
                                         int32_t mode, uint32_t *lanes, double *ms);
 
 /* Parity probes (host buffers). sorted_keys[r] and perm[r] (original index of rank r) may be NULL; min3/inv3 are
- * the Morton bounds (3 doubles each, may be NULL). */
+ * the Morton bounds (3 doubles each, may be NULL). Keys, permutation, bounds and centroids are those of the last
+ * rebuild: a refit keeps the order and does not recompute them. The slab probes compute from the present
+ * vertices. */
 BVHG_API bvhg_status bvhg_get_morton(bvhg_ctx *ctx, int32_t obj, uint64_t *sorted_keys, uint32_t *perm, double *min3,
                             double *inv3);
 /* Per-element slabs in original element order, slabs[(i * K/2 + a) * 2 + {0 min, 1 max}]. FP64 form only. */
