@@ -37,6 +37,8 @@ class Ref:
         L.ref_self_pairs.restype = _U
         L.ref_radix_sort_u64.argtypes = [_P, _U, _P, _P]
         L.ref_cluster.argtypes = [_P, _U, _I, _U, _P, _P]
+        L.ref_sort_and_sweep.argtypes = [_P, _U, _P, _U, _I, _D, _I, _P, _P, _U]
+        L.ref_sort_and_sweep.restype = _U
         self.lib = L
         self.tree_k = L.ref_tree_k()
         assert self.tree_k == tree_k
@@ -94,6 +96,15 @@ class Ref:
         perm = np.zeros(keys.shape[0], dtype=np.uint64)
         self.lib.ref_radix_sort_u64(keys.ctypes.data, keys.shape[0], out.ctypes.data, perm.ctypes.data)
         return out, perm
+
+    def sort_and_sweep(self, a, b, eps=0.0, axis=-1, cap=1 << 20):
+        """sort_and_sweep_local with each set as one patch: (count, pairs in the functor's order, axis swept)."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        used = ctypes.c_int(-1)
+        cnt, pairs = self._pairs(self.lib.ref_sort_and_sweep, a.ctypes.data, a.shape[0], b.ctypes.data, b.shape[0],
+                                 a.shape[1], eps, axis, ctypes.byref(used), cap=cap)
+        return cnt, pairs, used.value
 
     def cluster(self, xyz, clusters):
         """morton_cluster: (element order, clusters - 1 split positions)."""

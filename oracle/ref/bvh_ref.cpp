@@ -11,6 +11,7 @@
 #include <bvh/contact_entity.hpp>
 #include <bvh/hash.hpp>
 #include <bvh/kdop.hpp>
+#include <bvh/narrowphase/kokkos.hpp>
 #include <bvh/snapshot.hpp>
 #include <bvh/split/cluster.hpp>
 #include <bvh/tree_build.hpp>
@@ -232,5 +233,31 @@ void ref_cluster(const double *xyz, uint64_t n, int V, uint64_t clusters, uint64
   mc( ev, idx, sp );
   for ( uint64_t i = 0; i < n; ++i ) order[i] = idx( i );
   for ( uint64_t k = 0; k + 1 < clusters; ++k ) splits[k] = sp( k );
+}
+
+// sort_and_sweep_local (src/bvh/narrowphase/kokkos.hpp:164-248) with each element set as one patch (the patch's
+// k-DOP is the union of its elements', patch.hpp), axis = max_variant_axis (kokkos.hpp:125-160) when axis < 0.
+// Returns the pair count; the first cap pairs (index in A, index in B) in the order the functor sees them.
+uint64_t ref_sort_and_sweep(const double *xa, uint64_t na, const double *xb, uint64_t nb, int V, double eps,
+                            int axis, int *axis_used, uint64_t *out, uint64_t cap)
+{
+  auto a = make_elements( xa, na, V, eps );
+  auto b = make_elements( xb, nb, V, eps );
+  using elem_view = Kokkos::View< ref_element *, Kokkos::HostSpace, Kokkos::MemoryTraits< Kokkos::Unmanaged > >;
+  elem_view va( a.data(), a.size() ), vb( b.data(), b.size() );
+  bvh::patch<> pa( 0, bvh::span< const ref_element >( a.data(), a.size() ) );
+  bvh::patch<> pb( 1, bvh::span< const ref_element >( b.data(), b.size() ) );
+  const int ax = axis >= 0 ? axis : bvh::max_variant_axis( va, vb );
+  if ( axis_used ) *axis_used = ax;
+  uint64_t cnt = 0;
+  bvh::sort_and_sweep_local( pa, va, pb, vb, ax, [&]( const ref_element &e, const ref_element &f ) {
+    if ( cnt < cap )
+    {
+      out[2 * cnt] = e.gid;
+      out[2 * cnt + 1] = f.gid;
+    }
+    ++cnt;
+  } );
+  return cnt;
 }
 }

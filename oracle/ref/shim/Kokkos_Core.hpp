@@ -87,6 +87,30 @@ private:
   std::size_t m_size = 0;
 };
 
+// Two-dimensional views with a static second extent (DataType = T*[N]): element (i, j) at i * N + j.
+template< class T, std::size_t N, class... Props >
+class View< T *[N], Props... >
+{
+public:
+  using value_type = T;
+  using size_type = std::size_t;
+
+  View() = default;
+  explicit View(const std::string &, std::size_t n = 0)
+      : m_store( std::make_shared< std::vector< std::remove_const_t< T > > >( n * N ) ), m_rows( n )
+  {}
+  T &operator()(std::size_t i, std::size_t j) const { return ( *m_store )[i * N + j]; }
+  T *data() const { return m_store ? m_store->data() : nullptr; }
+  std::size_t size() const { return m_rows * N; }
+  std::size_t extent(int d) const { return d == 0 ? m_rows : N; }
+
+private:
+  std::shared_ptr< std::vector< std::remove_const_t< T > > > m_store;
+  std::size_t m_rows = 0;
+};
+
+inline void fence() {}
+
 template< class V >
 void resize(V &v, std::size_t n)
 {
@@ -174,11 +198,22 @@ void parallel_reduce(std::size_t n, const F &f, R &&result)
   using RR = std::remove_cv_t< std::remove_reference_t< R > >;
   if constexpr ( detail::has_value_type< F >::value )
   {
-    typename F::value_type acc;
-    f.init( acc );
-    for ( std::size_t i = 0; i < n; ++i ) f( i, acc );
-    if constexpr ( detail::is_view< RR >::value ) result() = acc;
-    else result = acc;
+    using VT = typename F::value_type;
+    if constexpr ( std::is_array_v< VT > && std::extent_v< VT > == 0 )
+    {
+      // array reducer (value_type = T[], F::value_count entries), result an array of as many
+      F g = f;  // Kokkos runs a copy of the functor (its init need not be const)
+      std::vector< std::remove_extent_t< VT > > acc( F::value_count );
+      g.init( acc.data() );
+      for ( std::size_t i = 0; i < n; ++i ) g( i, acc.data() );
+      for ( std::size_t k = 0; k < F::value_count; ++k ) result[k] = acc[k];
+    } else {
+      VT acc;
+      f.init( acc );
+      for ( std::size_t i = 0; i < n; ++i ) f( i, acc );
+      if constexpr ( detail::is_view< RR >::value ) result() = acc;
+      else result = acc;
+    }
   } else {
     RR acc{};
     for ( std::size_t i = 0; i < n; ++i ) f( static_cast< int >( i ), acc );

@@ -10,7 +10,8 @@ the shape of the reference's two-plate contact case, each with inflation 0 and 0
 case and object: vertices; k-DOP slabs for K = 6, 18, 26 (kdop_base::from_vertices; 18 through dop_18's
 normals); centroids; Morton bounds and 64-bit codes (compute_bounds + morton); pair counts of
 potential_collision_set over top-down trees of dop_26 and of dop_6; self_collision_set pairs of object a for
-both; the 18-DOP pair set by brute force with the reference's overlap.
+both; the 18-DOP pair set by brute force with the reference's overlap; the pairs and axis of sort_and_sweep_local
+with max_variant_axis (narrowphase/kokkos.hpp) over dop_26 and dop_6 k-DOPs (soups only).
 
 Run from the repository root: python tests/golden/make_golden.py
 """
@@ -71,6 +72,11 @@ def main():
             out[f"{name}/tree_count{tk}"] = np.int64(r.tree_pairs(a, b, eps)[0])
             out[f"{name}/self{tk}"] = r.self_pairs(a, eps)[1]
         out[f"{name}/pairs18"] = r26.brute_pairs18(a, b, eps)[1]
+        if name.startswith("soup"):
+            for tk, r in ((26, r26), (6, r6)):
+                _, pairs, axis = r.sort_and_sweep(a, b, eps, -1)
+                out[f"{name}/sweep{tk}/pairs"] = np.unique(pairs, axis=0)
+                out[f"{name}/sweep{tk}/axis"] = np.int64(axis)
     out["cases"] = np.array(names)
     # Morton clustering into patches (morton_cluster) for the collision_world mirror, and the 1-bit radix sort
     cl = meshes.random_soup(700, 3, seed=4242, size=0.03)

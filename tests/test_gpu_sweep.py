@@ -142,3 +142,24 @@ def test_reference_known_answers(k):
             assert got.shape[0] == 12 and set(got[:, 1].tolist()) == {0} and sorted(got[:, 0].tolist()) == list(range(12))
             got, _ = ctx.sort_and_sweep(ob, oa, 0)
             assert got.shape[0] == 12 and set(got[:, 0].tolist()) == {0}
+
+
+def test_gpu_sweep_matches_the_reference_vectors():
+    """bvhg_sort_and_sweep against the pairs and axis of the reference's own sort_and_sweep_local and
+    max_variant_axis (dop_26 and dop_6), stored in tests/golden/ref_vectors.npz."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_vectors.npz"))
+    checked = 0
+    for name in g["cases"]:
+        name = str(name)
+        if not name.startswith("soup"):
+            continue
+        a, b, eps = g[f"{name}/a"], g[f"{name}/b"], float(g[f"{name}/eps"])
+        for k in (26, 6):
+            with bvhg.Context(k=k, epsilon=eps) as ctx:
+                oa, ob = build_pair(ctx, a, b)
+                got, used = ctx.sort_and_sweep(oa, ob, -1)
+                assert used == int(g[f"{name}/sweep{k}/axis"])
+                assert np.array_equal(orc.canonical(got), orc.canonical(g[f"{name}/sweep{k}/pairs"])), (name, k)
+                checked += 1
+    assert checked == 12

@@ -262,3 +262,21 @@ def test_stable_sort_matches_the_reference_radix_sorter():
     perm = orc.stable_perm(keys)
     assert np.array_equal(perm.astype(np.uint64), GOLDEN["radix/perm"])
     assert np.array_equal(keys[perm], GOLDEN["radix/sorted"])
+
+
+def test_sort_and_sweep_matches_the_reference_vectors():
+    """The oracle's sort-and-sweep and axis choice against sort_and_sweep_local / max_variant_axis outputs of the
+    reference's own code (dop_26 and dop_6 builds) stored in the fixture."""
+    g = GOLDEN
+    checked = 0
+    for name in g["cases"]:
+        name = str(name)
+        if not name.startswith("soup"):
+            continue
+        for k in (26, 6):
+            axis = int(g[f"{name}/sweep{k}/axis"])
+            assert orc.max_variant_axis(g[f"{name}/a/centroids"], g[f"{name}/b/centroids"]) == axis
+            mine = orc.sort_and_sweep(g[f"{name}/a/kdops{k}"], g[f"{name}/b/kdops{k}"], k, axis).astype(np.int64)
+            assert np.array_equal(np.unique(mine, axis=0), g[f"{name}/sweep{k}/pairs"].astype(np.int64)), (name, k)
+            checked += 1
+    assert checked == 12

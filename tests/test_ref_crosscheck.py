@@ -73,3 +73,24 @@ def test_radix_sorter_and_cluster(refs):
     s, p = refs[26].radix_sort_u64(keys)
     assert np.array_equal(p.astype(np.int64), orc.stable_perm(keys).astype(np.int64))
     assert np.array_equal(s, np.sort(keys, kind="stable"))
+
+
+@pytest.mark.parametrize("V", [3, 4, 8])
+@pytest.mark.parametrize("eps", [0.0, 0.003])
+def test_sort_and_sweep_against_the_reference(refs, V, eps):
+    """The oracle's sort-and-sweep and axis choice against the reference's sort_and_sweep_local and
+    max_variant_axis (dop_26 and dop_6 builds): the same axis, the same emitted pairs on every axis."""
+    a = meshes.random_soup(900, V, seed=1300 + V, size=0.05)
+    b = meshes.random_soup(700, V, seed=1400 + V, size=0.05, stream=1)
+    for k, r in refs.items():
+        sa, sb = orc.kdops(a, k, eps), orc.kdops(b, k, eps)
+        cnt, pairs, axis = r.sort_and_sweep(a, b, eps, -1)
+        assert axis == orc.max_variant_axis(orc.centroids(a), orc.centroids(b))
+        assert cnt > 0
+        mine = orc.sort_and_sweep(sa, sb, k, axis).astype(np.int64)
+        assert np.array_equal(np.unique(pairs, axis=0), np.unique(mine, axis=0)), (k, axis)
+        for ax in (0, 1, 2):
+            cnt2, pairs2, used = r.sort_and_sweep(a, b, eps, ax)
+            assert used == ax
+            mine2 = orc.sort_and_sweep(sa, sb, k, ax).astype(np.int64)
+            assert np.array_equal(np.unique(pairs2, axis=0), np.unique(mine2, axis=0)), (k, ax)
