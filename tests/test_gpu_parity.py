@@ -414,7 +414,7 @@ def test_objects_with_different_vertex_counts(precision):
             objs[name] = ctx.object()
             ctx.set_elements(objs[name], x)
             ctx.build(objs[name])
-        for rep in range(2):  # the second round runs after the density decision of the first
+        for rep in range(2):  # the second pass runs after the density decision of the first
             for a, b in (("tri", "tet"), ("tet", "tri"), ("tri", "hex"), ("hex", "tet")):
                 xa, xb = {"tri": tri, "tet": tet, "hex": hexa}[a], {"tri": tri, "tet": tet, "hex": hexa}[b]
                 got = orc.canonical(ctx.broadphase(objs[a], objs[b]))
