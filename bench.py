@@ -35,7 +35,19 @@ os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 METRIC = "build+broadphase Mprims/s, FP32-filter vs FP64 plain on B200, same exact pair set"
 K = 18
 EPS = 0.0
-WORKLOAD = "sphere_plate: icosphere L9 (5,242,880 tris, r=0.5, penetration 0.01) + plate 2048x1024 quads (4,194,304 tris)"
+
+
+def workload_name(args):
+    tris = 20 * 4 ** args.level
+    return (f"sphere_plate: icosphere L{args.level} ({tris:,} tris, r=0.5, penetration 0.01) + plate "
+            f"{args.nx}x{args.ny} quads ({2 * args.nx * args.ny:,} tris)")
+
+
+def bench_config(args, world, elements, pairs):
+    """The config object of both arms' lines (the same keys and values for the same workload)."""
+    return {"workload": workload_name(args), "k": K, "epsilon": EPS, "elements": int(elements), "pairs": int(pairs),
+            "form": "plain FP64", "l2": "inputs 680 MB > L2 (126 MB)",
+            "parallelism": f"independent scene per rank x{world}"}
 
 
 def parse():
@@ -260,6 +272,7 @@ def run_gpu(args, world, rank, local):
     cand32 = ctx32.last_candidates()
     # identical exact pair sets (checked as sorted sets once, outside the timed regions)
     same = False
+    p64 = None
     if rank == 0:
         step_device(ctx64, a64, b64)
         p64 = d_out[:pairs64].cpu().numpy().copy()
@@ -319,9 +332,8 @@ def run_gpu(args, world, rank, local):
         "metric": METRIC, "value": prims * world / (ms64 * 1e-3) / 1e6, "unit": "Mprims/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded icosphere + plate)",
-        "config": {"workload": WORKLOAD, "k": K, "epsilon": EPS, "elements": prims, "pairs": int(pairs64),
-                   "form": "plain FP64", "sort_digit_bits": 8, "l2": "inputs 680 MB > L2 (126 MB)",
-                   "parallelism": f"independent scene per rank x{world}"},
+        "config": bench_config(args, world, prims, pairs64),
+        "sort_digit_bits": 8,
         "filter_fp32": {"ms_per_step": ms32, "value": prims * world / (ms32 * 1e-3) / 1e6, "pairs": int(pairs32),
                         "candidates": int(cand32), "same_pair_set": bool(same),
                         "speedup_vs_fp64": ms64 / ms32,
@@ -338,7 +350,7 @@ def run_gpu(args, world, rank, local):
     ctx64.close()
     ctx32.close()
     ctxt.close()
-    return result, sphere, plate
+    return result, sphere, plate, p64
 
 
 def run_precision(args, world, rank, local):
@@ -590,22 +602,24 @@ def run_timestep(args, world, rank, local):
     }
 
 
-def cpu_baseline_sample(sphere_level=8, nx=1024, ny=512, threads=0):
-    """The reference's algorithms on all host cores over a quarter-size sample of the same scene."""
+def cpu_baseline_full(sphere, plate, gpu_pairs, threads=0):
+    """The reference's algorithms on all host cores over the whole benchmark scene (one pass, about 4 s on 16
+    cores), with the pair list kept: it is both the CPU baseline and the oracle's pair set for the GPU's."""
     from oracle import oracle as orc
-    from distbvh_b200 import meshes
-    s, p = meshes.sphere_plate(sphere_level, nx, ny)
     t = time.perf_counter()
-    cnt, stages = orc.pipeline(s, p, K, EPS, threads)
+    cnt, stages, want = orc.pipeline(sphere, plate, K, EPS, threads, keep_pairs=True)
     dt = time.perf_counter() - t
-    n = s.shape[0] + p.shape[0]
+    n = sphere.shape[0] + plate.shape[0]
+    got = np.asarray(gpu_pairs).astype(np.uint64)
+    got = got[np.lexsort((got[:, 1], got[:, 0]))] if got.shape[0] else got.reshape(0, 2)
     out = {"value": n / dt / 1e6, "unit": "Mprims/s", "cores": orc.max_threads() if threads == 0 else threads,
-           "kind": "port", "sample": f"icosphere L{sphere_level} + plate {nx}x{ny} quads ({n} tris, same scene "
-           f"at 1/4 size), 18-DOP, one pass", "seconds": dt, "pairs": int(cnt),
-           "stages_s": stages}
+           "kind": "port", "sample": f"the whole benchmark scene ({n} tris), 18-DOP, one pass with the pair list "
+           "kept", "seconds": dt, "pairs": int(cnt), "stages_s": stages,
+           "pairs_match_oracle": bool(np.array_equal(got, want))}
     # The reference's own serial element path (its headers, built into oracle/_ref when the sources were present):
     # from_vertices, top-down tree of dop_26 snapshots, potential_collision_set; 26-DOP, its only tree form.
     from oracle import ref
+    from distbvh_b200 import meshes
     if ref.available():
         s6, p6 = meshes.sphere_plate(6, 256, 128)
         r = ref.Ref(26)
@@ -620,13 +634,15 @@ def cpu_baseline_sample(sphere_level=8, nx=1024, ny=512, threads=0):
 
 
 def run_reference(args, world, rank):
-    """Reference arm: the reference's algorithms for this path on the host cores (OpenMP restatement:
-    from_vertices, compute_bounds, morton, one-bit radix sort, serial top-down tree, parallel query_tree)."""
+    """Reference arm: the reference's algorithms for this path on all host cores (OpenMP restatement of the Kokkos
+    path: from_vertices, compute_bounds, morton, one-bit radix sort, then the serial top-down tree and a parallel
+    query_tree), one pass over the whole benchmark scene per step, the pair list kept. Only the oracle and the mesh
+    generators are imported: the CUDA library is never loaded here."""
     if rank != 0:
         return None
     from oracle import oracle as orc
     from distbvh_b200 import meshes
-    s, p = meshes.sphere_plate(8, 1024, 512)
+    s, p = meshes.sphere_plate(args.level, args.nx, args.ny)
     n = s.shape[0] + p.shape[0]
     for _ in range(args.warmup):
         orc.pipeline(s, p, K, EPS)
@@ -638,12 +654,13 @@ def run_reference(args, world, rank):
         times.append(time.perf_counter() - t)
     ms = float(np.mean(times)) * 1e3
     value = n / (ms * 1e-3) / 1e6
-    sample = f"icosphere L8 + plate 1024x512 quads ({n} tris, the benchmark scene at 1/4 size) per step"
+    sample = f"the whole benchmark scene ({n} tris) per step"
     return {
         "metric": METRIC, "value": value, "unit": "Mprims/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded icosphere + plate)",
-        "config": {"workload": WORKLOAD, "k": K, "epsilon": EPS, "elements": n, "pairs": int(cnt)},
+        "config": bench_config(args, world, n, cnt),
+        "sort_digit_bits": 1,
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "Mprims/s", "cores": orc.max_threads(), "kind": "port",
                          "sample": sample},
@@ -749,10 +766,12 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    result, _, _ = run_gpu(args, world, rank, local)
+    result, sphere, plate, p64 = run_gpu(args, world, rank, local)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline_sample()
+            cb = cpu_baseline_full(sphere, plate, p64)
+            result["pairs_match_oracle"] = cb["pairs_match_oracle"]
+            result["cpu_baseline"] = cb
         print(json.dumps(result))
     if world > 1:
         import torch.distributed as dist

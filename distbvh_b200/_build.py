@@ -22,6 +22,7 @@ NVCC_FLAGS = [
     # __dmul_rn/__dadd_rn explicitly, and contraction is disabled as a second guard.
     "-fmad=false",
 ]
+LINK_GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
 def nvcc():
@@ -64,7 +65,7 @@ def build(force=False, verbose=False, extra=()):
     if errors:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs,
+    cmd = [nvcc(), *LINK_GENCODE, "-shared", "-o", tmp, *objs,
            "-Xcompiler", "-fPIC", "-lcudart"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)

@@ -75,7 +75,7 @@ struct object
   dev_buf verts_own, gid_own;
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
-  dev_buf hist, status;
+  dev_buf hist, status, runs;
   dev_buf warp_box, bucket_box, node_box, child, range, parent, exch, bdel, queue, elem_cache;
   dev_buf scal;  // obj_scalars
   // Each object's build runs on its own stream, forked from and joined back into the context stream with
@@ -366,6 +366,7 @@ bvhg_status reserve_object(bvhg_ctx *ctx, object &o)
   BVHG_CUDA( ctx, o.vals_alt.reserve( n * 4 ) );
   BVHG_CUDA( ctx, o.hist.reserve( passes * radix * 4 ) );
   BVHG_CUDA( ctx, o.status.reserve( passes * ( tiles + 1 ) * radix * 4 ) );
+  BVHG_CUDA( ctx, o.runs.reserve( long_run_capacity( n ) * 4 ) );
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;  // leaf buckets
   BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.bucket_box.reserve( m * D * 2 * sb ) );
@@ -494,9 +495,12 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
     }
   }
   {
-    // the fix-up reads the last pass's output and writes the other buffers
+    // the fix-up reads the last pass's output and writes the other buffers; runs too long for it are sorted in
+    // place afterwards, with the fix-up's input as scratch
     stage_scope st( ctx, BVHG_STAGE_FIXUP );
-    BVHG_CUDA( ctx, launch_sort_fixup( kin, vin, kout, vout, n, o.sc(), s ) );
+    BVHG_CUDA( ctx, launch_sort_fixup( kin, vin, kout, vout, n, o.runs.as< uint32_t >(), o.sc(), s ) );
+    st.launched();
+    BVHG_CUDA( ctx, launch_sort_runs( kout, vout, kin, vin, n, o.runs.as< uint32_t >(), o.sc(), s ) );
     st.launched();
     o.sort_result_alt = ( kout == o.keys_alt.as< uint64_t >() ) ? 1 : 0;
   }
@@ -1323,26 +1327,8 @@ bvhg_status bvhg_get_morton(bvhg_ctx *ctx, int32_t obj, uint64_t *sorted_keys, u
   if ( st != BVHG_OK ) return st;
   obj_scalars h;
   BVHG_CUDA( ctx, cudaMemcpy( &h, o.sc(), sizeof( h ), cudaMemcpyDeviceToHost ) );
-  if ( h.sort_approx )
-  {
-    // A run of equal high key halves was too long for the device fix-up: the build order is valid but not the
-    // stable order. The stable order is the order of (key, element index) pairs.
-    std::vector< std::pair< uint64_t, uint32_t > > kv( o.n );
-    std::vector< uint64_t > k( o.n );
-    std::vector< uint32_t > v( o.n );
-    BVHG_CUDA( ctx, cudaMemcpy( k.data(), o.sorted_keys(), o.n * 8, cudaMemcpyDeviceToHost ) );
-    BVHG_CUDA( ctx, cudaMemcpy( v.data(), o.sorted_vals(), o.n * 4, cudaMemcpyDeviceToHost ) );
-    for ( uint64_t i = 0; i < o.n; ++i ) kv[i] = { k[i], v[i] };
-    std::sort( kv.begin(), kv.end() );
-    for ( uint64_t i = 0; i < o.n; ++i )
-    {
-      if ( sorted_keys ) sorted_keys[i] = kv[i].first;
-      if ( perm ) perm[i] = kv[i].second;
-    }
-  } else {
-    if ( sorted_keys ) BVHG_CUDA( ctx, cudaMemcpy( sorted_keys, o.sorted_keys(), o.n * 8, cudaMemcpyDeviceToHost ) );
-    if ( perm ) BVHG_CUDA( ctx, cudaMemcpy( perm, o.sorted_vals(), o.n * 4, cudaMemcpyDeviceToHost ) );
-  }
+  if ( sorted_keys ) BVHG_CUDA( ctx, cudaMemcpy( sorted_keys, o.sorted_keys(), o.n * 8, cudaMemcpyDeviceToHost ) );
+  if ( perm ) BVHG_CUDA( ctx, cudaMemcpy( perm, o.sorted_vals(), o.n * 4, cudaMemcpyDeviceToHost ) );
   if ( min3 ) std::memcpy( min3, h.min3, sizeof( h.min3 ) );
   if ( inv3 ) std::memcpy( inv3, h.inv3, sizeof( h.inv3 ) );
   return BVHG_OK;

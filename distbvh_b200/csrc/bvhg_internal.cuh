@@ -36,7 +36,7 @@ struct obj_scalars
   int root;                          // root internal node, or ~elem when n == 1
   int error;                         // bvhg_status raised by a kernel (first one wins)
   unsigned int climb_count;          // subtrees queued for the global phase of the tree build
-  unsigned int sort_approx;          // 1: a run of equal high key halves was too long for the low-half fix-up
+  unsigned int long_runs;            // runs of equal high key halves too long for the fix-up (sorted by k_sort_runs)
   alignas( 16 ) unsigned char root_box[26 * 8];  // the root's slabs, D (min, max) pairs of the slab type
   unsigned int sort_tile_counter[64];// tile dispenser per radix pass
 };
@@ -96,8 +96,15 @@ cudaError_t launch_keys_hist(int bits, const double *cx, const double *cy, const
                              obj_scalars *sc, uint64_t *keys, uint32_t *hist, cudaStream_t s);
 
 // Stable sort of each run of equal high key halves by the low half (in -> out), after the passes over bits 32..62.
+// Runs longer than the fix-up's neighbour scan are copied in order and their starts listed in runs[] (capacity
+// n / 33 + 1, count in sc->long_runs); launch_sort_runs then sorts them.
 cudaError_t launch_sort_fixup(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
-                              uint32_t *vals_out, uint64_t n, obj_scalars *sc, cudaStream_t s);
+                              uint32_t *vals_out, uint64_t n, uint32_t *runs, obj_scalars *sc, cudaStream_t s);
+// Stable sort by the low key half of every run listed by the fix-up, in place in keys/vals, with tkeys/tvals (the
+// fix-up's input, no longer needed) as scratch. Exits at once when no run is listed.
+cudaError_t launch_sort_runs(uint64_t *keys, uint32_t *vals, uint64_t *tkeys, uint32_t *tvals, uint64_t n,
+                             const uint32_t *runs, obj_scalars *sc, cudaStream_t s);
+inline uint64_t long_run_capacity(uint64_t n) { return n / 33 + 1; }
 
 // Passes of the sort that build() runs: those whose digit lies in the high key half (the fix-up sorts the rest).
 inline int sort_first_pass(int bits) { return 32 / bits; }

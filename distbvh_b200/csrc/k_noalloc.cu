@@ -1,18 +1,20 @@
-// k_noalloc.cu — a stable radix sort of Morton keys that allocates no memory.
+// k_noalloc.cu — a stable radix sort of 64-bit keys that allocates no memory.
 //
 // Some callers cannot call cudaMalloc: a host that has handed all device memory to its own pool allocator (as
-// solid-mechanics codes and frameworks with caching allocators commonly do), code running where allocation
-// would stall or is not allowed (a real-time step loop with a fixed memory budget, work issued while a CUDA
-// stream is being captured), or a library boundary that forbids the callee from owning device memory. For them
-// bvhg_radix_sort_noalloc sorts caller-owned device keys into caller-owned outputs and takes every byte of scratch
-// (digit histograms, look-back status words, tile counters, the ping-pong key/index buffer) from one file-scope
-// static device array of fixed size. The sort itself is the library's radix pass kernel (k_sort.cu), unchanged.
+// solid-mechanics codes and frameworks with caching allocators commonly do, so a cudaMalloc beside the pool fails
+// or fragments it), a step loop that runs under a fixed device-memory budget, or a library boundary that forbids
+// the callee from owning device memory. For them bvhg_radix_sort_noalloc sorts caller-owned device keys into
+// caller-owned outputs and takes every byte of scratch (digit histograms, look-back status words, tile counters,
+// the ping-pong key/index buffer) from one file-scope static device array of fixed size. The sort itself is the
+// library's radix pass kernel (k_sort.cu), unchanged, over all 8 digits of the keys.
 //
 // The array exists on every GPU that loads this library, for the life of the process. Its device address is
 // resolved once per device, on the first call made with that device current (cudaGetSymbolAddress); make that
-// first call before any stream capture. All calls share the array and it keeps the last call's contents: each
-// call clears the parts that must start at zero, and calls that overlap on the GPU (different streams, or
-// different host threads) race on it.
+// first call before any stream capture. The cached address belongs to the CUDA context it was resolved in: after
+// cudaDeviceReset on a device, the library must not be called on that device again in the same process. All
+// calls share the array and it keeps the last call's contents: each call clears the parts that must start at
+// zero, and calls that overlap on the GPU (different streams, or different host threads) race on it. A call waits
+// for its stream before it returns (it reads back the sort's error word).
 #include "../../include/bvhg.h"
 #include "bvhg_internal.cuh"
 

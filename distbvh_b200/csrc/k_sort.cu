@@ -348,14 +348,14 @@ cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64
 // of a run at the run's start plus its rank by (full key, position) -- a stable sort of the run by the low half --
 // then gives the stable order of the full keys. One thread per element, out of place (in -> out), so that no
 // thread reads what another writes. Runs are found by scanning neighbours (cache hits: a warp reads contiguous
-// keys). A run longer than kFixRun keeps its order and is flagged in sc->sort_approx (still a valid build order;
-// exact probes sort such runs again on the host).
+// keys). A run longer than kFixRun is copied in order; the thread at its start lists it for k_sort_runs, which
+// sorts it by the low half on the device.
 constexpr int kFixRun = 32;
 
 __global__ void __launch_bounds__( 256 ) k_sort_fixup(const uint64_t *__restrict__ keys_in,
                                                       const uint32_t *__restrict__ vals_in,
                                                       uint64_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
-                                                      uint32_t n, obj_scalars *sc)
+                                                      uint32_t n, uint32_t *__restrict__ runs, obj_scalars *sc)
 {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if ( i >= n ) return;
@@ -384,7 +384,9 @@ __global__ void __launch_bounds__( 256 ) k_sort_fixup(const uint64_t *__restrict
   uint32_t pos = i;
   if ( limit || e - s + 1 > kFixRun )
   {
-    atomicOr( &sc->sort_approx, 1u );
+    // s == i only at the run's first element (the backward scan stops before its limit there); the run holds at
+    // least kFixRun + 1 elements, so at most n / 33 runs are listed
+    if ( s == i ) runs[atomicAdd( &sc->long_runs, 1u )] = i;
   } else if ( e > s ) {
     uint32_t rank = 0;
     for ( uint32_t j = s; j <= e; ++j )
@@ -398,14 +400,183 @@ __global__ void __launch_bounds__( 256 ) k_sort_fixup(const uint64_t *__restrict
   vals_out[pos] = vals_in[i];
 }
 
+// Stable sort of the long runs by the low key half. Block r takes runs r, r + grid, ...; a run is the range of
+// equal high halves that starts at its listed index (its end by binary search: the keys are ordered by the high
+// half). A run of up to kRunSmem elements is sorted in shared memory by a bitonic network over the distinct
+// composite keys (low half << 32 | position in the run), whose order is the stable order. A longer run takes four
+// stable 8-bit LSD passes over the low half through the scratch arrays (ping-pong, ending back in keys/vals): per
+// pass, 512 elements at a time are ranked by warp match in element order and placed at the digit's running offset.
+constexpr int kRunThreads = 512;
+constexpr int kRunWarps = kRunThreads / 32;
+constexpr int kRunSmem = 2048;
+
+__global__ void __launch_bounds__( kRunThreads ) k_sort_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                             uint64_t *__restrict__ tkeys,
+                                                             uint32_t *__restrict__ tvals, uint32_t n,
+                                                             const uint32_t *__restrict__ runs, const obj_scalars *sc)
+{
+  // bitonic: 2048 composite keys + 2048 indices (24 KB); LSD: per-warp digit counts, running offsets, tile totals,
+  // the four digit histograms (22.5 KB)
+  __shared__ __align__( 16 ) unsigned char s_raw[kRunSmem * 12];
+  __shared__ uint32_t s_scan[kRunWarps];
+  __shared__ uint32_t s_run_start, s_run_len;
+  const uint32_t nruns = *reinterpret_cast< const volatile unsigned int * >( &sc->long_runs );
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned lt_mask = ( 1u << lane ) - 1u;
+  for ( uint32_t r = blockIdx.x; r < nruns; r += gridDim.x )
+  {
+    if ( tid == 0 )
+    {
+      const uint32_t s = runs[r];
+      const uint32_t hi = static_cast< uint32_t >( keys[s] >> 32 );
+      uint32_t lo = s + 1, up = n;  // first index past s whose high half differs
+      while ( lo < up )
+      {
+        const uint32_t mid = lo + ( up - lo ) / 2;
+        if ( static_cast< uint32_t >( keys[mid] >> 32 ) == hi ) lo = mid + 1;
+        else up = mid;
+      }
+      s_run_start = s;
+      s_run_len = lo - s;
+    }
+    __syncthreads();
+    const uint32_t s = s_run_start, L = s_run_len;
+    const uint64_t hi_bits = keys[s] & 0xffffffff00000000ull;
+    if ( L <= kRunSmem )
+    {
+      uint64_t *c = reinterpret_cast< uint64_t * >( s_raw );
+      uint32_t *v = reinterpret_cast< uint32_t * >( s_raw + kRunSmem * 8 );
+      uint32_t P = 1;
+      while ( P < L ) P <<= 1;
+      for ( uint32_t j = tid; j < P; j += kRunThreads )
+      {
+        if ( j < L )
+        {
+          c[j] = ( ( keys[s + j] & 0xffffffffull ) << 32 ) | j;
+          v[j] = vals[s + j];
+        } else {
+          c[j] = ~0ull;
+        }
+      }
+      __syncthreads();
+      for ( uint32_t k = 2; k <= P; k <<= 1 )
+        for ( uint32_t j = k >> 1; j > 0; j >>= 1 )
+        {
+          for ( uint32_t t = tid; t < P; t += kRunThreads )
+          {
+            const uint32_t u = t ^ j;
+            if ( u > t )
+            {
+              const uint64_t a = c[t], b = c[u];
+              if ( ( a > b ) == ( ( t & k ) == 0 ) )
+              {
+                c[t] = b;
+                c[u] = a;
+              }
+            }
+          }
+          __syncthreads();
+        }
+      for ( uint32_t j = tid; j < L; j += kRunThreads )
+      {
+        const uint64_t x = c[j];
+        keys[s + j] = hi_bits | ( x >> 32 );
+        vals[s + j] = v[x & 0xffffffffull];
+      }
+    } else {
+      uint32_t( *cnt )[256] = reinterpret_cast< uint32_t( * )[256] >( s_raw );  // [kRunWarps][256]
+      uint32_t *run_off = reinterpret_cast< uint32_t * >( s_raw + kRunWarps * 256 * 4 );
+      uint32_t *tot = run_off + 256;
+      uint32_t( *hist )[256] = reinterpret_cast< uint32_t( * )[256] >( tot + 256 );  // [4][256]
+      for ( int q = tid; q < kRunWarps * 256; q += kRunThreads ) ( &cnt[0][0] )[q] = 0;
+      for ( int q = tid; q < 4 * 256; q += kRunThreads ) ( &hist[0][0] )[q] = 0;
+      __syncthreads();
+      for ( uint32_t j = tid; j < L; j += kRunThreads )
+      {
+        const uint32_t low = static_cast< uint32_t >( keys[s + j] );
+#pragma unroll
+        for ( int p = 0; p < 4; ++p ) atomicAdd( &hist[p][( low >> ( 8 * p ) ) & 255u], 1u );
+      }
+      __syncthreads();
+      uint64_t *sk = keys, *dk = tkeys;
+      uint32_t *sv = vals, *dv = tvals;
+      for ( int p = 0; p < 4; ++p )
+      {
+        const uint32_t x = tid < 256 ? hist[p][tid] : 0u;
+        const uint32_t ex = block_exclusive_scan( x, s_scan );
+        if ( tid < 256 ) run_off[tid] = ex;
+        __syncthreads();
+        for ( uint32_t base = 0; base < L; base += kRunThreads )
+        {
+          const uint32_t j = base + tid;
+          const bool valid = j < L;
+          const uint64_t key = valid ? sk[s + j] : 0ull;
+          const uint32_t val = valid ? sv[s + j] : 0u;
+          const uint32_t d = valid ? ( static_cast< uint32_t >( key ) >> ( 8 * p ) ) & 255u : 256u;
+          const unsigned peers = __match_any_sync( 0xffffffffu, d );
+          const uint32_t rank = __popc( peers & lt_mask );
+          if ( valid && lane == __ffs( peers ) - 1 ) cnt[warp][d] = __popc( peers );
+          __syncthreads();
+          if ( tid < 256 )
+          {
+            uint32_t t = 0;
+#pragma unroll
+            for ( int w = 0; w < kRunWarps; ++w )
+            {
+              const uint32_t c = cnt[w][tid];
+              cnt[w][tid] = t;
+              t += c;
+            }
+            tot[tid] = t;
+          }
+          __syncthreads();
+          if ( valid )
+          {
+            const uint32_t pos = run_off[d] + cnt[warp][d] + rank;
+            dk[s + pos] = key;
+            dv[s + pos] = val;
+          }
+          __syncthreads();
+          if ( tid < 256 )
+          {
+            run_off[tid] += tot[tid];
+#pragma unroll
+            for ( int w = 0; w < kRunWarps; ++w ) cnt[w][tid] = 0;
+          }
+          __syncthreads();
+        }
+        uint64_t *tk = sk;
+        sk = dk;
+        dk = tk;
+        uint32_t *tv = sv;
+        sv = dv;
+        dv = tv;
+      }
+    }
+    __syncthreads();  // shared memory and the run bounds are reused by the next run
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_sort_fixup(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
-                              uint32_t *vals_out, uint64_t n, obj_scalars *sc, cudaStream_t s)
+                              uint32_t *vals_out, uint64_t n, uint32_t *runs, obj_scalars *sc, cudaStream_t s)
 {
   if ( n == 0 ) return cudaSuccess;
   k_sort_fixup<<< static_cast< unsigned >( ( n + 255 ) / 256 ), 256, 0, s >>>( keys_in, vals_in, keys_out, vals_out,
-                                                                             static_cast< uint32_t >( n ), sc );
+                                                                             static_cast< uint32_t >( n ), runs, sc );
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sort_runs(uint64_t *keys, uint32_t *vals, uint64_t *tkeys, uint32_t *tvals, uint64_t n,
+                             const uint32_t *runs, obj_scalars *sc, cudaStream_t s)
+{
+  // a run has at least 33 elements: never more blocks than possible runs, at most one per SM
+  if ( n <= static_cast< uint64_t >( kFixRun ) ) return cudaSuccess;
+  const uint64_t most = long_run_capacity( n );
+  const uint64_t cap = static_cast< uint64_t >( device_sm_count() );
+  k_sort_runs<<< static_cast< unsigned >( most < cap ? most : cap ), kRunThreads, 0, s >>>(
+    keys, vals, tkeys, tvals, static_cast< uint32_t >( n ), runs, sc );
   return cudaGetLastError();
 }
 

@@ -205,10 +205,11 @@ BVHG_API bvhg_status bvhg_test_stall_sort(bvhg_ctx *ctx, int32_t enable);
 /* Stable sort of n device-resident 64-bit keys (Morton keys or any others): keys_out[r] is the r-th smallest key,
  * perm_out[r] its index in keys_in (ties keep input order). No counterpart in the reference: it is the library's
  * radix sort for callers that cannot allocate device memory (a host whose pool allocator owns all device memory, a
- * step loop with a fixed memory budget, work issued during stream capture). It allocates nothing: its scratch is a
- * fixed static device array (about 14 MB on every GPU that loads the library, held until the process exits), so n
- * is limited to 1,048,576 (BVHG_ERR_ARG beyond). The first call on a device resolves the array's address; make it
- * before any stream capture. Calls share the array: calls that overlap on the GPU race. Runs on `stream` (NULL =
+ * step loop with a fixed device-memory budget, a library boundary that forbids the callee from owning device
+ * memory). It allocates nothing: its scratch is a fixed static device array (about 14 MB on every GPU that loads
+ * the library, held until the process exits), so n is limited to 1,048,576 (BVHG_ERR_ARG beyond). The first call
+ * on a device resolves the array's address; make it before any stream capture, and do not call again on a device
+ * after cudaDeviceReset of it. Calls share the array: calls that overlap on the GPU race. Runs on `stream` (NULL =
  * the default stream) and returns when the sort is complete. keys_in, keys_out and perm_out must not overlap. */
 BVHG_API bvhg_status bvhg_radix_sort_noalloc(const uint64_t *keys_in, uint64_t *keys_out, uint32_t *perm_out,
                                              uint64_t n, void *stream);

@@ -788,9 +788,11 @@ double now_s()
 extern "C" {
 
 // Runs the whole path for objects A and B with `threads` OpenMP threads (0 = all). stage_s[7] receives the
-// seconds of: slabs+centroids, bounds, keys, sort, tree build, traversal, total. Returns |S(A, B)|.
+// seconds of: slabs+centroids, bounds, keys, sort, tree build, traversal (pair list included), total. The pair
+// list (index in A, index in B), in no particular order, goes to pairs[2p], pairs[2p + 1] for p < cap when pairs
+// is given. Returns |S(A, B)|.
 std::int64_t orc_pipeline(const double *xa, std::uint64_t na, const double *xb, std::uint64_t nb, std::uint32_t V,
-                          int K, double eps, int threads, double *stage_s)
+                          int K, double eps, int threads, double *stage_s, std::uint32_t *pairs, std::uint64_t cap)
 {
   if ( threads > 0 ) omp_set_num_threads( threads );
   const int D = K / 2;
@@ -828,11 +830,13 @@ std::int64_t orc_pipeline(const double *xa, std::uint64_t na, const double *xb, 
   td_tree TB;
   td_make( TB, sb.data(), cb.data(), nb, K );
   const double t5 = now_s();
-  std::int64_t total = 0;
+  // every thread keeps the pairs it finds (the path's output is the pair list, not only its size)
+  std::vector< std::vector< std::uint32_t > > found( omp_get_max_threads() );
   if ( na && nb )
   {
-#pragma omp parallel reduction(+ : total)
+#pragma omp parallel
     {
+      std::vector< std::uint32_t > &mine = found[omp_get_thread_num()];
       std::vector< std::uint32_t > out;
 #pragma omp for schedule(dynamic, 1024)
       for ( std::int64_t r = 0; r < static_cast< std::int64_t >( na ); ++r )
@@ -841,11 +845,26 @@ std::int64_t orc_pipeline(const double *xa, std::uint64_t na, const double *xb, 
         const std::uint32_t e = static_cast< std::uint32_t >( ia[r] );
         out.clear();
         query_node( TB, 0, sa.data() + static_cast< std::uint64_t >( e ) * D * 2, D, e, out );
-        total += static_cast< std::int64_t >( out.size() / 2 );
+        mine.insert( mine.end(), out.begin(), out.end() );
       }
     }
   }
   const double t6 = now_s();
+  std::int64_t total = 0;
+  for ( const auto &f : found )
+  {
+    if ( pairs )
+      for ( std::size_t j = 0; j + 1 < f.size(); j += 2 )
+      {
+        const std::uint64_t p = static_cast< std::uint64_t >( total ) + j / 2;
+        if ( p < cap )
+        {
+          pairs[2 * p] = f[j];
+          pairs[2 * p + 1] = f[j + 1];
+        }
+      }
+    total += static_cast< std::int64_t >( f.size() / 2 );
+  }
   if ( stage_s )
   {
     stage_s[0] = t1 - t0;

@@ -48,7 +48,7 @@ def _load():
         "orc_tree_node_count": (I64, [P, P, U64, I32]),
         "orc_max_variant_axis": (I32, [P, U64, P, U64]),
         "orc_sort_and_sweep": (I64, [P, U64, P, U64, I32, I32, P, U64]),
-        "orc_pipeline": (I64, [P, U64, P, U64, U32, I32, D, I32, P]),
+        "orc_pipeline": (I64, [P, U64, P, U64, U32, I32, D, I32, P, P, U64]),
         "orc_max_threads": (I32, []),
     }
     for name, (res, args) in sig.items():
@@ -229,14 +229,25 @@ def self_pair_set(xyz, k, eps=0.0, method="tree", gid=None):
 PIPELINE_STAGES = ("slabs", "bounds", "keys", "sort", "tree", "traverse", "total")
 
 
-def pipeline(xyz_a, xyz_b, k, eps=0.0, threads=0):
-    """The whole path on the CPU (all threads by default). Returns (|S|, {stage: seconds})."""
+def pipeline(xyz_a, xyz_b, k, eps=0.0, threads=0, keep_pairs=False):
+    """The whole path on the CPU (all threads by default). Returns (|S|, {stage: seconds}), and with keep_pairs
+    the pair set as a third item (canonical: sorted (m, 2) uint64 of (index in A, index in B))."""
     xa, xb = _c(xyz_a, np.float64), _c(xyz_b, np.float64)
     assert xa.shape[1] == xb.shape[1]
     st = np.zeros(7)
-    cnt = lib.orc_pipeline(xa.ctypes.data, xa.shape[0], xb.ctypes.data, xb.shape[0], xa.shape[1], k, eps, threads,
-                           st.ctypes.data)
-    return cnt, dict(zip(PIPELINE_STAGES, st.tolist()))
+    if not keep_pairs:
+        cnt = lib.orc_pipeline(xa.ctypes.data, xa.shape[0], xb.ctypes.data, xb.shape[0], xa.shape[1], k, eps,
+                               threads, st.ctypes.data, None, 0)
+        return cnt, dict(zip(PIPELINE_STAGES, st.tolist()))
+    cap = 4 * (xa.shape[0] + xb.shape[0]) + 1
+    while True:
+        out = np.empty((cap, 2), dtype=np.uint32)
+        cnt = lib.orc_pipeline(xa.ctypes.data, xa.shape[0], xb.ctypes.data, xb.shape[0], xa.shape[1], k, eps,
+                               threads, st.ctypes.data, out.ctypes.data, cap)
+        if cnt <= cap:
+            break
+        cap = cnt
+    return cnt, dict(zip(PIPELINE_STAGES, st.tolist())), canonical(out[:cnt])
 
 
 def max_threads():

@@ -5,9 +5,14 @@
 #   libbvhref26.so  element trees of dop_26 (the reference's default bphase_kdop)
 #   libbvhref6.so   element trees of dop_6 (built with BVH_BROADPHASE_6_DOP)
 # The reference's own build system (CMake with Kokkos and DARMA/vt) is not used.
+# Usage: ref_build.sh <reference src directory> (or REF_SRC in the environment).
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF_SRC="${REF_SRC:-/root/reference/src}"
+REF_SRC="${1:-${REF_SRC:-}}"
+if [ -z "$REF_SRC" ]; then
+  echo "usage: ref_build.sh <reference src directory>" >&2
+  exit 2
+fi
 CXX="${ORACLE_CXX:-/usr/bin/g++}"
 FMT_INC="$(python3 -c 'import os, flashinfer; print(os.path.join(os.path.dirname(flashinfer.__file__), "data", "spdlog", "include"))' 2>/dev/null || true)"
 if [ ! -d "$REF_SRC/bvh" ] || [ -z "$FMT_INC" ] || [ ! -f "$FMT_INC/spdlog/fmt/bundled/format.h" ]; then

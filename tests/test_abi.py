@@ -30,10 +30,24 @@ def test_library_exports_every_declared_symbol():
     assert sorted(bvhg.EXPORTS) == names
 
 
-def test_library_is_sm100a_only():
-    # the fat binary carries sm_100a code and nothing else (cuobjdump is not used: the ELF note names are enough)
-    data = open(bvhg.LIB_PATH, "rb").read()
-    assert b"sm_100a" in data
+def test_build_recipe_targets_sm100a_only():
+    # every nvcc invocation of the recipe (compile and link) names one target, sm_100a, and no other
+    from distbvh_b200 import _build
+    flags = list(_build.NVCC_FLAGS)
+    gencodes = [flags[i + 1] for i, f in enumerate(flags) if f == "-gencode"]
+    assert gencodes == ["arch=compute_100a,code=sm_100a"]
+    assert not any(f.startswith(("-arch", "--gpu-architecture", "--generate-code")) for f in flags)
+    assert _build.LINK_GENCODE == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_package_import_does_not_load_the_library():
+    # the mesh generators (used by the CPU reference arm) import without mapping libbvhg.so
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); from distbvh_b200 import meshes; "
+            "print(any('libbvhg' in l for l in open('/proc/self/maps')))" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True).stdout.strip()
+    assert out == "False"
 
 
 @pytest.mark.parametrize("k", [6, 18, 26])

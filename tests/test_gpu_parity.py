@@ -2,7 +2,8 @@
 
 Bit-exact for everything integer or FP64 (slabs, centroids, Morton bounds and keys, permutation, pair sets).
 The FP32 precision form must give the identical pair set after its FP64 recheck, and its FP32 slabs must
-enclose the FP64 slabs. Sizes keep the oracle to seconds; full-size properties are checked in test_gpu_scale.py.
+enclose the FP64 slabs. Sizes keep the oracle to seconds; the benchmark-sized scenes are checked against the
+oracle in test_gpu_full_size.py.
 """
 import numpy as np
 import pytest
@@ -85,27 +86,36 @@ def test_many_tiles_sort():
         check_stages(ctx, oa, a, 18, 0.0)
 
 
-def clustered_soup(counts, seed):
+def clustered_soup(counts, seed, cells=None):
     """Tiny triangles in clusters of the given sizes, each inside one cell of the top 31 Morton bits (10 bits of
     x, 10 of y, 11 of z: the clusters sit at cell centres of a 1024 x 1024 x 2048 grid over the unit cube, 2e-4
     wide), plus two corner elements that fix the Morton bounds to the unit cube. Members of a cluster share the
-    high key half and differ in the low."""
+    high key half and differ in the low. cells: the (ix, iy, iz) cell of each cluster (distinct), else a fixed
+    diagonal of cells."""
     rng = np.random.default_rng(seed)
     parts = [np.array([[[0, 0, 0], [1e-3, 0, 0], [0, 1e-3, 0]]]),
              np.array([[[1, 1, 1], [1 - 1e-3, 1, 1], [1, 1 - 1e-3, 1]]])]
     for j, c in enumerate(counts):
-        centre = (np.array([307, 511 - 40 * j, 2 * (129 + 17 * j)]) + 0.5) / np.array([1024.0, 1024.0, 2048.0])
+        cell = np.array([307, 511 - 40 * j, 2 * (129 + 17 * j)]) if cells is None else np.asarray(cells[j])
+        centre = (cell + 0.5) / np.array([1024.0, 1024.0, 2048.0])
         pts = centre + rng.uniform(-1e-4, 1e-4, (c, 1, 3)) + rng.uniform(-2e-6, 2e-6, (c, 3, 3))
         parts.append(pts)
     xyz = np.concatenate(parts).astype(np.float64)
     return np.ascontiguousarray(xyz[rng.permutation(xyz.shape[0])])
 
 
-@pytest.mark.parametrize("counts", [(2, 5, 31, 32), (33, 3), (500, 40, 7)])
+def distinct_cells(count, seed):
+    rng = np.random.default_rng(seed)
+    flat = rng.choice(1000 * 1000 * 2000, size=count, replace=False)
+    return np.stack([flat % 1000 + 12, (flat // 1000) % 1000 + 12, flat // 1000000 + 24], axis=1)
+
+
+@pytest.mark.parametrize("counts", [(2, 5, 31, 32), (33, 3), (500, 40, 7), (2048, 2049, 1), (100000, 34)])
 def test_runs_of_equal_high_key_halves(counts):
-    """The build sorts by the high key half and fixes each run of equal high halves by the low half: short runs
-    on the device, runs beyond its limit through the exact host order of the probe. Either way the probe returns
-    the stable order and the pair sets are exact."""
+    """The build sorts by the high key half, then orders each run of equal high halves by the low half on the
+    device: runs of up to 32 in the fix-up, longer ones in the run sort (a shared-memory network up to 2048
+    elements, LSD passes beyond). The permutation read back is the device's own, and it must be the stable order
+    of the oracle's keys; the pair sets must be exact."""
     a = clustered_soup(counts, seed=sum(counts))
     b = clustered_soup(counts[::-1], seed=7 + sum(counts))
     with bvhg.Context(k=18) as ctx:
@@ -114,6 +124,33 @@ def test_runs_of_equal_high_key_halves(counts):
         check_stages(ctx, ob, b, 18, 0.0)
         assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b, 18))
         assert np.array_equal(orc.canonical(ctx.self_collision(oa)), orc.self_pair_set(a, 18))
+
+
+@pytest.mark.parametrize("bits", [1, 8])
+def test_many_long_runs(bits):
+    """Hundreds of runs beyond the fix-up's limit, more than there are blocks of the run sort, at two digit
+    widths of the high-half passes."""
+    rng = np.random.default_rng(77)
+    counts = rng.integers(33, 300, size=400)
+    a = clustered_soup(counts, seed=78, cells=distinct_cells(counts.shape[0], 79))
+    with bvhg.Context(k=18, digit_bits=bits) as ctx:
+        o = ctx.object()
+        ctx.set_elements(o, a)
+        ctx.build(o)
+        check_stages(ctx, o, a, 18, 0.0)
+
+
+def test_all_keys_equal():
+    """Every element identical: one run covering the whole object (the LSD path), key ties kept in index order."""
+    tri = meshes.random_soup(1, 3, seed=4, size=0.1)
+    a = np.ascontiguousarray(np.repeat(tri, 5000, axis=0))
+    with bvhg.Context(k=18) as ctx:
+        o = ctx.object()
+        ctx.set_elements(o, a)
+        ctx.build(o)
+        check_stages(ctx, o, a, 18, 0.0)
+        keys, perm, _, _ = ctx.morton(o, a.shape[0])
+        assert np.all(keys == keys[0]) and np.array_equal(perm, np.arange(a.shape[0], dtype=np.uint32))
 
 
 def test_two_plates_config():
@@ -325,8 +362,8 @@ def test_stage_timing_and_launch_count():
         ctx.build(oa)
         ctx.self_collision(oa)
         ms, launches = ctx.stage_times()
-        # four radix passes over the high key half, then the low-half fix-up
-        assert launches["sort"] == 4 and launches["fixup"] == 1 and launches["slabs"] == 1 and launches["build"] == 1 and launches["climb"] == 1
+        # four radix passes over the high key half, then the low-half fix-up and the sort of long runs
+        assert launches["sort"] == 4 and launches["fixup"] == 2 and launches["slabs"] == 1 and launches["build"] == 1 and launches["climb"] == 1
         assert launches["traverse"] >= 1
         assert all(v >= 0 for v in ms.values()) and ms["sort"] > 0
         assert ctx.launch_count() >= 12
