@@ -67,6 +67,8 @@ def parse():
                         "two-body scenes in one graph; timestep: 32 tumbling tori, refit vs rebuild; sweep: "
                         "sort-and-sweep between two patch-sized objects")
     p.add_argument("--lattice", type=int, default=256, help="tet_lattice cells per axis (256 = 16,777,216 tets)")
+    p.add_argument("--kdop", type=int, default=26, choices=[6, 18, 26], help="tet_lattice k-DOP (26 = the precision case)")
+    p.add_argument("--no-oracle", action="store_true", help="skip the full-size oracle pair-set check")
     return p.parse_args()
 
 
@@ -372,7 +374,7 @@ def run_precision(args, world, rank, local):
     d_a, d_b = torch.from_numpy(a_np).to(dev), torch.from_numpy(b_np).to(dev)
     prims = a_np.shape[0] + b_np.shape[0]
     stream = torch.cuda.Stream(device=dev)
-    k = 26
+    k = args.kdop
 
     def run(precision):
         ctx = bvhg.Context(k=k, precision=precision, device=local, stream=stream.cuda_stream)
@@ -402,8 +404,33 @@ def run_precision(args, world, rank, local):
         cand = ctx.last_candidates() if precision == bvhg.FILTER_FP32 else cnt
         return ctx, oa, ms, cnt, cand, out[:cnt]
 
+    def stage_ms(precision, reps=2):
+        """Per-stage device times of one step (library CUDA events around each stage, stream-serialised)."""
+        ctx = bvhg.Context(k=k, precision=precision, device=local, stream=stream.cuda_stream, stage_timing=True)
+        oa, ob = ctx.object(), ctx.object()
+
+        def step(cap, out):
+            ctx.set_elements(oa, d_a, mem=bvhg.MEM_DEVICE)
+            ctx.set_elements(ob, d_b, mem=bvhg.MEM_DEVICE)
+            ctx.build(oa)
+            ctx.build(ob)
+            return ctx.broadphase_raw(oa, ob, out.data_ptr() if out is not None else None, cap, bvhg.MEM_DEVICE)
+
+        _, cnt = step(0, None)
+        out = torch.empty((max(cnt, 1), 2), dtype=torch.int64, device=dev)
+        step(out.shape[0], out)
+        ctx.stage_times()
+        for _ in range(reps):
+            step(out.shape[0], out)
+        ms, _ = ctx.stage_times()
+        ctx.close()
+        del out
+        return {s_: v / reps for s_, v in ms.items() if v > 0}
+
     ctx64, oa64, ms64, n64, _, p64 = run(bvhg.PLAIN_FP64)
     ctx32, oa32, ms32, n32, cand32, p32 = run(bvhg.FILTER_FP32)
+    stages64 = stage_ms(bvhg.PLAIN_FP64)
+    stages32 = stage_ms(bvhg.FILTER_FP32)
     key64 = torch.sort(p64[:, 0] * (1 << 32) + p64[:, 1])[0]
     key32 = torch.sort(p32[:, 0] * (1 << 32) + p32[:, 1])[0]
     same = n64 == n32 and bool(torch.equal(key64, key32))
@@ -421,16 +448,33 @@ def run_precision(args, world, rank, local):
     del s64, s32, err_lo, err_hi, width, err, rel
     ctx64.close()
     ctx32.close()
+    oracle = None
+    if rank == 0 and not args.no_oracle:
+        # the oracle's OpenMP pipeline on the same objects, its pair list against the FP64 one (rank 0 only)
+        from oracle import oracle as orc
+        t = time.perf_counter()
+        ocnt, _, want = orc.pipeline(a_np, b_np, k, 0.0, keep_pairs=True)
+        dt = time.perf_counter() - t
+        got = p64.cpu().numpy().astype(np.uint64)
+        got = got[np.lexsort((got[:, 1], got[:, 0]))]
+        oracle = {"pairs_match_oracle": bool(np.array_equal(got, want)), "oracle_pairs": int(ocnt),
+                  "cpu_baseline": {"value": prims / dt / 1e6, "unit": "Mprims/s", "cores": orc.max_threads(),
+                                   "kind": "port", "sample": "the whole workload, one pass with the pair list kept",
+                                   "seconds": dt}}
+        del want, got
     return {
         "metric": METRIC, "value": prims * world / (ms32 * 1e-3) / 1e6, "unit": "Mprims/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded tet lattice)",
         "config": {"workload": f"tet_lattice: {m}^3 jittered cells, one tet each ({prims} tets), checkerboard "
-                               f"objects A/B, 26-DOP", "k": k, "epsilon": 0.0, "elements": prims,
+                               f"objects A/B, {k}-DOP", "k": k, "epsilon": 0.0, "elements": prims,
                    "l2": "inputs larger than L2"},
+        "oracle": oracle,
         "form": "FP32 filter + FP64 recheck (value); FP64 plain below",
-        "fp64_plain": {"ms_per_step": ms64, "value": prims * world / (ms64 * 1e-3) / 1e6, "pairs": int(n64)},
+        "fp64_plain": {"ms_per_step": ms64, "value": prims * world / (ms64 * 1e-3) / 1e6, "pairs": int(n64),
+                       "stages_ms": stages64},
         "filter_fp32": {"ms_per_step": ms32, "pairs": int(n32), "candidates": int(cand32), "same_pair_set": same,
+                        "stages_ms": stages32,
                         "speedup_vs_fp64": ms64 / ms32,
                         "false_positive_rate": (cand32 - n32) / cand32 if cand32 else 0.0},
         "fp32_bound_error": bound,

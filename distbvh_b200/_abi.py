@@ -25,7 +25,7 @@ EXPORTS = (
     "bvhg_get_kdops", "bvhg_get_kdops_f32", "bvhg_get_centroids", "bvhg_validate_tree", "bvhg_last_candidates",
     "bvhg_get_stage_times", "bvhg_launch_count", "bvhg_set_spin_limit", "bvhg_test_stall_sort", "bvhg_debug_normal",
     "bvhg_synchronize", "bvhg_last_error", "bvhg_status_string", "bvhg_radix_sort_noalloc",
-    "bvhg_batch_broadphase", "bvhg_batch_autotune", "bvhg_sort_and_sweep",
+    "bvhg_batch_broadphase", "bvhg_batch_autotune", "bvhg_sort_and_sweep", "bvhg_test_dense_stack",
 )
 
 
@@ -73,6 +73,7 @@ def _load():
         "bvhg_launch_count": (I32, [P, ctypes.POINTER(U64)]),
         "bvhg_set_spin_limit": (I32, [P, U32]),
         "bvhg_test_stall_sort": (I32, [P, I32]),
+        "bvhg_test_dense_stack": (I32, [P, I32]),
         "bvhg_debug_normal": (I32, [I32, I32, I32, P, P, P]),
         "bvhg_synchronize": (I32, [P]),
         "bvhg_last_error": (ctypes.c_char_p, [P]),
@@ -309,6 +310,9 @@ class Context:
 
     def test_stall_sort(self, enable):
         self._check(lib.bvhg_test_stall_sort(self._h, 1 if enable else 0))
+
+    def test_dense_stack(self, limit):
+        self._check(lib.bvhg_test_dense_stack(self._h, limit))
 
     def synchronize(self):
         self._check(lib.bvhg_synchronize(self._h))

@@ -12,6 +12,18 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p)
   return static_cast< uint32_t >( __cvta_generic_to_shared( p ) );
 }
 
+// 16 bytes global -> shared without a register round trip (cached in L1 as well); both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+  asm volatile( "cp.async.ca.shared.global [%0], [%1], 16;" ::"r"( smem_addr( dst ) ), "l"( src ) : "memory" );
+}
+
+// Waits for all of this thread's cp_async16 copies (a __syncwarp / __syncthreads then publishes them to the others).
+__device__ __forceinline__ void cp_async_wait_all()
+{
+  asm volatile( "cp.async.wait_all;" ::: "memory" );
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 {
   asm volatile( "mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"( smem_addr( bar ) ), "r"( count ) : "memory" );

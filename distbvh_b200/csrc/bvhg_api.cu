@@ -72,6 +72,9 @@ struct object
   // test from the vertices instead of storing all of them.
   bool store_slabs = false;
   bool stored = false;  // the last build stored them
+  // The batched dense walk reached its stack bound on this object's tree: its traversals use the single-node walk
+  // until the element count changes.
+  bool dense_ok = true;
   dev_buf verts_own, gid_own;
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
@@ -186,6 +189,7 @@ struct bvhg_ctx
   bool own_stream = false;
   uint32_t spin_limit = kDefaultSpinLimit;
   int stall_sort = 0;  // test hook: radix look-back polls a status row nobody publishes
+  int dense_stack = 0;  // test hook: lower stack bound of the batched dense walk (0 = its own)
   std::vector< std::unique_ptr< object > > objs;
   cudaEvent_t fork_evt = nullptr;
   std::string err;
@@ -370,7 +374,7 @@ bvhg_status reserve_object(bvhg_ctx *ctx, object &o)
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;  // leaf buckets
   BVHG_CUDA( ctx, o.warp_box.reserve( ( ( n + 31 ) / 32 ) * D * 2 * sb ) );
   BVHG_CUDA( ctx, o.bucket_box.reserve( m * D * 2 * sb ) );
-  BVHG_CUDA( ctx, o.elem_cache.reserve( n * D * 2 * sb ) );
+  BVHG_CUDA( ctx, o.elem_cache.reserve( m * kLeafSize * D * 2 * sb ) );  // whole buckets (slab-major tiles)
   BVHG_CUDA( ctx, o.node_box.reserve( ( m - 1 ) * D * 4 * sb + 16 ) );
   BVHG_CUDA( ctx, o.child.reserve( ( m - 1 ) * 8 + 8 ) );
   BVHG_CUDA( ctx, o.range.reserve( ( m - 1 ) * 8 + 8 ) );
@@ -570,13 +574,14 @@ bvhg_status find_pairs(bvhg_ctx *ctx, object &a, object &b, bool self, const uin
     BVHG_CUDA( ctx, ctx->pairs2.reserve( ctx->pair2_cap * sizeof( uint2 ) ) );
   }
   pair_scalars *ps = ctx->pscal.as< pair_scalars >();
-  for ( int attempt = 0; attempt < 3; ++attempt )
+  for ( int attempt = 0; attempt < 4; ++attempt )
   {
     BVHG_CUDA( ctx, cudaMemsetAsync( ps, 0, sizeof( pair_scalars ), s ) );
+    const bool dense = a.dense_ok && b.dense_ok;
     {
       stage_scope st( ctx, BVHG_STAGE_TRAVERSE );
-      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( a ), view_of( b ), self, ctx->cfg.epsilon, ctx->pairs.as< uint2 >(),
-                                       ctx->pair_cap, ps, s ) );
+      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( a ), view_of( b ), self, dense, ctx->cfg.epsilon,
+                                       ctx->pairs.as< uint2 >(), ctx->pair_cap, ps, s, ctx->dense_stack ) );
       st.launched();
     }
     if ( fp32 )
@@ -593,6 +598,13 @@ bvhg_status find_pairs(bvhg_ctx *ctx, object &a, object &b, bool self, const uin
     bvhg_status st = object_error( ctx, ctx->host_err[0] );
     if ( st == BVHG_OK ) st = object_error( ctx, ctx->host_err[1] );
     if ( st != BVHG_OK ) return st;
+    if ( ctx->host_ps->error == kErrOverflowStack && dense && a.stored && b.stored )
+    {
+      // the batched dense walk reached its stack bound: search again with the single-node walk
+      a.dense_ok = false;
+      b.dense_ok = false;
+      continue;
+    }
     if ( ctx->host_ps->error ) return fail( ctx, BVHG_ERR_CUDA, "traversal stack overflow" );
     const uint64_t ncand = ctx->host_ps->count;
     ctx->last_candidates = ncand;
@@ -725,7 +737,8 @@ bvhg_status capture_batch(bvhg_ctx *ctx, batch_state &B, const batch_args &x, co
       const bool self = x.a[sc] == x.b[sc];
       if ( oa.n == 0 || ob.n == 0 || ( self && oa.n < 2 ) ) continue;
       uint2 *cand = B.cand.as< uint2 >() + B.off[sc];
-      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( oa ), view_of( ob ), self, ctx->cfg.epsilon, cand, B.cap[sc], ps + sc, ls ) );
+      BVHG_CUDA( ctx, launch_traverse( K, fp32, view_of( oa ), view_of( ob ), self, oa.dense_ok && ob.dense_ok,
+                                       ctx->cfg.epsilon, cand, B.cap[sc], ps + sc, ls, ctx->dense_stack ) );
       const uint2 *fin = cand;
       const unsigned long long *cnt = &ps[sc].count;
       if ( fp32 )
@@ -851,6 +864,7 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
     {
       const object &ob = *ctx->objs[o];
       for ( uint64_t v : { ob.n, static_cast< uint64_t >( ob.V ), static_cast< uint64_t >( ob.store_slabs ),
+                           static_cast< uint64_t >( ob.dense_ok ),
                            reinterpret_cast< uint64_t >( ob.verts ),
                            reinterpret_cast< uint64_t >( ob.gid ), reinterpret_cast< uint64_t >( ob.scal.p ),
                            reinterpret_cast< uint64_t >( ob.keys.p ), reinterpret_cast< uint64_t >( ob.bucket_box.p ),
@@ -888,6 +902,15 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
     for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
     {
       const pair_scalars &h = B.host_ps[sc];
+      if ( h.error == kErrOverflowStack && ctx->objs[x.a[sc]]->dense_ok && ctx->objs[x.b[sc]]->dense_ok )
+      {
+        // the batched dense walk reached its stack bound: this scene's objects take the single-node walk and the
+        // batch runs again (a new layout: the graph is captured again)
+        ctx->objs[x.a[sc]]->dense_ok = false;
+        ctx->objs[x.b[sc]]->dense_ok = false;
+        grown = true;
+        continue;
+      }
       if ( h.error ) return fail( ctx, BVHG_ERR_CUDA, "traversal stack overflow in batch scene " + std::to_string( sc ) );
       const uint64_t need = fp32 ? std::max( h.count, h.count2 ) : h.count;
       cand_total += h.count;
@@ -1025,7 +1048,11 @@ bvhg_status bvhg_set_elements(bvhg_ctx *ctx, int32_t obj, const double *xyz, uin
   cudaSetDevice( ctx->cfg.device );
   object &o = *ctx->objs[obj];
   join_object( ctx, o );  // the last build may still read the owned vertex buffer
-  if ( n != o.n || V != o.V ) o.topo = false;
+  if ( n != o.n || V != o.V )
+  {
+    o.topo = false;
+    o.dense_ok = true;
+  }
   o.n = n;
   o.V = V;
   o.built = false;
@@ -1566,6 +1593,13 @@ bvhg_status bvhg_test_stall_sort(bvhg_ctx *ctx, int32_t enable)
 {
   if ( !ctx ) return BVHG_ERR_ARG;
   ctx->stall_sort = enable ? 1 : 0;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_test_dense_stack(bvhg_ctx *ctx, int32_t limit)
+{
+  if ( !ctx || limit < 0 ) return BVHG_ERR_ARG;
+  ctx->dense_stack = limit;
   return BVHG_OK;
 }
 

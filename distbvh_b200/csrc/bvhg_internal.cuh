@@ -192,9 +192,12 @@ struct tree_view
   const obj_scalars *sc;
 };
 
-// Queries every leaf of q against tree t; writes (q element, t element) local index pairs.
-cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, double eps, uint2 *pairs,
-                            uint64_t cap, pair_scalars *ps, cudaStream_t s);
+// Queries every leaf of q against tree t; writes (q element, t element) local index pairs. dense (both objects'
+// element slabs stored): the walk that pops nodes in batches and tests leaves in batches; its deeper stack bound can
+// be reached (ps->error = kErrOverflowStack), and the single-node walk (dense = false) then always completes.
+// dense_stack_limit > 0 lowers that bound (test hook); 0 keeps it.
+cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, bool dense, double eps, uint2 *pairs,
+                            uint64_t cap, pair_scalars *ps, cudaStream_t s, int dense_stack_limit = 0);
 
 // FP64 recheck of FP32 candidates: keeps (a, b) iff the FP64 slabs of a and b overlap, compacted into out.
 // The candidate count is min(ps->count, cand_cap), read on the device.

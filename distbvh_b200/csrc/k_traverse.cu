@@ -15,6 +15,7 @@
 // Self-collision (self_collision_set, collision_query.hpp:331-368): the query of rank i only visits subtrees
 // holding ranks > i (internal node k splits its bucket range [l, r] into [l, k] and [k + 1, r]) and tests only
 // bucket elements of rank > i, so every unordered pair is found once and no element is paired with itself.
+#include "bulk_copy.cuh"
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
 
@@ -56,10 +57,8 @@ struct slab_pair< float >
 template< int K, typename T >
 constexpr int kNodeChunk = ( K / 2 ) <= 4 ? K / 2 : ( sizeof( T ) == 4 ? ( K / 2 + 1 ) / 2 : 5 );
 
-// Resident blocks per SM of the walk: 4 for the variants that compute slabs (128 registers), 6 for the one that
-// reads stored slabs.
-template< int K, typename T, bool LAZY >
-constexpr int kTravBlocksPerSM = LAZY ? 4 : 6;
+// Resident blocks per SM of the single-node walk, which computes the element slabs it tests (128 registers).
+constexpr int kTravBlocksPerSM = 4;
 
 // Slots for k outputs of each calling lane, one atomic per group of converged lanes: the lanes' exclusive prefix of
 // k is formed from one ballot per bit of k (k < 64), the lowest lane reserves the group's total.
@@ -150,28 +149,25 @@ struct trav_args
   uint2 *pairs;
   uint64_t cap;
   pair_scalars *ps;
+  int dense_stack;  // stack bound of the batched dense walk (kDenseStack, lower under a test hook)
 };
 
 // Target leaf bucket bb for the lanes in `mine`: the warp first computes the bucket's element slabs into its cache
-// (lane j: element of rank 8 bb + j; the stored variant reads the stored rows instead), then every lane of the mask tests its query against them (ranks above its own
+// (lane j: element of rank 8 bb + j), then every lane of the mask tests its query against them (ranks above its own
 // in self-collision). Hits go out through one warp-aggregated reservation. Called by the whole warp.
-template< int K, typename T, int VT, bool LAZY >
+template< int K, typename T, int VT >
 __device__ __forceinline__ void test_bucket(const trav_args< T > &x, const T *qlo, const T *qhi, uint32_t qe, int bb,
                                             int skip, bool mine, T *cache, unsigned lane)
 {
   constexpr int D = K / 2;
   const int t0 = kLeafSize * bb;
   const int cnt = min( kLeafSize, static_cast< int >( x.nt ) - t0 );
-  // The bucket's element slabs: the stored rows (dense contact), or computed from the vertices into the warp's
-  // shared-memory cache by lanes 0..7 (sparse contact: a bucket is tested by few packets, so nothing is kept).
-  const T *rows = x.tcache + static_cast< size_t >( t0 ) * 2 * D;
-  if constexpr ( LAZY )
-  {
-    if ( static_cast< int >( lane ) < cnt )
-      slabs_to_row< K, T, VT >( x.tverts, x.tV, __ldg( x.tperm + t0 + lane ), x.eps, x.eps_hi, cache + lane * 2 * D );
-    __syncwarp();
-    rows = cache;
-  }
+  // The bucket's element slabs, computed from the vertices into the warp's shared-memory cache by lanes 0..7
+  // (sparse contact: a bucket is tested by few packets, so nothing is kept).
+  if ( static_cast< int >( lane ) < cnt )
+    slabs_to_row< K, T, VT >( x.tverts, x.tV, __ldg( x.tperm + t0 + lane ), x.eps, x.eps_hi, cache + lane * 2 * D );
+  __syncwarp();
+  const T *rows = cache;
   if ( mine )
   {
     const int r0 = max( t0, skip + 1 );
@@ -184,8 +180,7 @@ __device__ __forceinline__ void test_bucket(const trav_args< T > &x, const T *ql
       for ( int a = 0; a < D; ++a )
       {
         if ( !o ) break;
-        if constexpr ( LAZY ) o = qlo[a] < eb[2 * a + 1] && eb[2 * a] < qhi[a];
-        else o = qlo[a] < __ldg( eb + 2 * a + 1 ) && __ldg( eb + 2 * a ) < qhi[a];
+        o = qlo[a] < eb[2 * a + 1] && eb[2 * a] < qhi[a];
       }
       if ( o ) hits |= 1u << ( r - t0 );
     }
@@ -197,7 +192,7 @@ __device__ __forceinline__ void test_bucket(const trav_args< T > &x, const T *ql
 }
 
 // One packet: the union box of ranks pk*32 .. pk*32 + 31 against the target root, then the walk (see k_traverse).
-template< int K, typename T, int VT, bool LAZY >
+template< int K, typename T, int VT >
 __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const uint32_t i, const unsigned lane,
                                                 int2 *stack, T *cache, const T *rb)
 {
@@ -219,18 +214,7 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
   const uint32_t qe = valid ? __ldg( x.qperm + i ) : 0u;
   T qlo[D], qhi[D];
   bool in_root = valid;
-  if constexpr ( LAZY )
-  {
-    if ( valid ) leaf_slabs< K, T, VT >( x.qverts, x.qV, qe, x.eps, x.eps_hi, qlo, qhi );
-  } else {
-    const T *qs = x.qrows + static_cast< size_t >( valid ? i : 0 ) * D * 2;
-#pragma unroll
-    for ( int a = 0; a < D; ++a )
-    {
-      qlo[a] = __ldg( qs + 2 * a );
-      qhi[a] = __ldg( qs + 2 * a + 1 );
-    }
-  }
+  if ( valid ) leaf_slabs< K, T, VT >( x.qverts, x.qV, qe, x.eps, x.eps_hi, qlo, qhi );
 #pragma unroll
   for ( int a = 0; a < D; ++a )
   {
@@ -247,7 +231,7 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
   const int root = x.tsc->root;
   if ( root < 0 )
   {
-    test_bucket< K, T, VT, LAZY >( x, qlo, qhi, qe, ~root, skip, in_root, cache, lane );
+    test_bucket< K, T, VT >( x, qlo, qhi, qe, ~root, skip, in_root, cache, lane );
     return;
   }
   int sp = 0;
@@ -289,7 +273,7 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
     unsigned nmask = 0;
     if ( m0 )
     {
-      if ( c.x < 0 ) test_bucket< K, T, VT, LAZY >( x, qlo, qhi, qe, ~c.x, skip, o0, cache, lane );
+      if ( c.x < 0 ) test_bucket< K, T, VT >( x, qlo, qhi, qe, ~c.x, skip, o0, cache, lane );
       else
       {
         next = c.x;
@@ -298,7 +282,7 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
     }
     if ( m1 )
     {
-      if ( c.y < 0 ) test_bucket< K, T, VT, LAZY >( x, qlo, qhi, qe, ~c.y, skip, o1, cache, lane );
+      if ( c.y < 0 ) test_bucket< K, T, VT >( x, qlo, qhi, qe, ~c.y, skip, o1, cache, lane );
       else if ( next < 0 )
       {
         next = c.y;
@@ -332,10 +316,10 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
 // current node (the node row is read once for the warp, a broadcast), and a child is entered with the mask of the
 // lanes that overlap it (a lane that misses a node misses all of its descendants). Stack entries are (node, lane
 // mask), in shared memory. At a leaf bucket the lanes of the mask test their element against the bucket's element
-// slabs: the stored rows (dense contact) or, computed once by the warp from the vertices, a shared cache.
-template< int K, typename T, int VT, bool LAZY >
-__global__ void __launch_bounds__( kTravThreads, kTravBlocksPerSM< K, T, LAZY > ) k_traverse(const trav_args< T > x,
-                                                                         const obj_scalars *__restrict__ qsc)
+// slabs, computed once by the warp from the vertices into a shared cache.
+template< int K, typename T, int VT >
+__global__ void __launch_bounds__( kTravThreads, kTravBlocksPerSM ) k_traverse(const trav_args< T > x,
+                                                                           const obj_scalars *__restrict__ qsc)
 {
   constexpr int D = K / 2;
   constexpr int D0 = D < 4 ? D : 4;
@@ -359,14 +343,7 @@ __global__ void __launch_bounds__( kTravThreads, kTravBlocksPerSM< K, T, LAZY > 
     if ( !o ) return;
   }
   const uint32_t packets = ( x.nq + 31 ) / 32;
-  if constexpr ( !LAZY )
-  {
-    // Dense contact (stored slabs): one packet per warp, the hardware balances the walks.
-    const uint32_t pk = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
-    if ( pk < packets ) traverse_packet< K, T, VT, LAZY >( x, pk * 32 + lane, lane, stack, cache, rb );
-    return;
-  }
-  // Sparse contact: packets (32 query ranks) in a persistent grid. A warp takes chunks from the pair counters'
+  // Packets (32 query ranks) in a persistent grid. A warp takes chunks from the pair counters'
   // packet dispenser; chunk c holds the packets c, c + C, c + 2C, ... (C chunks), so a contact region (consecutive
   // Morton ranks) is spread over many chunks. Lane j tests the union box of the chunk's packet j against the target
   // root (one load per lane for the packets far from the target), then the warp walks the survivors one after the
@@ -390,14 +367,332 @@ __global__ void __launch_bounds__( kTravThreads, kTravBlocksPerSM< K, T, LAZY > 
     for ( unsigned m = __ballot_sync( 0xffffffffu, o ); m; m &= m - 1 )
     {
       const uint32_t p = c + static_cast< uint32_t >( __ffs( m ) - 1 ) * chunks;
-      traverse_packet< K, T, VT, LAZY >( x, p * 32 + lane, lane, stack, cache, rb );
+      traverse_packet< K, T, VT >( x, p * 32 + lane, lane, stack, cache, rb );
     }
   }
 }
 
+// ---- dense contact: both objects' element slabs stored ----------------------------------------------------------
+//
+// In dense contact a packet's walk visits a few hundred internal nodes and tens of leaf buckets, each shared by only
+// a fraction of the packet's 32 queries. Two changes over the walk of traverse_packet:
+//   - Nodes in batches. Each step pops up to kDenseBatch (node, lane mask) entries from the stack; the warp copies
+//     their rows (both children's slabs) into shared memory with one round of 16-byte asynchronous copies, and every
+//     lane tests its query against the children of each popped node whose mask holds it, from shared memory. One
+//     global round trip serves the whole batch instead of one per chunk of slabs per node.
+//   - Leaves in batches. The walk only queues (bucket, lane mask) entries; a flush spreads all (query, element)
+//     tests of the queued entries over the warp's lanes, 32 at a time, with every query's slabs staged in shared
+//     memory and the target elements' stored rows read from global memory. Hits leave through one ballot and one
+//     atomic per 32 tests.
+// The stack grows by at most kDenseBatch entries per step, so its depth bound is kDenseStack; a walk that would pass
+// it raises kErrOverflowStack, and the host then runs the pair search again with the single-node walk (whose stack
+// is bounded by the tree depth).
+constexpr int kLeafQueue = 32;  // queued (bucket, mask) entries per warp
+
+// A (min, max) pair: from global memory (read-only path) or from shared memory, as one vector load.
+__device__ __forceinline__ void load_pair(const double *p, double &lo, double &hi)
+{
+  const double2 v = __ldg( reinterpret_cast< const double2 * >( p ) );
+  lo = v.x;
+  hi = v.y;
+}
+__device__ __forceinline__ void load_pair(const float *p, float &lo, float &hi)
+{
+  const float2 v = __ldg( reinterpret_cast< const float2 * >( p ) );
+  lo = v.x;
+  hi = v.y;
+}
+__device__ __forceinline__ void shared_pair(const double *p, double &lo, double &hi)
+{
+  const double2 v = *reinterpret_cast< const double2 * >( p );
+  lo = v.x;
+  hi = v.y;
+}
+__device__ __forceinline__ void shared_pair(const float *p, float &lo, float &hi)
+{
+  const float2 v = *reinterpret_cast< const float2 * >( p );
+  lo = v.x;
+  hi = v.y;
+}
+constexpr int kDenseBatch = 4;  // nodes popped per step
+constexpr int kDenseStack = 256;
+
 template< int K, typename T >
-cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, double eps, uint2 *pairs, uint64_t cap,
-                          pair_scalars *ps, cudaStream_t s)
+struct dense_smem
+{
+  T q[32][K];                           // query slabs of the packet, (min, max) per slab
+  T rows[kDenseBatch][2 * K];           // node rows of the batch: [slab][child][min, max]
+  uint32_t qe[32];                      // query element indices
+  int2 stack[kDenseStack];              // (node, lane mask)
+  int2 leaf[kLeafQueue];                // (bucket, lane mask)
+  uint32_t pre[kLeafQueue];             // exclusive prefix of the entries' test counts (8 per query)
+};
+
+// Tests every (query, element) pair of the queued entries; i0 = the packet's first query rank.
+template< int K, typename T >
+__device__ __forceinline__ void flush_leaves(const trav_args< T > &x, dense_smem< K, T > &sm, int nleaf, uint32_t i0,
+                                             unsigned lane)
+{
+  constexpr int D = K / 2;
+  __syncwarp();
+  const int2 ent = static_cast< int >( lane ) < nleaf ? sm.leaf[lane] : make_int2( 0, 0 );
+  const uint32_t c = 8u * static_cast< uint32_t >( __popc( static_cast< unsigned >( ent.y ) ) );
+  uint32_t inc = c;
+#pragma unroll
+  for ( int o = 1; o < 32; o <<= 1 )
+  {
+    const uint32_t y = __shfl_up_sync( 0xffffffffu, inc, o );
+    if ( lane >= static_cast< unsigned >( o ) ) inc += y;
+  }
+  if ( static_cast< int >( lane ) < nleaf ) sm.pre[lane] = inc - c;
+  const uint32_t total = __shfl_sync( 0xffffffffu, inc, 31 );
+  __syncwarp();
+  const unsigned lt = ( 1u << lane ) - 1u;
+  for ( uint32_t base = 0; base < total; base += 32 )
+  {
+    const uint32_t g = base + lane;
+    bool hit = false;
+    uint32_t q = 0, r = 0;
+    if ( g < total )
+    {
+      int lo = 0, hi = nleaf - 1;  // the last entry whose prefix is <= g
+      while ( lo < hi )
+      {
+        const int mid = ( lo + hi + 1 ) >> 1;
+        if ( sm.pre[mid] <= g ) lo = mid;
+        else hi = mid - 1;
+      }
+      const uint32_t rr = g - sm.pre[lo];
+      const int2 en = sm.leaf[lo];
+      unsigned m = static_cast< unsigned >( en.y );
+      for ( uint32_t k = rr >> 3; k > 0; --k ) m &= m - 1;  // the (rr / 8)-th query of the entry's mask
+      q = static_cast< uint32_t >( __ffs( m ) - 1 );
+      r = static_cast< uint32_t >( en.x ) * kLeafSize + ( rr & 7u );
+      if ( r < x.nt && ( !x.self || r > i0 + q ) )
+      {
+        // a chunk of slabs of the element (global) and of the query (shared) is loaded before it is tested
+        const T *er = x.tcache + static_cast< size_t >( r >> 3 ) * ( kLeafSize * K ) + 2 * ( r & 7u );
+        const T *qr = sm.q[q];
+        hit = true;
+#pragma unroll
+        for ( int a0 = 0; a0 < D; a0 += kNodeChunk< K, T > )
+        {
+          if ( !hit ) break;
+          T ev[2 * kNodeChunk< K, T >], qv[2 * kNodeChunk< K, T >];
+#pragma unroll
+          for ( int j = 0; j < kNodeChunk< K, T >; ++j )
+          {
+            if ( a0 + j >= D ) break;
+            load_pair( er + 2 * kLeafSize * ( a0 + j ), ev[2 * j], ev[2 * j + 1] );
+            shared_pair( qr + 2 * ( a0 + j ), qv[2 * j], qv[2 * j + 1] );
+          }
+#pragma unroll
+          for ( int j = 0; j < kNodeChunk< K, T >; ++j )
+          {
+            if ( a0 + j >= D ) break;
+            hit = hit && qv[2 * j] < ev[2 * j + 1] && ev[2 * j] < qv[2 * j + 1];
+          }
+        }
+      }
+    }
+    const unsigned bal = __ballot_sync( 0xffffffffu, hit );
+    if ( bal )
+    {
+      unsigned long long pos = 0;
+      if ( lane == 0 ) pos = atomicAdd( &x.ps->count, static_cast< unsigned long long >( __popc( bal ) ) );
+      pos = __shfl_sync( 0xffffffffu, pos, 0 ) + static_cast< unsigned >( __popc( bal & lt ) );
+      if ( hit && pos < x.cap ) x.pairs[pos] = make_uint2( sm.qe[q], __ldg( x.tperm + r ) );
+    }
+  }
+  __syncwarp();
+}
+
+// One packet in dense contact (see above). Returns false when the stack bound was reached (error raised).
+template< int K, typename T >
+__device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, const uint32_t i0, const unsigned lane,
+                                                       dense_smem< K, T > &sm, const T *rb)
+{
+  constexpr int D = K / 2;
+  constexpr int D0 = D < 4 ? D : 4;
+  constexpr int R16 = 2 * K * static_cast< int >( sizeof( T ) ) / 16;  // 16-byte pieces of a node row
+  const uint32_t i = i0 + lane;
+  {
+    const T *wb = x.qwarp + static_cast< size_t >( i0 >> 5 ) * K;
+    bool o = true;
+#pragma unroll
+    for ( int a = 0; a < D0; ++a ) o = o && ( __ldg( wb + 2 * a ) < rb[2 * a + 1] && rb[2 * a] < __ldg( wb + 2 * a + 1 ) );
+    if ( !o ) return;
+#pragma unroll
+    for ( int a = D0; a < D; ++a ) o = o && ( __ldg( wb + 2 * a ) < rb[2 * a + 1] && rb[2 * a] < __ldg( wb + 2 * a + 1 ) );
+    if ( !o ) return;
+  }
+  const bool valid = i < x.nq;
+  T qlo[D], qhi[D];
+  bool in_root = valid;
+  {
+    const uint32_t iv = valid ? i : 0u;
+    const T *qs = x.qrows + static_cast< size_t >( iv >> 3 ) * ( kLeafSize * K ) + 2 * ( iv & 7u );
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      load_pair( qs + 2 * kLeafSize * a, qlo[a], qhi[a] );
+      if ( !valid )
+      {
+        qlo[a] = T( 0 );
+        qhi[a] = T( 0 );
+      }
+      sm.q[lane][2 * a] = qlo[a];
+      sm.q[lane][2 * a + 1] = qhi[a];
+      in_root = in_root && ( qlo[a] < rb[2 * a + 1] && rb[2 * a] < qhi[a] );
+    }
+  }
+  sm.qe[lane] = valid ? __ldg( x.qperm + i ) : 0u;
+  const unsigned mask = __ballot_sync( 0xffffffffu, in_root );
+  if ( !mask ) return;
+  const int root = x.tsc->root;
+  int nleaf = 0;
+  if ( root < 0 )
+  {
+    if ( lane == 0 ) sm.leaf[0] = make_int2( ~root, static_cast< int >( mask ) );
+    flush_leaves< K, T >( x, sm, 1, i0, lane );
+    return;
+  }
+  if ( lane == 0 ) sm.stack[0] = make_int2( root, static_cast< int >( mask ) );
+  int sp = 1;
+  while ( sp > 0 )
+  {
+    __syncwarp();
+    const int nb = sp < kDenseBatch ? sp : kDenseBatch;
+    sp -= nb;
+    // the batch's node rows into shared memory (one round of asynchronous copies), their links into registers
+    for ( int t = static_cast< int >( lane ); t < nb * R16; t += 32 )
+    {
+      const int k = t / R16, piece = t - k * R16;
+      const int node = sm.stack[sp + k].x;
+      cp_async16( reinterpret_cast< char * >( sm.rows[k] ) + 16 * piece,
+                  reinterpret_cast< const char * >( x.nbox + static_cast< size_t >( node ) * 2 * K ) + 16 * piece );
+    }
+    int2 links = make_int2( 0, 0 ), span = make_int2( 0, 0 );
+    if ( static_cast< int >( lane ) < nb )
+    {
+      const int node = sm.stack[sp + lane].x;
+      links = __ldg( x.child + node );
+      if ( x.self ) span = make_int2( node, __ldg( &x.range[node].y ) );
+    }
+    unsigned emask[kDenseBatch];
+#pragma unroll
+    for ( int k = 0; k < kDenseBatch; ++k ) emask[k] = k < nb ? static_cast< unsigned >( sm.stack[sp + k].y ) : 0u;
+    cp_async_wait_all();
+    __syncwarp();
+    unsigned m0[kDenseBatch], m1[kDenseBatch];
+#pragma unroll
+    for ( int k = 0; k < kDenseBatch; ++k )
+    {
+      bool o0 = ( emask[k] >> lane ) & 1u, o1 = o0;
+      if ( x.self )
+      {
+        // left child covers buckets [l, node], right child [node + 1, r]: skip subtrees whose last rank <= i
+        const int node = __shfl_sync( 0xffffffffu, span.x, k ), last = __shfl_sync( 0xffffffffu, span.y, k );
+        o0 = o0 && kLeafSize * node + kLeafSize - 1 > static_cast< int >( i );
+        o1 = o1 && min( kLeafSize * last + kLeafSize - 1, static_cast< int >( x.nt ) - 1 ) > static_cast< int >( i );
+      }
+      // a chunk of slabs of the row is read from shared memory before it is tested
+      const T *row = sm.rows[k];
+#pragma unroll
+      for ( int a0 = 0; a0 < D; a0 += kNodeChunk< K, T > )
+      {
+        if ( !( o0 || o1 ) ) break;
+        T v[4 * kNodeChunk< K, T >];
+#pragma unroll
+        for ( int j = 0; j < kNodeChunk< K, T >; ++j )
+        {
+          if ( a0 + j >= D ) break;
+          shared_pair( row + 4 * ( a0 + j ), v[4 * j], v[4 * j + 1] );
+          shared_pair( row + 4 * ( a0 + j ) + 2, v[4 * j + 2], v[4 * j + 3] );
+        }
+#pragma unroll
+        for ( int j = 0; j < kNodeChunk< K, T >; ++j )
+        {
+          if ( a0 + j >= D ) break;
+          o0 = o0 && ( qlo[a0 + j] < v[4 * j + 1] && v[4 * j] < qhi[a0 + j] );
+          o1 = o1 && ( qlo[a0 + j] < v[4 * j + 3] && v[4 * j + 2] < qhi[a0 + j] );
+        }
+      }
+      m0[k] = __ballot_sync( 0xffffffffu, o0 );
+      m1[k] = __ballot_sync( 0xffffffffu, o1 );
+    }
+    // children: buckets to the leaf queue, internal nodes onto the stack (warp-uniform; lane 0 writes)
+#pragma unroll
+    for ( int k = 0; k < kDenseBatch; ++k )
+    {
+      const int cx = __shfl_sync( 0xffffffffu, links.x, k ), cy = __shfl_sync( 0xffffffffu, links.y, k );
+#pragma unroll
+      for ( int side = 0; side < 2; ++side )
+      {
+        const unsigned m = side ? m1[k] : m0[k];
+        const int ch = side ? cy : cx;
+        if ( !m ) continue;
+        if ( ch < 0 )
+        {
+          if ( lane == 0 ) sm.leaf[nleaf] = make_int2( ~ch, static_cast< int >( m ) );
+          ++nleaf;
+        } else {
+          if ( sp >= x.dense_stack )
+          {
+            if ( lane == 0 ) atomicCAS( &x.ps->error, 0, kErrOverflowStack );
+            return;
+          }
+          if ( lane == 0 ) sm.stack[sp] = make_int2( ch, static_cast< int >( m ) );
+          ++sp;
+        }
+      }
+    }
+    if ( nleaf > kLeafQueue - 2 * kDenseBatch )
+    {
+      flush_leaves< K, T >( x, sm, nleaf, i0, lane );
+      nleaf = 0;
+    }
+  }
+  if ( nleaf > 0 ) flush_leaves< K, T >( x, sm, nleaf, i0, lane );
+}
+
+// Resident blocks per SM of the dense walk: as many as its shared memory allows (228 KB per SM, 1 KB of it reserved
+// per block), at most 6; the register budget follows from it.
+template< int K, typename T >
+constexpr int kDenseBlocksPerSM =
+  ( 228 * 1024 ) / ( ( kTravThreads / 32 ) * static_cast< int >( sizeof( dense_smem< K, T > ) ) + 1024 ) < 6
+    ? ( 228 * 1024 ) / ( ( kTravThreads / 32 ) * static_cast< int >( sizeof( dense_smem< K, T > ) ) + 1024 )
+    : 6;
+
+// Dense contact: one warp per packet of 32 query ranks (the hardware balances the walks).
+template< int K, typename T >
+__global__ void __launch_bounds__( kTravThreads, kDenseBlocksPerSM< K, T > ) k_traverse_stored(const trav_args< T > x,
+                                                                                               const obj_scalars *__restrict__ qsc)
+{
+  constexpr int D = K / 2;
+  constexpr int D0 = D < 4 ? D : 4;
+  constexpr int WPB = kTravThreads / 32;
+  __shared__ __align__( 16 ) dense_smem< K, T > s_dense[WPB];
+  const unsigned lane = threadIdx.x & 31u;
+  if ( *reinterpret_cast< const volatile int * >( &x.tsc->error ) == kErrTimeout ||
+       *reinterpret_cast< const volatile int * >( &qsc->error ) == kErrTimeout )
+    return;
+  const T *rb = reinterpret_cast< const T * >( x.tsc->root_box );
+  {
+    const T *qr = reinterpret_cast< const T * >( qsc->root_box );
+    bool o = true;
+#pragma unroll
+    for ( int a = 0; a < D0; ++a ) o = o && ( qr[2 * a] < rb[2 * a + 1] && rb[2 * a] < qr[2 * a + 1] );
+    if ( !o ) return;
+  }
+  const uint32_t packets = ( x.nq + 31 ) / 32;
+  const uint32_t pk = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+  if ( pk < packets ) traverse_packet_stored< K, T >( x, pk * 32, lane, s_dense[threadIdx.x >> 5], rb );
+}
+
+template< int K, typename T >
+cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, bool dense, double eps, uint2 *pairs, uint64_t cap,
+                          pair_scalars *ps, cudaStream_t s, int dense_stack_limit)
 {
   trav_args< T > x;
   x.qwarp = static_cast< const T * >( q.warp_box );
@@ -421,29 +716,31 @@ cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, double eps, uint2
   x.pairs = pairs;
   x.cap = cap;
   x.ps = ps;
+  x.dense_stack = dense_stack_limit > 0 && dense_stack_limit < kDenseStack ? dense_stack_limit : kDenseStack;
   // Dense contact: one warp per packet. Sparse: a persistent grid of at most the resident blocks (4 per SM), one
   // warp per chunk of 32 packets at most.
   constexpr uint64_t kWarps = kTravThreads / 32;
   const uint64_t packets = ( q.n + 31 ) / 32;
   const uint64_t chunks = ( packets + 31 ) / 32;
-  const uint64_t resident = static_cast< uint64_t >( device_sm_count() ) * kTravBlocksPerSM< K, T, true >;
-  uint64_t blocks = ( q.stored && t.stored ) ? ( packets + kWarps - 1 ) / kWarps : ( chunks + kWarps - 1 ) / kWarps;
-  if ( !( q.stored && t.stored ) && blocks > resident ) blocks = resident;
+  const uint64_t resident = static_cast< uint64_t >( device_sm_count() ) * kTravBlocksPerSM;
+  dense = dense && q.stored && t.stored;
+  uint64_t blocks = dense ? ( packets + kWarps - 1 ) / kWarps : ( chunks + kWarps - 1 ) / kWarps;
+  if ( !dense && blocks > resident ) blocks = resident;
   const unsigned grid = static_cast< unsigned >( blocks < ( 1ull << 30 ) ? ( blocks ? blocks : 1 ) : ( 1ull << 30 ) );
-  // both objects' element slabs stored (dense contact): the variant that only reads them; else the one that
+  // both objects' element slabs stored (dense contact): the batched walk that only reads them; else the one that
   // computes the slabs it tests from the vertices (unrolled when both objects have the same vertex count)
-  if ( q.stored && t.stored )
+  if ( dense )
   {
-    k_traverse< K, T, 3, false ><<< grid, kTravThreads, 0, s >>>( x, q.sc );
+    k_traverse_stored< K, T ><<< grid, kTravThreads, 0, s >>>( x, q.sc );
     return cudaGetLastError();
   }
   const uint32_t V = q.V == t.V ? q.V : 0;
   switch ( V )
   {
-    case 3: k_traverse< K, T, 3, true ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
-    case 4: k_traverse< K, T, 4, true ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
-    case 8: k_traverse< K, T, 8, true ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
-    default: k_traverse< K, T, 0, true ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+    case 3: k_traverse< K, T, 3 ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+    case 4: k_traverse< K, T, 4 ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+    case 8: k_traverse< K, T, 8 ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+    default: k_traverse< K, T, 0 ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
   }
   return cudaGetLastError();
 }
@@ -590,17 +887,17 @@ cudaError_t launch_gather_words(const int *const *src, int n, int *dst, cudaStre
   return cudaGetLastError();
 }
 
-cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, double eps, uint2 *pairs,
-                            uint64_t cap, pair_scalars *ps, cudaStream_t s)
+cudaError_t launch_traverse(int K, bool fp32, tree_view q, tree_view t, bool self, bool dense, double eps, uint2 *pairs,
+                            uint64_t cap, pair_scalars *ps, cudaStream_t s, int dense_stack_limit)
 {
   switch ( K )
   {
-    case 6: return fp32 ? launch_trav_t< 6, float >( q, t, self, eps, pairs, cap, ps, s )
-                        : launch_trav_t< 6, double >( q, t, self, eps, pairs, cap, ps, s );
-    case 18: return fp32 ? launch_trav_t< 18, float >( q, t, self, eps, pairs, cap, ps, s )
-                         : launch_trav_t< 18, double >( q, t, self, eps, pairs, cap, ps, s );
-    case 26: return fp32 ? launch_trav_t< 26, float >( q, t, self, eps, pairs, cap, ps, s )
-                         : launch_trav_t< 26, double >( q, t, self, eps, pairs, cap, ps, s );
+    case 6: return fp32 ? launch_trav_t< 6, float >( q, t, self, dense, eps, pairs, cap, ps, s, dense_stack_limit )
+                        : launch_trav_t< 6, double >( q, t, self, dense, eps, pairs, cap, ps, s, dense_stack_limit );
+    case 18: return fp32 ? launch_trav_t< 18, float >( q, t, self, dense, eps, pairs, cap, ps, s, dense_stack_limit )
+                         : launch_trav_t< 18, double >( q, t, self, dense, eps, pairs, cap, ps, s, dense_stack_limit );
+    case 26: return fp32 ? launch_trav_t< 26, float >( q, t, self, dense, eps, pairs, cap, ps, s, dense_stack_limit )
+                         : launch_trav_t< 26, double >( q, t, self, dense, eps, pairs, cap, ps, s, dense_stack_limit );
     default: return cudaErrorInvalidValue;
   }
 }

@@ -120,8 +120,9 @@ constexpr int kSlabThreads = 128;  // ranks per block of the element slab kernel
 // Element slabs in rank order, one thread per rank (the element perm[r] of rank r), staged in shared memory (padded
 // to C + 1 components against bank conflicts); per block of 128 ranks, the unions of its 16 leaf buckets and its 4
 // query groups of 32 ranks are written out coalesced: bucket_box row b and warp_box row g each hold the C = 2 D
-// values (min, max) per slab. The element slabs themselves go to elem_rows (row r: rank r) only when given (objects
-// in dense contact, whose traversals test most buckets); otherwise the traversal computes the few it tests from the
+// values (min, max) per slab. The element slabs themselves go to elem_rows (slab-major per leaf bucket: rank
+// r = 8 b + j, slab a at elem_rows[b * 8 C + 16 a + 2 j + {0 min, 1 max}]) only when given (objects in dense
+// contact, whose traversals test most buckets); otherwise the traversal computes the few it tests from the
 // vertices. A one-bucket object also gets its root box here. A rank whose index is not an element index marks a failed sort.
 template< int K, typename T, int VT >
 __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( VT == 8 ? 3 : 4 ) ) k_elem_slabs(const double *__restrict__ verts, uint32_t Vrt,
@@ -168,11 +169,16 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
   __syncthreads();
   if ( elem_rows )
   {
+    // slab-major per leaf bucket: [bucket][slab][element j < 8][min, max], so the 8 elements' values of one slab are
+    // contiguous (the dense traversal reads them 8 lanes at a time)
     T *eb = elem_rows + static_cast< size_t >( r0 ) * C;
-    for ( int k = tid; k < rows * C; k += kSlabThreads )
+    const int nbk = ( rows + kLeafSize - 1 ) / kLeafSize;
+    for ( int k = tid; k < nbk * kLeafSize * C; k += kSlabThreads )
     {
-      const int q = k / C;
-      eb[k] = s_el[q * P + ( k - q * C )];
+      const int lb = k / ( kLeafSize * C ), rem = k - lb * ( kLeafSize * C );
+      const int a = rem / ( 2 * kLeafSize ), j = ( rem >> 1 ) & ( kLeafSize - 1 ), side = rem & 1;
+      const int q = lb * kLeafSize + j;
+      if ( q < rows ) eb[k] = s_el[q * P + 2 * a + side];
     }
   }
   // bucket unions (ranks in order, as the serial union of the reference merges them)

@@ -201,6 +201,9 @@ BVHG_API bvhg_status bvhg_set_spin_limit(bvhg_ctx *ctx, uint32_t limit);
 /* Test hook: when enabled, every radix-sort look-back after the first tile polls a status word that no block
  * publishes, so the bounded wait runs out and the build reports BVHG_ERR_TIMEOUT (the context stays usable). */
 BVHG_API bvhg_status bvhg_test_stall_sort(bvhg_ctx *ctx, int32_t enable);
+/* Test hook: lowers the stack bound of the dense-contact walk to `limit` entries (0 restores it), so that it is
+ * reached and the library's fallback to the single-node walk runs (the pair set stays exact). */
+BVHG_API bvhg_status bvhg_test_dense_stack(bvhg_ctx *ctx, int32_t limit);
 
 /* Stable sort of n device-resident 64-bit keys (Morton keys or any others): keys_out[r] is the r-th smallest key,
  * perm_out[r] its index in keys_in (ties keep input order). No counterpart in the reference: it is the library's

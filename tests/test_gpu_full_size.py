@@ -20,15 +20,20 @@ pytestmark = pytest.mark.gpu
 
 
 def gpu_pairs(a, b, k, precision):
+    """Pair sets of two builds: the first traversal computes the element slabs it tests; when it finds the contact
+    dense, the second build stores every element's slabs and the second traversal reads them."""
     with bvhg.Context(k=k, precision=precision) as ctx:
         oa, ob = ctx.object(), ctx.object()
         ctx.set_elements(oa, a)
         ctx.set_elements(ob, b)
         ctx.build(oa)
         ctx.build(ob)
-        pairs = orc.canonical(ctx.broadphase(oa, ob))
+        first = orc.canonical(ctx.broadphase(oa, ob))
+        ctx.build(oa)
+        ctx.build(ob)
+        second = orc.canonical(ctx.broadphase(oa, ob))
         _, perm, mn, inv = ctx.morton(oa, a.shape[0])
-    return pairs, perm, mn, inv
+    return (first, second), perm, mn, inv
 
 
 def check_scene(a, b, k):
@@ -37,9 +42,11 @@ def check_scene(a, b, k):
     okeys = orc.morton_keys(orc.centroids(a), *orc.morton_bounds(orc.kdops(a, k), k))
     operm = orc.stable_perm(okeys)
     for precision in (bvhg.PLAIN_FP64, bvhg.FILTER_FP32):
-        got, perm, _, _ = gpu_pairs(a, b, k, precision)
-        assert got.shape == want.shape, f"precision {precision}: {got.shape[0]} pairs, oracle {want.shape[0]}"
-        assert np.array_equal(got, want), f"precision {precision}: pair set differs from the oracle"
+        sets, perm, _, _ = gpu_pairs(a, b, k, precision)
+        for which, got in zip(("first", "second"), sets):
+            assert got.shape == want.shape, f"precision {precision}, {which} build: {got.shape[0]} pairs, " \
+                                            f"oracle {want.shape[0]}"
+            assert np.array_equal(got, want), f"precision {precision}, {which} build: pair set differs"
         assert np.array_equal(perm, operm), f"precision {precision}: Morton permutation differs"
 
 

@@ -418,16 +418,18 @@ def test_precision_form_on_the_tet_lattice():
 
 
 @pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
-def test_stored_and_computed_element_slabs_agree(precision):
+@pytest.mark.parametrize("k", [6, 18, 26])
+def test_stored_and_computed_element_slabs_agree(precision, k):
     """Traversals compute the element slabs they test from the vertices (sparse contact) or read the ones the build
-    stored (dense contact, decided from the previous broadphase's candidate count): both give the exact set."""
+    stored (dense contact, decided from the previous broadphase's candidate count; the walk then queues its leaf
+    buckets and tests them in batches): both give the exact set."""
     m = 14
     xyz = meshes.tet_lattice(m)
     even = meshes.checkerboard(m)
     a, b = np.ascontiguousarray(xyz[even]), np.ascontiguousarray(xyz[~even])
-    want = orc.pair_set(a, b, 26)
-    want_self = orc.self_pair_set(a, 26)
-    with bvhg.Context(k=26, precision=precision) as ctx:
+    want = orc.pair_set(a, b, k)
+    want_self = orc.self_pair_set(a, k)
+    with bvhg.Context(k=k, precision=precision) as ctx:
         for step in range(3):  # first build: computed; later builds: stored (the contact is dense)
             oa, ob = (build_pair(ctx, a, b) if step == 0 else (oa, ob))
             if step:
@@ -477,3 +479,30 @@ def test_signed_zeros_and_exact_cancellations(k, V, eps):
         check_stages(ctx, oa, a, k, eps)
         check_stages(ctx, ob, b, k, eps)
         assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b, k, eps))
+
+
+@pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
+def test_dense_walk_stack_bound_falls_back(precision):
+    """The dense-contact walk pops several nodes per step, so its stack can grow past the tree depth; when it
+    reaches its bound the library searches again with the single-node walk. A test hook lowers the bound until
+    it is reached: the pair sets (inter-object, self, and in a batch) stay exact."""
+    m = 14
+    xyz = meshes.tet_lattice(m)
+    even = meshes.checkerboard(m)
+    a, b = np.ascontiguousarray(xyz[even]), np.ascontiguousarray(xyz[~even])
+    want = orc.pair_set(a, b, 18)
+    with bvhg.Context(k=18, precision=precision) as ctx:
+        ctx.test_dense_stack(3)
+        oa, ob = build_pair(ctx, a, b)
+        assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), want)  # dense from now on
+        for _ in range(2):
+            ctx.build(oa)
+            ctx.build(ob)
+            assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), want)
+            assert np.array_equal(orc.canonical(ctx.self_collision(oa)), orc.self_pair_set(a, 18))
+    with bvhg.Context(k=18, precision=precision) as ctx:
+        ctx.test_dense_stack(3)
+        oa, ob = build_pair(ctx, a, b)
+        for _ in range(3):
+            got = ctx.batch_broadphase([(oa, ob)])
+            assert np.array_equal(orc.canonical(got[0]), want)
