@@ -9,6 +9,7 @@ first use raises ImportError when libbvhg.so is missing. Importing only the mesh
 (`from distbvh_b200 import meshes`) does not load the CUDA library.
 """
 _ABI_NAMES = (
+    "OK", "ERR_ARG", "ERR_CUDA", "ERR_OVERFLOW", "ERR_TIMEOUT", "ERR_STATE", "ERR_NOMEM",
     "BvhgError", "Context", "EXPORTS", "FILTER_FP32", "MEM_DEVICE", "MEM_HOST", "PLAIN_FP64", "REBUILD", "REFIT",
     "STAGES", "debug_normal", "lib", "LIB_PATH",
 )

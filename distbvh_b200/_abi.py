@@ -26,6 +26,7 @@ EXPORTS = (
     "bvhg_get_stage_times", "bvhg_launch_count", "bvhg_set_spin_limit", "bvhg_test_stall_sort", "bvhg_debug_normal",
     "bvhg_synchronize", "bvhg_last_error", "bvhg_status_string", "bvhg_radix_sort_noalloc",
     "bvhg_batch_broadphase", "bvhg_batch_autotune", "bvhg_sort_and_sweep", "bvhg_test_dense_stack",
+    "bvhg_cluster", "bvhg_patch_pairs",
 )
 
 
@@ -74,6 +75,8 @@ def _load():
         "bvhg_set_spin_limit": (I32, [P, U32]),
         "bvhg_test_stall_sort": (I32, [P, I32]),
         "bvhg_test_dense_stack": (I32, [P, I32]),
+        "bvhg_cluster": (I32, [P, I32, U32, P, P, I32]),
+        "bvhg_patch_pairs": (I32, [P, I32, I32, P, U64, ctypes.POINTER(U64), P, U64, ctypes.POINTER(U64), I32]),
         "bvhg_debug_normal": (I32, [I32, I32, I32, P, P, P]),
         "bvhg_synchronize": (I32, [P]),
         "bvhg_last_error": (ctypes.c_char_p, [P]),
@@ -259,6 +262,26 @@ class Context:
         self._check(lib.bvhg_batch_autotune(self._h, len(scenes), a.ctypes.data, b.ctypes.data, mode,
                                             ctypes.byref(lanes), ctypes.byref(ms)))
         return lanes.value, ms.value
+
+    def cluster(self, obj, patches, n):
+        """Patches of a built object: (bounds (patches + 1,) uint64, order (n,) uint32)."""
+        bounds = np.empty(patches + 1, dtype=np.uint64)
+        order = np.empty(max(n, 1), dtype=np.uint32)
+        self._check(lib.bvhg_cluster(self._h, obj, patches, bounds.ctypes.data, order.ctypes.data, MEM_HOST))
+        return bounds, order[:n]
+
+    def patch_pairs(self, a, b):
+        """Element pairs grouped by patch pair: (groups (g, 4) uint32 rows (patch a, patch b, first, count),
+        pairs (m, 2) uint32 of (position in patch a, position in patch b))."""
+        ng, npairs = ctypes.c_uint64(), ctypes.c_uint64()
+        st = lib.bvhg_patch_pairs(self._h, a, b, None, 0, ctypes.byref(ng), None, 0, ctypes.byref(npairs), MEM_HOST)
+        if st not in (OK, ERR_OVERFLOW):
+            self._check(st)
+        groups = np.empty((max(ng.value, 1), 4), dtype=np.uint32)
+        pairs = np.empty((max(npairs.value, 1), 2), dtype=np.uint32)
+        self._check(lib.bvhg_patch_pairs(self._h, a, b, groups.ctypes.data, ng.value, ctypes.byref(ng),
+                                         pairs.ctypes.data, npairs.value, ctypes.byref(npairs), MEM_HOST))
+        return groups[:ng.value], pairs[:npairs.value]
 
     def morton(self, obj, n):
         keys = np.empty(n, dtype=np.uint64)

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbvhg.so")
-SOURCES = ["bvhg_api.cu", "k_element.cu", "k_sort.cu", "k_tree.cu", "k_traverse.cu", "k_sweep.cu", "k_noalloc.cu"]
+SOURCES = ["bvhg_api.cu", "k_element.cu", "k_sort.cu", "k_tree.cu", "k_traverse.cu", "k_sweep.cu", "k_cluster.cu", "k_noalloc.cu"]
 HEADERS = ["bvhg_internal.cuh", "kdop_math.cuh", "bulk_copy.cuh", os.path.join("..", "..", "include", "bvhg.h")]
 
 NVCC_FLAGS = [

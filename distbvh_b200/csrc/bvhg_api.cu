@@ -75,6 +75,10 @@ struct object
   // The batched dense walk reached its stack bound on this object's tree: its traversals use the single-node walk
   // until the element count changes.
   bool dense_ok = true;
+  // Patches (bvhg_cluster): valid until the next set_elements or rebuild.
+  bool clustered = false;
+  uint32_t cl_patches = 0;
+  dev_buf cl_order, cl_rank, cl_tmp, cl_runs, cl_bhist, cl_bbase, cl_splits, cl_bounds, cl_scal;
   dev_buf verts_own, gid_own;
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
@@ -197,6 +201,8 @@ struct bvhg_ctx
   dev_buf sw_keys, sw_vals, sw_rows, sw_srows, sw_sbmax, sw_hist, sw_status, sw_sc, sw_params, sw_partial;
   // pairs
   dev_buf pairs, pairs2, pairs_out, pscal;
+  // element pairs grouped by patch pair
+  dev_buf grp_count, grp_off, grp_rows, grp_pairs, grp_scal;
   uint64_t pair_cap = 0, pair2_cap = 0;
   pair_scalars *host_ps = nullptr;  // pinned: pair counters + the two objects' error words after a broadphase
   int *host_err = nullptr;          // pinned [2]
@@ -458,6 +464,7 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
     const bvhg_status rs = reserve_object( ctx, o );
     if ( rs != BVHG_OK ) return rs;
   }
+  o.clustered = false;  // a rebuild recomputes the keys and their order
   {
     stage_scope st( ctx, BVHG_STAGE_BOUNDS );
     {
@@ -1058,6 +1065,7 @@ bvhg_status bvhg_set_elements(bvhg_ctx *ctx, int32_t obj, const double *xyz, uin
   o.built = false;
   o.fresh = false;
   o.has_data = true;
+  o.clustered = false;
   if ( n == 0 )
   {
     o.verts = nullptr;
@@ -1338,6 +1346,124 @@ bvhg_status bvhg_sort_and_sweep(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, int
     return emit_pairs( ctx, a, b, false, ctx->pairs.as< uint2 >(), np, pairs, capacity, count, mem );
   }
   return fail( ctx, BVHG_ERR_CUDA, "pair buffer did not converge" );
+}
+
+bvhg_status bvhg_cluster(bvhg_ctx *ctx, int32_t obj, uint32_t patches, uint64_t *bounds, uint32_t *order,
+                         int32_t mem)
+{
+  if ( !valid_obj( ctx, obj ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  if ( patches == 0 || patches > ( 1u << 24 ) ) return fail( ctx, BVHG_ERR_ARG, "patches must be in [1, 2^24]" );
+  if ( mem != BVHG_MEM_HOST && mem != BVHG_MEM_DEVICE ) return fail( ctx, BVHG_ERR_ARG, "bad memory kind" );
+  object &o = *ctx->objs[obj];
+  if ( !o.built || ( o.n > 0 && !o.topo ) ) return fail( ctx, BVHG_ERR_STATE, "cluster before a rebuild" );
+  cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, o );
+  const uint64_t n = o.n;
+  const uint64_t nb = cluster_block_count( n ) + 1;
+  BVHG_CUDA( ctx, o.cl_order.reserve( n * 4 ) );
+  BVHG_CUDA( ctx, o.cl_rank.reserve( n * 4 ) );
+  BVHG_CUDA( ctx, o.cl_tmp.reserve( n * 4 ) );
+  BVHG_CUDA( ctx, o.cl_runs.reserve( long_run_capacity( n ) * 4 ) );
+  BVHG_CUDA( ctx, o.cl_bhist.reserve( nb * 33 * 4 ) );
+  BVHG_CUDA( ctx, o.cl_bbase.reserve( nb * 2 * 4 ) );
+  BVHG_CUDA( ctx, o.cl_splits.reserve( static_cast< size_t >( patches ) * 4 ) );
+  BVHG_CUDA( ctx, o.cl_bounds.reserve( ( static_cast< size_t >( patches ) + 1 ) * 8 ) );
+  BVHG_CUDA( ctx, o.cl_scal.reserve( sizeof( cluster_scalars ) ) );
+  if ( n > 0 )
+  {
+    // the keys' order must be the build's valid one
+    const bvhg_status st = check_scalar_errors( ctx, o );
+    if ( st != BVHG_OK ) return st;
+  }
+  cluster_launch x;
+  x.keys = o.n ? o.sorted_keys() : nullptr;
+  x.perm = o.n ? o.sorted_vals() : nullptr;
+  x.n = n;
+  x.patches = patches;
+  x.order = o.cl_order.as< uint32_t >();
+  x.rank = o.cl_rank.as< uint32_t >();
+  x.tmp = o.cl_tmp.as< uint32_t >();
+  x.runs = o.cl_runs.as< uint32_t >();
+  x.bhist = o.cl_bhist.as< uint32_t >();
+  x.bbase = o.cl_bbase.as< uint32_t >();
+  x.splits = o.cl_splits.as< uint32_t >();
+  x.bounds = o.cl_bounds.as< uint64_t >();
+  x.cs = o.cl_scal.as< cluster_scalars >();
+  x.s = ctx->stream;
+  BVHG_CUDA( ctx, launch_cluster( x ) );
+  ctx->launches += 8;
+  const cudaMemcpyKind kind = mem == BVHG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  if ( bounds )
+    BVHG_CUDA( ctx, cudaMemcpyAsync( bounds, x.bounds, ( static_cast< size_t >( patches ) + 1 ) * 8, kind, ctx->stream ) );
+  if ( order && n ) BVHG_CUDA( ctx, cudaMemcpyAsync( order, x.order, n * 4, kind, ctx->stream ) );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
+  o.clustered = true;
+  o.cl_patches = patches;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_patch_pairs(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, uint32_t *groups, uint64_t group_capacity,
+                             uint64_t *group_count, uint32_t *pairs, uint64_t pair_capacity, uint64_t *pair_count,
+                             int32_t mem)
+{
+  if ( !valid_obj( ctx, obj_a ) || !valid_obj( ctx, obj_b ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  if ( obj_a == obj_b ) return fail( ctx, BVHG_ERR_ARG, "patch pairs need two distinct objects" );
+  if ( !group_count || !pair_count ) return fail( ctx, BVHG_ERR_ARG, "null count" );
+  if ( ( group_capacity > 0 && !groups ) || ( pair_capacity > 0 && !pairs ) )
+    return fail( ctx, BVHG_ERR_ARG, "null output buffer" );
+  if ( mem != BVHG_MEM_HOST && mem != BVHG_MEM_DEVICE ) return fail( ctx, BVHG_ERR_ARG, "bad memory kind" );
+  object &a = *ctx->objs[obj_a];
+  object &b = *ctx->objs[obj_b];
+  if ( !a.built || !b.built ) return fail( ctx, BVHG_ERR_STATE, "patch pairs before build" );
+  if ( !a.clustered || !b.clustered ) return fail( ctx, BVHG_ERR_STATE, "patch pairs before bvhg_cluster" );
+  cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, a );
+  join_object( ctx, b );
+  *group_count = 0;
+  *pair_count = 0;
+  if ( a.n == 0 || b.n == 0 )
+  {
+    ctx->last_candidates = 0;
+    return BVHG_OK;
+  }
+  const uint2 *lp = nullptr;
+  uint64_t np = 0;
+  bvhg_status st = find_pairs( ctx, a, b, false, &lp, &np );
+  if ( st != BVHG_OK ) return st;
+  note_density( a, b, false, ctx->last_candidates );
+  if ( np >= ( 1ull << 32 ) ) return fail( ctx, BVHG_ERR_ARG, "more than 2^32 - 1 pairs" );
+  const uint64_t bins = static_cast< uint64_t >( a.cl_patches ) * b.cl_patches;
+  const uint64_t rows = std::min< uint64_t >( bins, np );
+  cudaStream_t s = ctx->stream;
+  BVHG_CUDA( ctx, ctx->grp_count.reserve( bins * 4 ) );
+  BVHG_CUDA( ctx, ctx->grp_off.reserve( bins * 4 ) );
+  BVHG_CUDA( ctx, ctx->grp_rows.reserve( ( rows + 1 ) * 16 ) );
+  BVHG_CUDA( ctx, ctx->grp_pairs.reserve( ( np + 1 ) * 8 ) );
+  BVHG_CUDA( ctx, ctx->grp_scal.reserve( sizeof( cluster_scalars ) ) );
+  group_launch g;
+  g.bounds_a = a.cl_bounds.as< uint64_t >();
+  g.bounds_b = b.cl_bounds.as< uint64_t >();
+  g.rank_a = a.cl_rank.as< uint32_t >();
+  g.rank_b = b.cl_rank.as< uint32_t >();
+  g.patches_a = a.cl_patches;
+  g.patches_b = b.cl_patches;
+  cluster_scalars *cs = ctx->grp_scal.as< cluster_scalars >();
+  BVHG_CUDA( ctx, launch_group_pairs( lp, np, g, ctx->grp_count.as< uint32_t >(), ctx->grp_off.as< uint32_t >(),
+                                      ctx->grp_rows.as< uint32_t >(), rows, ctx->grp_pairs.as< uint32_t >(), cs, s ) );
+  ctx->launches += 3;
+  cluster_scalars h{};
+  BVHG_CUDA( ctx, cudaMemcpyAsync( &h, cs, sizeof( h ), cudaMemcpyDeviceToHost, s ) );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( s ) );
+  *group_count = h.groups;
+  *pair_count = np;
+  const cudaMemcpyKind kind = mem == BVHG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  if ( h.groups > group_capacity || np > pair_capacity )
+    return fail( ctx, BVHG_ERR_OVERFLOW, "patch pair buffers too small: " + std::to_string( h.groups ) + " groups, " +
+                                           std::to_string( np ) + " pairs" );
+  if ( h.groups ) BVHG_CUDA( ctx, cudaMemcpyAsync( groups, ctx->grp_rows.p, h.groups * 16, kind, s ) );
+  if ( np ) BVHG_CUDA( ctx, cudaMemcpyAsync( pairs, ctx->grp_pairs.p, np * 8, kind, s ) );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( s ) );
+  return BVHG_OK;
 }
 
 bvhg_status bvhg_get_morton(bvhg_ctx *ctx, int32_t obj, uint64_t *sorted_keys, uint32_t *perm, double *min3,

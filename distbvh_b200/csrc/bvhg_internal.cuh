@@ -106,6 +106,50 @@ cudaError_t launch_sort_runs(uint64_t *keys, uint32_t *vals, uint64_t *tkeys, ui
                              const uint32_t *runs, obj_scalars *sc, cudaStream_t s);
 inline uint64_t long_run_capacity(uint64_t n) { return n / 33 + 1; }
 
+// ---- patches (k_cluster.cu) ----
+struct cluster_scalars
+{
+  unsigned int runs;    // equal-hash runs listed for k_cluster_runs
+  unsigned int t;       // threshold split depth
+  unsigned int need;    // positions of depth t taken
+  unsigned int groups;  // non-empty patch pairs of the last grouping
+};
+
+// Arguments of the Morton clustering of one object (src/bvh/split/cluster.hpp:89-179) from its build's sorted keys.
+struct cluster_launch
+{
+  const uint64_t *keys;  // n sorted Morton keys (the build's)
+  const uint32_t *perm;  // n element indices in key order (the build's)
+  uint64_t n;
+  uint32_t patches;      // od_factor >= 1
+  uint32_t *order;       // n: element indices in patch order (stable by the 32-bit hash)
+  uint32_t *rank;        // n: position of every element in the patch order
+  uint32_t *tmp;         // n: scratch of the long-run sort
+  uint32_t *runs;        // n / 33 + 1: long equal-hash runs
+  uint32_t *bhist;       // cluster_block_count(n) * 33: per-block depth histograms
+  uint32_t *bbase;       // cluster_block_count(n) * 2
+  uint32_t *splits;      // max(patches - 1, 1)
+  uint64_t *bounds;      // patches + 1: patch p = positions [bounds[p], bounds[p + 1])
+  cluster_scalars *cs;
+  cudaStream_t s;
+};
+size_t cluster_block_count(uint64_t n);
+cudaError_t launch_cluster(const cluster_launch &x);
+
+// Two clustered objects: element pairs (local indices) grouped by patch pair.
+struct group_launch
+{
+  const uint64_t *bounds_a, *bounds_b;
+  const uint32_t *rank_a, *rank_b;
+  uint32_t patches_a, patches_b;
+};
+// pairs: np (a, b) local index pairs. bin_count, bin_off: patches_a * patches_b words each. groups: rows (patch a,
+// patch b, first pair, pair count) of the non-empty patch pairs in (a, b) order, at most group_cap (their number in
+// cs->groups). out: np (index in patch a, index in patch b) pairs grouped by patch pair.
+cudaError_t launch_group_pairs(const uint2 *pairs, uint64_t np, const group_launch &g, uint32_t *bin_count,
+                               uint32_t *bin_off, uint32_t *groups, uint64_t group_cap, uint32_t *out,
+                               cluster_scalars *cs, cudaStream_t s);
+
 // Passes of the sort that build() runs: those whose digit lies in the high key half (the fix-up sorts the rest).
 inline int sort_first_pass(int bits) { return 32 / bits; }
 

@@ -17,12 +17,13 @@
 //     get_entity_global_id(e)). The library computes the k-DOP exactly as kdop_base::from_vertices
 //     (src/bvh/kdop.hpp:238-264) with world_config::k (26 by default: the reference's bphase_kdop).
 //   - Patches: an object's elements are split into od_factor patches exactly as the reference's Morton clustering
-//     splits them (morton_cluster, src/bvh/split/cluster.hpp:89-179; every split algorithm uses it here). The
-//     functor is called once for every patch pair that holds at least one overlapping element pair (the reference
-//     calls it for every pair of overlapping patch k-DOPs, a superset), with both patches' elements as spans in
-//     the reference's order and, in addition, the exact element pairs of that patch pair
-//     (broadphase_collision::candidates, indices into the two spans). A functor that only reports overlapping
-//     elements gives the same results.
+//     splits them (morton_cluster, src/bvh/split/cluster.hpp:89-179; every split algorithm uses it here), on the
+//     device (bvhg_cluster). The functor is called once for every patch pair that holds at least one overlapping
+//     element pair (the reference calls it for every pair of overlapping patch k-DOPs, a superset), with both
+//     patches' elements as spans in the reference's order and, in addition, the exact element pairs of that patch
+//     pair (broadphase_collision::candidates, indices into the two spans; grouped by patch pair on the device,
+//     bvhg_patch_pairs; unordered within a patch pair). A functor that only reports overlapping elements gives
+//     the same results.
 //   - The element bytes handed to the functor are copies made at init_broadphase (the reference ships copies to
 //     the narrowphase rank too); the caller's array is read only during set_entity_data.
 //   - Errors throw bvhg::error (the reference asserts and terminates).
@@ -36,7 +37,6 @@
 #include <cstdint>
 #include <cstring>
 #include <functional>
-#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -202,46 +202,6 @@ const void *type_id()
   static const char id = 0;
   return &id;
 }
-// The reference's Morton clustering (src/bvh/split/cluster.hpp:89-179) from the library's sorted 63-bit keys and
-// permutation (order[r] = element of rank r): the 32-bit Morton hash of an element is its 63-bit key shifted right
-// by 33 (quantize32 keeps the top 10 of the 21 bits per axis); the order becomes the stable one of the hashes
-// (equal hashes in element order); the split depth of neighbours i, i + 1 is 31 - floor(log2(h_i ^ h_{i+1})) (all
-// ones for equal hashes); the P - 1 smallest depths (ties: the lower position) are the splits; and patch k spans
-// positions [split[k - 1], split[k]) of that order, as set_entity_data_impl cuts it
-// (src/bvh/collision_object.cpp:125-133). Returns the P + 1 patch boundaries.
-inline std::vector< std::size_t > morton_cluster(const std::vector< uint64_t > &keys, std::vector< uint32_t > &order,
-                                                 std::size_t P)
-{
-  const std::size_t n = keys.size();
-  for ( std::size_t r = 0; r < n; )
-  {
-    std::size_t e = r + 1;
-    while ( e < n && ( keys[e] >> 33 ) == ( keys[r] >> 33 ) ) ++e;
-    std::sort( order.begin() + r, order.begin() + e );
-    r = e;
-  }
-  const std::size_t nsplit = P - 1;
-  std::vector< std::size_t > split( nsplit, n > 0 ? n - 1 : 0 );
-  if ( n > 1 && nsplit > 0 )
-  {
-    std::vector< std::pair< uint32_t, uint32_t > > d( n - 1 );
-    for ( std::size_t i = 0; i + 1 < n; ++i )
-    {
-      const uint32_t mask = static_cast< uint32_t >( ( keys[i] >> 33 ) ^ ( keys[i + 1] >> 33 ) );
-      d[i] = { mask ? static_cast< uint32_t >( __builtin_clz( mask ) ) : 0xffffffffu, static_cast< uint32_t >( i ) };
-    }
-    const std::size_t take = std::min( nsplit, n - 1 );
-    std::nth_element( d.begin(), d.begin() + ( take - 1 ), d.end() );
-    std::vector< std::size_t > chosen;
-    for ( std::size_t k = 0; k < take; ++k ) chosen.push_back( d[k].second );
-    std::sort( chosen.begin(), chosen.end() );
-    for ( std::size_t k = 0; k < take; ++k ) split[k] = chosen[k];
-  }
-  std::vector< std::size_t > pbeg( P + 1, 0 );
-  for ( std::size_t k = 1; k < P; ++k ) pbeg[k] = split[k - 1];
-  pbeg[P] = n;
-  return pbeg;
-}
 }  // namespace detail
 
 class collision_world;
@@ -316,10 +276,8 @@ public:
   std::vector< std::vector< uint64_t > > patch_global_ids() const
   {
     std::vector< std::vector< uint64_t > > out( num_patches() );
-    std::vector< uint32_t > order( m_n );
-    for ( std::size_t i = 0; i < m_n; ++i ) order[m_rank[i]] = static_cast< uint32_t >( i );
     for ( std::size_t p = 0; p < out.size(); ++p )
-      for ( std::size_t r = m_pbeg[p]; r < m_pbeg[p + 1]; ++r ) out[p].push_back( m_gid[order[r]] );
+      for ( std::size_t r = m_pbeg[p]; r < m_pbeg[p + 1]; ++r ) out[p].push_back( m_gid[m_order[r]] );
     return out;
   }
 
@@ -337,11 +295,7 @@ private:
   collision_object(collision_world &w, std::size_t id);
   bvhg_ctx *ctx() const;
 
-  // the patch holding position r of the patch order, and where patch p starts (m_pbeg has od_factor + 1 entries)
-  std::size_t patch_of_rank(std::size_t r) const
-  {
-    return static_cast< std::size_t >( std::upper_bound( m_pbeg.begin(), m_pbeg.end(), r ) - m_pbeg.begin() ) - 1;
-  }
+  // where patch p starts in the patch order (m_pbeg has od_factor + 1 entries)
   std::size_t patch_begin(std::size_t p) const { return m_pbeg[p]; }
 
   collision_world &m_world;
@@ -352,7 +306,7 @@ private:
   std::vector< uint64_t > m_gid;
   std::vector< unsigned char > m_src;  // the caller's elements, original order
   detail::element_store m_elems;       // patch order (after init_broadphase)
-  std::vector< uint32_t > m_rank;      // position of element i in the patch order
+  std::vector< uint32_t > m_order;     // element index of every position of the patch order
   std::vector< std::size_t > m_pbeg;   // patch p = positions [m_pbeg[p], m_pbeg[p + 1])
   std::vector< narrowphase_result > m_results;
   std::vector< std::pair< uint64_t, uint64_t > > m_last_pairs;
@@ -448,60 +402,64 @@ inline std::size_t collision_object::num_patches() const noexcept { return m_wor
 inline void collision_object::init_broadphase()
 {
   detail::check( ctx(), bvhg_build( ctx(), m_obj, BVHG_REBUILD ), "init_broadphase" );
+  // patches by the reference's Morton clustering, cut on the device (bvhg_cluster): only the patch bounds and the
+  // element order come back
+  const std::size_t P = m_world.m_od;
+  std::vector< uint64_t > bounds( P + 1 );
   std::vector< uint32_t > order( m_n );
-  std::vector< uint64_t > keys( m_n );
-  if ( m_n )
-    detail::check( ctx(), bvhg_get_morton( ctx(), m_obj, keys.data(), order.data(), nullptr, nullptr ), "init_broadphase" );
-  m_pbeg = detail::morton_cluster( keys, order, m_world.m_od );
-  m_rank.assign( m_n, 0 );
+  detail::check( ctx(), bvhg_cluster( ctx(), m_obj, static_cast< uint32_t >( P ), bounds.data(), m_n ? order.data() : nullptr,
+                                      BVHG_MEM_HOST ),
+                 "init_broadphase" );
+  m_pbeg.assign( bounds.begin(), bounds.end() );
+  m_order = order;
   m_elems.bytes.assign( m_n * m_elems.elem_size, 0 );
   for ( std::size_t r = 0; r < m_n; ++r )
-  {
-    m_rank[order[r]] = static_cast< uint32_t >( r );
     std::memcpy( m_elems.bytes.data() + r * m_elems.elem_size, m_src.data() + order[r] * m_elems.elem_size,
                  m_elems.elem_size );
-  }
   m_built = true;
 }
 
 inline void collision_object::broadphase(collision_object &other)
 {
   if ( !m_built || !other.m_built ) throw error( BVHG_ERR_STATE, "broadphase before init_broadphase" );
-  // element pairs as local indices (the objects were given no library gids)
-  std::vector< uint64_t > buf( 2 * 4096 );
-  uint64_t count = 0;
-  bvhg_status s = bvhg_broadphase( ctx(), m_obj, other.m_obj, buf.data(), buf.size() / 2, &count, BVHG_MEM_HOST );
+  // the exact element pairs, grouped by patch pair on the device (bvhg_patch_pairs): rows (patch here, patch there,
+  // first pair, pair count) and pairs (position in this patch, position in the other patch)
+  std::vector< uint32_t > groups( 4 * 64 ), pairs( 2 * 4096 );
+  uint64_t ngroups = 0, npairs = 0;
+  bvhg_status s = bvhg_patch_pairs( ctx(), m_obj, other.m_obj, groups.data(), groups.size() / 4, &ngroups, pairs.data(),
+                                    pairs.size() / 2, &npairs, BVHG_MEM_HOST );
   if ( s == BVHG_ERR_OVERFLOW )
   {
-    buf.resize( 2 * count );
-    s = bvhg_broadphase( ctx(), m_obj, other.m_obj, buf.data(), count, &count, BVHG_MEM_HOST );
+    groups.resize( 4 * ngroups );
+    pairs.resize( 2 * npairs );
+    s = bvhg_patch_pairs( ctx(), m_obj, other.m_obj, groups.data(), ngroups, &ngroups, pairs.data(), npairs, &npairs,
+                          BVHG_MEM_HOST );
   }
   detail::check( ctx(), s, "broadphase" );
-  m_last_pairs.resize( count );
-  // group by patch pair; indices within the patches' rank-ordered spans
-  std::map< std::pair< std::size_t, std::size_t >, std::vector< std::pair< uint32_t, uint32_t > > > groups;
-  for ( uint64_t p = 0; p < count; ++p )
+  m_last_pairs.resize( npairs );
+  for ( uint64_t g = 0; g < ngroups; ++g )
   {
-    const std::size_t i = buf[2 * p], j = buf[2 * p + 1];
-    m_last_pairs[p] = { m_gid[i], other.m_gid[j] };
-    const std::size_t ra = m_rank[i], rb = other.m_rank[j];
-    const std::size_t pa = patch_of_rank( ra ), pb = other.patch_of_rank( rb );
-    groups[{ pa, pb }].emplace_back( static_cast< uint32_t >( ra - patch_begin( pa ) ),
-                                     static_cast< uint32_t >( rb - other.patch_begin( pb ) ) );
+    const std::size_t pa = groups[4 * g], pb = groups[4 * g + 1], first = groups[4 * g + 2], cnt = groups[4 * g + 3];
+    for ( std::size_t q = first; q < first + cnt; ++q )
+      m_last_pairs[q] = { m_gid[m_order[patch_begin( pa ) + pairs[2 * q]]],
+                          other.m_gid[other.m_order[other.patch_begin( pb ) + pairs[2 * q + 1]]] };
   }
   if ( !m_world.m_functor ) return;
   if ( m_world.m_functor_type != m_elems.type || m_world.m_functor_type != other.m_elems.type )
     throw error( BVHG_ERR_ARG, "narrowphase functor element type differs from the objects' element type" );
-  for ( auto &g : groups )
+  std::vector< std::pair< uint32_t, uint32_t > > cand;
+  for ( uint64_t g = 0; g < ngroups; ++g )
   {
-    const std::size_t pa = g.first.first, pb = g.first.second;
+    const std::size_t pa = groups[4 * g], pb = groups[4 * g + 1], first = groups[4 * g + 2], cnt = groups[4 * g + 3];
+    cand.resize( cnt );
+    for ( std::size_t q = 0; q < cnt; ++q ) cand[q] = { pairs[2 * ( first + q )], pairs[2 * ( first + q ) + 1] };
     const std::size_t a0 = patch_begin( pa ), a1 = patch_begin( pa + 1 );
     const std::size_t b0 = other.patch_begin( pb ), b1 = other.patch_begin( pb + 1 );
     const patch_meta ma{ m_id * m_world.m_od + pa, a1 - a0 }, mb{ other.m_id * m_world.m_od + pb, b1 - b0 };
     narrowphase_result_pair res = m_world.m_functor(
       *this, ma, m_elems.bytes.data() + a0 * m_elems.elem_size, a1 - a0, other, mb,
       other.m_elems.bytes.data() + b0 * other.m_elems.elem_size, b1 - b0,
-      span< const std::pair< uint32_t, uint32_t > >( g.second.data(), g.second.size() ) );
+      span< const std::pair< uint32_t, uint32_t > >( cand.data(), cand.size() ) );
     if ( res.a.size() ) m_results.push_back( std::move( res.a ) );
     if ( res.b.size() ) other.m_results.push_back( std::move( res.b ) );
   }

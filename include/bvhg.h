@@ -171,6 +171,27 @@ BVHG_API bvhg_status bvhg_batch_broadphase(bvhg_ctx *ctx, uint32_t nscenes, cons
 BVHG_API bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a, const int32_t *obj_b,
                                         int32_t mode, uint32_t *lanes, double *ms);
 
+/* Patches: the reference's Morton clustering of an object (morton_cluster, src/bvh/split/cluster.hpp:89-179, as
+ * set_entity_data_clustering uses it, src/bvh/collision_object.hpp:89-131), on the device from the last rebuild's
+ * keys. The elements are ordered stably by their 32-bit Morton hash (the 63-bit key >> 33; equal hashes in element
+ * order), and the order is cut at the `patches` - 1 neighbouring positions whose hashes split highest in the Morton
+ * tree (smallest 31 - floor(log2(h_i ^ h_i+1)); equal hashes last; ties by position); patch p holds positions
+ * [bounds[p], bounds[p + 1]) (src/bvh/collision_object.cpp:134-141). bounds (patches + 1 values, may be NULL) and
+ * order (n element indices in patch order, may be NULL) are in `mem`. The object keeps the patches for
+ * bvhg_patch_pairs until its next bvhg_set_elements or rebuild. Blocks until done. */
+BVHG_API bvhg_status bvhg_cluster(bvhg_ctx *ctx, int32_t obj, uint32_t patches, uint64_t *bounds, uint32_t *order,
+                                  int32_t mem);
+/* The exact element pairs of two clustered objects (the set of bvhg_broadphase) grouped by patch pair on the device,
+ * for a narrowphase functor per patch pair (collision_world::set_narrowphase_functor, src/bvh/collision_world.hpp:
+ * 58-94, run per patch pair in src/bvh/collision_object/impl.cpp:269-350). groups: 4 words per non-empty patch pair
+ * (patch in obj_a, patch in obj_b, first pair, pair count), in (patch a, patch b) order; pairs: 2 words per element
+ * pair (position in the patch of obj_a, position in the patch of obj_b; positions within a patch follow the
+ * patch order of bvhg_cluster), grouped in that order, unordered within a group. BVHG_ERR_OVERFLOW when either
+ * capacity is too small (*group_count and *pair_count are then the required sizes). Blocks until done. */
+BVHG_API bvhg_status bvhg_patch_pairs(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, uint32_t *groups,
+                                      uint64_t group_capacity, uint64_t *group_count, uint32_t *pairs,
+                                      uint64_t pair_capacity, uint64_t *pair_count, int32_t mem);
+
 /* Parity probes (host buffers). sorted_keys[r] and perm[r] (original index of rank r) may be NULL; min3/inv3 are
  * the Morton bounds (3 doubles each, may be NULL). Keys, permutation, bounds and centroids are those of the last
  * rebuild: a refit keeps the order and does not recompute them. The slab probes compute from the present

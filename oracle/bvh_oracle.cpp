@@ -878,6 +878,53 @@ std::int64_t orc_pipeline(const double *xa, std::uint64_t na, const double *xb, 
   return total;
 }
 
+// morton_cluster (src/bvh/split/cluster.hpp:89-179) with its hashes from morton_impl over the 32-bit type
+// (src/bvh/contact_entity.hpp:104-118: morton32(quantize32(centroid, min, inv_diag)), hash.hpp:106-110, 148-166):
+// the element indices stably sorted by hash; the depth of every neighbouring pair, 31 - floor(log2(h_i ^ h_{i+1}))
+// or all ones for equal hashes (cluster.hpp:143-151); the positions stably sorted by depth; the first `patches` - 1
+// of them, in position order, are the splits, and positions that cannot be chosen hold n - 1 (cluster.hpp:109-116,
+// 156-169). order_out receives the n element indices in hash order, bounds_out the patches + 1 patch boundaries
+// [0, splits..., n] (set_entity_data_impl, src/bvh/collision_object.cpp:134-141).
+void orc_morton_cluster(const double *centroids, std::uint64_t n, const double *min3, const double *inv3,
+                        std::uint32_t patches, std::uint32_t *order_out, std::uint64_t *bounds_out)
+{
+  const std::uint64_t nsplit = patches > 0 ? patches - 1 : 0;
+  std::vector< std::uint64_t > splits( nsplit, 0 );
+  std::vector< std::uint32_t > hash( n ), idx( n );
+  for ( std::uint64_t i = 0; i < n; ++i )
+  {
+    std::uint32_t q[3];
+    orc_quantize32( centroids + 3 * i, min3, inv3, q );
+    hash[i] = orc_morton32( q[0], q[1], q[2] );
+  }
+  std::iota( idx.begin(), idx.end(), 0u );
+  std::stable_sort( idx.begin(), idx.end(), [&hash](std::uint32_t a, std::uint32_t b) { return hash[a] < hash[b]; } );
+  if ( n > 0 )
+  {
+    const std::uint64_t max_idx = n - 1;
+    if ( nsplit > max_idx ) std::fill( splits.begin(), splits.end(), max_idx );
+    std::vector< std::uint32_t > depth( n - 1 ), pos( n - 1 );
+    for ( std::uint64_t i = 0; i + 1 < n; ++i )
+    {
+      const std::uint32_t mask = hash[idx[i]] ^ hash[idx[i + 1]];
+      depth[i] = mask ? 31u - static_cast< std::uint32_t >( 31 - __builtin_clz( mask ) ) : 0xffffffffu;
+      pos[i] = static_cast< std::uint32_t >( i );
+    }
+    std::stable_sort( pos.begin(), pos.end(), [&depth](std::uint32_t a, std::uint32_t b) { return depth[a] < depth[b]; } );
+    const std::uint64_t take = std::min< std::uint64_t >( nsplit, n - 1 );
+    std::vector< std::uint32_t > chosen( pos.begin(), pos.begin() + take );
+    std::sort( chosen.begin(), chosen.end() );
+    for ( std::uint64_t k = 0; k < take; ++k ) splits[k] = chosen[k];
+  }
+  if ( order_out ) std::memcpy( order_out, idx.data(), n * sizeof( std::uint32_t ) );
+  if ( bounds_out && patches > 0 )
+  {
+    bounds_out[0] = 0;
+    for ( std::uint64_t k = 1; k < patches; ++k ) bounds_out[k] = splits[k - 1];
+    bounds_out[patches] = n;
+  }
+}
+
 int orc_max_threads() { return omp_get_max_threads(); }
 
 }  // extern "C"

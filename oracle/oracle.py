@@ -50,6 +50,7 @@ def _load():
         "orc_sort_and_sweep": (I64, [P, U64, P, U64, I32, I32, P, U64]),
         "orc_pipeline": (I64, [P, U64, P, U64, U32, I32, D, I32, P, P, U64]),
         "orc_max_threads": (I32, []),
+        "orc_morton_cluster": (None, [P, U64, P, P, U32, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -248,6 +249,19 @@ def pipeline(xyz_a, xyz_b, k, eps=0.0, threads=0, keep_pairs=False):
             break
         cap = cnt
     return cnt, dict(zip(PIPELINE_STAGES, st.tolist())), canonical(out[:cnt])
+
+
+def morton_cluster(xyz, k, patches, eps=0.0):
+    """The reference's Morton clustering of elements into `patches` patches: (element order (n,) uint32, patch
+    bounds (patches + 1,) uint64), from the 32-bit hashes of the centroids over the k-DOP Morton bounds."""
+    c = centroids(xyz)
+    mn, inv = morton_bounds(kdops(xyz, k, eps), k)
+    n = c.shape[0]
+    order = np.empty(max(n, 1), dtype=np.uint32)
+    bounds = np.empty(patches + 1, dtype=np.uint64)
+    lib.orc_morton_cluster(c.ctypes.data, n, mn.ctypes.data, inv.ctypes.data, patches, order.ctypes.data,
+                           bounds.ctypes.data)
+    return order[:n], bounds
 
 
 def max_threads():

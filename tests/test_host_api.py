@@ -55,32 +55,3 @@ def test_host_api_pairs_match_the_oracle(tmp_path, od, k):
     assert count == want.shape[0] > 0
     assert 1 <= calls <= od * od
     assert np.array_equal(got, want[np.lexsort((want[:, 1], want[:, 0]))])
-
-
-CLUSTER_SRC = os.path.join(ROOT, "tests", "host_api", "cluster_test.cpp")
-GOLDEN = np.load(os.path.join(ROOT, "tests", "golden", "ref_vectors.npz"))
-
-
-@pytest.mark.parametrize("od", [1, 8, 64])
-def test_patches_match_the_reference_clustering(tmp_path, od):
-    """The mirror's patches are the reference's morton_cluster patches (golden vectors from the reference's own
-    code): the same elements in the same order, cut at the same positions. Keys and permutation come from the
-    oracle, which the GPU path matches bit for bit."""
-    exe = str(tmp_path / "cl")
-    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I" + os.path.join(LIBDIR, "host"),
-                    CLUSTER_SRC, "-o", exe], check=True, capture_output=True, text=True)
-    xyz = GOLDEN["cluster/xyz"]
-    keys = orc.morton_keys(orc.centroids(xyz), *orc.morton_bounds(orc.kdops(xyz, 26), 26))
-    perm = orc.stable_perm(keys).astype(np.uint32)
-    with open(tmp_path / "k.bin", "wb") as f:
-        f.write(np.uint64(keys.shape[0]).tobytes())
-        f.write(keys[perm].tobytes())
-        f.write(perm.tobytes())
-    out = subprocess.run([exe, str(tmp_path / "k.bin"), str(od)], check=True, capture_output=True, text=True).stdout
-    lines = out.strip().split("\n")
-    pbeg = np.array([int(x) for x in lines[0].split()])
-    order = np.array([int(x) for x in lines[1].split()])
-    ref_order = GOLDEN[f"cluster/od{od}/order"].astype(np.int64)
-    ref_splits = GOLDEN[f"cluster/od{od}/splits"].astype(np.int64)
-    assert np.array_equal(order, ref_order)
-    assert np.array_equal(pbeg, np.concatenate([[0], ref_splits, [xyz.shape[0]]]))

@@ -280,3 +280,23 @@ def test_sort_and_sweep_matches_the_reference_vectors():
             assert np.array_equal(np.unique(mine, axis=0), g[f"{name}/sweep{k}/pairs"].astype(np.int64)), (name, k)
             checked += 1
     assert checked == 12
+
+
+@pytest.mark.parametrize("od", [1, 8, 64])
+def test_oracle_morton_cluster_matches_the_reference_vectors(od):
+    """morton_cluster restated (32-bit hashes, stable sorts by hash and by split depth) against the element order and
+    splits that the reference's own code wrote."""
+    xyz = GOLDEN["cluster/xyz"]
+    order, bounds = orc.morton_cluster(xyz, 26, od)
+    assert np.array_equal(order.astype(np.int64), GOLDEN[f"cluster/od{od}/order"].astype(np.int64))
+    want = np.concatenate([[0], GOLDEN[f"cluster/od{od}/splits"].astype(np.int64), [xyz.shape[0]]])
+    assert np.array_equal(bounds.astype(np.int64), want)
+
+
+def test_oracle_morton_cluster_edge_cases():
+    # no elements: every split is 0; fewer elements than patches: unchosen splits hold n - 1
+    order, bounds = orc.morton_cluster(np.zeros((0, 3, 3)), 18, 4)
+    assert order.shape == (0,) and np.array_equal(bounds, np.zeros(5, dtype=np.uint64))
+    xyz = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]], [[5, 5, 5], [6, 5, 5], [5, 6, 5]]], dtype=np.float64)
+    order, bounds = orc.morton_cluster(xyz, 18, 4)
+    assert np.array_equal(order, [0, 1]) and np.array_equal(bounds, [0, 0, 1, 1, 2])
