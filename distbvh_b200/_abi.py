@@ -26,7 +26,7 @@ EXPORTS = (
     "bvhg_get_stage_times", "bvhg_launch_count", "bvhg_set_spin_limit", "bvhg_test_stall_sort", "bvhg_debug_normal",
     "bvhg_synchronize", "bvhg_last_error", "bvhg_status_string", "bvhg_radix_sort_noalloc",
     "bvhg_batch_broadphase", "bvhg_batch_autotune", "bvhg_sort_and_sweep", "bvhg_test_dense_stack",
-    "bvhg_cluster", "bvhg_patch_pairs",
+    "bvhg_cluster", "bvhg_patch_pairs", "bvhg_patch_kdops",
 )
 
 
@@ -76,6 +76,7 @@ def _load():
         "bvhg_test_stall_sort": (I32, [P, I32]),
         "bvhg_test_dense_stack": (I32, [P, I32]),
         "bvhg_cluster": (I32, [P, I32, U32, P, P, I32]),
+        "bvhg_patch_kdops": (I32, [P, I32, P, I32]),
         "bvhg_patch_pairs": (I32, [P, I32, I32, P, U64, ctypes.POINTER(U64), P, U64, ctypes.POINTER(U64), I32]),
         "bvhg_debug_normal": (I32, [I32, I32, I32, P, P, P]),
         "bvhg_synchronize": (I32, [P]),
@@ -269,6 +270,12 @@ class Context:
         order = np.empty(max(n, 1), dtype=np.uint32)
         self._check(lib.bvhg_cluster(self._h, obj, patches, bounds.ctypes.data, order.ctypes.data, MEM_HOST))
         return bounds, order[:n]
+
+    def patch_kdops(self, obj, patches):
+        """Patch boxes of a clustered object: (patches, K/2, 2) float64 (min, max) per slab."""
+        out = np.empty((patches, self.k // 2, 2), dtype=np.float64)
+        self._check(lib.bvhg_patch_kdops(self._h, obj, out.ctypes.data, MEM_HOST))
+        return out
 
     def patch_pairs(self, a, b):
         """Element pairs grouped by patch pair: (groups (g, 4) uint32 rows (patch a, patch b, first, count),

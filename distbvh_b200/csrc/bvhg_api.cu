@@ -78,7 +78,7 @@ struct object
   // Patches (bvhg_cluster): valid until the next set_elements or rebuild.
   bool clustered = false;
   uint32_t cl_patches = 0;
-  dev_buf cl_order, cl_rank, cl_tmp, cl_runs, cl_bhist, cl_bbase, cl_splits, cl_bounds, cl_scal;
+  dev_buf cl_order, cl_rank, cl_tmp, cl_runs, cl_bhist, cl_bbase, cl_splits, cl_bounds, cl_scal, cl_enc, cl_boxes;
   dev_buf verts_own, gid_own;
   dev_buf cx, cy, cz;
   dev_buf keys, keys_alt, vals, vals_alt;
@@ -1399,6 +1399,30 @@ bvhg_status bvhg_cluster(bvhg_ctx *ctx, int32_t obj, uint32_t patches, uint64_t 
   BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
   o.clustered = true;
   o.cl_patches = patches;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_patch_kdops(bvhg_ctx *ctx, int32_t obj, double *boxes, int32_t mem)
+{
+  if ( !valid_obj( ctx, obj ) ) return fail( ctx, BVHG_ERR_ARG, "invalid object" );
+  if ( !boxes ) return fail( ctx, BVHG_ERR_ARG, "null box buffer" );
+  if ( mem != BVHG_MEM_HOST && mem != BVHG_MEM_DEVICE ) return fail( ctx, BVHG_ERR_ARG, "bad memory kind" );
+  object &o = *ctx->objs[obj];
+  if ( !o.clustered ) return fail( ctx, BVHG_ERR_STATE, "patch k-DOPs before bvhg_cluster" );
+  cudaSetDevice( ctx->cfg.device );
+  join_object( ctx, o );
+  const uint32_t P = o.cl_patches;
+  const int K = ctx->cfg.k;
+  const size_t bytes = static_cast< size_t >( P ) * K * 8;
+  BVHG_CUDA( ctx, o.cl_enc.reserve( bytes ) );
+  BVHG_CUDA( ctx, o.cl_boxes.reserve( bytes ) );
+  BVHG_CUDA( ctx, launch_patch_kdops( K, o.verts, o.V, o.n, ctx->cfg.epsilon, o.cl_order.as< uint32_t >(),
+                                      o.cl_bounds.as< uint64_t >(), P, o.cl_enc.as< unsigned long long >(),
+                                      o.cl_boxes.as< double >(), ctx->stream ) );
+  ctx->launches += o.n ? 3 : 2;
+  BVHG_CUDA( ctx, cudaMemcpyAsync( boxes, o.cl_boxes.p, bytes,
+                                   mem == BVHG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream ) );
+  BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
   return BVHG_OK;
 }
 

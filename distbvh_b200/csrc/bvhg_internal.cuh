@@ -136,6 +136,12 @@ struct cluster_launch
 size_t cluster_block_count(uint64_t n);
 cudaError_t launch_cluster(const cluster_launch &x);
 
+// Patch boxes of a clustered object: out[(p * K/2 + a) * 2 + {0 min, 1 max}] = the union of the FP64 slabs of patch
+// p's elements (+inf / -inf for an empty patch); enc: patches * K words of scratch.
+cudaError_t launch_patch_kdops(int K, const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *order,
+                               const uint64_t *bounds, uint32_t patches, unsigned long long *enc, double *out,
+                               cudaStream_t s);
+
 // Two clustered objects: element pairs (local indices) grouped by patch pair.
 struct group_launch
 {

@@ -15,6 +15,7 @@
 //     a stable block-scan compaction then writes the chosen positions in order.
 // Every kernel is a bounded loop; nothing waits on another block.
 #include "bvhg_internal.cuh"
+#include "kdop_math.cuh"
 
 namespace bvhg {
 int device_sm_count();
@@ -449,6 +450,73 @@ __global__ void k_group_scatter(const uint2 *__restrict__ pairs, uint64_t np, gr
   }
 }
 
+// ---- patch k-DOPs ----------------------------------------------------------------------------------------------
+
+// Patch boxes: the union of the FP64 slabs (kdop_base::from_vertices, src/bvh/kdop.hpp:238-264) of every element of
+// each patch, as the reference's patch snapshot unions its elements' k-DOPs (make_snapshot,
+// src/bvh/snapshot.hpp:139-149). One thread per position of the patch order; a warp whose positions all lie in one
+// patch reduces in registers and updates the patch's order-preserving encodings once per slab, other warps per lane.
+template< int K, int VT >
+__global__ void __launch_bounds__( 256 ) k_patch_kdops(const double *__restrict__ verts, uint32_t Vrt, uint32_t n,
+                                                       double eps, const uint32_t *__restrict__ order,
+                                                       const uint64_t *__restrict__ bounds, uint32_t patches,
+                                                       unsigned long long *__restrict__ enc)
+{
+  constexpr int D = K / 2;
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31u;
+  const bool valid = r < n;
+  const uint32_t p = valid ? patch_of( bounds, patches, r ) : 0xffffffffu;
+  const uint32_t p0 = __shfl_sync( 0xffffffffu, p, 0 );
+  const bool uniform = __all_sync( 0xffffffffu, valid && p == p0 );
+  double lo[D], hi[D];
+  if ( valid ) leaf_slabs< K, double, VT >( verts, Vrt, __ldg( order + r ), eps, 0.f, lo, hi );
+#pragma unroll
+  for ( int a = 0; a < D; ++a )
+  {
+    unsigned long long emin = valid ? ord_encode( lo[a] ) : ~0ull, emax = valid ? ord_encode( hi[a] ) : 0ull;
+    if ( uniform )
+    {
+#pragma unroll
+      for ( int o = 16; o > 0; o >>= 1 )
+      {
+        const unsigned long long om = __shfl_xor_sync( 0xffffffffu, emin, o );
+        const unsigned long long oM = __shfl_xor_sync( 0xffffffffu, emax, o );
+        emin = om < emin ? om : emin;
+        emax = oM > emax ? oM : emax;
+      }
+      if ( lane == 0 )
+      {
+        atomicMin( enc + ( static_cast< size_t >( p0 ) * D + a ) * 2, emin );
+        atomicMax( enc + ( static_cast< size_t >( p0 ) * D + a ) * 2 + 1, emax );
+      }
+    } else if ( valid ) {
+      atomicMin( enc + ( static_cast< size_t >( p ) * D + a ) * 2, emin );
+      atomicMax( enc + ( static_cast< size_t >( p ) * D + a ) * 2 + 1, emax );
+    }
+  }
+}
+
+__global__ void k_patch_kdops_init(unsigned long long *enc, uint64_t words)
+{
+  for ( uint64_t i = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; i < words;
+        i += static_cast< uint64_t >( gridDim.x ) * blockDim.x )
+    enc[i] = ( i & 1 ) ? 0ull : ~0ull;
+}
+
+// Decoded boxes; an empty patch gets (+inf, -inf) on every slab.
+__global__ void k_patch_kdops_decode(const unsigned long long *__restrict__ enc, uint64_t words, double *__restrict__ out)
+{
+  for ( uint64_t i = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; i < words;
+        i += static_cast< uint64_t >( gridDim.x ) * blockDim.x )
+  {
+    const unsigned long long e = enc[i];
+    const bool untouched = ( i & 1 ) ? e == 0ull : e == ~0ull;
+    out[i] = untouched ? ( ( i & 1 ) ? -__longlong_as_double( 0x7ff0000000000000LL ) : __longlong_as_double( 0x7ff0000000000000LL ) )
+                       : ord_decode( e );
+  }
+}
+
 unsigned grid_for(uint64_t work, unsigned threads, unsigned per_sm)
 {
   const uint64_t blocks = ( work + threads - 1 ) / threads;
@@ -488,6 +556,27 @@ cudaError_t launch_cluster(const cluster_launch &x)
   }
   k_cluster_bounds<<< 1, 256, 0, x.s >>>( x.splits, take, x.patches, n, x.bounds );
   k_cluster_rank<<< grid_for( n, 256, 8 ), 256, 0, x.s >>>( x.order, n, x.rank );
+  return cudaGetLastError();
+}
+
+cudaError_t launch_patch_kdops(int K, const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *order,
+                               const uint64_t *bounds, uint32_t patches, unsigned long long *enc, double *out,
+                               cudaStream_t s)
+{
+  const uint64_t words = static_cast< uint64_t >( patches ) * K;
+  k_patch_kdops_init<<< grid_for( words, 256, 4 ), 256, 0, s >>>( enc, words );
+  if ( n > 0 )
+  {
+    const unsigned grid = static_cast< unsigned >( ( n + 255 ) / 256 );
+    const uint32_t n32 = static_cast< uint32_t >( n );
+#define BVHG_PK( KK, VV ) k_patch_kdops< KK, VV ><<< grid, 256, 0, s >>>( verts, V, n32, eps, order, bounds, patches, enc )
+    if ( K == 6 ) { if ( V == 3 ) BVHG_PK( 6, 3 ); else if ( V == 4 ) BVHG_PK( 6, 4 ); else if ( V == 8 ) BVHG_PK( 6, 8 ); else BVHG_PK( 6, 0 ); }
+    else if ( K == 18 ) { if ( V == 3 ) BVHG_PK( 18, 3 ); else if ( V == 4 ) BVHG_PK( 18, 4 ); else if ( V == 8 ) BVHG_PK( 18, 8 ); else BVHG_PK( 18, 0 ); }
+    else if ( K == 26 ) { if ( V == 3 ) BVHG_PK( 26, 3 ); else if ( V == 4 ) BVHG_PK( 26, 4 ); else if ( V == 8 ) BVHG_PK( 26, 8 ); else BVHG_PK( 26, 0 ); }
+    else return cudaErrorInvalidValue;
+#undef BVHG_PK
+  }
+  k_patch_kdops_decode<<< grid_for( words, 256, 4 ), 256, 0, s >>>( enc, words, out );
   return cudaGetLastError();
 }
 

@@ -15,6 +15,8 @@
 // Self-collision (self_collision_set, collision_query.hpp:331-368): the query of rank i only visits subtrees
 // holding ranks > i (internal node k splits its bucket range [l, r] into [l, k] and [k + 1, r]) and tests only
 // bucket elements of rank > i, so every unordered pair is found once and no element is paired with itself.
+#include <cstddef>
+
 #include "bulk_copy.cuh"
 #include "bvhg_internal.cuh"
 #include "kdop_math.cuh"
@@ -420,13 +422,27 @@ constexpr int kDenseStack = 256;
 template< int K, typename T >
 struct dense_smem
 {
-  T q[32][K];                           // query slabs of the packet, (min, max) per slab
-  T rows[kDenseBatch][2 * K];           // node rows of the batch: [slab][child][min, max]
-  uint32_t qe[32];                      // query element indices
-  int2 stack[kDenseStack];              // (node, lane mask)
-  int2 leaf[kLeafQueue];                // (bucket, lane mask)
-  uint32_t pre[kLeafQueue];             // exclusive prefix of the entries' test counts (8 per query)
+  // every array starts on a 16-byte boundary: rows[] receives 16-byte asynchronous copies, and q[] and rows[] are
+  // read as 8- or 16-byte (min, max) pairs
+  alignas( 16 ) T q[32][K];                  // query slabs of the packet, (min, max) per slab
+  alignas( 16 ) T rows[kDenseBatch][2 * K];  // node rows of the batch: [slab][child][min, max]
+  alignas( 16 ) uint32_t qe[32];             // query element indices
+  alignas( 16 ) int2 stack[kDenseStack];     // (node, lane mask)
+  alignas( 16 ) int2 leaf[kLeafQueue];       // (bucket, lane mask)
+  alignas( 16 ) uint32_t pre[kLeafQueue];    // exclusive prefix of the entries' test counts (8 per query)
 };
+
+template< int K, typename T >
+constexpr bool dense_smem_aligned()
+{
+  using S = dense_smem< K, T >;
+  return offsetof( S, q ) % 16 == 0 && offsetof( S, rows ) % 16 == 0 && sizeof( S ) % 16 == 0 &&
+         ( 2 * K * sizeof( T ) ) % 16 == 0;  // node rows: whole 16-byte pieces
+}
+static_assert( dense_smem_aligned< 6, double >() && dense_smem_aligned< 18, double >() &&
+                 dense_smem_aligned< 26, double >() && dense_smem_aligned< 6, float >() &&
+                 dense_smem_aligned< 18, float >() && dense_smem_aligned< 26, float >(),
+               "dense walk shared memory must keep 16-byte alignment" );
 
 // Tests every (query, element) pair of the queued entries; i0 = the packet's first query rank.
 template< int K, typename T >

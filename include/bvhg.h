@@ -181,6 +181,12 @@ BVHG_API bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const 
  * bvhg_patch_pairs until its next bvhg_set_elements or rebuild. Blocks until done. */
 BVHG_API bvhg_status bvhg_cluster(bvhg_ctx *ctx, int32_t obj, uint32_t patches, uint64_t *bounds, uint32_t *order,
                                   int32_t mem);
+/* Patch boxes of a clustered object (the k-DOP of the reference's patch snapshot, make_snapshot,
+ * src/bvh/snapshot.hpp:139-149, which the reference gathers to build its patch tree, src/bvh/collision_object/
+ * top_down.cpp:103-127): boxes[(p * K/2 + a) * 2 + {0 min, 1 max}] is the union of the FP64 slabs
+ * (kdop_base::from_vertices with the context's epsilon) of patch p's elements, from their present vertices; an
+ * empty patch gets (+inf, -inf). `mem` is the memory kind of boxes. Blocks until done. */
+BVHG_API bvhg_status bvhg_patch_kdops(bvhg_ctx *ctx, int32_t obj, double *boxes, int32_t mem);
 /* The exact element pairs of two clustered objects (the set of bvhg_broadphase) grouped by patch pair on the device,
  * for a narrowphase functor per patch pair (collision_world::set_narrowphase_functor, src/bvh/collision_world.hpp:
  * 58-94, run per patch pair in src/bvh/collision_object/impl.cpp:269-350). groups: 4 words per non-empty patch pair

@@ -482,3 +482,25 @@ def test_dense_walk_stack_bound_falls_back(precision):
         for _ in range(3):
             got = ctx.batch_broadphase([(oa, ob)])
             assert np.array_equal(orc.canonical(got[0]), want)
+
+
+@pytest.mark.parametrize("k", [6, 18, 26])
+@pytest.mark.parametrize("eps", [0.0, 1e-3])
+def test_fp32_dense_contact_of_touching_elements(k, eps):
+    """Hexahedra of a grid touch their neighbours exactly, and the grid is split checkerboard-wise into two objects
+    in dense contact: with epsilon 0 the touching faces are FP32 candidates (the outward-rounded slabs overlap) but
+    not pairs, and the FP64 recheck must drop every one of them, in the computed-slab walk and in the dense walk over
+    stored slabs; coordinates are scaled by an irrational factor so the 18- and 26-DOP projections round."""
+    xyz, _ = element_grid(12, 12, 12)
+    xyz = np.ascontiguousarray(xyz * np.sqrt(2.0) + 0.1)
+    idx = np.arange(xyz.shape[0])
+    i, j, l = idx % 12, (idx // 12) % 12, idx // 144
+    even = (i + j + l) % 2 == 0
+    a, b = np.ascontiguousarray(xyz[even]), np.ascontiguousarray(xyz[~even])
+    want = orc.pair_set(a, b, k, eps)
+    with bvhg.Context(k=k, precision=bvhg.FILTER_FP32, epsilon=eps) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        for _ in range(3):  # the first pass decides dense contact; later builds store the slabs
+            assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), want)
+            ctx.build(oa)
+            ctx.build(ob)
