@@ -107,11 +107,15 @@ struct object
 
 // Batching form: every object and scene of a batch as one CUDA graph (builds and traversals spread over lanes of
 // concurrent streams, no host round trip between scenes), captured once per batch layout and replayed.
+// Device tables (item arguments, block starts) of a fused batch graph's batched launches.
+using launch_tables = std::vector< std::unique_ptr< dev_buf > >;
+
 struct batch_graph
 {
   std::vector< uint64_t > key;  // layout the graph was captured for
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  std::shared_ptr< launch_tables > tables;  // read by the graph's kernels (fused form)
 };
 
 struct batch_state
@@ -121,7 +125,10 @@ struct batch_state
   std::vector< uint64_t > key;  // layout of the graph in use
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  int lanes = 16;  // concurrent streams (bvhg_batch_autotune picks it)
+  std::shared_ptr< launch_tables > tables;
+  // 0: the fused form (one batched launch per pipeline stage for all objects and scenes); else the laned form with
+  // this many concurrent streams of per-object launches (bvhg_batch_autotune picks it)
+  int lanes = 0;
   std::vector< cudaStream_t > lane;
   std::vector< cudaEvent_t > obj_done, lane_done;
   cudaEvent_t fork = nullptr;
@@ -139,6 +146,7 @@ struct batch_state
         key = g.key;
         graph = g.graph;
         exec = g.exec;
+        tables = g.tables;
         return true;
       }
     return false;
@@ -152,7 +160,7 @@ struct batch_state
       cudaGraphDestroy( graphs.front().graph );
       graphs.erase( graphs.begin() );
     }
-    graphs.push_back( { key, graph, exec } );
+    graphs.push_back( { key, graph, exec, tables } );
   }
   void drop_graph()
   {
@@ -164,6 +172,7 @@ struct batch_state
     graphs.clear();
     exec = nullptr;
     graph = nullptr;
+    tables.reset();
     key.clear();
   }
   ~batch_state()
@@ -506,13 +515,11 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
     }
   }
   {
-    // the fix-up reads the last pass's output and writes the other buffers; runs too long for it are sorted in
-    // place afterwards, with the fix-up's input as scratch
+    // the fix-up reads the last pass's output and writes the other buffers
     stage_scope st( ctx, BVHG_STAGE_FIXUP );
     BVHG_CUDA( ctx, launch_sort_fixup( kin, vin, kout, vout, n, o.runs.as< uint32_t >(), o.sc(), s ) );
     st.launched();
-    BVHG_CUDA( ctx, launch_sort_runs( kout, vout, kin, vin, n, o.runs.as< uint32_t >(), o.sc(), s ) );
-    st.launched();
+    if ( sort_runs_blocks( n ) ) st.launched();
     o.sort_result_alt = ( kout == o.keys_alt.as< uint64_t >() ) ? 1 : 0;
   }
   {
@@ -784,6 +791,250 @@ bvhg_status capture_batch(bvhg_ctx *ctx, batch_state &B, const batch_args &x, co
   return BVHG_OK;
 }
 
+// One batched launch's tables on the device (before capture: a synchronous upload).
+template< typename A >
+bvhg_status make_launch(bvhg_ctx *ctx, launch_tables &keep, const std::vector< A > &items,
+                        const std::vector< uint32_t > &blocks, batch_launch *out)
+{
+  *out = batch_launch{};
+  if ( items.empty() ) return BVHG_OK;
+  std::vector< uint32_t > starts( items.size() + 1, 0 );
+  for ( size_t i = 0; i < items.size(); ++i ) starts[i + 1] = starts[i] + blocks[i];
+  keep.emplace_back( new dev_buf );
+  dev_buf &bi = *keep.back();
+  BVHG_CUDA( ctx, bi.reserve( items.size() * sizeof( A ) ) );
+  BVHG_CUDA( ctx, cudaMemcpy( bi.p, items.data(), items.size() * sizeof( A ), cudaMemcpyHostToDevice ) );
+  keep.emplace_back( new dev_buf );
+  dev_buf &bs = *keep.back();
+  BVHG_CUDA( ctx, bs.reserve( starts.size() * sizeof( uint32_t ) ) );
+  BVHG_CUDA( ctx, cudaMemcpy( bs.p, starts.data(), starts.size() * sizeof( uint32_t ), cudaMemcpyHostToDevice ) );
+  out->items = bi.p;
+  out->starts = bs.as< uint32_t >();
+  out->nitems = static_cast< int >( items.size() );
+  out->blocks = starts.back();
+  return BVHG_OK;
+}
+
+// The vertex count shared by every non-empty object of the batch, or 0 when they differ (the laned form then runs).
+uint32_t batch_vertex_count(bvhg_ctx *ctx, const std::vector< int32_t > &uniq)
+{
+  uint32_t V = 0;
+  for ( int32_t o : uniq )
+  {
+    const object &ob = *ctx->objs[o];
+    if ( ob.n == 0 ) continue;
+    if ( V == 0 ) V = ob.V;
+    else if ( V != ob.V ) return 0;
+  }
+  return V ? V : 3;
+}
+
+// Fused form of a batch: every pipeline stage of every object, then every scene's traversal, recheck and gid
+// mapping, each as one batched launch (batch.cuh) whose blocks run the per-object (per-scene) launch's blocks back to
+// back. The per-object computation, its buffers and its host-side state are those of do_build_on; only the number of
+// launches changes (about a dozen per batch instead of a dozen per object).
+bvhg_status capture_batch_fused(bvhg_ctx *ctx, batch_state &B, const batch_args &x, const std::vector< int32_t > &uniq,
+                                uint32_t V)
+{
+  const int K = ctx->cfg.k;
+  const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
+  const int bits = ctx->cfg.sort_digit_bits;
+  const int passes = sort_passes( bits );
+  const int first = sort_first_pass( bits );
+  const uint64_t radix = 1ull << bits;
+  const double eps = ctx->cfg.epsilon;
+  auto tables = std::make_shared< launch_tables >();
+  std::vector< init_args > it_init;
+  std::vector< cb_args > it_cb;
+  std::vector< kh_args > it_kh;
+  std::vector< std::vector< sort_pass_args > > it_pass( passes );
+  std::vector< fixup_args > it_fix, it_runs;
+  std::vector< slabs_args > it_slabs;
+  std::vector< tree_args > it_tree;  // objects with more than one bucket (build + climb, or refit)
+  std::vector< uint32_t > b_init, b_cb, b_kh, b_fix, b_runs, b_slabs, b_build, b_climb, b_refit;
+  std::vector< std::vector< uint32_t > > b_pass( passes );
+  bool tma = V == 3 || V == 4 || V == 8;
+  for ( int32_t oi : uniq )
+    if ( ctx->objs[oi]->n && ( reinterpret_cast< uintptr_t >( ctx->objs[oi]->verts ) & 15 ) ) tma = false;
+  for ( int32_t oi : uniq )
+  {
+    object &o = *ctx->objs[oi];
+    if ( o.n == 0 )
+    {
+      o.built = true;
+      o.fresh = x.mode == BVHG_REBUILD;
+      continue;
+    }
+    const uint64_t n = o.n;
+    const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
+    const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
+    if ( x.mode == BVHG_REBUILD )
+    {
+      const size_t first_words = static_cast< size_t >( first ) * ( tiles + 1 ) * radix;
+      const init_args ia{ o.sc(), o.hist.as< uint32_t >(), passes * radix, o.status.as< uint32_t >() + first_words,
+                          passes * ( tiles + 1 ) * radix - first_words, o.exch.as< int >(), m > 1 ? m - 1 : 0 };
+      it_init.push_back( ia );
+      b_init.push_back( obj_init_blocks( ia ) );
+      it_cb.push_back( cb_args{ o.verts, o.V, n, eps, o.cx.as< double >(), o.cy.as< double >(), o.cz.as< double >(),
+                                o.sc(), ctx->spin_limit } );
+      uint32_t cbb = 0;
+      BVHG_CUDA( ctx, centroid_bounds_blocks( K, V, n, tma, &cbb ) );
+      b_cb.push_back( cbb );
+      it_kh.push_back( kh_args{ o.cx.as< double >(), o.cy.as< double >(), o.cz.as< double >(), n, o.sc(),
+                                o.keys.as< uint64_t >(), o.hist.as< uint32_t >() } );
+      b_kh.push_back( keys_hist_blocks( n ) );
+      uint64_t *kin = o.keys.as< uint64_t >(), *kout = o.keys_alt.as< uint64_t >();
+      uint32_t *vin = nullptr, *vout = o.vals_alt.as< uint32_t >();
+      uint32_t *vother = o.vals.as< uint32_t >();
+      for ( int p = first; p < passes; ++p )
+      {
+        it_pass[p].push_back( onesweep_args( bits, kin, vin, kout, vout, n, p, o.hist.as< uint32_t >(),
+                                             o.status.as< uint32_t >(), o.sc(), ctx->spin_limit, ctx->stall_sort ) );
+        b_pass[p].push_back( onesweep_blocks( n ) );
+        std::swap( kin, kout );
+        uint32_t *next_out = vin ? vin : vother;
+        vin = vout;
+        vout = next_out;
+      }
+      const fixup_args fa{ kin, vin, kout, vout, n, o.runs.as< uint32_t >(), o.sc() };
+      it_fix.push_back( fa );
+      b_fix.push_back( sort_fixup_blocks( n ) );
+      if ( const uint32_t rb = sort_runs_blocks( n ) )
+      {
+        it_runs.push_back( fa );
+        b_runs.push_back( rb );
+      }
+      o.sort_result_alt = ( kout == o.keys_alt.as< uint64_t >() ) ? 1 : 0;
+    } else if ( m > 1 ) {
+      // refit: only the exchange slots start over
+      const init_args ia{ nullptr, nullptr, 0, nullptr, 0, o.exch.as< int >(), m - 1 };
+      it_init.push_back( ia );
+      b_init.push_back( obj_init_blocks( ia ) );
+    }
+    it_slabs.push_back( slabs_args{ o.verts, o.V, n, eps, f32_round_up( eps ), o.sorted_vals(), o.bucket_box.p,
+                                    o.warp_box.p, o.store_slabs ? o.elem_cache.p : nullptr, o.sc() } );
+    b_slabs.push_back( slabs_blocks( n ) );
+    o.stored = o.store_slabs;
+    if ( m > 1 )
+    {
+      it_tree.push_back( tree_args{ n, o.sorted_keys(), o.bdel.as< uint8_t >(), o.bucket_box.p, o.node_box.p,
+                                    o.child.as< int2 >(), o.range.as< int2 >(), o.parent.as< int >(), o.exch.as< int >(),
+                                    o.queue.as< int4 >(), o.sc() } );
+      b_build.push_back( build_blocks( n ) );
+      b_climb.push_back( climb_blocks( n ) );
+      b_refit.push_back( refit_blocks( n ) );
+    }
+    o.built = true;
+    if ( x.mode == BVHG_REBUILD )
+    {
+      o.topo = true;
+      o.fresh = true;
+      o.clustered = false;
+    } else {
+      o.fresh = false;
+    }
+  }
+  // scenes (after the objects' host state above: the views read which buffers hold the sorted order and slabs)
+  pair_scalars *ps = B.ps.as< pair_scalars >();
+  std::vector< trav_item > it_dense, it_sparse;
+  std::vector< uint32_t > b_dense, b_sparse, b_recheck, b_gid;
+  std::vector< recheck_args > it_recheck;
+  std::vector< gid_args > it_gid;
+  for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
+  {
+    object &oa = *ctx->objs[x.a[sc]];
+    object &ob = *ctx->objs[x.b[sc]];
+    const bool self = x.a[sc] == x.b[sc];
+    if ( oa.n == 0 || ob.n == 0 || ( self && oa.n < 2 ) ) continue;
+    uint2 *cand = B.cand.as< uint2 >() + B.off[sc];
+    trav_item ti;
+    uint32_t tb = 0;
+    bool dense = false;
+    traverse_item( K, fp32, view_of( oa ), view_of( ob ), self, oa.dense_ok && ob.dense_ok, eps, cand, B.cap[sc],
+                   ps + sc, ctx->dense_stack, &ti, &tb, &dense );
+    ( dense ? it_dense : it_sparse ).push_back( ti );
+    ( dense ? b_dense : b_sparse ).push_back( tb );
+    const uint2 *fin = cand;
+    const unsigned long long *cnt = &ps[sc].count;
+    if ( fp32 )
+    {
+      uint2 *ex = B.exact.as< uint2 >() + B.off[sc];
+      it_recheck.push_back( recheck_args{ oa.verts, oa.V, ob.verts, ob.V, eps, cand, B.cap[sc], ex, B.cap[sc], ps + sc } );
+      b_recheck.push_back( recheck_blocks( B.cap[sc] ) );
+      fin = ex;
+      cnt = &ps[sc].count2;
+    }
+    it_gid.push_back( gid_args{ fin, cnt, B.cap[sc], oa.gid, ob.gid, self ? 1 : 0, B.out.as< uint64_t >() + 2 * B.off[sc] } );
+    b_gid.push_back( gid_pairs_dev_blocks( B.cap[sc] ) );
+  }
+  // the tables on the device, then the graph
+  batch_launch l_init, l_cb, l_kh, l_fix, l_runs, l_slabs, l_build, l_climb, l_refit, l_dense, l_sparse, l_recheck, l_gid;
+  std::vector< batch_launch > l_pass( passes );
+  bvhg_status st = make_launch( ctx, *tables, it_init, b_init, &l_init );
+  if ( st == BVHG_OK && x.mode == BVHG_REBUILD )
+  {
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_cb, b_cb, &l_cb );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_kh, b_kh, &l_kh );
+    for ( int p = first; p < passes && st == BVHG_OK; ++p ) st = make_launch( ctx, *tables, it_pass[p], b_pass[p], &l_pass[p] );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_fix, b_fix, &l_fix );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_runs, b_runs, &l_runs );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_tree, b_build, &l_build );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_tree, b_climb, &l_climb );
+  } else if ( st == BVHG_OK ) {
+    st = make_launch( ctx, *tables, it_tree, b_refit, &l_refit );
+  }
+  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_slabs, b_slabs, &l_slabs );
+  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_dense, b_dense, &l_dense );
+  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_sparse, b_sparse, &l_sparse );
+  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_recheck, b_recheck, &l_recheck );
+  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_gid, b_gid, &l_gid );
+  if ( st != BVHG_OK ) return st;
+  const uint32_t Vt = V;  // every object shares it: the traversal and recheck unroll it
+  B.graph = nullptr;
+  B.exec = nullptr;
+  cudaStream_t s = ctx->stream;
+  BVHG_CUDA( ctx, cudaStreamBeginCapture( s, cudaStreamCaptureModeRelaxed ) );
+  auto body = [&]() -> bvhg_status {
+    BVHG_CUDA( ctx, cudaMemsetAsync( ps, 0, x.nscenes * sizeof( pair_scalars ), s ) );
+    BVHG_CUDA( ctx, launch_obj_init_batch( l_init, s ) );
+    if ( x.mode == BVHG_REBUILD )
+    {
+      BVHG_CUDA( ctx, launch_centroid_bounds_batch( K, V, tma, l_cb, s ) );
+      BVHG_CUDA( ctx, launch_keys_hist_batch( bits, l_kh, s ) );
+      for ( int p = first; p < passes; ++p ) BVHG_CUDA( ctx, launch_onesweep_batch( bits, l_pass[p], s ) );
+      BVHG_CUDA( ctx, launch_sort_fixup_batch( l_fix, s ) );
+      BVHG_CUDA( ctx, launch_sort_runs_batch( l_runs, s ) );
+      BVHG_CUDA( ctx, launch_slabs_batch( K, fp32, V, l_slabs, s ) );
+      BVHG_CUDA( ctx, launch_build_batch( K, fp32, l_build, s ) );
+      BVHG_CUDA( ctx, launch_climb_batch( K, fp32, l_climb, s ) );
+    } else {
+      BVHG_CUDA( ctx, launch_slabs_batch( K, fp32, V, l_slabs, s ) );
+      BVHG_CUDA( ctx, launch_refit_batch( K, fp32, l_refit, s ) );
+    }
+    BVHG_CUDA( ctx, launch_traverse_batch( K, fp32, true, Vt, l_dense, s ) );
+    BVHG_CUDA( ctx, launch_traverse_batch( K, fp32, false, Vt, l_sparse, s ) );
+    if ( fp32 ) BVHG_CUDA( ctx, launch_recheck_batch( K, Vt, l_recheck, s ) );
+    BVHG_CUDA( ctx, launch_gid_pairs_dev_batch( l_gid, s ) );
+    BVHG_CUDA( ctx, launch_gather_words( B.err_src.as< const int *const >(), static_cast< int >( uniq.size() ),
+                                         B.err_words.as< int >(), s ) );
+    ctx->launches += 16;
+    return BVHG_OK;
+  };
+  st = body();
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture( s, &g );
+  if ( st != BVHG_OK )
+  {
+    if ( g ) cudaGraphDestroy( g );
+    return st;
+  }
+  if ( ce != cudaSuccess ) return cuda_fail( ctx, ce, "cudaStreamEndCapture" );
+  B.graph = g;
+  BVHG_CUDA( ctx, cudaGraphInstantiate( &B.exec, B.graph, 0 ) );
+  B.tables = tables;
+  return BVHG_OK;
+}
+
 // Runs a batch: returns the per-scene exact counts in `counts` (host) and leaves scene sc's pairs in
 // B.out[2 * B.off[sc] ...]. Grows per-scene capacities and recaptures until every scene fits.
 bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
@@ -885,13 +1136,21 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
     BVHG_CUDA( ctx, cudaStreamSynchronize( ctx->stream ) );
     if ( !B.select( key ) )
     {
-      const bvhg_status st = capture_batch( ctx, B, x, uniq, slot );
+      const uint32_t V = batch_vertex_count( ctx, uniq );
+      const bvhg_status st = B.lanes == 0 && V ? capture_batch_fused( ctx, B, x, uniq, V )
+                                               : capture_batch( ctx, B, x, uniq, slot );
       if ( st != BVHG_OK ) return st;
       B.key = key;
       B.keep();
     } else {
       // a replay rebuilds the same objects: their host-side state is what the capture left
-      for ( int32_t o : uniq ) ctx->objs[o]->built = true;
+      for ( int32_t o : uniq )
+      {
+        object &ob = *ctx->objs[o];
+        ob.built = true;
+        ob.fresh = x.mode == BVHG_REBUILD;
+        if ( x.mode == BVHG_REBUILD ) ob.clustered = false;
+      }
     }
     BVHG_CUDA( ctx, cudaGraphLaunch( B.exec, ctx->stream ) );
     BVHG_CUDA( ctx, cudaMemcpyAsync( B.host_ps, B.ps.p, x.nscenes * sizeof( pair_scalars ), cudaMemcpyDeviceToHost,
@@ -1181,7 +1440,7 @@ bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *
   int best = ctx->batch->lanes;
   float best_ms = 0.f;
   bvhg_status st = BVHG_OK;
-  for ( int L : { 1, 4, 8, 16, 32, 64 } )
+  for ( int L : { 0, 1, 4, 8, 16, 32, 64 } )
   {
     ctx->batch->lanes = L;
     st = run_batch( ctx, x, counts.data() );  // captures this lane count's graph and settles the capacities

@@ -25,6 +25,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "batch.cuh"
+
 namespace bvhg {
 
 // Device-side scalars of one object (one allocation, read back for probes).
@@ -36,7 +38,7 @@ struct obj_scalars
   int root;                          // root internal node, or ~elem when n == 1
   int error;                         // bvhg_status raised by a kernel (first one wins)
   unsigned int climb_count;          // subtrees queued for the global phase of the tree build
-  unsigned int long_runs;            // runs of equal high key halves too long for the fix-up (sorted by k_sort_runs)
+  unsigned int long_runs;            // runs of equal high key halves listed by the fix-up for the run sort
   alignas( 16 ) unsigned char root_box[26 * 8];  // the root's slabs, D (min, max) pairs of the slab type
   unsigned int sort_tile_counter[64];// tile dispenser per radix pass
 };
@@ -86,6 +88,96 @@ constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;
 inline int sort_passes(int bits) { return ( kKeyBits + bits - 1 ) / bits; }
 
+// ---- kernel arguments: every pipeline kernel is a body over one of these structs, launched per object or, for
+// a batch, for many objects at once (batch.cuh) ----
+
+struct init_args  // reset state of a rebuild
+{
+  obj_scalars *sc;
+  uint32_t *hist;
+  uint64_t hist_words;
+  uint32_t *status;
+  uint64_t status_words;
+  int *exch;
+  uint64_t exch_words;
+};
+
+struct cb_args  // K1: centroids and Morton bounds
+{
+  const double *verts;
+  uint32_t V;
+  uint64_t n;
+  double eps;
+  double *cx, *cy, *cz;
+  obj_scalars *sc;
+  uint32_t spin_limit;
+};
+
+struct kh_args  // K2: Morton keys and digit histograms
+{
+  const double *cx, *cy, *cz;
+  uint64_t n;
+  obj_scalars *sc;
+  uint64_t *keys;
+  uint32_t *hist;
+};
+
+struct sort_pass_args  // one radix pass of one object
+{
+  const uint64_t *keys_in;
+  const uint32_t *vals_in;  // NULL: the element index
+  uint64_t *keys_out;
+  uint32_t *vals_out;
+  uint64_t n;
+  int pass;
+  const uint32_t *hist;     // this pass's digit histogram
+  uint32_t *status;         // this pass's look-back words
+  obj_scalars *sc;
+  uint32_t spin_limit;
+  int stall;
+  int use_tma;
+};
+
+struct fixup_args  // the low-half fix-up and the sort of the long runs it lists
+{
+  const uint64_t *keys_in;
+  const uint32_t *vals_in;
+  uint64_t *keys_out;
+  uint32_t *vals_out;
+  uint64_t n;
+  uint32_t *runs;  // long_run_capacity(n) first elements of long runs
+  obj_scalars *sc;
+};
+
+struct slabs_args  // element slabs, leaf-bucket and query-group boxes
+{
+  const double *verts;
+  uint32_t V;
+  uint64_t n;
+  double eps;
+  float eps_hi;
+  const uint32_t *vals;
+  void *bucket_box;
+  void *warp_box;
+  void *elem_rows;  // NULL: not stored
+  obj_scalars *sc;
+};
+
+struct tree_args  // the block-local build, the climb and the refit of one object's tree
+{
+  uint64_t n;
+  const uint64_t *keys;
+  uint8_t *bdel;
+  const void *bucket_box;
+  void *node_box;
+  int2 *child;
+  int2 *range;
+  int *parent;
+  int *exch;
+  int4 *queue;
+  obj_scalars *sc;
+};
+
 // ---- launch wrappers (one per kernel family), implemented in the k_*.cu files ----
 // All return cudaGetLastError() of the launch.
 
@@ -95,15 +187,20 @@ cudaError_t launch_centroid_bounds(int K, const double *verts, uint32_t V, uint6
 cudaError_t launch_keys_hist(int bits, const double *cx, const double *cy, const double *cz, uint64_t n,
                              obj_scalars *sc, uint64_t *keys, uint32_t *hist, cudaStream_t s);
 
-// Stable sort of each run of equal high key halves by the low half (in -> out), after the passes over bits 32..62.
-// Runs longer than the fix-up's neighbour scan are copied in order and their starts listed in runs[] (capacity
-// n / 33 + 1, count in sc->long_runs); launch_sort_runs then sorts them.
+// Batched forms (items: the per-object argument structs, blocks per item from the *_blocks functions).
+uint32_t obj_init_blocks(const init_args &a);
+cudaError_t launch_obj_init_batch(const batch_launch &b, cudaStream_t s);
+// tma: every item's vertices 16-byte aligned and V in {3, 4, 8} (then the bulk-copy form), else the plain form.
+cudaError_t centroid_bounds_blocks(int K, uint32_t V, uint64_t n, bool tma, uint32_t *blocks);
+cudaError_t launch_centroid_bounds_batch(int K, uint32_t V, bool tma, const batch_launch &b, cudaStream_t s);
+uint32_t keys_hist_blocks(uint64_t n);
+cudaError_t launch_keys_hist_batch(int bits, const batch_launch &b, cudaStream_t s);
+
+// Stable sort of each run of equal high key halves by the low half (in -> out), after the passes over bits 32..62:
+// the fix-up ranks runs of up to 32 elements in place and lists longer ones (runs[], count in sc->long_runs), which
+// a second small launch sorts with the input arrays as scratch (nothing else reads them afterwards).
 cudaError_t launch_sort_fixup(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
                               uint32_t *vals_out, uint64_t n, uint32_t *runs, obj_scalars *sc, cudaStream_t s);
-// Stable sort by the low key half of every run listed by the fix-up, in place in keys/vals, with tkeys/tvals (the
-// fix-up's input, no longer needed) as scratch. Exits at once when no run is listed.
-cudaError_t launch_sort_runs(uint64_t *keys, uint32_t *vals, uint64_t *tkeys, uint32_t *tvals, uint64_t n,
-                             const uint32_t *runs, obj_scalars *sc, cudaStream_t s);
 inline uint64_t long_run_capacity(uint64_t n) { return n / 33 + 1; }
 
 // ---- patches (k_cluster.cu) ----
@@ -202,6 +299,16 @@ cudaError_t launch_sweep(const sweep_launch &x);
 cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
                             obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s);
+// Batched: the argument struct of one object's pass (hist and status offset to the pass), and its blocks.
+sort_pass_args onesweep_args(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
+                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
+                             obj_scalars *sc, uint32_t spin_limit, int stall);
+uint32_t onesweep_blocks(uint64_t n);
+cudaError_t launch_onesweep_batch(int bits, const batch_launch &b, cudaStream_t s);
+uint32_t sort_fixup_blocks(uint64_t n);
+uint32_t sort_runs_blocks(uint64_t n);  // 0: no launch (no run can be long)
+cudaError_t launch_sort_fixup_batch(const batch_launch &b, cudaStream_t s);
+cudaError_t launch_sort_runs_batch(const batch_launch &b, cudaStream_t s);
 
 // Element slabs + agglomerative LBVH build over leaf buckets with bottom-up refit (FP64 or FP32 slabs): the
 // block-local phase, which queues unfinished subtrees for launch_climb.
@@ -223,6 +330,17 @@ cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, uin
 cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint8_t *bdel, void *node_box, int2 *child, int2 *range,
                          int *parent, int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s);
 
+// Batched forms of the slab kernel (items: slabs_args; one V for all items), the block-local build, the climb and
+// the refit (items: tree_args of objects with more than one bucket), with the blocks of one item.
+uint32_t slabs_blocks(uint64_t n);
+cudaError_t launch_slabs_batch(int K, bool fp32, uint32_t V, const batch_launch &b, cudaStream_t s);
+uint32_t build_blocks(uint64_t n);
+cudaError_t launch_build_batch(int K, bool fp32, const batch_launch &b, cudaStream_t s);
+uint32_t climb_blocks(uint64_t n);
+cudaError_t launch_climb_batch(int K, bool fp32, const batch_launch &b, cudaStream_t s);
+uint32_t refit_blocks(uint64_t n);
+cudaError_t launch_refit_batch(int K, bool fp32, const batch_launch &b, cudaStream_t s);
+
 // Refit with the topology of the last build, after launch_slabs recomputed the bucket boxes: every internal node.
 cudaError_t launch_refit(int K, bool fp32, uint64_t n, const void *bucket_box, void *node_box, const int *parent,
                          int *exch, obj_scalars *sc, cudaStream_t s);
@@ -241,6 +359,72 @@ struct tree_view
   uint64_t n;
   const obj_scalars *sc;
 };
+
+// The traversal of one scene (query object q against target tree t) as kernel arguments: the pointer members that
+// hold slabs point to FP64 or FP32 values per the context's form.
+struct trav_item
+{
+  const void *qwarp;
+  const double *qverts;
+  uint32_t qV;
+  const void *qrows;
+  const uint32_t *qperm;
+  uint32_t nq;
+  const int2 *child;
+  const void *nbox;
+  const int2 *range;
+  const double *tverts;
+  uint32_t tV;
+  const void *tcache;
+  const uint32_t *tperm;
+  const obj_scalars *tsc;
+  uint32_t nt;
+  int self;
+  double eps;
+  float eps_hi;
+  uint2 *pairs;
+  uint64_t cap;
+  pair_scalars *ps;
+  int dense_stack;
+  const obj_scalars *qsc;
+};
+
+// One scene's traversal for a batched launch: its item, its blocks and whether it takes the dense walk (the batch
+// launches the dense and the other scenes separately).
+void traverse_item(int K, bool fp32, tree_view q, tree_view t, bool self, bool dense, double eps, uint2 *pairs,
+                   uint64_t cap, pair_scalars *ps, int dense_stack_limit, trav_item *item, uint32_t *blocks,
+                   bool *dense_out);
+// V: the vertex count of every query and target object of the items (0: mixed).
+cudaError_t launch_traverse_batch(int K, bool fp32, bool dense, uint32_t V, const batch_launch &b, cudaStream_t s);
+
+struct recheck_args
+{
+  const double *va;
+  uint32_t Va;
+  const double *vb;
+  uint32_t Vb;
+  double eps;
+  const uint2 *cand;
+  uint64_t cand_cap;
+  uint2 *out;
+  uint64_t cap;
+  pair_scalars *ps;
+};
+uint32_t recheck_blocks(uint64_t ncand);
+cudaError_t launch_recheck_batch(int K, uint32_t V, const batch_launch &b, cudaStream_t s);
+
+struct gid_args
+{
+  const uint2 *pairs;
+  const unsigned long long *count;
+  uint64_t cap;
+  const uint64_t *gid_a;
+  const uint64_t *gid_b;
+  int normalize;
+  uint64_t *out;
+};
+uint32_t gid_pairs_dev_blocks(uint64_t cap);
+cudaError_t launch_gid_pairs_dev_batch(const batch_launch &b, cudaStream_t s);
 
 // Queries every leaf of q against tree t; writes (q element, t element) local index pairs. dense (both objects'
 // element slabs stored): the walk that pops nodes in batches and tests leaves in batches; its deeper stack bound can

@@ -95,20 +95,24 @@ __device__ __forceinline__ void element_centroid_bounds(const double *p, int V, 
 // K1. Each block stages a tile of 256 elements (256 * V * 24 bytes, contiguous) into shared memory with
 // coalesced 16-byte loads, then each thread reduces its own element. Grid-stride over tiles.
 template< int K, int VT >
-__global__ void __launch_bounds__( kElemThreads ) k_centroid_bounds(const double *__restrict__ verts, uint32_t Vrt,
-                                                                  uint64_t n, double eps, double *__restrict__ cx,
-                                                                  double *__restrict__ cy, double *__restrict__ cz,
-                                                                  obj_scalars *__restrict__ sc)
+__device__ void cb_body(const cb_args &args, uint32_t bid, uint32_t nblk)
 {
+  const double *__restrict__ verts = args.verts;
+  const uint64_t n = args.n;
+  const double eps = args.eps;
+  double *__restrict__ cx = args.cx;
+  double *__restrict__ cy = args.cy;
+  double *__restrict__ cz = args.cz;
+  obj_scalars *__restrict__ sc = args.sc;
   extern __shared__ double s_v[];
-  const int V = VT > 0 ? VT : static_cast< int >( Vrt );
+  const int V = VT > 0 ? VT : static_cast< int >( args.V );
   const int per = V * 3;
   const double inf = __longlong_as_double( 0x7ff0000000000000LL );
   double mn[3] = { inf, inf, inf };  // identity of min
   double mx[3] = { -inf, -inf, -inf };
   bool bad = false;
-  for ( uint64_t t0 = static_cast< uint64_t >( blockIdx.x ) * kElemThreads; t0 < n;
-        t0 += static_cast< uint64_t >( gridDim.x ) * kElemThreads )
+  for ( uint64_t t0 = static_cast< uint64_t >( bid ) * kElemThreads; t0 < n;
+        t0 += static_cast< uint64_t >( nblk ) * kElemThreads )
   {
     const int cnt = static_cast< int >( min( static_cast< uint64_t >( kElemThreads ), n - t0 ) );
     const double *src = verts + t0 * per;
@@ -137,11 +141,16 @@ __global__ void __launch_bounds__( kElemThreads ) k_centroid_bounds(const double
 // partial tile through plain loads. Every wait on a copy is bounded: past spin_limit polls the block raises the
 // object's error word, waits (bounded) for its copies in flight and stops.
 template< int K, int VT >
-__global__ void __launch_bounds__( kElemThreads, VT == 8 ? 2 : 3 ) k_centroid_bounds_tma(const double *__restrict__ verts, uint64_t n,
-                                                                      double eps, double *__restrict__ cx,
-                                                                      double *__restrict__ cy, double *__restrict__ cz,
-                                                                      obj_scalars *__restrict__ sc, uint32_t spin_limit)
+__device__ void cb_tma_body(const cb_args &args, uint32_t bid, uint32_t nblk)
 {
+  const double *__restrict__ verts = args.verts;
+  const uint64_t n = args.n;
+  const double eps = args.eps;
+  double *__restrict__ cx = args.cx;
+  double *__restrict__ cy = args.cy;
+  double *__restrict__ cz = args.cz;
+  obj_scalars *__restrict__ sc = args.sc;
+  const uint32_t spin_limit = args.spin_limit;
   constexpr int per = VT * 3;
   constexpr uint32_t kTileD = kElemThreads * per;  // doubles per tile
   extern __shared__ __align__( 128 ) double s_stage[];  // 2 stages of kTileD doubles
@@ -152,7 +161,7 @@ __global__ void __launch_bounds__( kElemThreads, VT == 8 ? 2 : 3 ) k_centroid_bo
   bool bad = false;
   const uint64_t tiles = ( n + kElemThreads - 1 ) / kElemThreads;
   const uint64_t full = n / kElemThreads;  // tiles that are bulk-copied
-  const uint64_t G = gridDim.x;
+  const uint64_t G = nblk;
   const int tid = threadIdx.x;
   auto issue = [&](uint64_t t, int st) {
     mbar_expect_tx( &s_mbar[st], kTileD * 8 );
@@ -164,21 +173,21 @@ __global__ void __launch_bounds__( kElemThreads, VT == 8 ? 2 : 3 ) k_centroid_bo
     mbar_init( &s_mbar[0], 1 );
     mbar_init( &s_mbar[1], 1 );
     mbar_init_fence();
-    if ( blockIdx.x < full )
+    if ( bid < full )
     {
-      issue( blockIdx.x, 0 );
+      issue( bid, 0 );
       pend |= 1u;
     }
-    if ( blockIdx.x + G < full )
+    if ( bid + G < full )
     {
-      issue( blockIdx.x + G, 1 );
+      issue( bid + G, 1 );
       pend |= 2u;
     }
   }
   __syncthreads();
   uint32_t phases = 0;  // bit s: parity of stage s's next completion
   int st = 0;
-  for ( uint64_t t = blockIdx.x; t < tiles; t += G, st ^= 1 )
+  for ( uint64_t t = bid; t < tiles; t += G, st ^= 1 )
   {
     double *sv = s_stage + st * kTileD;
     const int cnt = static_cast< int >( min( static_cast< uint64_t >( kElemThreads ), n - t * kElemThreads ) );
@@ -240,12 +249,15 @@ __device__ __forceinline__ uint64_t quant21(double c, double mn, double inv)
 // runs, those over the high key half (warp-aggregated shared-memory counters, one global atomic per nonzero bin
 // per block).
 template< int BITS >
-__global__ void __launch_bounds__( kElemThreads ) k_keys_hist(const double *__restrict__ cx,
-                                                            const double *__restrict__ cy,
-                                                            const double *__restrict__ cz, uint64_t n,
-                                                            obj_scalars *__restrict__ sc, uint64_t *__restrict__ keys,
-                                                            uint32_t *__restrict__ hist)
+__device__ void kh_body(const kh_args &args, uint32_t bid, uint32_t nblk)
 {
+  const double *__restrict__ cx = args.cx;
+  const double *__restrict__ cy = args.cy;
+  const double *__restrict__ cz = args.cz;
+  const uint64_t n = args.n;
+  obj_scalars *__restrict__ sc = args.sc;
+  uint64_t *__restrict__ keys = args.keys;
+  uint32_t *__restrict__ hist = args.hist;
   constexpr int RADIX = 1 << BITS;
   constexpr int PASSES = ( kKeyBits + BITS - 1 ) / BITS;
   constexpr int FIRST = 32 / BITS;  // only the passes over the high key half run (the fix-up sorts the low half)
@@ -262,7 +274,7 @@ __global__ void __launch_bounds__( kElemThreads ) k_keys_hist(const double *__re
     const double inv = __ddiv_rn( 1.0, width );
     s_min[c] = mn;
     s_inv[c] = inv;
-    if ( blockIdx.x == 0 )
+    if ( bid == 0 )
     {
       sc->min3[c] = mn;
       sc->inv3[c] = inv;
@@ -275,8 +287,8 @@ __global__ void __launch_bounds__( kElemThreads ) k_keys_hist(const double *__re
   // Each warp takes runs of kKeyUnroll * 32 consecutive elements (element w0 + 32 u + lane in step u): the loads of
   // all steps are issued before the first key is formed, which keeps kKeyUnroll loads per thread in flight.
   constexpr int U = kKeyUnroll;
-  const uint64_t stride = static_cast< uint64_t >( gridDim.x ) * kElemThreads * U;
-  const uint64_t base = static_cast< uint64_t >( blockIdx.x ) * kElemThreads * U;
+  const uint64_t stride = static_cast< uint64_t >( nblk ) * kElemThreads * U;
+  const uint64_t base = static_cast< uint64_t >( bid ) * kElemThreads * U;
   // Every warp runs the same number of iterations so that the warp-wide match below sees all 32 lanes.
   for ( uint64_t w0 = base + ( threadIdx.x & ~31u ) * U; w0 < n; w0 += stride )
   {
@@ -338,73 +350,152 @@ int sm_count()
 }
 
 template< int K, int VT >
-cudaError_t launch_cb_t(const double *verts, uint32_t V, uint64_t n, double eps, double *cx, double *cy, double *cz,
-                        obj_scalars *sc, uint32_t spin_limit, cudaStream_t s)
+constexpr int kCbTmaMinBlocks = VT == 8 ? 2 : 3;
+
+// Shared memory of the centroid/bounds kernels: two TMA stages of 256 elements, or one plain tile.
+size_t cb_smem(uint32_t V, bool tma)
+{
+  return static_cast< size_t >( tma ? 2 : 1 ) * kElemThreads * V * 3 * sizeof( double );
+}
+
+// Per device: the shared-memory opt-in of both launch forms of the TMA kernel and its resident blocks per SM.
+template< int K, int VT >
+cudaError_t cb_tma_setup(int *per_sm_out)
+{
+  static int per_sm[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice( &dev );
+  if ( e != cudaSuccess ) return e;
+  if ( dev < 0 || dev >= 64 ) return cudaErrorInvalidDevice;
+  if ( !per_sm[dev] )
+  {
+    const int smem2 = static_cast< int >( cb_smem( VT, true ) );
+    constexpr int MB = kCbTmaMinBlocks< K, VT >;
+    e = cudaFuncSetAttribute( k_single< cb_args, cb_tma_body< K, VT >, kElemThreads, MB >,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem2 );
+    if ( e != cudaSuccess ) return e;
+    e = cudaFuncSetAttribute( k_batched< cb_args, cb_tma_body< K, VT >, kElemThreads, MB >,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem2 );
+    if ( e != cudaSuccess ) return e;
+    int b = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &b, k_single< cb_args, cb_tma_body< K, VT >, kElemThreads, MB >,
+                                                       kElemThreads, smem2 );
+    if ( e != cudaSuccess ) return e;
+    per_sm[dev] = b > 0 ? b : 1;
+  }
+  *per_sm_out = per_sm[dev];
+  return cudaSuccess;
+}
+
+template< int K, int VT >
+cudaError_t cb_plain_setup(uint32_t V)
+{
+  const size_t smem = cb_smem( V, false );
+  // Static shared memory counts against the same 48 KB default: opt in whenever the tile is large.
+  if ( smem < 40 * 1024 ) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute( k_single< cb_args, cb_body< K, VT >, kElemThreads, 4 >,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( smem ) );
+  if ( e != cudaSuccess ) return e;
+  return cudaFuncSetAttribute( k_batched< cb_args, cb_body< K, VT >, kElemThreads, 4 >,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( smem ) );
+}
+
+// Blocks of one object's centroid/bounds launch.
+uint32_t cb_grid(uint64_t n, bool tma, int per_sm)
+{
+  const uint64_t tiles = ( n + kElemThreads - 1 ) / kElemThreads;
+  const uint64_t cap = static_cast< uint64_t >( sm_count() ) * ( tma ? per_sm : 8 );
+  return static_cast< uint32_t >( tiles < cap ? ( tiles ? tiles : 1 ) : cap );
+}
+
+template< int K, int VT >
+cudaError_t launch_cb_t(const cb_args &a, cudaStream_t s)
 {
   if constexpr ( VT > 0 )
   {
-    if ( ( reinterpret_cast< uintptr_t >( verts ) & 15 ) == 0 )
+    if ( ( reinterpret_cast< uintptr_t >( a.verts ) & 15 ) == 0 )
     {
-      const size_t smem2 = static_cast< size_t >( 2 ) * kElemThreads * VT * 3 * sizeof( double );
-      // per device: the shared-memory opt-in and the resident blocks per SM of the persistent grid
-      static int per_sm[64] = {};
-      int dev = 0;
-      cudaError_t e = cudaGetDevice( &dev );
+      int per_sm = 1;
+      cudaError_t e = cb_tma_setup< K, VT >( &per_sm );
       if ( e != cudaSuccess ) return e;
-      if ( dev < 0 || dev >= 64 ) return cudaErrorInvalidDevice;
-      if ( !per_sm[dev] )
-      {
-        e = cudaFuncSetAttribute( k_centroid_bounds_tma< K, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast< int >( smem2 ) );
-        if ( e != cudaSuccess ) return e;
-        int b = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &b, k_centroid_bounds_tma< K, VT >, kElemThreads, smem2 );
-        if ( e != cudaSuccess ) return e;
-        per_sm[dev] = b > 0 ? b : 1;
-      }
-      const uint64_t tiles = ( n + kElemThreads - 1 ) / kElemThreads;
-      const uint64_t cap = static_cast< uint64_t >( sm_count() ) * per_sm[dev];
-      const unsigned grid = static_cast< unsigned >( tiles < cap ? ( tiles ? tiles : 1 ) : cap );
-      k_centroid_bounds_tma< K, VT ><<< grid, kElemThreads, smem2, s >>>( verts, n, eps, cx, cy, cz, sc, spin_limit );
+      k_single< cb_args, cb_tma_body< K, VT >, kElemThreads, kCbTmaMinBlocks< K, VT > >
+        <<< cb_grid( a.n, true, per_sm ), kElemThreads, cb_smem( VT, true ), s >>>( a );
       return cudaGetLastError();
     }
   }
-  const size_t smem = static_cast< size_t >( kElemThreads ) * V * 3 * sizeof( double );
-  // Static shared memory counts against the same 48 KB default: opt in whenever the tile is large.
-  if ( smem >= 40 * 1024 )
+  cudaError_t e = cb_plain_setup< K, VT >( a.V );
+  if ( e != cudaSuccess ) return e;
+  k_single< cb_args, cb_body< K, VT >, kElemThreads, 4 ><<< cb_grid( a.n, false, 0 ), kElemThreads, cb_smem( a.V, false ), s >>>( a );
+  return cudaGetLastError();
+}
+
+// Batched: every item's verts 16-byte aligned and VT > 0 for the TMA form (tma), one V for all items.
+template< int K, int VT >
+cudaError_t launch_cb_batch_t(uint32_t V, bool tma, const batch_launch &b, cudaStream_t s)
+{
+  const cb_args *items = static_cast< const cb_args * >( b.items );
+  if constexpr ( VT > 0 )
   {
-    cudaError_t e = cudaFuncSetAttribute( k_centroid_bounds< K, VT >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast< int >( smem ) );
-    if ( e != cudaSuccess ) return e;
+    if ( tma )
+    {
+      int per_sm = 1;
+      cudaError_t e = cb_tma_setup< K, VT >( &per_sm );
+      if ( e != cudaSuccess ) return e;
+      k_batched< cb_args, cb_tma_body< K, VT >, kElemThreads, kCbTmaMinBlocks< K, VT > >
+        <<< b.blocks, kElemThreads, cb_smem( VT, true ), s >>>( items, b.starts, b.nitems );
+      return cudaGetLastError();
+    }
   }
-  const uint64_t tiles = ( n + kElemThreads - 1 ) / kElemThreads;
-  const uint64_t cap = static_cast< uint64_t >( sm_count() ) * 8;
-  const unsigned grid = static_cast< unsigned >( tiles < cap ? ( tiles ? tiles : 1 ) : cap );
-  k_centroid_bounds< K, VT ><<< grid, kElemThreads, smem, s >>>( verts, V, n, eps, cx, cy, cz, sc );
+  cudaError_t e = cb_plain_setup< K, VT >( V );
+  if ( e != cudaSuccess ) return e;
+  k_batched< cb_args, cb_body< K, VT >, kElemThreads, 4 ><<< b.blocks, kElemThreads, cb_smem( V, false ), s >>>(
+    items, b.starts, b.nitems );
   return cudaGetLastError();
 }
 
 template< int K >
-cudaError_t launch_cb_k(const double *verts, uint32_t V, uint64_t n, double eps, double *cx, double *cy, double *cz,
-                        obj_scalars *sc, uint32_t spin_limit, cudaStream_t s)
+cudaError_t launch_cb_k(const cb_args &a, cudaStream_t s)
 {
-  switch ( V )
+  switch ( a.V )
   {
-    case 3: return launch_cb_t< K, 3 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
-    case 4: return launch_cb_t< K, 4 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
-    case 8: return launch_cb_t< K, 8 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
-    default: return launch_cb_t< K, 0 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
+    case 3: return launch_cb_t< K, 3 >( a, s );
+    case 4: return launch_cb_t< K, 4 >( a, s );
+    case 8: return launch_cb_t< K, 8 >( a, s );
+    default: return launch_cb_t< K, 0 >( a, s );
   }
 }
 
-template< int BITS >
-cudaError_t launch_kh_t(const double *cx, const double *cy, const double *cz, uint64_t n, obj_scalars *sc,
-                        uint64_t *keys, uint32_t *hist, cudaStream_t s)
+template< int K >
+cudaError_t launch_cb_batch_k(uint32_t V, bool tma, const batch_launch &b, cudaStream_t s)
+{
+  switch ( V )
+  {
+    case 3: return launch_cb_batch_t< K, 3 >( V, tma, b, s );
+    case 4: return launch_cb_batch_t< K, 4 >( V, tma, b, s );
+    case 8: return launch_cb_batch_t< K, 8 >( V, tma, b, s );
+    default: return launch_cb_batch_t< K, 0 >( V, false, b, s );
+  }
+}
+
+uint32_t kh_grid(uint64_t n)
 {
   const uint64_t blocks = ( n + kElemThreads * kKeyUnroll - 1 ) / ( kElemThreads * kKeyUnroll );
   const uint64_t cap = static_cast< uint64_t >( sm_count() ) * 8;
-  const unsigned grid = static_cast< unsigned >( blocks < cap ? ( blocks ? blocks : 1 ) : cap );
-  k_keys_hist< BITS ><<< grid, kElemThreads, 0, s >>>( cx, cy, cz, n, sc, keys, hist );
+  return static_cast< uint32_t >( blocks < cap ? ( blocks ? blocks : 1 ) : cap );
+}
+
+template< int BITS >
+cudaError_t launch_kh_t(const kh_args &a, cudaStream_t s)
+{
+  k_single< kh_args, kh_body< BITS >, kElemThreads, 1 ><<< kh_grid( a.n ), kElemThreads, 0, s >>>( a );
+  return cudaGetLastError();
+}
+
+template< int BITS >
+cudaError_t launch_kh_batch_t(const batch_launch &b, cudaStream_t s)
+{
+  k_batched< kh_args, kh_body< BITS >, kElemThreads, 1 ><<< b.blocks, kElemThreads, 0, s >>>(
+    static_cast< const kh_args * >( b.items ), b.starts, b.nitems );
   return cudaGetLastError();
 }
 
@@ -416,22 +507,32 @@ namespace {
 
 // The reset state of a rebuild in one launch: the object's scalars (zero, Morton-bound minima at the largest
 // encoding), the digit histograms, the look-back words of the passes that run, the climb's exchange slots (-1).
-__global__ void k_obj_init(obj_scalars *sc, uint32_t *hist, uint64_t hist_words, uint32_t *status,
-                           uint64_t status_words, int *exch, uint64_t exch_words)
+__device__ void init_body(const init_args &a, uint32_t bid, uint32_t nblk)
 {
-  const uint64_t stride = static_cast< uint64_t >( gridDim.x ) * blockDim.x;
-  const uint64_t t = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x;
-  constexpr uint64_t sc_words = sizeof( obj_scalars ) / 4;
-  for ( uint64_t i = t; i < sc_words; i += stride ) reinterpret_cast< uint32_t * >( sc )[i] = 0u;
-  for ( uint64_t i = t; i < hist_words; i += stride ) hist[i] = 0u;
-  for ( uint64_t i = t; i < status_words; i += stride ) status[i] = 0u;
-  for ( uint64_t i = t; i < exch_words; i += stride ) exch[i] = -1;
+  const uint64_t stride = static_cast< uint64_t >( nblk ) * blockDim.x;
+  const uint64_t t = static_cast< uint64_t >( bid ) * blockDim.x + threadIdx.x;
+  const uint64_t sc_words = a.sc ? sizeof( obj_scalars ) / 4 : 0;  // no scalars: only the exchange slots (refit)
+  for ( uint64_t i = t; i < sc_words; i += stride ) reinterpret_cast< uint32_t * >( a.sc )[i] = 0u;
+  for ( uint64_t i = t; i < a.hist_words; i += stride ) a.hist[i] = 0u;
+  for ( uint64_t i = t; i < a.status_words; i += stride ) a.status[i] = 0u;
+  for ( uint64_t i = t; i < a.exch_words; i += stride ) a.exch[i] = -1;
   // the minima start at the largest encoding (written after the zeroing by the same thread)
   for ( uint64_t i = t; i < sc_words; i += stride )
   {
     const uint64_t byte = i * 4;
-    if ( byte < 3 * sizeof( unsigned long long ) ) reinterpret_cast< uint32_t * >( sc )[i] = 0xffffffffu;
+    if ( byte < 3 * sizeof( unsigned long long ) ) reinterpret_cast< uint32_t * >( a.sc )[i] = 0xffffffffu;
   }
+}
+
+uint32_t init_blocks(const init_args &a)
+{
+  uint64_t most = sizeof( obj_scalars ) / 4;
+  if ( a.hist_words > most ) most = a.hist_words;
+  if ( a.status_words > most ) most = a.status_words;
+  if ( a.exch_words > most ) most = a.exch_words;
+  const uint64_t blocks = ( most + 255 ) / 256;
+  const uint64_t cap = static_cast< uint64_t >( sm_count() ) * 4;
+  return static_cast< uint32_t >( blocks < cap ? blocks : cap );
 }
 
 }  // namespace
@@ -439,25 +540,67 @@ __global__ void k_obj_init(obj_scalars *sc, uint32_t *hist, uint64_t hist_words,
 cudaError_t launch_obj_init(obj_scalars *sc, uint32_t *hist, uint64_t hist_words, uint32_t *status,
                             uint64_t status_words, int *exch, uint64_t exch_words, cudaStream_t s)
 {
-  uint64_t most = sizeof( obj_scalars ) / 4;
-  if ( hist_words > most ) most = hist_words;
-  if ( status_words > most ) most = status_words;
-  if ( exch_words > most ) most = exch_words;
-  const uint64_t blocks = ( most + 255 ) / 256;
-  const uint64_t cap = static_cast< uint64_t >( sm_count() ) * 4;
-  k_obj_init<<< static_cast< unsigned >( blocks < cap ? blocks : cap ), 256, 0, s >>>( sc, hist, hist_words, status,
-                                                                                     status_words, exch, exch_words );
+  const init_args a{ sc, hist, hist_words, status, status_words, exch, exch_words };
+  k_single< init_args, init_body, 256, 1 ><<< init_blocks( a ), 256, 0, s >>>( a );
+  return cudaGetLastError();
+}
+
+uint32_t obj_init_blocks(const init_args &a) { return init_blocks( a ); }
+
+cudaError_t launch_obj_init_batch(const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+  k_batched< init_args, init_body, 256, 1 ><<< b.blocks, 256, 0, s >>>( static_cast< const init_args * >( b.items ),
+                                                                      b.starts, b.nitems );
   return cudaGetLastError();
 }
 
 cudaError_t launch_centroid_bounds(int K, const double *verts, uint32_t V, uint64_t n, double eps, double *cx,
                                    double *cy, double *cz, obj_scalars *sc, uint32_t spin_limit, cudaStream_t s)
 {
+  const cb_args a{ verts, V, n, eps, cx, cy, cz, sc, spin_limit };
   switch ( K )
   {
-    case 6: return launch_cb_k< 6 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
-    case 18: return launch_cb_k< 18 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
-    case 26: return launch_cb_k< 26 >( verts, V, n, eps, cx, cy, cz, sc, spin_limit, s );
+    case 6: return launch_cb_k< 6 >( a, s );
+    case 18: return launch_cb_k< 18 >( a, s );
+    case 26: return launch_cb_k< 26 >( a, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t centroid_bounds_blocks(int K, uint32_t V, uint64_t n, bool tma, uint32_t *blocks)
+{
+  int per_sm = 0;
+  if ( tma )
+  {
+    cudaError_t e = cudaSuccess;
+    switch ( K * 100 + static_cast< int >( V ) )
+    {
+      case 603: e = cb_tma_setup< 6, 3 >( &per_sm ); break;
+      case 604: e = cb_tma_setup< 6, 4 >( &per_sm ); break;
+      case 608: e = cb_tma_setup< 6, 8 >( &per_sm ); break;
+      case 1803: e = cb_tma_setup< 18, 3 >( &per_sm ); break;
+      case 1804: e = cb_tma_setup< 18, 4 >( &per_sm ); break;
+      case 1808: e = cb_tma_setup< 18, 8 >( &per_sm ); break;
+      case 2603: e = cb_tma_setup< 26, 3 >( &per_sm ); break;
+      case 2604: e = cb_tma_setup< 26, 4 >( &per_sm ); break;
+      case 2608: e = cb_tma_setup< 26, 8 >( &per_sm ); break;
+      default: return cudaErrorInvalidValue;
+    }
+    if ( e != cudaSuccess ) return e;
+  }
+  *blocks = cb_grid( n, tma, per_sm );
+  return cudaSuccess;
+}
+
+cudaError_t launch_centroid_bounds_batch(int K, uint32_t V, bool tma, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+  switch ( K )
+  {
+    case 6: return launch_cb_batch_k< 6 >( V, tma, b, s );
+    case 18: return launch_cb_batch_k< 18 >( V, tma, b, s );
+    case 26: return launch_cb_batch_k< 26 >( V, tma, b, s );
     default: return cudaErrorInvalidValue;
   }
 }
@@ -465,12 +608,28 @@ cudaError_t launch_centroid_bounds(int K, const double *verts, uint32_t V, uint6
 cudaError_t launch_keys_hist(int bits, const double *cx, const double *cy, const double *cz, uint64_t n,
                              obj_scalars *sc, uint64_t *keys, uint32_t *hist, cudaStream_t s)
 {
+  const kh_args a{ cx, cy, cz, n, sc, keys, hist };
   switch ( bits )
   {
-    case 1: return launch_kh_t< 1 >( cx, cy, cz, n, sc, keys, hist, s );
-    case 2: return launch_kh_t< 2 >( cx, cy, cz, n, sc, keys, hist, s );
-    case 4: return launch_kh_t< 4 >( cx, cy, cz, n, sc, keys, hist, s );
-    case 8: return launch_kh_t< 8 >( cx, cy, cz, n, sc, keys, hist, s );
+    case 1: return launch_kh_t< 1 >( a, s );
+    case 2: return launch_kh_t< 2 >( a, s );
+    case 4: return launch_kh_t< 4 >( a, s );
+    case 8: return launch_kh_t< 8 >( a, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+uint32_t keys_hist_blocks(uint64_t n) { return kh_grid( n ); }
+
+cudaError_t launch_keys_hist_batch(int bits, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+  switch ( bits )
+  {
+    case 1: return launch_kh_batch_t< 1 >( b, s );
+    case 2: return launch_kh_batch_t< 2 >( b, s );
+    case 4: return launch_kh_batch_t< 4 >( b, s );
+    case 8: return launch_kh_batch_t< 8 >( b, s );
     default: return cudaErrorInvalidValue;
   }
 }

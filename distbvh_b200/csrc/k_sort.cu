@@ -56,13 +56,20 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s
 // written out. Every wait is bounded (look-back polls and mbarrier waits); on a timeout the block raises the
 // object's error word and stops, and blocks that may have read a garbage prefix write nothing.
 template< int BITS >
-__global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *__restrict__ keys_in,
-                                                           const uint32_t *__restrict__ vals_in,
-                                                           uint64_t *__restrict__ keys_out,
-                                                           uint32_t *__restrict__ vals_out, uint64_t n64, int pass,
-                                                           const uint32_t *__restrict__ hist, uint32_t *status,
-                                                           obj_scalars *sc, uint32_t spin_limit, int stall, int use_tma)
+__device__ void onesweep_body(const sort_pass_args &a, uint32_t, uint32_t)
 {
+  const uint64_t *__restrict__ keys_in = a.keys_in;
+  const uint32_t *__restrict__ vals_in = a.vals_in;
+  uint64_t *__restrict__ keys_out = a.keys_out;
+  uint32_t *__restrict__ vals_out = a.vals_out;
+  const uint64_t n64 = a.n;
+  const int pass = a.pass;
+  const uint32_t *__restrict__ hist = a.hist;
+  uint32_t *status = a.status;
+  obj_scalars *sc = a.sc;
+  const uint32_t spin_limit = a.spin_limit;
+  const int stall = a.stall;
+  const int use_tma = a.use_tma;
   constexpr int RADIX = 1 << BITS;
   constexpr uint32_t MASK = RADIX - 1;
   extern __shared__ __align__( 128 ) unsigned char s_raw[];  // 2 stages of [kSortTile keys][kSortTile indices]
@@ -311,35 +318,53 @@ __global__ void __launch_bounds__( kSortThreads, 2 ) k_onesweep(const uint64_t *
   }
 }
 
+// The attribute is per device and per kernel: set it once for each device this process launches on.
 template< int BITS >
-cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out, uint32_t *vals_out,
-                        uint64_t n, int pass, const uint32_t *hist, uint32_t *status, obj_scalars *sc,
-                        uint32_t spin_limit, int stall, cudaStream_t s)
+cudaError_t onesweep_setup()
 {
-  constexpr int RADIX = 1 << BITS;
-  const size_t smem = static_cast< size_t >( 2 ) * kSortTile * ( sizeof( uint64_t ) + sizeof( uint32_t ) );
-  // The attribute is per device: set it once for each device this process launches on.
   static std::atomic< unsigned long long > configured{ 0 };
   int dev = 0;
   cudaError_t e = cudaGetDevice( &dev );
   if ( e != cudaSuccess ) return e;
   const unsigned long long bit = 1ull << ( dev & 63 );
-  if ( !( configured.load() & bit ) )
-  {
-    e = cudaFuncSetAttribute( k_onesweep< BITS >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast< int >( smem ) );
-    if ( e != cudaSuccess ) return e;
-    configured.fetch_or( bit );
-  }
+  if ( configured.load() & bit ) return cudaSuccess;
+  const int smem = static_cast< int >( 2 * kSortTile * ( sizeof( uint64_t ) + sizeof( uint32_t ) ) );
+  e = cudaFuncSetAttribute( k_single< sort_pass_args, onesweep_body< BITS >, kSortThreads, 2 >,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem );
+  if ( e != cudaSuccess ) return e;
+  e = cudaFuncSetAttribute( k_batched< sort_pass_args, onesweep_body< BITS >, kSortThreads, 2 >,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem );
+  if ( e != cudaSuccess ) return e;
+  configured.fetch_or( bit );
+  return cudaSuccess;
+}
+
+constexpr size_t kOnesweepSmem = static_cast< size_t >( 2 ) * kSortTile * ( sizeof( uint64_t ) + sizeof( uint32_t ) );
+
+// persistent: two blocks per SM (shared memory for two 48 KB stages each), never more blocks than tiles
+uint32_t os_grid(uint64_t n)
+{
   const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
-  // persistent: two blocks per SM (shared memory for two 48 KB stages each), never more blocks than tiles
   const uint64_t cap = static_cast< uint64_t >( device_sm_count() ) * 2;
-  const unsigned grid = static_cast< unsigned >( tiles < cap ? tiles : cap );
-  const int use_tma = ( ( reinterpret_cast< uintptr_t >( keys_in ) | reinterpret_cast< uintptr_t >( vals_in ) ) & 15 ) == 0;
-  k_onesweep< BITS ><<< grid, kSortThreads, smem, s >>>( keys_in, vals_in, keys_out, vals_out, n, pass,
-                                                        hist + static_cast< size_t >( pass ) * RADIX,
-                                                        status + static_cast< size_t >( pass ) * ( tiles + 1 ) * RADIX,
-                                                        sc, spin_limit, stall, use_tma );
+  return static_cast< uint32_t >( tiles < cap ? tiles : cap );
+}
+
+template< int BITS >
+cudaError_t launch_os_t(const sort_pass_args &a, cudaStream_t s)
+{
+  cudaError_t e = onesweep_setup< BITS >();
+  if ( e != cudaSuccess ) return e;
+  k_single< sort_pass_args, onesweep_body< BITS >, kSortThreads, 2 ><<< os_grid( a.n ), kSortThreads, kOnesweepSmem, s >>>( a );
+  return cudaGetLastError();
+}
+
+template< int BITS >
+cudaError_t launch_os_batch_t(const batch_launch &b, cudaStream_t s)
+{
+  cudaError_t e = onesweep_setup< BITS >();
+  if ( e != cudaSuccess ) return e;
+  k_batched< sort_pass_args, onesweep_body< BITS >, kSortThreads, 2 ><<< b.blocks, kSortThreads, kOnesweepSmem, s >>>(
+    static_cast< const sort_pass_args * >( b.items ), b.starts, b.nitems );
   return cudaGetLastError();
 }
 
@@ -348,16 +373,156 @@ cudaError_t launch_os_t(const uint64_t *keys_in, const uint32_t *vals_in, uint64
 // of a run at the run's start plus its rank by (full key, position) -- a stable sort of the run by the low half --
 // then gives the stable order of the full keys. One thread per element, out of place (in -> out), so that no
 // thread reads what another writes. Runs are found by scanning neighbours (cache hits: a warp reads contiguous
-// keys). A run longer than kFixRun is copied in order; the thread at its start lists it for k_sort_runs, which
-// sorts it by the low half on the device.
+// keys). A run longer than kFixRun is listed and sorted from `in` to `out` by runs_body (sort_run_block); no thread
+// of the fix-up writes its elements.
 constexpr int kFixRun = 32;
+constexpr int kFixThreads = 512;
+constexpr int kFixWarps = kFixThreads / 32;
+constexpr int kRunSmem = 2048;
 
-__global__ void __launch_bounds__( 256 ) k_sort_fixup(const uint64_t *__restrict__ keys_in,
-                                                      const uint32_t *__restrict__ vals_in,
-                                                      uint64_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
-                                                      uint32_t n, uint32_t *__restrict__ runs, obj_scalars *sc)
+// Stable sort by the low key half of the run [s, s + L) of equal high halves, by one block of kFixThreads threads,
+// from (src keys, src vals) into (dst keys, dst vals). Up to kRunSmem elements: a bitonic network in shared memory
+// over the distinct composite keys (low half << 32 | position in the run), whose order is the stable order. Longer:
+// the run is copied to dst, then four stable 8-bit LSD passes over the low half ping-pong between dst and src (src
+// is scratch then: nothing reads it after the radix passes but this block, and the high halves every neighbour
+// scan compares stay in place), ending in dst; per pass, 512 elements at a time are ranked by warp match in
+// element order and placed at the digit's running offset.
+__device__ void sort_run_block(uint64_t *__restrict__ skeys, uint32_t *__restrict__ svals, uint64_t *__restrict__ dkeys,
+                               uint32_t *__restrict__ dvals, uint32_t s, uint32_t L, unsigned char *s_raw,
+                               uint32_t *s_scan)
 {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned lt_mask = ( 1u << lane ) - 1u;
+  const uint64_t hi_bits = skeys[s] & 0xffffffff00000000ull;
+  if ( L <= kRunSmem )
+  {
+    uint64_t *c = reinterpret_cast< uint64_t * >( s_raw );
+    uint32_t *v = reinterpret_cast< uint32_t * >( s_raw + kRunSmem * 8 );
+    uint32_t P = 1;
+    while ( P < L ) P <<= 1;
+    for ( uint32_t j = tid; j < P; j += kFixThreads )
+    {
+      if ( j < L )
+      {
+        c[j] = ( ( skeys[s + j] & 0xffffffffull ) << 32 ) | j;
+        v[j] = svals[s + j];
+      } else {
+        c[j] = ~0ull;
+      }
+    }
+    __syncthreads();
+    for ( uint32_t k = 2; k <= P; k <<= 1 )
+      for ( uint32_t j = k >> 1; j > 0; j >>= 1 )
+      {
+        for ( uint32_t t = tid; t < P; t += kFixThreads )
+        {
+          const uint32_t u = t ^ j;
+          if ( u > t )
+          {
+            const uint64_t a = c[t], b = c[u];
+            if ( ( a > b ) == ( ( t & k ) == 0 ) )
+            {
+              c[t] = b;
+              c[u] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    for ( uint32_t j = tid; j < L; j += kFixThreads )
+    {
+      const uint64_t x = c[j];
+      dkeys[s + j] = hi_bits | ( x >> 32 );
+      dvals[s + j] = v[x & 0xffffffffull];
+    }
+    __syncthreads();
+    return;
+  }
+  uint32_t( *cnt )[256] = reinterpret_cast< uint32_t( * )[256] >( s_raw );  // [kFixWarps][256]
+  uint32_t *run_off = reinterpret_cast< uint32_t * >( s_raw + kFixWarps * 256 * 4 );
+  uint32_t *tot = run_off + 256;
+  uint32_t( *hist )[256] = reinterpret_cast< uint32_t( * )[256] >( tot + 256 );  // [4][256]
+  for ( int q = tid; q < kFixWarps * 256; q += kFixThreads ) ( &cnt[0][0] )[q] = 0;
+  for ( int q = tid; q < 4 * 256; q += kFixThreads ) ( &hist[0][0] )[q] = 0;
+  for ( uint32_t j = tid; j < L; j += kFixThreads )
+  {
+    dkeys[s + j] = skeys[s + j];
+    dvals[s + j] = svals[s + j];
+  }
+  __syncthreads();
+  for ( uint32_t j = tid; j < L; j += kFixThreads )
+  {
+    const uint32_t low = static_cast< uint32_t >( dkeys[s + j] );
+#pragma unroll
+    for ( int p = 0; p < 4; ++p ) atomicAdd( &hist[p][( low >> ( 8 * p ) ) & 255u], 1u );
+  }
+  __syncthreads();
+  uint64_t *sk = dkeys, *dk = skeys;
+  uint32_t *sv = dvals, *dv = svals;
+  for ( int p = 0; p < 4; ++p )
+  {
+    const uint32_t x = tid < 256 ? hist[p][tid] : 0u;
+    const uint32_t ex = block_exclusive_scan( x, s_scan );
+    if ( tid < 256 ) run_off[tid] = ex;
+    __syncthreads();
+    for ( uint32_t base = 0; base < L; base += kFixThreads )
+    {
+      const uint32_t j = base + tid;
+      const bool valid = j < L;
+      const uint64_t key = valid ? sk[s + j] : 0ull;
+      const uint32_t val = valid ? sv[s + j] : 0u;
+      const uint32_t d = valid ? ( static_cast< uint32_t >( key ) >> ( 8 * p ) ) & 255u : 256u;
+      const unsigned peers = __match_any_sync( 0xffffffffu, d );
+      const uint32_t rank = __popc( peers & lt_mask );
+      if ( valid && lane == __ffs( peers ) - 1 ) cnt[warp][d] = __popc( peers );
+      __syncthreads();
+      if ( tid < 256 )
+      {
+        uint32_t t = 0;
+#pragma unroll
+        for ( int w = 0; w < kFixWarps; ++w )
+        {
+          const uint32_t c = cnt[w][tid];
+          cnt[w][tid] = t;
+          t += c;
+        }
+        tot[tid] = t;
+      }
+      __syncthreads();
+      if ( valid )
+      {
+        const uint32_t pos = run_off[d] + cnt[warp][d] + rank;
+        dk[s + pos] = key;
+        dv[s + pos] = val;
+      }
+      __syncthreads();
+      if ( tid < 256 )
+      {
+        run_off[tid] += tot[tid];
+#pragma unroll
+        for ( int w = 0; w < kFixWarps; ++w ) cnt[w][tid] = 0;
+      }
+      __syncthreads();
+    }
+    uint64_t *tk = sk;
+    sk = dk;
+    dk = tk;
+    uint32_t *tv = sv;
+    sv = dv;
+    dv = tv;
+  }
+}
+
+// The fix-up proper: one lean thread per element. A run longer than kFixRun is left in place and its first element
+// listed (runs[], count in sc->long_runs) for runs_body.
+__device__ void fixup_body(const fixup_args &a, uint32_t bid, uint32_t)
+{
+  const uint64_t *__restrict__ keys_in = a.keys_in;
+  const uint32_t *__restrict__ vals_in = a.vals_in;
+  uint64_t *__restrict__ keys_out = a.keys_out;
+  uint32_t *__restrict__ vals_out = a.vals_out;
+  const uint32_t n = static_cast< uint32_t >( a.n );
+  const uint32_t i = bid * blockDim.x + threadIdx.x;
   if ( i >= n ) return;
   const uint64_t ki = keys_in[i];
   const uint32_t hi = static_cast< uint32_t >( ki >> 32 );
@@ -381,13 +546,16 @@ __global__ void __launch_bounds__( 256 ) k_sort_fixup(const uint64_t *__restrict
       break;
     }
   }
-  uint32_t pos = i;
   if ( limit || e - s + 1 > kFixRun )
   {
-    // s == i only at the run's first element (the backward scan stops before its limit there); the run holds at
-    // least kFixRun + 1 elements, so at most n / 33 runs are listed
-    if ( s == i ) runs[atomicAdd( &sc->long_runs, 1u )] = i;
-  } else if ( e > s ) {
+    // s == i only at the run's first element (the backward scan stops before its limit there); a run has more
+    // than kFixRun elements, so at most n / 33 runs are listed
+    if ( s == i ) a.runs[atomicAdd( &a.sc->long_runs, 1u )] = i;
+    return;
+  }
+  uint32_t pos = i;
+  if ( e > s )
+  {
     uint32_t rank = 0;
     for ( uint32_t j = s; j <= e; ++j )
     {
@@ -400,196 +568,115 @@ __global__ void __launch_bounds__( 256 ) k_sort_fixup(const uint64_t *__restrict
   vals_out[pos] = vals_in[i];
 }
 
-// Stable sort of the long runs by the low key half. Block r takes runs r, r + grid, ...; a run is the range of
-// equal high halves that starts at its listed index (its end by binary search: the keys are ordered by the high
-// half). A run of up to kRunSmem elements is sorted in shared memory by a bitonic network over the distinct
-// composite keys (low half << 32 | position in the run), whose order is the stable order. A longer run takes four
-// stable 8-bit LSD passes over the low half through the scratch arrays (ping-pong, ending back in keys/vals): per
-// pass, 512 elements at a time are ranked by warp match in element order and placed at the digit's running offset.
-constexpr int kRunThreads = 512;
-constexpr int kRunWarps = kRunThreads / 32;
-constexpr int kRunSmem = 2048;
+// The long runs the fix-up listed, by a few blocks: block r takes runs r, r + grid, ... (sort_run_block, from the
+// pass output into the fix-up output). Exits at once when none was listed.
+constexpr uint32_t kRunBlocks = 8;
 
-__global__ void __launch_bounds__( kRunThreads ) k_sort_runs(uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
-                                                             uint64_t *__restrict__ tkeys,
-                                                             uint32_t *__restrict__ tvals, uint32_t n,
-                                                             const uint32_t *__restrict__ runs, const obj_scalars *sc)
+__device__ void runs_body(const fixup_args &a, uint32_t bid, uint32_t nblk)
 {
-  // bitonic: 2048 composite keys + 2048 indices (24 KB); LSD: per-warp digit counts, running offsets, tile totals,
-  // the four digit histograms (22.5 KB)
   __shared__ __align__( 16 ) unsigned char s_raw[kRunSmem * 12];
-  __shared__ uint32_t s_scan[kRunWarps];
-  __shared__ uint32_t s_run_start, s_run_len;
-  const uint32_t nruns = *reinterpret_cast< const volatile unsigned int * >( &sc->long_runs );
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const unsigned lt_mask = ( 1u << lane ) - 1u;
-  for ( uint32_t r = blockIdx.x; r < nruns; r += gridDim.x )
+  __shared__ uint32_t s_scan[kFixWarps];
+  __shared__ uint32_t s_start, s_len;
+  const uint32_t n = static_cast< uint32_t >( a.n );
+  const uint32_t nruns = *reinterpret_cast< const volatile unsigned int * >( &a.sc->long_runs );
+  for ( uint32_t r = bid; r < nruns; r += nblk )
   {
-    if ( tid == 0 )
+    if ( threadIdx.x == 0 )
     {
-      const uint32_t s = runs[r];
-      const uint32_t hi = static_cast< uint32_t >( keys[s] >> 32 );
+      const uint32_t s = a.runs[r];
+      const uint32_t hi = static_cast< uint32_t >( a.keys_in[s] >> 32 );
       uint32_t lo = s + 1, up = n;  // first index past s whose high half differs
       while ( lo < up )
       {
         const uint32_t mid = lo + ( up - lo ) / 2;
-        if ( static_cast< uint32_t >( keys[mid] >> 32 ) == hi ) lo = mid + 1;
+        if ( static_cast< uint32_t >( a.keys_in[mid] >> 32 ) == hi ) lo = mid + 1;
         else up = mid;
       }
-      s_run_start = s;
-      s_run_len = lo - s;
+      s_start = s;
+      s_len = lo - s;
     }
     __syncthreads();
-    const uint32_t s = s_run_start, L = s_run_len;
-    const uint64_t hi_bits = keys[s] & 0xffffffff00000000ull;
-    if ( L <= kRunSmem )
-    {
-      uint64_t *c = reinterpret_cast< uint64_t * >( s_raw );
-      uint32_t *v = reinterpret_cast< uint32_t * >( s_raw + kRunSmem * 8 );
-      uint32_t P = 1;
-      while ( P < L ) P <<= 1;
-      for ( uint32_t j = tid; j < P; j += kRunThreads )
-      {
-        if ( j < L )
-        {
-          c[j] = ( ( keys[s + j] & 0xffffffffull ) << 32 ) | j;
-          v[j] = vals[s + j];
-        } else {
-          c[j] = ~0ull;
-        }
-      }
-      __syncthreads();
-      for ( uint32_t k = 2; k <= P; k <<= 1 )
-        for ( uint32_t j = k >> 1; j > 0; j >>= 1 )
-        {
-          for ( uint32_t t = tid; t < P; t += kRunThreads )
-          {
-            const uint32_t u = t ^ j;
-            if ( u > t )
-            {
-              const uint64_t a = c[t], b = c[u];
-              if ( ( a > b ) == ( ( t & k ) == 0 ) )
-              {
-                c[t] = b;
-                c[u] = a;
-              }
-            }
-          }
-          __syncthreads();
-        }
-      for ( uint32_t j = tid; j < L; j += kRunThreads )
-      {
-        const uint64_t x = c[j];
-        keys[s + j] = hi_bits | ( x >> 32 );
-        vals[s + j] = v[x & 0xffffffffull];
-      }
-    } else {
-      uint32_t( *cnt )[256] = reinterpret_cast< uint32_t( * )[256] >( s_raw );  // [kRunWarps][256]
-      uint32_t *run_off = reinterpret_cast< uint32_t * >( s_raw + kRunWarps * 256 * 4 );
-      uint32_t *tot = run_off + 256;
-      uint32_t( *hist )[256] = reinterpret_cast< uint32_t( * )[256] >( tot + 256 );  // [4][256]
-      for ( int q = tid; q < kRunWarps * 256; q += kRunThreads ) ( &cnt[0][0] )[q] = 0;
-      for ( int q = tid; q < 4 * 256; q += kRunThreads ) ( &hist[0][0] )[q] = 0;
-      __syncthreads();
-      for ( uint32_t j = tid; j < L; j += kRunThreads )
-      {
-        const uint32_t low = static_cast< uint32_t >( keys[s + j] );
-#pragma unroll
-        for ( int p = 0; p < 4; ++p ) atomicAdd( &hist[p][( low >> ( 8 * p ) ) & 255u], 1u );
-      }
-      __syncthreads();
-      uint64_t *sk = keys, *dk = tkeys;
-      uint32_t *sv = vals, *dv = tvals;
-      for ( int p = 0; p < 4; ++p )
-      {
-        const uint32_t x = tid < 256 ? hist[p][tid] : 0u;
-        const uint32_t ex = block_exclusive_scan( x, s_scan );
-        if ( tid < 256 ) run_off[tid] = ex;
-        __syncthreads();
-        for ( uint32_t base = 0; base < L; base += kRunThreads )
-        {
-          const uint32_t j = base + tid;
-          const bool valid = j < L;
-          const uint64_t key = valid ? sk[s + j] : 0ull;
-          const uint32_t val = valid ? sv[s + j] : 0u;
-          const uint32_t d = valid ? ( static_cast< uint32_t >( key ) >> ( 8 * p ) ) & 255u : 256u;
-          const unsigned peers = __match_any_sync( 0xffffffffu, d );
-          const uint32_t rank = __popc( peers & lt_mask );
-          if ( valid && lane == __ffs( peers ) - 1 ) cnt[warp][d] = __popc( peers );
-          __syncthreads();
-          if ( tid < 256 )
-          {
-            uint32_t t = 0;
-#pragma unroll
-            for ( int w = 0; w < kRunWarps; ++w )
-            {
-              const uint32_t c = cnt[w][tid];
-              cnt[w][tid] = t;
-              t += c;
-            }
-            tot[tid] = t;
-          }
-          __syncthreads();
-          if ( valid )
-          {
-            const uint32_t pos = run_off[d] + cnt[warp][d] + rank;
-            dk[s + pos] = key;
-            dv[s + pos] = val;
-          }
-          __syncthreads();
-          if ( tid < 256 )
-          {
-            run_off[tid] += tot[tid];
-#pragma unroll
-            for ( int w = 0; w < kRunWarps; ++w ) cnt[w][tid] = 0;
-          }
-          __syncthreads();
-        }
-        uint64_t *tk = sk;
-        sk = dk;
-        dk = tk;
-        uint32_t *tv = sv;
-        sv = dv;
-        dv = tv;
-      }
-    }
-    __syncthreads();  // shared memory and the run bounds are reused by the next run
+    sort_run_block( const_cast< uint64_t * >( a.keys_in ), const_cast< uint32_t * >( a.vals_in ), a.keys_out,
+                    a.vals_out, s_start, s_len, s_raw, s_scan );
+    __syncthreads();  // the next run reuses shared memory and the run bounds
   }
 }
 
 }  // namespace
 
+uint32_t sort_fixup_blocks(uint64_t n) { return static_cast< uint32_t >( ( n + 255 ) / 256 ); }
+
+uint32_t sort_runs_blocks(uint64_t n)
+{
+  if ( n <= static_cast< uint64_t >( kFixRun ) ) return 0;  // no run can be long
+  const uint64_t most = long_run_capacity( n );
+  return static_cast< uint32_t >( most < kRunBlocks ? most : kRunBlocks );
+}
+
 cudaError_t launch_sort_fixup(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
                               uint32_t *vals_out, uint64_t n, uint32_t *runs, obj_scalars *sc, cudaStream_t s)
 {
   if ( n == 0 ) return cudaSuccess;
-  k_sort_fixup<<< static_cast< unsigned >( ( n + 255 ) / 256 ), 256, 0, s >>>( keys_in, vals_in, keys_out, vals_out,
-                                                                             static_cast< uint32_t >( n ), runs, sc );
+  const fixup_args a{ keys_in, vals_in, keys_out, vals_out, n, runs, sc };
+  k_single< fixup_args, fixup_body, 256, 8 ><<< sort_fixup_blocks( n ), 256, 0, s >>>( a );
+  if ( const uint32_t rb = sort_runs_blocks( n ) ) k_single< fixup_args, runs_body, kFixThreads, 1 ><<< rb, kFixThreads, 0, s >>>( a );
   return cudaGetLastError();
 }
 
-cudaError_t launch_sort_runs(uint64_t *keys, uint32_t *vals, uint64_t *tkeys, uint32_t *tvals, uint64_t n,
-                             const uint32_t *runs, obj_scalars *sc, cudaStream_t s)
+cudaError_t launch_sort_fixup_batch(const batch_launch &b, cudaStream_t s)
 {
-  // a run has at least 33 elements: never more blocks than possible runs, at most one per SM
-  if ( n <= static_cast< uint64_t >( kFixRun ) ) return cudaSuccess;
-  const uint64_t most = long_run_capacity( n );
-  const uint64_t cap = static_cast< uint64_t >( device_sm_count() );
-  k_sort_runs<<< static_cast< unsigned >( most < cap ? most : cap ), kRunThreads, 0, s >>>(
-    keys, vals, tkeys, tvals, static_cast< uint32_t >( n ), runs, sc );
+  if ( !b.nitems ) return cudaSuccess;
+  k_batched< fixup_args, fixup_body, 256, 8 ><<< b.blocks, 256, 0, s >>>( static_cast< const fixup_args * >( b.items ),
+                                                                        b.starts, b.nitems );
   return cudaGetLastError();
 }
+
+cudaError_t launch_sort_runs_batch(const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+  k_batched< fixup_args, runs_body, kFixThreads, 1 ><<< b.blocks, kFixThreads, 0, s >>>(
+    static_cast< const fixup_args * >( b.items ), b.starts, b.nitems );
+  return cudaGetLastError();
+}
+
+sort_pass_args onesweep_args(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
+                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
+                             obj_scalars *sc, uint32_t spin_limit, int stall)
+{
+  const uint64_t radix = 1ull << bits;
+  const uint64_t tiles = ( n + kSortTile - 1 ) / kSortTile;
+  const int use_tma = ( ( reinterpret_cast< uintptr_t >( keys_in ) | reinterpret_cast< uintptr_t >( vals_in ) ) & 15 ) == 0;
+  return sort_pass_args{ keys_in, vals_in, keys_out, vals_out, n, pass, hist + static_cast< size_t >( pass ) * radix,
+                         status + static_cast< size_t >( pass ) * ( tiles + 1 ) * radix, sc, spin_limit, stall, use_tma };
+}
+
+uint32_t onesweep_blocks(uint64_t n) { return os_grid( n ); }
 
 cudaError_t launch_onesweep(int bits, const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out,
                             uint32_t *vals_out, uint64_t n, int pass, const uint32_t *hist, uint32_t *status,
                             obj_scalars *sc, uint32_t spin_limit, int stall, cudaStream_t s)
 {
+  const sort_pass_args a = onesweep_args( bits, keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc,
+                                          spin_limit, stall );
   switch ( bits )
   {
-    case 1: return launch_os_t< 1 >( keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc, spin_limit, stall, s );
-    case 2: return launch_os_t< 2 >( keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc, spin_limit, stall, s );
-    case 4: return launch_os_t< 4 >( keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc, spin_limit, stall, s );
-    case 8: return launch_os_t< 8 >( keys_in, vals_in, keys_out, vals_out, n, pass, hist, status, sc, spin_limit, stall, s );
+    case 1: return launch_os_t< 1 >( a, s );
+    case 2: return launch_os_t< 2 >( a, s );
+    case 4: return launch_os_t< 4 >( a, s );
+    case 8: return launch_os_t< 8 >( a, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_onesweep_batch(int bits, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+  switch ( bits )
+  {
+    case 1: return launch_os_batch_t< 1 >( b, s );
+    case 2: return launch_os_batch_t< 2 >( b, s );
+    case 4: return launch_os_batch_t< 4 >( b, s );
+    case 8: return launch_os_batch_t< 8 >( b, s );
     default: return cudaErrorInvalidValue;
   }
 }

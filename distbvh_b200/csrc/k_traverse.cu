@@ -154,6 +154,36 @@ struct trav_args
   int dense_stack;  // stack bound of the batched dense walk (kDenseStack, lower under a test hook)
 };
 
+// The typed view of a scene's traversal item.
+template< typename T >
+__device__ __forceinline__ trav_args< T > typed(const trav_item &it)
+{
+  trav_args< T > x;
+  x.qwarp = static_cast< const T * >( it.qwarp );
+  x.qverts = it.qverts;
+  x.qV = it.qV;
+  x.qrows = static_cast< const T * >( it.qrows );
+  x.qperm = it.qperm;
+  x.nq = it.nq;
+  x.child = it.child;
+  x.nbox = static_cast< const T * >( it.nbox );
+  x.range = it.range;
+  x.tverts = it.tverts;
+  x.tV = it.tV;
+  x.tcache = static_cast< const T * >( it.tcache );
+  x.tperm = it.tperm;
+  x.tsc = it.tsc;
+  x.nt = it.nt;
+  x.self = it.self;
+  x.eps = it.eps;
+  x.eps_hi = it.eps_hi;
+  x.pairs = it.pairs;
+  x.cap = it.cap;
+  x.ps = it.ps;
+  x.dense_stack = it.dense_stack;
+  return x;
+}
+
 // Target leaf bucket bb for the lanes in `mine`: the warp first computes the bucket's element slabs into its cache
 // (lane j: element of rank 8 bb + j), then every lane of the mask tests its query against them (ranks above its own
 // in self-collision). Hits go out through one warp-aggregated reservation. Called by the whole warp.
@@ -320,9 +350,10 @@ __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const u
 // mask), in shared memory. At a leaf bucket the lanes of the mask test their element against the bucket's element
 // slabs, computed once by the warp from the vertices into a shared cache.
 template< int K, typename T, int VT >
-__global__ void __launch_bounds__( kTravThreads, kTravBlocksPerSM ) k_traverse(const trav_args< T > x,
-                                                                           const obj_scalars *__restrict__ qsc)
+__device__ void traverse_body(const trav_item &item, uint32_t, uint32_t)
 {
+  const trav_args< T > x = typed< T >( item );
+  const obj_scalars *__restrict__ qsc = item.qsc;
   constexpr int D = K / 2;
   constexpr int D0 = D < 4 ? D : 4;
   constexpr int WPB = kTravThreads / 32;
@@ -682,9 +713,10 @@ constexpr int kDenseBlocksPerSM =
 
 // Dense contact: one warp per packet of 32 query ranks (the hardware balances the walks).
 template< int K, typename T >
-__global__ void __launch_bounds__( kTravThreads, kDenseBlocksPerSM< K, T > ) k_traverse_stored(const trav_args< T > x,
-                                                                                               const obj_scalars *__restrict__ qsc)
+__device__ void stored_body(const trav_item &item, uint32_t bid, uint32_t)
 {
+  const trav_args< T > x = typed< T >( item );
+  const obj_scalars *__restrict__ qsc = item.qsc;
   constexpr int D = K / 2;
   constexpr int D0 = D < 4 ? D : 4;
   constexpr int WPB = kTravThreads / 32;
@@ -702,80 +734,117 @@ __global__ void __launch_bounds__( kTravThreads, kDenseBlocksPerSM< K, T > ) k_t
     if ( !o ) return;
   }
   const uint32_t packets = ( x.nq + 31 ) / 32;
-  const uint32_t pk = ( blockIdx.x * blockDim.x + threadIdx.x ) >> 5;
+  const uint32_t pk = ( bid * blockDim.x + threadIdx.x ) >> 5;
   if ( pk < packets ) traverse_packet_stored< K, T >( x, pk * 32, lane, s_dense[threadIdx.x >> 5], rb );
+}
+
+// One scene's item and grid. Dense contact: one warp per packet. Sparse: a persistent grid of at most the resident
+// blocks (4 per SM), one warp per chunk of 32 packets at most.
+template< int K, typename T >
+void trav_item_t(tree_view q, tree_view t, bool self, bool dense, double eps, uint2 *pairs, uint64_t cap,
+                 pair_scalars *ps, int dense_stack_limit, trav_item *it, uint32_t *blocks, bool *dense_out)
+{
+  it->qwarp = q.warp_box;
+  it->qverts = q.verts;
+  it->qV = q.V;
+  it->qrows = q.elem_cache;
+  it->qperm = q.perm;
+  it->nq = static_cast< uint32_t >( q.n );
+  it->child = t.child;
+  it->nbox = t.node_box;
+  it->range = t.range;
+  it->tverts = t.verts;
+  it->tV = t.V;
+  it->tcache = t.elem_cache;
+  it->tperm = t.perm;
+  it->tsc = t.sc;
+  it->nt = static_cast< uint32_t >( t.n );
+  it->self = self ? 1 : 0;
+  it->eps = eps;
+  it->eps_hi = f32_round_up( eps );
+  it->pairs = pairs;
+  it->cap = cap;
+  it->ps = ps;
+  it->dense_stack = dense_stack_limit > 0 && dense_stack_limit < kDenseStack ? dense_stack_limit : kDenseStack;
+  it->qsc = q.sc;
+  constexpr uint64_t kWarps = kTravThreads / 32;
+  const uint64_t packets = ( q.n + 31 ) / 32;
+  const uint64_t chunks = ( packets + 31 ) / 32;
+  const uint64_t resident = static_cast< uint64_t >( device_sm_count() ) * kTravBlocksPerSM;
+  dense = dense && q.stored && t.stored;
+  uint64_t b = dense ? ( packets + kWarps - 1 ) / kWarps : ( chunks + kWarps - 1 ) / kWarps;
+  if ( !dense && b > resident ) b = resident;
+  *blocks = static_cast< uint32_t >( b < ( 1ull << 30 ) ? ( b ? b : 1 ) : ( 1ull << 30 ) );
+  *dense_out = dense;
 }
 
 template< int K, typename T >
 cudaError_t launch_trav_t(tree_view q, tree_view t, bool self, bool dense, double eps, uint2 *pairs, uint64_t cap,
                           pair_scalars *ps, cudaStream_t s, int dense_stack_limit)
 {
-  trav_args< T > x;
-  x.qwarp = static_cast< const T * >( q.warp_box );
-  x.qverts = q.verts;
-  x.qV = q.V;
-  x.qrows = static_cast< const T * >( q.elem_cache );
-  x.qperm = q.perm;
-  x.nq = static_cast< uint32_t >( q.n );
-  x.child = t.child;
-  x.nbox = static_cast< const T * >( t.node_box );
-  x.range = t.range;
-  x.tverts = t.verts;
-  x.tV = t.V;
-  x.tcache = static_cast< const T * >( t.elem_cache );
-  x.tperm = t.perm;
-  x.tsc = t.sc;
-  x.nt = static_cast< uint32_t >( t.n );
-  x.self = self ? 1 : 0;
-  x.eps = eps;
-  x.eps_hi = f32_round_up( eps );
-  x.pairs = pairs;
-  x.cap = cap;
-  x.ps = ps;
-  x.dense_stack = dense_stack_limit > 0 && dense_stack_limit < kDenseStack ? dense_stack_limit : kDenseStack;
-  // Dense contact: one warp per packet. Sparse: a persistent grid of at most the resident blocks (4 per SM), one
-  // warp per chunk of 32 packets at most.
-  constexpr uint64_t kWarps = kTravThreads / 32;
-  const uint64_t packets = ( q.n + 31 ) / 32;
-  const uint64_t chunks = ( packets + 31 ) / 32;
-  const uint64_t resident = static_cast< uint64_t >( device_sm_count() ) * kTravBlocksPerSM;
-  dense = dense && q.stored && t.stored;
-  uint64_t blocks = dense ? ( packets + kWarps - 1 ) / kWarps : ( chunks + kWarps - 1 ) / kWarps;
-  if ( !dense && blocks > resident ) blocks = resident;
-  const unsigned grid = static_cast< unsigned >( blocks < ( 1ull << 30 ) ? ( blocks ? blocks : 1 ) : ( 1ull << 30 ) );
+  trav_item it;
+  uint32_t grid = 0;
+  trav_item_t< K, T >( q, t, self, dense, eps, pairs, cap, ps, dense_stack_limit, &it, &grid, &dense );
   // both objects' element slabs stored (dense contact): the batched walk that only reads them; else the one that
   // computes the slabs it tests from the vertices (unrolled when both objects have the same vertex count)
   if ( dense )
   {
-    k_traverse_stored< K, T ><<< grid, kTravThreads, 0, s >>>( x, q.sc );
+    k_single< trav_item, stored_body< K, T >, kTravThreads, kDenseBlocksPerSM< K, T > ><<< grid, kTravThreads, 0, s >>>( it );
     return cudaGetLastError();
   }
   const uint32_t V = q.V == t.V ? q.V : 0;
   switch ( V )
   {
-    case 3: k_traverse< K, T, 3 ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
-    case 4: k_traverse< K, T, 4 ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
-    case 8: k_traverse< K, T, 8 ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
-    default: k_traverse< K, T, 0 ><<< grid, kTravThreads, 0, s >>>( x, q.sc ); break;
+    case 3: k_single< trav_item, traverse_body< K, T, 3 >, kTravThreads, kTravBlocksPerSM ><<< grid, kTravThreads, 0, s >>>( it ); break;
+    case 4: k_single< trav_item, traverse_body< K, T, 4 >, kTravThreads, kTravBlocksPerSM ><<< grid, kTravThreads, 0, s >>>( it ); break;
+    case 8: k_single< trav_item, traverse_body< K, T, 8 >, kTravThreads, kTravBlocksPerSM ><<< grid, kTravThreads, 0, s >>>( it ); break;
+    default: k_single< trav_item, traverse_body< K, T, 0 >, kTravThreads, kTravBlocksPerSM ><<< grid, kTravThreads, 0, s >>>( it ); break;
+  }
+  return cudaGetLastError();
+}
+
+template< int K, typename T >
+cudaError_t launch_trav_batch_t(bool dense, uint32_t V, const batch_launch &b, cudaStream_t s)
+{
+  const trav_item *items = static_cast< const trav_item * >( b.items );
+  if ( dense )
+  {
+    k_batched< trav_item, stored_body< K, T >, kTravThreads, kDenseBlocksPerSM< K, T > ><<< b.blocks, kTravThreads, 0, s >>>(
+      items, b.starts, b.nitems );
+    return cudaGetLastError();
+  }
+  switch ( V )
+  {
+    case 3: k_batched< trav_item, traverse_body< K, T, 3 >, kTravThreads, kTravBlocksPerSM ><<< b.blocks, kTravThreads, 0, s >>>( items, b.starts, b.nitems ); break;
+    case 4: k_batched< trav_item, traverse_body< K, T, 4 >, kTravThreads, kTravBlocksPerSM ><<< b.blocks, kTravThreads, 0, s >>>( items, b.starts, b.nitems ); break;
+    case 8: k_batched< trav_item, traverse_body< K, T, 8 >, kTravThreads, kTravBlocksPerSM ><<< b.blocks, kTravThreads, 0, s >>>( items, b.starts, b.nitems ); break;
+    default: k_batched< trav_item, traverse_body< K, T, 0 >, kTravThreads, kTravBlocksPerSM ><<< b.blocks, kTravThreads, 0, s >>>( items, b.starts, b.nitems ); break;
   }
   return cudaGetLastError();
 }
 
 // K7: FP64 slabs of both elements from their vertices, slab by slab with early exit.
 template< int K, int VA, int VB >
-__global__ void __launch_bounds__( 256 ) k_recheck(const double *__restrict__ va, uint32_t Var,
-                                                 const double *__restrict__ vb, uint32_t Vbr, double eps,
-                                                 const uint2 *__restrict__ cand, uint64_t cand_cap, uint2 *out,
-                                                 uint64_t cap, pair_scalars *ps)
+__device__ void recheck_body(const recheck_args &args, uint32_t bid, uint32_t nblk)
 {
+  const double *__restrict__ va = args.va;
+  const uint32_t Var = args.Va;
+  const double *__restrict__ vb = args.vb;
+  const uint32_t Vbr = args.Vb;
+  const double eps = args.eps;
+  const uint2 *__restrict__ cand = args.cand;
+  const uint64_t cand_cap = args.cand_cap;
+  uint2 *out = args.out;
+  const uint64_t cap = args.cap;
+  pair_scalars *ps = args.ps;
   constexpr int D = K / 2;
   // The candidate count is read on the device: no host round trip between traversal and recheck.
   const uint64_t ncand = min( static_cast< uint64_t >( *reinterpret_cast< volatile unsigned long long * >( &ps->count ) ),
                               cand_cap );
   const int Va = VA > 0 ? VA : static_cast< int >( Var );
   const int Vb = VB > 0 ? VB : static_cast< int >( Vbr );
-  for ( uint64_t p = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; p < ncand;
-        p += static_cast< uint64_t >( gridDim.x ) * blockDim.x )
+  for ( uint64_t p = static_cast< uint64_t >( bid ) * blockDim.x + threadIdx.x; p < ncand;
+        p += static_cast< uint64_t >( nblk ) * blockDim.x )
   {
     const uint2 c = __ldg( cand + p );
     const double *pa = va + static_cast< size_t >( c.x ) * Va * 3;
@@ -829,18 +898,33 @@ __global__ void __launch_bounds__( 256 ) k_recheck(const double *__restrict__ va
   }
 }
 
-template< int K >
-cudaError_t recheck_k(const double *va, uint32_t Va, const double *vb, uint32_t Vb, double eps, const uint2 *cand,
-                      uint64_t ncand, uint2 *out, uint64_t cap, pair_scalars *ps, cudaStream_t s)
+// grid-stride over the candidates (their count is read on the device): at most 4 blocks per SM
+uint32_t recheck_grid(uint64_t ncand)
 {
-  // grid-stride over the candidates (their count is read on the device): at most 4 blocks per SM
   const uint64_t blocks = ( ncand + 255 ) / 256;
   const uint64_t capb = static_cast< uint64_t >( device_sm_count() ) * 4;
-  const unsigned grid = static_cast< unsigned >( blocks < capb ? ( blocks ? blocks : 1 ) : capb );
-  if ( Va == 3 && Vb == 3 ) k_recheck< K, 3, 3 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
-  else if ( Va == 4 && Vb == 4 ) k_recheck< K, 4, 4 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
-  else if ( Va == 8 && Vb == 8 ) k_recheck< K, 8, 8 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
-  else k_recheck< K, 0, 0 ><<< grid, 256, 0, s >>>( va, Va, vb, Vb, eps, cand, ncand, out, cap, ps );
+  return static_cast< uint32_t >( blocks < capb ? ( blocks ? blocks : 1 ) : capb );
+}
+
+template< int K >
+cudaError_t recheck_k(const recheck_args &a, cudaStream_t s)
+{
+  const uint32_t grid = recheck_grid( a.cand_cap );
+  if ( a.Va == 3 && a.Vb == 3 ) k_single< recheck_args, recheck_body< K, 3, 3 >, 256, 2 ><<< grid, 256, 0, s >>>( a );
+  else if ( a.Va == 4 && a.Vb == 4 ) k_single< recheck_args, recheck_body< K, 4, 4 >, 256, 2 ><<< grid, 256, 0, s >>>( a );
+  else if ( a.Va == 8 && a.Vb == 8 ) k_single< recheck_args, recheck_body< K, 8, 8 >, 256, 2 ><<< grid, 256, 0, s >>>( a );
+  else k_single< recheck_args, recheck_body< K, 0, 0 >, 256, 2 ><<< grid, 256, 0, s >>>( a );
+  return cudaGetLastError();
+}
+
+template< int K >
+cudaError_t recheck_batch_k(uint32_t V, const batch_launch &b, cudaStream_t s)
+{
+  const recheck_args *it = static_cast< const recheck_args * >( b.items );
+  if ( V == 3 ) k_batched< recheck_args, recheck_body< K, 3, 3 >, 256, 2 ><<< b.blocks, 256, 0, s >>>( it, b.starts, b.nitems );
+  else if ( V == 4 ) k_batched< recheck_args, recheck_body< K, 4, 4 >, 256, 2 ><<< b.blocks, 256, 0, s >>>( it, b.starts, b.nitems );
+  else if ( V == 8 ) k_batched< recheck_args, recheck_body< K, 8, 8 >, 256, 2 ><<< b.blocks, 256, 0, s >>>( it, b.starts, b.nitems );
+  else k_batched< recheck_args, recheck_body< K, 0, 0 >, 256, 2 ><<< b.blocks, 256, 0, s >>>( it, b.starts, b.nitems );
   return cudaGetLastError();
 }
 
@@ -860,19 +944,18 @@ __global__ void k_gid_pairs(const uint2 *__restrict__ pairs, uint64_t count, con
 
 // k_gid_pairs with the count read on the device (at most cap): for launches whose count is unknown when they are
 // enqueued (batched scenes in a CUDA graph).
-__global__ void k_gid_pairs_dev(const uint2 *__restrict__ pairs, const unsigned long long *count, uint64_t cap,
-                                const uint64_t *__restrict__ gid_a, const uint64_t *__restrict__ gid_b, int normalize,
-                                uint64_t *__restrict__ out)
+__device__ void gid_dev_body(const gid_args &a, uint32_t bid, uint32_t nblk)
 {
-  const uint64_t n = min( static_cast< uint64_t >( *reinterpret_cast< const volatile unsigned long long * >( count ) ), cap );
-  for ( uint64_t p = static_cast< uint64_t >( blockIdx.x ) * blockDim.x + threadIdx.x; p < n;
-        p += static_cast< uint64_t >( gridDim.x ) * blockDim.x )
+  const uint64_t n = min( static_cast< uint64_t >( *reinterpret_cast< const volatile unsigned long long * >( a.count ) ),
+                          a.cap );
+  for ( uint64_t p = static_cast< uint64_t >( bid ) * blockDim.x + threadIdx.x; p < n;
+        p += static_cast< uint64_t >( nblk ) * blockDim.x )
   {
-    uint2 c = pairs[p];
-    if ( normalize && c.x > c.y ) c = make_uint2( c.y, c.x );
-    const uint64_t a = gid_a ? __ldg( gid_a + c.x ) : c.x;
-    const uint64_t b = gid_b ? __ldg( gid_b + c.y ) : c.y;
-    reinterpret_cast< ulonglong2 * >( out )[p] = make_ulonglong2( a, b );
+    uint2 c = a.pairs[p];
+    if ( a.normalize && c.x > c.y ) c = make_uint2( c.y, c.x );
+    const uint64_t ga = a.gid_a ? __ldg( a.gid_a + c.x ) : c.x;
+    const uint64_t gb = a.gid_b ? __ldg( a.gid_b + c.y ) : c.y;
+    reinterpret_cast< ulonglong2 * >( a.out )[p] = make_ulonglong2( ga, gb );
   }
 }
 
@@ -885,14 +968,27 @@ __global__ void k_gather_words(const int *const *__restrict__ src, int n, int *_
 
 }  // namespace
 
+uint32_t gid_pairs_dev_blocks(uint64_t cap)
+{
+  const uint64_t blocks = ( cap + 255 ) / 256;
+  return static_cast< uint32_t >( blocks < 148 * 2 ? ( blocks ? blocks : 1 ) : 148 * 2 );
+}
+
 cudaError_t launch_gid_pairs_dev(const uint2 *pairs, const unsigned long long *count, uint64_t cap,
                                  const uint64_t *gid_a, const uint64_t *gid_b, bool normalize, uint64_t *out,
                                  cudaStream_t s)
 {
   if ( cap == 0 ) return cudaSuccess;
-  const uint64_t blocks = ( cap + 255 ) / 256;
-  const unsigned grid = static_cast< unsigned >( blocks < 148 * 2 ? blocks : 148 * 2 );
-  k_gid_pairs_dev<<< grid, 256, 0, s >>>( pairs, count, cap, gid_a, gid_b, normalize ? 1 : 0, out );
+  const gid_args a{ pairs, count, cap, gid_a, gid_b, normalize ? 1 : 0, out };
+  k_single< gid_args, gid_dev_body, 256, 1 ><<< gid_pairs_dev_blocks( cap ), 256, 0, s >>>( a );
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gid_pairs_dev_batch(const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+  k_batched< gid_args, gid_dev_body, 256, 1 ><<< b.blocks, 256, 0, s >>>( static_cast< const gid_args * >( b.items ),
+                                                                        b.starts, b.nitems );
   return cudaGetLastError();
 }
 
@@ -922,11 +1018,48 @@ cudaError_t launch_recheck(int K, const double *verts_a, uint32_t Va, const doub
                            const uint2 *cand, uint64_t ncand, uint2 *out, uint64_t cap, pair_scalars *ps,
                            cudaStream_t s)
 {
+  const recheck_args a{ verts_a, Va, verts_b, Vb, eps, cand, ncand, out, cap, ps };
   switch ( K )
   {
-    case 6: return recheck_k< 6 >( verts_a, Va, verts_b, Vb, eps, cand, ncand, out, cap, ps, s );
-    case 18: return recheck_k< 18 >( verts_a, Va, verts_b, Vb, eps, cand, ncand, out, cap, ps, s );
-    case 26: return recheck_k< 26 >( verts_a, Va, verts_b, Vb, eps, cand, ncand, out, cap, ps, s );
+    case 6: return recheck_k< 6 >( a, s );
+    case 18: return recheck_k< 18 >( a, s );
+    case 26: return recheck_k< 26 >( a, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+uint32_t recheck_blocks(uint64_t ncand) { return recheck_grid( ncand ); }
+
+cudaError_t launch_recheck_batch(int K, uint32_t V, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+  switch ( K )
+  {
+    case 6: return recheck_batch_k< 6 >( V, b, s );
+    case 18: return recheck_batch_k< 18 >( V, b, s );
+    case 26: return recheck_batch_k< 26 >( V, b, s );
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+void traverse_item(int K, bool fp32, tree_view q, tree_view t, bool self, bool dense, double eps, uint2 *pairs,
+                   uint64_t cap, pair_scalars *ps, int dense_stack_limit, trav_item *item, uint32_t *blocks,
+                   bool *dense_out)
+{
+  // the item's fields do not depend on K or the slab type; only the grid depends on K through nothing either
+  if ( fp32 ) trav_item_t< 18, float >( q, t, self, dense, eps, pairs, cap, ps, dense_stack_limit, item, blocks, dense_out );
+  else trav_item_t< 18, double >( q, t, self, dense, eps, pairs, cap, ps, dense_stack_limit, item, blocks, dense_out );
+  (void)K;
+}
+
+cudaError_t launch_traverse_batch(int K, bool fp32, bool dense, uint32_t V, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+  switch ( K )
+  {
+    case 6: return fp32 ? launch_trav_batch_t< 6, float >( dense, V, b, s ) : launch_trav_batch_t< 6, double >( dense, V, b, s );
+    case 18: return fp32 ? launch_trav_batch_t< 18, float >( dense, V, b, s ) : launch_trav_batch_t< 18, double >( dense, V, b, s );
+    case 26: return fp32 ? launch_trav_batch_t< 26, float >( dense, V, b, s ) : launch_trav_batch_t< 26, double >( dense, V, b, s );
     default: return cudaErrorInvalidValue;
   }
 }

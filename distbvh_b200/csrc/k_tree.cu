@@ -124,13 +124,22 @@ constexpr int kSlabThreads = 128;  // ranks per block of the element slab kernel
 // r = 8 b + j, slab a at elem_rows[b * 8 C + 16 a + 2 j + {0 min, 1 max}]) only when given (objects in dense
 // contact, whose traversals test most buckets); otherwise the traversal computes the few it tests from the
 // vertices. A one-bucket object also gets its root box here. A rank whose index is not an element index marks a failed sort.
+template< int K, int VT >
+constexpr int kSlabMinBlocks = ( VT == 3 && K <= 18 ) ? 8 : ( VT == 8 ? 3 : 4 );
+
 template< int K, typename T, int VT >
-__global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( VT == 8 ? 3 : 4 ) ) k_elem_slabs(const double *__restrict__ verts, uint32_t Vrt,
-                                                                  int n, double eps, float eps_hi,
-                                                                  const uint32_t *__restrict__ vals,
-                                                                  T *__restrict__ bucket_box, T *__restrict__ warp_box,
-                                                                  T *__restrict__ elem_rows, obj_scalars *sc)
+__device__ void slabs_body(const slabs_args &args, uint32_t bid, uint32_t)
 {
+  const double *__restrict__ verts = args.verts;
+  const uint32_t Vrt = args.V;
+  const int n = static_cast< int >( args.n );
+  const double eps = args.eps;
+  const float eps_hi = args.eps_hi;
+  const uint32_t *__restrict__ vals = args.vals;
+  T *__restrict__ bucket_box = static_cast< T * >( args.bucket_box );
+  T *__restrict__ warp_box = static_cast< T * >( args.warp_box );
+  T *__restrict__ elem_rows = static_cast< T * >( args.elem_rows );
+  obj_scalars *sc = args.sc;
   constexpr int D = K / 2;
   constexpr int C = 2 * D;
   constexpr int P = C + 1;
@@ -140,7 +149,7 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
   __shared__ T s_bk[( kSlabThreads / kLeafSize ) * P];
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;  // no valid permutation
   const int tid = threadIdx.x;
-  const int r0 = static_cast< int >( blockIdx.x ) * kSlabThreads;
+  const int r0 = static_cast< int >( bid ) * kSlabThreads;
   const int rows = min( kSlabThreads, n - r0 );
   if ( tid < rows )
   {
@@ -237,13 +246,18 @@ __global__ void __launch_bounds__( kSlabThreads, ( VT == 3 && K <= 18 ) ? 8 : ( 
 //    (parent * 2 + side, l, r, node).
 // e. Coalesced write-out of the topology of every node closed in the block (child, range, parent).
 template< int K, typename T >
-__global__ void __launch_bounds__( kBuildThreads, 8 ) k_build_leaf(int n, const uint64_t *__restrict__ keys,
-                                                              uint8_t *__restrict__ bdel,
-                                                              const T *__restrict__ bucket_box,
-                                                              T *__restrict__ node_box, int *__restrict__ child,
-                                                              int2 *__restrict__ range, int *__restrict__ parent,
-                                                              int4 *__restrict__ queue, obj_scalars *sc)
+__device__ void build_leaf_body(const tree_args &args, uint32_t bid, uint32_t)
 {
+  const int n = static_cast< int >( args.n );
+  const uint64_t *__restrict__ keys = args.keys;
+  uint8_t *__restrict__ bdel = args.bdel;
+  const T *__restrict__ bucket_box = static_cast< const T * >( args.bucket_box );
+  T *__restrict__ node_box = static_cast< T * >( args.node_box );
+  int *__restrict__ child = reinterpret_cast< int * >( args.child );
+  int2 *__restrict__ range = args.range;
+  int *__restrict__ parent = args.parent;
+  int4 *__restrict__ queue = args.queue;
+  obj_scalars *sc = args.sc;
   constexpr int D = K / 2;
   constexpr int C = 2 * D;
   constexpr int W = kBuildThreads / 32;
@@ -261,7 +275,7 @@ __global__ void __launch_bounds__( kBuildThreads, 8 ) k_build_leaf(int n, const 
   __shared__ int s_npairs, s_root_ref;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int b = static_cast< int >( blockIdx.x * blockDim.x ) + tid;
+  const int b = static_cast< int >( bid * blockDim.x ) + tid;
   const int wbase = b - lane, bbase = b - tid;
   const int m = ( n + kLeafSize - 1 ) / kLeafSize;  // buckets
   auto box = [&](int ref, int c) -> T & { return s_box[ref * ( C + 1 ) + c]; };
@@ -501,16 +515,23 @@ __global__ void __launch_bounds__( kBuildThreads, 8 ) k_build_leaf(int n, const 
 // acq_rel atomic exchange that orders its slab stores before it; the second arrival's slab loads (through L2)
 // are ordered after its acquire load or exchange. Slabs written by phase 1 are visible here (kernel boundary).
 template< int K, typename T >
-__global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint8_t *__restrict__ bdel, T *node_box,
-                                                     int *child, int2 *__restrict__ range, int *__restrict__ parent,
-                                                     int *exch, const int4 *__restrict__ queue, obj_scalars *sc)
+__device__ void climb_body(const tree_args &args, uint32_t bid, uint32_t nblk)
 {
+  const int n = static_cast< int >( args.n );
+  const uint8_t *__restrict__ bdel = args.bdel;
+  T *node_box = static_cast< T * >( args.node_box );
+  int *child = reinterpret_cast< int * >( args.child );
+  int2 *__restrict__ range = args.range;
+  int *__restrict__ parent = args.parent;
+  int *exch = args.exch;
+  const int4 *__restrict__ queue = args.queue;
+  obj_scalars *sc = args.sc;
   constexpr int D = K / 2;
   using io = box_io< T >;
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
   const int m = ( n + kLeafSize - 1 ) / kLeafSize;
   const unsigned count = *reinterpret_cast< volatile unsigned * >( &sc->climb_count );
-  for ( unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x )
+  for ( unsigned q = bid * blockDim.x + threadIdx.x; q < count; q += nblk * blockDim.x )
   {
     const int4 w = queue[q];
     int par = w.x >> 1, side = w.x & 1, l = w.y, r = w.z;
@@ -567,13 +588,17 @@ __global__ void __launch_bounds__( 128 ) k_build_climb(int n, const uint8_t *__r
 // boxes; elements keep their ranks): the first/second-arrival climb along the stored parent links. exch must
 // hold -1.
 template< int K, typename T >
-__global__ void __launch_bounds__( kBuildThreads ) k_refit(int n, const T *__restrict__ bucket_box, T *node_box,
-                                                         const int *__restrict__ parent, int *exch,
-                                                         obj_scalars *__restrict__ sc)
+__device__ void refit_body(const tree_args &args, uint32_t bid, uint32_t)
 {
+  const int n = static_cast< int >( args.n );
+  const T *__restrict__ bucket_box = static_cast< const T * >( args.bucket_box );
+  T *node_box = static_cast< T * >( args.node_box );
+  const int *__restrict__ parent = args.parent;
+  int *exch = args.exch;
+  obj_scalars *__restrict__ sc = args.sc;
   constexpr int D = K / 2;
   using io = box_io< T >;
-  const int b = static_cast< int >( blockIdx.x * blockDim.x + threadIdx.x );
+  const int b = static_cast< int >( bid * blockDim.x + threadIdx.x );
   const int m = ( n + kLeafSize - 1 ) / kLeafSize;
   if ( b >= m || m == 1 ) return;  // a one-bucket object's root box came from the slab kernel
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
@@ -618,71 +643,130 @@ __global__ void __launch_bounds__( kBuildThreads ) k_refit(int n, const T *__res
   }
 }
 
+uint32_t slab_grid(uint64_t n) { return static_cast< uint32_t >( ( n + kSlabThreads - 1 ) / kSlabThreads ); }
+
 template< int K, typename T, int VT >
-cudaError_t launch_slabs_t(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals,
-                           void *bucket_box, void *warp_box, void *elem_rows, obj_scalars *sc, cudaStream_t s)
+cudaError_t launch_slabs_t(const slabs_args &a, cudaStream_t s)
 {
-  const unsigned grid = static_cast< unsigned >( ( n + kSlabThreads - 1 ) / kSlabThreads );
-  k_elem_slabs< K, T, VT ><<< grid, kSlabThreads, 0, s >>>( verts, V, static_cast< int >( n ), eps, f32_round_up( eps ),
-                                                           vals, static_cast< T * >( bucket_box ),
-                                                           static_cast< T * >( warp_box ),
-                                                           static_cast< T * >( elem_rows ), sc );
+  k_single< slabs_args, slabs_body< K, T, VT >, kSlabThreads, kSlabMinBlocks< K, VT > ><<< slab_grid( a.n ), kSlabThreads, 0, s >>>( a );
+  return cudaGetLastError();
+}
+
+template< int K, typename T, int VT >
+cudaError_t launch_slabs_batch_t(const batch_launch &b, cudaStream_t s)
+{
+  k_batched< slabs_args, slabs_body< K, T, VT >, kSlabThreads, kSlabMinBlocks< K, VT > ><<< b.blocks, kSlabThreads, 0, s >>>(
+    static_cast< const slabs_args * >( b.items ), b.starts, b.nitems );
   return cudaGetLastError();
 }
 
 template< int K, typename T >
-cudaError_t slabs_v(const double *verts, uint32_t V, uint64_t n, double eps, const uint32_t *vals, void *bb, void *wb,
-                    void *er, obj_scalars *sc, cudaStream_t s)
+cudaError_t slabs_v(const slabs_args &a, cudaStream_t s)
 {
-  switch ( V )
+  switch ( a.V )
   {
-    case 3: return launch_slabs_t< K, T, 3 >( verts, V, n, eps, vals, bb, wb, er, sc, s );
-    case 4: return launch_slabs_t< K, T, 4 >( verts, V, n, eps, vals, bb, wb, er, sc, s );
-    case 8: return launch_slabs_t< K, T, 8 >( verts, V, n, eps, vals, bb, wb, er, sc, s );
-    default: return launch_slabs_t< K, T, 0 >( verts, V, n, eps, vals, bb, wb, er, sc, s );
+    case 3: return launch_slabs_t< K, T, 3 >( a, s );
+    case 4: return launch_slabs_t< K, T, 4 >( a, s );
+    case 8: return launch_slabs_t< K, T, 8 >( a, s );
+    default: return launch_slabs_t< K, T, 0 >( a, s );
   }
 }
 
 template< int K, typename T >
-cudaError_t launch_build_t(uint64_t n, const uint64_t *keys, uint8_t *bdel, const void *bucket_box, void *node_box,
-                           int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc, cudaStream_t s)
+cudaError_t slabs_batch_v(uint32_t V, const batch_launch &b, cudaStream_t s)
+{
+  switch ( V )
+  {
+    case 3: return launch_slabs_batch_t< K, T, 3 >( b, s );
+    case 4: return launch_slabs_batch_t< K, T, 4 >( b, s );
+    case 8: return launch_slabs_batch_t< K, T, 8 >( b, s );
+    default: return launch_slabs_batch_t< K, T, 0 >( b, s );
+  }
+}
+
+uint32_t build_grid(uint64_t n)
 {
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
-  if ( m <= 1 ) return cudaSuccess;  // the slab kernel stored a one-bucket object's root
-  const unsigned grid = static_cast< unsigned >( ( m + kBuildThreads - 1 ) / kBuildThreads );
-  const size_t smem = static_cast< size_t >( kBuildThreads ) * ( 2 * ( K / 2 ) + 1 ) * sizeof( T );  // [rows][C + 1]
-  const cudaError_t e = cudaFuncSetAttribute( k_build_leaf< K, T >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              static_cast< int >( smem ) );
+  return m <= 1 ? 0u : static_cast< uint32_t >( ( m + kBuildThreads - 1 ) / kBuildThreads );
+}
+
+template< int K, typename T >
+constexpr size_t kBuildSmem = static_cast< size_t >( kBuildThreads ) * ( 2 * ( K / 2 ) + 1 ) * sizeof( T );  // [rows][C + 1]
+
+template< int K, typename T >
+cudaError_t build_setup()
+{
+  cudaError_t e = cudaFuncSetAttribute( k_single< tree_args, build_leaf_body< K, T >, kBuildThreads, 8 >,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( kBuildSmem< K, T > ) );
   if ( e != cudaSuccess ) return e;
-  k_build_leaf< K, T ><<< grid, kBuildThreads, smem, s >>>( static_cast< int >( n ), keys, bdel,
-                                                           static_cast< const T * >( bucket_box ),
-                                                           static_cast< T * >( node_box ),
-                                                           reinterpret_cast< int * >( child ), range, parent, queue, sc );
+  return cudaFuncSetAttribute( k_batched< tree_args, build_leaf_body< K, T >, kBuildThreads, 8 >,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast< int >( kBuildSmem< K, T > ) );
+}
+
+template< int K, typename T >
+cudaError_t launch_build_t(const tree_args &a, cudaStream_t s)
+{
+  const uint32_t grid = build_grid( a.n );
+  if ( !grid ) return cudaSuccess;  // the slab kernel stored a one-bucket object's root
+  const cudaError_t e = build_setup< K, T >();
+  if ( e != cudaSuccess ) return e;
+  k_single< tree_args, build_leaf_body< K, T >, kBuildThreads, 8 ><<< grid, kBuildThreads, kBuildSmem< K, T >, s >>>( a );
   return cudaGetLastError();
 }
 
 template< int K, typename T >
-cudaError_t launch_climb_t(uint64_t n, const uint8_t *bdel, void *node_box, int2 *child, int2 *range, int *parent,
-                           int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s)
+cudaError_t launch_build_batch_t(const batch_launch &b, cudaStream_t s)
+{
+  const cudaError_t e = build_setup< K, T >();
+  if ( e != cudaSuccess ) return e;
+  k_batched< tree_args, build_leaf_body< K, T >, kBuildThreads, 8 ><<< b.blocks, kBuildThreads, kBuildSmem< K, T >, s >>>(
+    static_cast< const tree_args * >( b.items ), b.starts, b.nitems );
+  return cudaGetLastError();
+}
+
+// The queue length is known only on the device: a grid-stride grid sized for the usual fraction.
+uint32_t climb_grid(uint64_t n)
 {
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
-  // The queue length is known only on the device: a grid-stride grid sized for the usual fraction.
   const uint64_t want = ( m / 8 + 127 ) / 128;
-  const unsigned cgrid = static_cast< unsigned >( want < 148 * 16 ? ( want ? want : 1 ) : 148 * 16 );
-  k_build_climb< K, T ><<< cgrid, 128, 0, s >>>( static_cast< int >( n ), bdel, static_cast< T * >( node_box ),
-                                                reinterpret_cast< int * >( child ), range, parent, exch, queue, sc );
+  return static_cast< uint32_t >( want < 148 * 16 ? ( want ? want : 1 ) : 148 * 16 );
+}
+
+template< int K, typename T >
+cudaError_t launch_climb_t(const tree_args &a, cudaStream_t s)
+{
+  k_single< tree_args, climb_body< K, T >, 128, 7 ><<< climb_grid( a.n ), 128, 0, s >>>( a );
   return cudaGetLastError();
 }
 
 template< int K, typename T >
-cudaError_t launch_refit_t(uint64_t n, const void *bucket_box, void *node_box, const int *parent, int *exch,
-                           obj_scalars *sc, cudaStream_t s)
+cudaError_t launch_climb_batch_t(const batch_launch &b, cudaStream_t s)
+{
+  k_batched< tree_args, climb_body< K, T >, 128, 7 ><<< b.blocks, 128, 0, s >>>( static_cast< const tree_args * >( b.items ),
+                                                                               b.starts, b.nitems );
+  return cudaGetLastError();
+}
+
+uint32_t refit_grid(uint64_t n)
 {
   const uint64_t m = ( n + kLeafSize - 1 ) / kLeafSize;
-  if ( m <= 1 ) return cudaSuccess;
-  const unsigned grid = static_cast< unsigned >( ( m + kBuildThreads - 1 ) / kBuildThreads );
-  k_refit< K, T ><<< grid, kBuildThreads, 0, s >>>( static_cast< int >( n ), static_cast< const T * >( bucket_box ),
-                                                   static_cast< T * >( node_box ), parent, exch, sc );
+  return m <= 1 ? 0u : static_cast< uint32_t >( ( m + kBuildThreads - 1 ) / kBuildThreads );
+}
+
+template< int K, typename T >
+cudaError_t launch_refit_t(const tree_args &a, cudaStream_t s)
+{
+  const uint32_t grid = refit_grid( a.n );
+  if ( !grid ) return cudaSuccess;
+  k_single< tree_args, refit_body< K, T >, kBuildThreads, 7 ><<< grid, kBuildThreads, 0, s >>>( a );
+  return cudaGetLastError();
+}
+
+template< int K, typename T >
+cudaError_t launch_refit_batch_t(const batch_launch &b, cudaStream_t s)
+{
+  k_batched< tree_args, refit_body< K, T >, kBuildThreads, 7 ><<< b.blocks, kBuildThreads, 0, s >>>(
+    static_cast< const tree_args * >( b.items ), b.starts, b.nitems );
   return cudaGetLastError();
 }
 
@@ -717,67 +801,112 @@ cudaError_t probe_v(const double *verts, uint32_t V, uint64_t n, double eps, voi
 
 }  // namespace
 
-cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
-                         const uint32_t *vals, void *bucket_box, void *warp_box, void *elem_rows,
-                         obj_scalars *sc, cudaStream_t s)
-{
-  switch ( K )
-  {
-    case 6: return fp32 ? slabs_v< 6, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s )
-                        : slabs_v< 6, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s );
-    case 18: return fp32 ? slabs_v< 18, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s )
-                         : slabs_v< 18, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s );
-    case 26: return fp32 ? slabs_v< 26, float >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s )
-                         : slabs_v< 26, double >( verts, V, n, eps, vals, bucket_box, warp_box, elem_rows, sc, s );
-    default: return cudaErrorInvalidValue;
+#define BVHG_BY_K( CALL_F, CALL_D )                                                                                    \
+  switch ( K )                                                                                                         \
+  {                                                                                                                    \
+    case 6: return fp32 ? CALL_F( 6 ) : CALL_D( 6 );                                                                   \
+    case 18: return fp32 ? CALL_F( 18 ) : CALL_D( 18 );                                                                \
+    case 26: return fp32 ? CALL_F( 26 ) : CALL_D( 26 );                                                                \
+    default: return cudaErrorInvalidValue;                                                                             \
   }
+
+cudaError_t launch_slabs(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps,
+                         const uint32_t *vals, void *bucket_box, void *warp_box, void *elem_rows, obj_scalars *sc,
+                         cudaStream_t s)
+{
+  const slabs_args a{ verts, V, n, eps, f32_round_up( eps ), vals, bucket_box, warp_box, elem_rows, sc };
+#define F( KK ) slabs_v< KK, float >( a, s )
+#define D( KK ) slabs_v< KK, double >( a, s )
+  BVHG_BY_K( F, D )
+#undef F
+#undef D
+}
+
+uint32_t slabs_blocks(uint64_t n) { return slab_grid( n ); }
+
+cudaError_t launch_slabs_batch(int K, bool fp32, uint32_t V, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+#define F( KK ) slabs_batch_v< KK, float >( V, b, s )
+#define D( KK ) slabs_batch_v< KK, double >( V, b, s )
+  BVHG_BY_K( F, D )
+#undef F
+#undef D
 }
 
 cudaError_t launch_build(int K, bool fp32, uint64_t n, const uint64_t *keys, uint8_t *bdel, const void *bucket_box,
                          void *node_box, int2 *child, int2 *range, int *parent, int4 *queue, obj_scalars *sc,
                          cudaStream_t s)
 {
-  switch ( K )
-  {
-    case 6: return fp32 ? launch_build_t< 6, float >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s )
-                        : launch_build_t< 6, double >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s );
-    case 18: return fp32 ? launch_build_t< 18, float >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s )
-                         : launch_build_t< 18, double >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s );
-    case 26: return fp32 ? launch_build_t< 26, float >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s )
-                         : launch_build_t< 26, double >( n, keys, bdel, bucket_box, node_box, child, range, parent, queue, sc, s );
-    default: return cudaErrorInvalidValue;
-  }
+  const tree_args a{ n, keys, bdel, bucket_box, node_box, child, range, parent, nullptr, queue, sc };
+#define F( KK ) launch_build_t< KK, float >( a, s )
+#define D( KK ) launch_build_t< KK, double >( a, s )
+  BVHG_BY_K( F, D )
+#undef F
+#undef D
+}
+
+uint32_t build_blocks(uint64_t n) { return build_grid( n ); }
+
+cudaError_t launch_build_batch(int K, bool fp32, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+#define F( KK ) launch_build_batch_t< KK, float >( b, s )
+#define D( KK ) launch_build_batch_t< KK, double >( b, s )
+  BVHG_BY_K( F, D )
+#undef F
+#undef D
 }
 
 cudaError_t launch_climb(int K, bool fp32, uint64_t n, const uint8_t *bdel, void *node_box, int2 *child, int2 *range,
                          int *parent, int *exch, const int4 *queue, obj_scalars *sc, cudaStream_t s)
 {
-  switch ( K )
-  {
-    case 6: return fp32 ? launch_climb_t< 6, float >( n, bdel, node_box, child, range, parent, exch, queue, sc, s )
-                        : launch_climb_t< 6, double >( n, bdel, node_box, child, range, parent, exch, queue, sc, s );
-    case 18: return fp32 ? launch_climb_t< 18, float >( n, bdel, node_box, child, range, parent, exch, queue, sc, s )
-                         : launch_climb_t< 18, double >( n, bdel, node_box, child, range, parent, exch, queue, sc, s );
-    case 26: return fp32 ? launch_climb_t< 26, float >( n, bdel, node_box, child, range, parent, exch, queue, sc, s )
-                         : launch_climb_t< 26, double >( n, bdel, node_box, child, range, parent, exch, queue, sc, s );
-    default: return cudaErrorInvalidValue;
-  }
+  const tree_args a{ n, nullptr, const_cast< uint8_t * >( bdel ), nullptr, node_box, child, range, parent, exch,
+                     const_cast< int4 * >( queue ), sc };
+#define F( KK ) launch_climb_t< KK, float >( a, s )
+#define D( KK ) launch_climb_t< KK, double >( a, s )
+  BVHG_BY_K( F, D )
+#undef F
+#undef D
+}
+
+uint32_t climb_blocks(uint64_t n) { return climb_grid( n ); }
+
+cudaError_t launch_climb_batch(int K, bool fp32, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+#define F( KK ) launch_climb_batch_t< KK, float >( b, s )
+#define D( KK ) launch_climb_batch_t< KK, double >( b, s )
+  BVHG_BY_K( F, D )
+#undef F
+#undef D
 }
 
 cudaError_t launch_refit(int K, bool fp32, uint64_t n, const void *bucket_box, void *node_box, const int *parent,
                          int *exch, obj_scalars *sc, cudaStream_t s)
 {
-  switch ( K )
-  {
-    case 6: return fp32 ? launch_refit_t< 6, float >( n, bucket_box, node_box, parent, exch, sc, s )
-                        : launch_refit_t< 6, double >( n, bucket_box, node_box, parent, exch, sc, s );
-    case 18: return fp32 ? launch_refit_t< 18, float >( n, bucket_box, node_box, parent, exch, sc, s )
-                         : launch_refit_t< 18, double >( n, bucket_box, node_box, parent, exch, sc, s );
-    case 26: return fp32 ? launch_refit_t< 26, float >( n, bucket_box, node_box, parent, exch, sc, s )
-                         : launch_refit_t< 26, double >( n, bucket_box, node_box, parent, exch, sc, s );
-    default: return cudaErrorInvalidValue;
-  }
+  const tree_args a{ n, nullptr, nullptr, bucket_box, node_box, nullptr, nullptr, const_cast< int * >( parent ), exch,
+                     nullptr, sc };
+#define F( KK ) launch_refit_t< KK, float >( a, s )
+#define D( KK ) launch_refit_t< KK, double >( a, s )
+  BVHG_BY_K( F, D )
+#undef F
+#undef D
 }
+
+uint32_t refit_blocks(uint64_t n) { return refit_grid( n ); }
+
+cudaError_t launch_refit_batch(int K, bool fp32, const batch_launch &b, cudaStream_t s)
+{
+  if ( !b.nitems ) return cudaSuccess;
+#define F( KK ) launch_refit_batch_t< KK, float >( b, s )
+#define D( KK ) launch_refit_batch_t< KK, double >( b, s )
+  BVHG_BY_K( F, D )
+#undef F
+#undef D
+}
+
+#undef BVHG_BY_K
 
 cudaError_t launch_probe_kdops(int K, bool fp32, const double *verts, uint32_t V, uint64_t n, double eps, void *out,
                                cudaStream_t s)

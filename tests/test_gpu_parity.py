@@ -89,8 +89,8 @@ def test_many_tiles_sort():
 @pytest.mark.parametrize("counts", [(2, 5, 31, 32), (33, 3), (500, 40, 7), (2048, 2049, 1), (100000, 34)])
 def test_runs_of_equal_high_key_halves(counts):
     """The build sorts by the high key half, then orders each run of equal high halves by the low half on the
-    device: runs of up to 32 in the fix-up, longer ones in the run sort (a shared-memory network up to 2048
-    elements, LSD passes beyond). The permutation read back is the device's own, and it must be the stable order
+    device: runs of up to 32 by every element's own rank, longer ones by the run sort (a shared-memory network up to
+    2048 elements, LSD passes beyond). The permutation read back is the device's own, and it must be the stable order
     of the oracle's keys; the pair sets must be exact."""
     a = clustered_soup(counts, seed=sum(counts))
     b = clustered_soup(counts[::-1], seed=7 + sum(counts))
@@ -338,7 +338,7 @@ def test_stage_timing_and_launch_count():
         ctx.build(oa)
         ctx.self_collision(oa)
         ms, launches = ctx.stage_times()
-        # four radix passes over the high key half, then the low-half fix-up and the sort of long runs
+        # four radix passes over the high key half, then the low-half fix-up and the sort of its long runs
         assert launches["sort"] == 4 and launches["fixup"] == 2 and launches["slabs"] == 1 and launches["build"] == 1 and launches["climb"] == 1
         assert launches["traverse"] >= 1
         assert all(v >= 0 for v in ms.values()) and ms["sort"] > 0
