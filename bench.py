@@ -503,7 +503,7 @@ def run_batch_form(args, world, rank, local):
         ctx.set_elements(ob, db, mem=bvhg.MEM_DEVICE)
         tensors += [da, db]
         objs.append((oa, ob))
-    lanes, tune_ms = ctx.batch_autotune(objs)
+    groups, lanes, tune_ms = ctx.batch_autotune(objs)
     ia = np.ascontiguousarray([o[0] for o in objs], dtype=np.int32)
     ib = np.ascontiguousarray([o[1] for o in objs], dtype=np.int32)
     counts = np.zeros(len(objs), dtype=np.uint64)
@@ -544,7 +544,7 @@ def run_batch_form(args, world, rank, local):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded two-body scenes)",
         "config": {"workload": f"batch: 512 two-body scenes, per-scene elements LogUniform[1k, 200k] ({prims} tris),"
                                " 18-DOP, one CUDA graph", "k": K, "elements": prims, "pairs": total,
-                   "lanes": lanes, "autotune_ms": tune_ms},
+                   "groups": groups, "lanes": lanes, "autotune_ms": tune_ms},
         "parity": {"scenes_checked_against_single_scene_path": checked, "same_pair_sets": bool(same)},
     }
 

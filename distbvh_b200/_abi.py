@@ -26,7 +26,7 @@ EXPORTS = (
     "bvhg_get_stage_times", "bvhg_launch_count", "bvhg_set_spin_limit", "bvhg_test_stall_sort", "bvhg_debug_normal",
     "bvhg_synchronize", "bvhg_last_error", "bvhg_status_string", "bvhg_radix_sort_noalloc",
     "bvhg_batch_broadphase", "bvhg_batch_autotune", "bvhg_sort_and_sweep", "bvhg_test_dense_stack",
-    "bvhg_cluster", "bvhg_patch_pairs", "bvhg_patch_kdops",
+    "bvhg_cluster", "bvhg_patch_pairs", "bvhg_patch_kdops", "bvhg_test_batch_form",
 )
 
 
@@ -75,6 +75,7 @@ def _load():
         "bvhg_set_spin_limit": (I32, [P, U32]),
         "bvhg_test_stall_sort": (I32, [P, I32]),
         "bvhg_test_dense_stack": (I32, [P, I32]),
+        "bvhg_test_batch_form": (I32, [P, U32, U32]),
         "bvhg_cluster": (I32, [P, I32, U32, P, P, I32]),
         "bvhg_patch_kdops": (I32, [P, I32, P, I32]),
         "bvhg_patch_pairs": (I32, [P, I32, I32, P, U64, ctypes.POINTER(U64), P, U64, ctypes.POINTER(U64), I32]),
@@ -84,7 +85,8 @@ def _load():
         "bvhg_status_string": (ctypes.c_char_p, [I32]),
         "bvhg_radix_sort_noalloc": (I32, [P, P, P, U64, P]),
         "bvhg_batch_broadphase": (I32, [P, U32, P, P, I32, P, U64, P, P, I32]),
-        "bvhg_batch_autotune": (I32, [P, U32, P, P, I32, ctypes.POINTER(U32), ctypes.POINTER(ctypes.c_double)]),
+        "bvhg_batch_autotune": (I32, [P, U32, P, P, I32, ctypes.POINTER(U32), ctypes.POINTER(U32),
+                                      ctypes.POINTER(ctypes.c_double)]),
         "bvhg_sort_and_sweep": (I32, [P, I32, I32, I32, P, U64, ctypes.POINTER(U64), ctypes.POINTER(I32), I32]),
     }
     for name, (res, args) in sig.items():
@@ -256,13 +258,15 @@ class Context:
         return lib.bvhg_batch_broadphase(self._h, n, a_ptr, b_ptr, mode, out_ptr, capacity, counts_ptr, None, mem)
 
     def batch_autotune(self, scenes, mode=0):
+        """Picks the batching form's configuration: returns (groups (0 = per-object launches), lanes, ms)."""
         a = np.ascontiguousarray([x[0] for x in scenes], dtype=np.int32)
         b = np.ascontiguousarray([x[1] for x in scenes], dtype=np.int32)
+        groups = ctypes.c_uint32()
         lanes = ctypes.c_uint32()
         ms = ctypes.c_double()
         self._check(lib.bvhg_batch_autotune(self._h, len(scenes), a.ctypes.data, b.ctypes.data, mode,
-                                            ctypes.byref(lanes), ctypes.byref(ms)))
-        return lanes.value, ms.value
+                                            ctypes.byref(groups), ctypes.byref(lanes), ctypes.byref(ms)))
+        return groups.value, lanes.value, ms.value
 
     def cluster(self, obj, patches, n):
         """Patches of a built object: (bounds (patches + 1,) uint64, order (n,) uint32)."""
@@ -340,6 +344,9 @@ class Context:
 
     def test_stall_sort(self, enable):
         self._check(lib.bvhg_test_stall_sort(self._h, 1 if enable else 0))
+
+    def test_batch_form(self, groups, lanes):
+        self._check(lib.bvhg_test_batch_form(self._h, groups, lanes))
 
     def test_dense_stack(self, limit):
         self._check(lib.bvhg_test_dense_stack(self._h, limit))

@@ -126,9 +126,11 @@ struct batch_state
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::shared_ptr< launch_tables > tables;
-  // 0: the fused form (one batched launch per pipeline stage for all objects and scenes); else the laned form with
-  // this many concurrent streams of per-object launches (bvhg_batch_autotune picks it)
-  int lanes = 0;
+  // groups > 0: the fused form (one batched launch per pipeline stage for each of `groups` groups of objects, on
+  // `lanes` streams); groups == 0: the laned form, per-object launches on `lanes` streams. bvhg_batch_autotune picks
+  // both.
+  int groups = 16;
+  int lanes = 16;
   std::vector< cudaStream_t > lane;
   std::vector< cudaEvent_t > obj_done, lane_done;
   cudaEvent_t fork = nullptr;
@@ -829,12 +831,36 @@ uint32_t batch_vertex_count(bvhg_ctx *ctx, const std::vector< int32_t > &uniq)
   return V ? V : 3;
 }
 
-// Fused form of a batch: every pipeline stage of every object, then every scene's traversal, recheck and gid
-// mapping, each as one batched launch (batch.cuh) whose blocks run the per-object (per-scene) launch's blocks back to
-// back. The per-object computation, its buffers and its host-side state are those of do_build_on; only the number of
-// launches changes (about a dozen per batch instead of a dozen per object).
+// The batched launches of one group of a fused batch: its objects' pipeline stages and its scenes' traversal,
+// recheck and gid mapping (items and blocks per launch; uploaded by make_launch before capture).
+struct fused_group
+{
+  std::vector< init_args > init;
+  std::vector< cb_args > cb;
+  std::vector< kh_args > kh;
+  std::vector< std::vector< sort_pass_args > > pass;
+  std::vector< fixup_args > fix, runs;
+  std::vector< slabs_args > slabs;
+  std::vector< tree_args > tree;  // objects with more than one bucket (build + climb, or refit)
+  std::vector< uint32_t > b_init, b_cb, b_kh, b_fix, b_runs, b_slabs, b_build, b_climb, b_refit;
+  std::vector< std::vector< uint32_t > > b_pass;
+  std::vector< trav_item > dense, sparse;
+  std::vector< recheck_args > recheck;
+  std::vector< gid_args > gid;
+  std::vector< uint32_t > b_dense, b_sparse, b_recheck, b_gid;
+  std::vector< int > needs;  // other groups whose objects this group's scenes read
+  batch_launch l_init, l_cb, l_kh, l_fix, l_runs, l_slabs, l_build, l_climb, l_refit, l_dense, l_sparse, l_recheck, l_gid;
+  std::vector< batch_launch > l_pass;
+};
+
+// Fused form of a batch: the objects are split into `groups` groups of about equal element counts (in first-use
+// order, so a scene's two objects mostly share a group); each group runs every pipeline stage of its objects as one
+// batched launch per stage (batch.cuh), then the traversal, recheck and gid mapping of the scenes whose later object
+// is in the group, on one of `lanes` streams. Groups small enough for their objects' working sets to stay in L2
+// between stages run faster than one group over the whole batch; the autotuner picks the group count. The
+// per-object computation, its buffers and its host-side state are those of do_build_on; only the launches change.
 bvhg_status capture_batch_fused(bvhg_ctx *ctx, batch_state &B, const batch_args &x, const std::vector< int32_t > &uniq,
-                                uint32_t V)
+                                uint32_t V, int groups, int lanes)
 {
   const int K = ctx->cfg.k;
   const bool fp32 = ctx->cfg.precision == BVHG_FILTER_FP32;
@@ -844,21 +870,34 @@ bvhg_status capture_batch_fused(bvhg_ctx *ctx, batch_state &B, const batch_args 
   const uint64_t radix = 1ull << bits;
   const double eps = ctx->cfg.epsilon;
   auto tables = std::make_shared< launch_tables >();
-  std::vector< init_args > it_init;
-  std::vector< cb_args > it_cb;
-  std::vector< kh_args > it_kh;
-  std::vector< std::vector< sort_pass_args > > it_pass( passes );
-  std::vector< fixup_args > it_fix, it_runs;
-  std::vector< slabs_args > it_slabs;
-  std::vector< tree_args > it_tree;  // objects with more than one bucket (build + climb, or refit)
-  std::vector< uint32_t > b_init, b_cb, b_kh, b_fix, b_runs, b_slabs, b_build, b_climb, b_refit;
-  std::vector< std::vector< uint32_t > > b_pass( passes );
+  // objects to groups by cumulative element count
+  uint64_t total = 0;
+  for ( int32_t oi : uniq ) total += ctx->objs[oi]->n;
+  const int G = std::max( 1, std::min< int >( groups, static_cast< int >( uniq.size() ) ) );
+  std::vector< int > group_of( ctx->objs.size(), 0 );
+  {
+    uint64_t acc = 0;
+    for ( int32_t oi : uniq )
+    {
+      const int g = total ? static_cast< int >( std::min< uint64_t >( G - 1, ( acc * G ) / total ) ) : 0;
+      group_of[oi] = g;
+      acc += ctx->objs[oi]->n;
+    }
+  }
+  std::vector< fused_group > grp( G );
+  for ( auto &fg : grp )
+  {
+    fg.pass.resize( passes );
+    fg.b_pass.resize( passes );
+    fg.l_pass.resize( passes );
+  }
   bool tma = V == 3 || V == 4 || V == 8;
   for ( int32_t oi : uniq )
     if ( ctx->objs[oi]->n && ( reinterpret_cast< uintptr_t >( ctx->objs[oi]->verts ) & 15 ) ) tma = false;
   for ( int32_t oi : uniq )
   {
     object &o = *ctx->objs[oi];
+    fused_group &fg = grp[group_of[oi]];
     if ( o.n == 0 )
     {
       o.built = true;
@@ -873,56 +912,56 @@ bvhg_status capture_batch_fused(bvhg_ctx *ctx, batch_state &B, const batch_args 
       const size_t first_words = static_cast< size_t >( first ) * ( tiles + 1 ) * radix;
       const init_args ia{ o.sc(), o.hist.as< uint32_t >(), passes * radix, o.status.as< uint32_t >() + first_words,
                           passes * ( tiles + 1 ) * radix - first_words, o.exch.as< int >(), m > 1 ? m - 1 : 0 };
-      it_init.push_back( ia );
-      b_init.push_back( obj_init_blocks( ia ) );
-      it_cb.push_back( cb_args{ o.verts, o.V, n, eps, o.cx.as< double >(), o.cy.as< double >(), o.cz.as< double >(),
+      fg.init.push_back( ia );
+      fg.b_init.push_back( obj_init_blocks( ia ) );
+      fg.cb.push_back( cb_args{ o.verts, o.V, n, eps, o.cx.as< double >(), o.cy.as< double >(), o.cz.as< double >(),
                                 o.sc(), ctx->spin_limit } );
       uint32_t cbb = 0;
       BVHG_CUDA( ctx, centroid_bounds_blocks( K, V, n, tma, &cbb ) );
-      b_cb.push_back( cbb );
-      it_kh.push_back( kh_args{ o.cx.as< double >(), o.cy.as< double >(), o.cz.as< double >(), n, o.sc(),
+      fg.b_cb.push_back( cbb );
+      fg.kh.push_back( kh_args{ o.cx.as< double >(), o.cy.as< double >(), o.cz.as< double >(), n, o.sc(),
                                 o.keys.as< uint64_t >(), o.hist.as< uint32_t >() } );
-      b_kh.push_back( keys_hist_blocks( n ) );
+      fg.b_kh.push_back( keys_hist_blocks( n ) );
       uint64_t *kin = o.keys.as< uint64_t >(), *kout = o.keys_alt.as< uint64_t >();
       uint32_t *vin = nullptr, *vout = o.vals_alt.as< uint32_t >();
       uint32_t *vother = o.vals.as< uint32_t >();
       for ( int p = first; p < passes; ++p )
       {
-        it_pass[p].push_back( onesweep_args( bits, kin, vin, kout, vout, n, p, o.hist.as< uint32_t >(),
+        fg.pass[p].push_back( onesweep_args( bits, kin, vin, kout, vout, n, p, o.hist.as< uint32_t >(),
                                              o.status.as< uint32_t >(), o.sc(), ctx->spin_limit, ctx->stall_sort ) );
-        b_pass[p].push_back( onesweep_blocks( n ) );
+        fg.b_pass[p].push_back( onesweep_blocks( n ) );
         std::swap( kin, kout );
         uint32_t *next_out = vin ? vin : vother;
         vin = vout;
         vout = next_out;
       }
       const fixup_args fa{ kin, vin, kout, vout, n, o.runs.as< uint32_t >(), o.sc() };
-      it_fix.push_back( fa );
-      b_fix.push_back( sort_fixup_blocks( n ) );
+      fg.fix.push_back( fa );
+      fg.b_fix.push_back( sort_fixup_blocks( n ) );
       if ( const uint32_t rb = sort_runs_blocks( n ) )
       {
-        it_runs.push_back( fa );
-        b_runs.push_back( rb );
+        fg.runs.push_back( fa );
+        fg.b_runs.push_back( rb );
       }
       o.sort_result_alt = ( kout == o.keys_alt.as< uint64_t >() ) ? 1 : 0;
     } else if ( m > 1 ) {
       // refit: only the exchange slots start over
       const init_args ia{ nullptr, nullptr, 0, nullptr, 0, o.exch.as< int >(), m - 1 };
-      it_init.push_back( ia );
-      b_init.push_back( obj_init_blocks( ia ) );
+      fg.init.push_back( ia );
+      fg.b_init.push_back( obj_init_blocks( ia ) );
     }
-    it_slabs.push_back( slabs_args{ o.verts, o.V, n, eps, f32_round_up( eps ), o.sorted_vals(), o.bucket_box.p,
+    fg.slabs.push_back( slabs_args{ o.verts, o.V, n, eps, f32_round_up( eps ), o.sorted_vals(), o.bucket_box.p,
                                     o.warp_box.p, o.store_slabs ? o.elem_cache.p : nullptr, o.sc() } );
-    b_slabs.push_back( slabs_blocks( n ) );
+    fg.b_slabs.push_back( slabs_blocks( n ) );
     o.stored = o.store_slabs;
     if ( m > 1 )
     {
-      it_tree.push_back( tree_args{ n, o.sorted_keys(), o.bdel.as< uint8_t >(), o.bucket_box.p, o.node_box.p,
+      fg.tree.push_back( tree_args{ n, o.sorted_keys(), o.bdel.as< uint8_t >(), o.bucket_box.p, o.node_box.p,
                                     o.child.as< int2 >(), o.range.as< int2 >(), o.parent.as< int >(), o.exch.as< int >(),
                                     o.queue.as< int4 >(), o.sc() } );
-      b_build.push_back( build_blocks( n ) );
-      b_climb.push_back( climb_blocks( n ) );
-      b_refit.push_back( refit_blocks( n ) );
+      fg.b_build.push_back( build_blocks( n ) );
+      fg.b_climb.push_back( climb_blocks( n ) );
+      fg.b_refit.push_back( refit_blocks( n ) );
     }
     o.built = true;
     if ( x.mode == BVHG_REBUILD )
@@ -934,102 +973,146 @@ bvhg_status capture_batch_fused(bvhg_ctx *ctx, batch_state &B, const batch_args 
       o.fresh = false;
     }
   }
-  // scenes (after the objects' host state above: the views read which buffers hold the sorted order and slabs)
+  // scenes (after the objects' host state above: the views read which buffers hold the sorted order and slabs), in
+  // the group of their later object
   pair_scalars *ps = B.ps.as< pair_scalars >();
-  std::vector< trav_item > it_dense, it_sparse;
-  std::vector< uint32_t > b_dense, b_sparse, b_recheck, b_gid;
-  std::vector< recheck_args > it_recheck;
-  std::vector< gid_args > it_gid;
   for ( uint32_t sc = 0; sc < x.nscenes; ++sc )
   {
     object &oa = *ctx->objs[x.a[sc]];
     object &ob = *ctx->objs[x.b[sc]];
     const bool self = x.a[sc] == x.b[sc];
     if ( oa.n == 0 || ob.n == 0 || ( self && oa.n < 2 ) ) continue;
+    const int ga = group_of[x.a[sc]], gb = group_of[x.b[sc]];
+    fused_group &fg = grp[std::max( ga, gb )];
+    const int other = std::min( ga, gb );
+    if ( other != std::max( ga, gb ) && std::find( fg.needs.begin(), fg.needs.end(), other ) == fg.needs.end() )
+      fg.needs.push_back( other );
     uint2 *cand = B.cand.as< uint2 >() + B.off[sc];
     trav_item ti;
     uint32_t tb = 0;
     bool dense = false;
     traverse_item( K, fp32, view_of( oa ), view_of( ob ), self, oa.dense_ok && ob.dense_ok, eps, cand, B.cap[sc],
                    ps + sc, ctx->dense_stack, &ti, &tb, &dense );
-    ( dense ? it_dense : it_sparse ).push_back( ti );
-    ( dense ? b_dense : b_sparse ).push_back( tb );
+    ( dense ? fg.dense : fg.sparse ).push_back( ti );
+    ( dense ? fg.b_dense : fg.b_sparse ).push_back( tb );
     const uint2 *fin = cand;
     const unsigned long long *cnt = &ps[sc].count;
     if ( fp32 )
     {
       uint2 *ex = B.exact.as< uint2 >() + B.off[sc];
-      it_recheck.push_back( recheck_args{ oa.verts, oa.V, ob.verts, ob.V, eps, cand, B.cap[sc], ex, B.cap[sc], ps + sc } );
-      b_recheck.push_back( recheck_blocks( B.cap[sc] ) );
+      fg.recheck.push_back( recheck_args{ oa.verts, oa.V, ob.verts, ob.V, eps, cand, B.cap[sc], ex, B.cap[sc], ps + sc } );
+      fg.b_recheck.push_back( recheck_blocks( B.cap[sc] ) );
       fin = ex;
       cnt = &ps[sc].count2;
     }
-    it_gid.push_back( gid_args{ fin, cnt, B.cap[sc], oa.gid, ob.gid, self ? 1 : 0, B.out.as< uint64_t >() + 2 * B.off[sc] } );
-    b_gid.push_back( gid_pairs_dev_blocks( B.cap[sc] ) );
+    fg.gid.push_back( gid_args{ fin, cnt, B.cap[sc], oa.gid, ob.gid, self ? 1 : 0, B.out.as< uint64_t >() + 2 * B.off[sc] } );
+    fg.b_gid.push_back( gid_pairs_dev_blocks( B.cap[sc] ) );
   }
-  // the tables on the device, then the graph
-  batch_launch l_init, l_cb, l_kh, l_fix, l_runs, l_slabs, l_build, l_climb, l_refit, l_dense, l_sparse, l_recheck, l_gid;
-  std::vector< batch_launch > l_pass( passes );
-  bvhg_status st = make_launch( ctx, *tables, it_init, b_init, &l_init );
-  if ( st == BVHG_OK && x.mode == BVHG_REBUILD )
+  // the tables on the device
+  for ( auto &fg : grp )
   {
-    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_cb, b_cb, &l_cb );
-    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_kh, b_kh, &l_kh );
-    for ( int p = first; p < passes && st == BVHG_OK; ++p ) st = make_launch( ctx, *tables, it_pass[p], b_pass[p], &l_pass[p] );
-    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_fix, b_fix, &l_fix );
-    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_runs, b_runs, &l_runs );
-    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_tree, b_build, &l_build );
-    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_tree, b_climb, &l_climb );
-  } else if ( st == BVHG_OK ) {
-    st = make_launch( ctx, *tables, it_tree, b_refit, &l_refit );
+    bvhg_status st = make_launch( ctx, *tables, fg.init, fg.b_init, &fg.l_init );
+    if ( st == BVHG_OK && x.mode == BVHG_REBUILD )
+    {
+      if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.cb, fg.b_cb, &fg.l_cb );
+      if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.kh, fg.b_kh, &fg.l_kh );
+      for ( int p = first; p < passes && st == BVHG_OK; ++p )
+        st = make_launch( ctx, *tables, fg.pass[p], fg.b_pass[p], &fg.l_pass[p] );
+      if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.fix, fg.b_fix, &fg.l_fix );
+      if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.runs, fg.b_runs, &fg.l_runs );
+      if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.tree, fg.b_build, &fg.l_build );
+      if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.tree, fg.b_climb, &fg.l_climb );
+    } else if ( st == BVHG_OK ) {
+      st = make_launch( ctx, *tables, fg.tree, fg.b_refit, &fg.l_refit );
+    }
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.slabs, fg.b_slabs, &fg.l_slabs );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.dense, fg.b_dense, &fg.l_dense );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.sparse, fg.b_sparse, &fg.l_sparse );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.recheck, fg.b_recheck, &fg.l_recheck );
+    if ( st == BVHG_OK ) st = make_launch( ctx, *tables, fg.gid, fg.b_gid, &fg.l_gid );
+    if ( st != BVHG_OK ) return st;
   }
-  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_slabs, b_slabs, &l_slabs );
-  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_dense, b_dense, &l_dense );
-  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_sparse, b_sparse, &l_sparse );
-  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_recheck, b_recheck, &l_recheck );
-  if ( st == BVHG_OK ) st = make_launch( ctx, *tables, it_gid, b_gid, &l_gid );
-  if ( st != BVHG_OK ) return st;
-  const uint32_t Vt = V;  // every object shares it: the traversal and recheck unroll it
+  // streams and events
+  const int L = std::max( 1, std::min( lanes, G ) );
+  while ( static_cast< int >( B.lane.size() ) < L )
+  {
+    cudaStream_t st = nullptr;
+    BVHG_CUDA( ctx, cudaStreamCreateWithFlags( &st, cudaStreamNonBlocking ) );
+    B.lane.push_back( st );
+    cudaEvent_t e = nullptr;
+    BVHG_CUDA( ctx, cudaEventCreateWithFlags( &e, cudaEventDisableTiming ) );
+    B.lane_done.push_back( e );
+  }
+  while ( B.obj_done.size() < static_cast< size_t >( G ) )
+  {
+    cudaEvent_t e = nullptr;
+    BVHG_CUDA( ctx, cudaEventCreateWithFlags( &e, cudaEventDisableTiming ) );
+    B.obj_done.push_back( e );
+  }
+  if ( !B.fork ) BVHG_CUDA( ctx, cudaEventCreateWithFlags( &B.fork, cudaEventDisableTiming ) );
   B.graph = nullptr;
   B.exec = nullptr;
   cudaStream_t s = ctx->stream;
   BVHG_CUDA( ctx, cudaStreamBeginCapture( s, cudaStreamCaptureModeRelaxed ) );
   auto body = [&]() -> bvhg_status {
     BVHG_CUDA( ctx, cudaMemsetAsync( ps, 0, x.nscenes * sizeof( pair_scalars ), s ) );
-    BVHG_CUDA( ctx, launch_obj_init_batch( l_init, s ) );
-    if ( x.mode == BVHG_REBUILD )
+    BVHG_CUDA( ctx, cudaEventRecord( B.fork, s ) );
+    for ( int l = 0; l < L; ++l ) BVHG_CUDA( ctx, cudaStreamWaitEvent( B.lane[l], B.fork, 0 ) );
+    // builds, group by group on its lane
+    for ( int g = 0; g < G; ++g )
     {
-      BVHG_CUDA( ctx, launch_centroid_bounds_batch( K, V, tma, l_cb, s ) );
-      BVHG_CUDA( ctx, launch_keys_hist_batch( bits, l_kh, s ) );
-      for ( int p = first; p < passes; ++p ) BVHG_CUDA( ctx, launch_onesweep_batch( bits, l_pass[p], s ) );
-      BVHG_CUDA( ctx, launch_sort_fixup_batch( l_fix, s ) );
-      BVHG_CUDA( ctx, launch_sort_runs_batch( l_runs, s ) );
-      BVHG_CUDA( ctx, launch_slabs_batch( K, fp32, V, l_slabs, s ) );
-      BVHG_CUDA( ctx, launch_build_batch( K, fp32, l_build, s ) );
-      BVHG_CUDA( ctx, launch_climb_batch( K, fp32, l_climb, s ) );
-    } else {
-      BVHG_CUDA( ctx, launch_slabs_batch( K, fp32, V, l_slabs, s ) );
-      BVHG_CUDA( ctx, launch_refit_batch( K, fp32, l_refit, s ) );
+      fused_group &fg = grp[g];
+      cudaStream_t ls = B.lane[g % L];
+      BVHG_CUDA( ctx, launch_obj_init_batch( fg.l_init, ls ) );
+      if ( x.mode == BVHG_REBUILD )
+      {
+        BVHG_CUDA( ctx, launch_centroid_bounds_batch( K, V, tma, fg.l_cb, ls ) );
+        BVHG_CUDA( ctx, launch_keys_hist_batch( bits, fg.l_kh, ls ) );
+        for ( int p = first; p < passes; ++p ) BVHG_CUDA( ctx, launch_onesweep_batch( bits, fg.l_pass[p], ls ) );
+        BVHG_CUDA( ctx, launch_sort_fixup_batch( fg.l_fix, ls ) );
+        BVHG_CUDA( ctx, launch_sort_runs_batch( fg.l_runs, ls ) );
+        BVHG_CUDA( ctx, launch_slabs_batch( K, fp32, V, fg.l_slabs, ls ) );
+        BVHG_CUDA( ctx, launch_build_batch( K, fp32, fg.l_build, ls ) );
+        BVHG_CUDA( ctx, launch_climb_batch( K, fp32, fg.l_climb, ls ) );
+      } else {
+        BVHG_CUDA( ctx, launch_slabs_batch( K, fp32, V, fg.l_slabs, ls ) );
+        BVHG_CUDA( ctx, launch_refit_batch( K, fp32, fg.l_refit, ls ) );
+      }
+      BVHG_CUDA( ctx, cudaEventRecord( B.obj_done[g], ls ) );
+      ctx->launches += x.mode == BVHG_REBUILD ? 9 + ( passes - first ) : 3;
     }
-    BVHG_CUDA( ctx, launch_traverse_batch( K, fp32, true, Vt, l_dense, s ) );
-    BVHG_CUDA( ctx, launch_traverse_batch( K, fp32, false, Vt, l_sparse, s ) );
-    if ( fp32 ) BVHG_CUDA( ctx, launch_recheck_batch( K, Vt, l_recheck, s ) );
-    BVHG_CUDA( ctx, launch_gid_pairs_dev_batch( l_gid, s ) );
+    // scenes, group by group after the builds they read
+    for ( int g = 0; g < G; ++g )
+    {
+      fused_group &fg = grp[g];
+      cudaStream_t ls = B.lane[g % L];
+      for ( int o : fg.needs )
+        if ( o % L != g % L ) BVHG_CUDA( ctx, cudaStreamWaitEvent( ls, B.obj_done[o], 0 ) );
+      BVHG_CUDA( ctx, launch_traverse_batch( K, fp32, true, V, fg.l_dense, ls ) );
+      BVHG_CUDA( ctx, launch_traverse_batch( K, fp32, false, V, fg.l_sparse, ls ) );
+      if ( fp32 ) BVHG_CUDA( ctx, launch_recheck_batch( K, V, fg.l_recheck, ls ) );
+      BVHG_CUDA( ctx, launch_gid_pairs_dev_batch( fg.l_gid, ls ) );
+      ctx->launches += fp32 ? 4 : 3;
+    }
+    for ( int l = 0; l < L; ++l )
+    {
+      BVHG_CUDA( ctx, cudaEventRecord( B.lane_done[l], B.lane[l] ) );
+      BVHG_CUDA( ctx, cudaStreamWaitEvent( s, B.lane_done[l], 0 ) );
+    }
     BVHG_CUDA( ctx, launch_gather_words( B.err_src.as< const int *const >(), static_cast< int >( uniq.size() ),
                                          B.err_words.as< int >(), s ) );
-    ctx->launches += 16;
     return BVHG_OK;
   };
-  st = body();
-  cudaGraph_t g = nullptr;
-  const cudaError_t ce = cudaStreamEndCapture( s, &g );
+  bvhg_status st = body();
+  cudaGraph_t gph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture( s, &gph );
   if ( st != BVHG_OK )
   {
-    if ( g ) cudaGraphDestroy( g );
+    if ( gph ) cudaGraphDestroy( gph );
     return st;
   }
   if ( ce != cudaSuccess ) return cuda_fail( ctx, ce, "cudaStreamEndCapture" );
-  B.graph = g;
+  B.graph = gph;
   BVHG_CUDA( ctx, cudaGraphInstantiate( &B.exec, B.graph, 0 ) );
   B.tables = tables;
   return BVHG_OK;
@@ -1107,6 +1190,7 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
     }
     // graph identity: everything a replay would read from the captured parameters
     std::vector< uint64_t > key{ static_cast< uint64_t >( x.mode ), x.nscenes, static_cast< uint64_t >( B.lanes ),
+                                 static_cast< uint64_t >( B.groups ),
                                  reinterpret_cast< uint64_t >( B.cand.p ), reinterpret_cast< uint64_t >( B.out.p ),
                                  reinterpret_cast< uint64_t >( B.exact.p ), reinterpret_cast< uint64_t >( B.ps.p ),
                                  reinterpret_cast< uint64_t >( B.err_src.p ),
@@ -1137,7 +1221,7 @@ bvhg_status run_batch(bvhg_ctx *ctx, const batch_args &x, uint64_t *counts)
     if ( !B.select( key ) )
     {
       const uint32_t V = batch_vertex_count( ctx, uniq );
-      const bvhg_status st = B.lanes == 0 && V ? capture_batch_fused( ctx, B, x, uniq, V )
+      const bvhg_status st = B.groups > 0 && V ? capture_batch_fused( ctx, B, x, uniq, V, B.groups, B.lanes )
                                                : capture_batch( ctx, B, x, uniq, slot );
       if ( st != BVHG_OK ) return st;
       B.key = key;
@@ -1425,7 +1509,7 @@ bvhg_status bvhg_batch_broadphase(bvhg_ctx *ctx, uint32_t nscenes, const int32_t
 }
 
 bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a, const int32_t *obj_b,
-                                int32_t mode, uint32_t *lanes, double *ms)
+                                int32_t mode, uint32_t *groups, uint32_t *lanes, double *ms)
 {
   if ( !ctx ) return BVHG_ERR_ARG;
   if ( nscenes == 0 || !obj_a || !obj_b ) return fail( ctx, BVHG_ERR_ARG, "empty batch" );
@@ -1437,13 +1521,17 @@ bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   BVHG_CUDA( ctx, cudaEventCreate( &e0 ) );
   BVHG_CUDA( ctx, cudaEventCreate( &e1 ) );
-  int best = ctx->batch->lanes;
+  int best_groups = ctx->batch->groups, best_lanes = ctx->batch->lanes;
   float best_ms = 0.f;
   bvhg_status st = BVHG_OK;
-  for ( int L : { 0, 1, 4, 8, 16, 32, 64 } )
+  // fused form: groups of objects (the batch's tile), one stream per group up to 16; laned form: per-object launches
+  const std::pair< int, int > configs[] = { { 1, 1 }, { 4, 4 }, { 16, 16 }, { 64, 16 }, { 256, 16 },
+                                            { 0, 16 }, { 0, 64 } };
+  for ( const auto &cfg : configs )
   {
-    ctx->batch->lanes = L;
-    st = run_batch( ctx, x, counts.data() );  // captures this lane count's graph and settles the capacities
+    ctx->batch->groups = cfg.first;
+    ctx->batch->lanes = cfg.second;
+    st = run_batch( ctx, x, counts.data() );  // captures this configuration's graph and settles the capacities
     if ( st != BVHG_OK ) break;
     float t = 0.f;
     cudaEventRecord( e0, ctx->stream );
@@ -1458,14 +1546,17 @@ bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *
     if ( best_ms == 0.f || t < best_ms )
     {
       best_ms = t;
-      best = L;
+      best_groups = cfg.first;
+      best_lanes = cfg.second;
     }
   }
   cudaEventDestroy( e0 );
   cudaEventDestroy( e1 );
-  ctx->batch->lanes = best;
+  ctx->batch->groups = best_groups;
+  ctx->batch->lanes = best_lanes;
   ctx->batch->drop_graph();
-  if ( lanes ) *lanes = static_cast< uint32_t >( best );
+  if ( lanes ) *lanes = static_cast< uint32_t >( best_lanes );
+  if ( groups ) *groups = static_cast< uint32_t >( best_groups );
   if ( ms ) *ms = best_ms;
   return st;
 }
@@ -2002,6 +2093,15 @@ bvhg_status bvhg_test_stall_sort(bvhg_ctx *ctx, int32_t enable)
 {
   if ( !ctx ) return BVHG_ERR_ARG;
   ctx->stall_sort = enable ? 1 : 0;
+  return BVHG_OK;
+}
+
+bvhg_status bvhg_test_batch_form(bvhg_ctx *ctx, uint32_t groups, uint32_t lanes)
+{
+  if ( !ctx || lanes == 0 || lanes > 64 || groups > 4096 ) return BVHG_ERR_ARG;
+  if ( !ctx->batch ) ctx->batch = std::make_unique< batch_state >();
+  ctx->batch->groups = static_cast< int >( groups );
+  ctx->batch->lanes = static_cast< int >( lanes );
   return BVHG_OK;
 }
 

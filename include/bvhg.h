@@ -156,20 +156,24 @@ BVHG_API bvhg_status bvhg_sort_and_sweep(bvhg_ctx *ctx, int32_t obj_a, int32_t o
  * src/bvh/collision_object.cpp:248 at once). Scene s pairs objects obj_a[s] and obj_b[s] (obj_a[s] == obj_b[s]: that
  * object's self-collision); objects already hold their elements (bvhg_set_elements) and may appear in several
  * scenes. Every object in the batch is built once (mode: BVHG_REBUILD, or BVHG_REFIT after a rebuild) and every
- * scene traversed, as one CUDA graph: builds and scenes spread over concurrent streams, no host round trip between
- * them. The graph is captured on the first call for a batch layout (objects, element counts, vertex pointers,
- * per-scene capacities) and replayed while the layout stays the same, so a time-stepped loop that updates
- * coordinates in place replays it. counts[s] (host, required) receives scene s's exact pair count; the pairs go
- * to `pairs` (mem) scene after scene, (gid_a, gid_b) like bvhg_broadphase, scene s starting at pair offsets[s]
- * (offsets may be NULL). BVHG_ERR_OVERFLOW when the total exceeds capacity (counts are then still valid). */
+ * scene traversed, as one CUDA graph with no host round trip between scenes. When every object has the same vertex
+ * count the graph is the fused form: the objects are split into groups, and each group runs each pipeline stage of
+ * all its objects as one launch, then the traversal of its scenes as one launch, groups on concurrent streams;
+ * otherwise per-object launches spread over concurrent streams. The graph is captured on the first call for a batch
+ * layout (objects, element counts, vertex pointers, per-scene capacities) and replayed while the layout stays the
+ * same, so a time-stepped loop that updates coordinates in place replays it. counts[s] (host, required) receives
+ * scene s's exact pair count; the pairs go to `pairs` (mem) scene after scene, (gid_a, gid_b) like bvhg_broadphase,
+ * scene s starting at pair offsets[s] (offsets may be NULL). BVHG_ERR_OVERFLOW when the total exceeds capacity
+ * (counts are then still valid). Objects built by a batch are built as by bvhg_build. */
 BVHG_API bvhg_status bvhg_batch_broadphase(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a,
                                           const int32_t *obj_b, int32_t mode, uint64_t *pairs, uint64_t capacity,
                                           uint64_t *counts, uint64_t *offsets, int32_t mem);
-/* Autotuner of the batching form: times the batch's graph with 1, 4, 8, 16, 32 and 64 concurrent streams and keeps
- * the fastest for later bvhg_batch_broadphase calls on this context. lanes and ms (may be NULL) receive the choice
- * and its time per batch. */
+/* Autotuner of the batching form: times the batch's graph in the fused form with 1, 4, 16, 64 and 256 groups of
+ * objects (the batch's tile: groups whose working sets stay in L2 between stages) and in the per-object form with 16
+ * and 64 streams, and keeps the fastest for later bvhg_batch_broadphase calls on this context. groups (0 = the
+ * per-object form), lanes (streams) and ms (may be NULL) receive the choice and its time per batch. */
 BVHG_API bvhg_status bvhg_batch_autotune(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a, const int32_t *obj_b,
-                                        int32_t mode, uint32_t *lanes, double *ms);
+                                        int32_t mode, uint32_t *groups, uint32_t *lanes, double *ms);
 
 /* Patches: the reference's Morton clustering of an object (morton_cluster, src/bvh/split/cluster.hpp:89-179, as
  * set_entity_data_clustering uses it, src/bvh/collision_object.hpp:89-131), on the device from the last rebuild's
@@ -228,6 +232,9 @@ BVHG_API bvhg_status bvhg_set_spin_limit(bvhg_ctx *ctx, uint32_t limit);
 /* Test hook: when enabled, every radix-sort look-back after the first tile polls a status word that no block
  * publishes, so the bounded wait runs out and the build reports BVHG_ERR_TIMEOUT (the context stays usable). */
 BVHG_API bvhg_status bvhg_test_stall_sort(bvhg_ctx *ctx, int32_t enable);
+/* Test hook: sets the batching form's configuration instead of the autotuner (groups 0: per-object launches on
+ * `lanes` streams; else the fused form with that many groups of objects on `lanes` streams, lanes 1..64). */
+BVHG_API bvhg_status bvhg_test_batch_form(bvhg_ctx *ctx, uint32_t groups, uint32_t lanes);
 /* Test hook: lowers the stack bound of the dense-contact walk to `limit` entries (0 restores it), so that it is
  * reached and the library's fallback to the single-node walk runs (the pair set stays exact). */
 BVHG_API bvhg_status bvhg_test_dense_stack(bvhg_ctx *ctx, int32_t limit);

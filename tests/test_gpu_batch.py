@@ -1,8 +1,10 @@
 """Batching form: many independent scenes as one CUDA graph (bvhg_batch_broadphase), against the oracle.
 
 Scenes of uneven sizes (including an empty object and a self-collision scene) must each give the exact pair set
-of the single-scene path; replays of the captured graph after coordinates change in place must too (REBUILD and
-REFIT); the autotuner must pick one of its lane counts and leave the context usable.
+of the single-scene path, in every form of the batch graph (fused: one launch per pipeline stage for one group of
+objects or several; per-object launches on concurrent streams); replays of the captured graph after coordinates
+change in place must too (REBUILD and REFIT); the autotuner must pick one of its configurations and leave the
+context usable.
 """
 import numpy as np
 import pytest
@@ -27,10 +29,15 @@ def make_scenes(seed, nscenes, k):
     return bodies
 
 
+FORMS = [(1, 1), (5, 3), (16, 16), (0, 4)]  # (groups, lanes): fused with 1, 5 or 16 groups; per-object launches
+
+
 @pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
-def test_batch_matches_single_scenes(precision):
+@pytest.mark.parametrize("form", FORMS)
+def test_batch_matches_single_scenes(precision, form):
     bodies = make_scenes(5, 12, 18)
     with bvhg.Context(k=18, precision=precision) as ctx:
+        ctx.test_batch_form(*form)
         objs = []
         for a, b in bodies:
             oa, ob = ctx.object(), ctx.object()
@@ -50,10 +57,12 @@ def test_batch_matches_single_scenes(precision):
         assert np.array_equal(orc.canonical(ctx.broadphase(*objs[3])), orc.pair_set(*bodies[3], 18))
 
 
-def test_batch_replay_after_motion_rebuild_and_refit():
+@pytest.mark.parametrize("form", FORMS)
+def test_batch_replay_after_motion_rebuild_and_refit(form):
     bodies = make_scenes(9, 8, 18)
     dev = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in bodies]
     with bvhg.Context(k=18) as ctx:
+        ctx.test_batch_form(*form)
         objs = []
         for da, db in dev:
             oa, ob = ctx.object(), ctx.object()
@@ -72,7 +81,7 @@ def test_batch_replay_after_motion_rebuild_and_refit():
                 assert np.array_equal(orc.canonical(got[s]), want), (step, s)
 
 
-def test_batch_autotune_picks_a_lane_count():
+def test_batch_autotune_picks_a_configuration():
     bodies = make_scenes(13, 24, 18)
     with bvhg.Context(k=18) as ctx:
         objs = []
@@ -81,8 +90,8 @@ def test_batch_autotune_picks_a_lane_count():
             ctx.set_elements(oa, a)
             ctx.set_elements(ob, b)
             objs.append((oa, ob))
-        lanes, ms = ctx.batch_autotune(objs)
-        assert lanes in (1, 4, 8, 16, 32, 64) and ms > 0
+        groups, lanes, ms = ctx.batch_autotune(objs)
+        assert (groups, lanes) in ((1, 1), (4, 4), (16, 16), (64, 16), (256, 16), (0, 16), (0, 64)) and ms > 0
         got = ctx.batch_broadphase(objs)
         for s, (a, b) in enumerate(bodies):
             assert np.array_equal(orc.canonical(got[s]), orc.pair_set(a, b, 18))
