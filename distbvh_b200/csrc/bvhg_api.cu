@@ -458,8 +458,8 @@ bvhg_status do_build_on(bvhg_ctx *ctx, object &o, int mode, cudaStream_t s)
     {
       stage_scope st( ctx, BVHG_STAGE_BUILD );
       BVHG_CUDA( ctx, cudaMemsetAsync( o.exch.p, 0xff, ( m - 1 ) * sizeof( int ), s ) );
-      BVHG_CUDA( ctx, launch_refit( K, fp32, n, o.bucket_box.p, o.node_box.p, o.parent.as< int >(),
-                                    o.exch.as< int >(), o.sc(), s ) );
+      BVHG_CUDA( ctx, launch_refit( K, fp32, n, o.bucket_box.p, o.node_box.p, o.child.as< int2 >(), o.range.as< int2 >(),
+                                    o.parent.as< int >(), o.exch.as< int >(), o.sc(), s ) );
       st.launched();
     }
     o.built = true;

@@ -342,8 +342,10 @@ uint32_t refit_blocks(uint64_t n);
 cudaError_t launch_refit_batch(int K, bool fp32, const batch_launch &b, cudaStream_t s);
 
 // Refit with the topology of the last build, after launch_slabs recomputed the bucket boxes: every internal node.
-cudaError_t launch_refit(int K, bool fp32, uint64_t n, const void *bucket_box, void *node_box, const int *parent,
-                         int *exch, obj_scalars *sc, cudaStream_t s);
+// Nodes inside one block's 128 buckets are refit in shared memory; the nodes whose ranges cross blocks by climbs with
+// the global exchange (exch must hold -1).
+cudaError_t launch_refit(int K, bool fp32, uint64_t n, const void *bucket_box, void *node_box, const int2 *child,
+                         const int2 *range, const int *parent, int *exch, obj_scalars *sc, cudaStream_t s);
 
 struct tree_view
 {

@@ -13,6 +13,7 @@
 // first arrival's slab stores are ordered before its acq_rel atomic exchange, and the second arrival, which sees
 // the slot taken with an acquire load (or learns it from its own exchange), reads them through L2 after it.
 #include "bvhg_internal.cuh"
+#include "bulk_copy.cuh"
 #include "kdop_math.cuh"
 
 namespace bvhg {
@@ -55,6 +56,17 @@ template<>
 struct box_io< double >
 {
   __device__ static void store2(double *p, double lo, double hi) { *reinterpret_cast< double2 * >( p ) = make_double2( lo, hi ); }
+  __device__ static void store4(double *p, double a, double b, double c, double d)
+  {
+    reinterpret_cast< double2 * >( p )[0] = make_double2( a, b );
+    reinterpret_cast< double2 * >( p )[1] = make_double2( c, d );
+  }
+  __device__ static void load2(const double *p, double &lo, double &hi)
+  {
+    const double2 v = *reinterpret_cast< const double2 * >( p );
+    lo = v.x;
+    hi = v.y;
+  }
   __device__ static void load2_cg(const double *p, double &lo, double &hi)
   {
     const double2 v = __ldcg( reinterpret_cast< const double2 * >( p ) );
@@ -69,6 +81,16 @@ template<>
 struct box_io< float >
 {
   __device__ static void store2(float *p, float lo, float hi) { *reinterpret_cast< float2 * >( p ) = make_float2( lo, hi ); }
+  __device__ static void store4(float *p, float a, float b, float c, float d)
+  {
+    *reinterpret_cast< float4 * >( p ) = make_float4( a, b, c, d );
+  }
+  __device__ static void load2(const float *p, float &lo, float &hi)
+  {
+    const float2 v = *reinterpret_cast< const float2 * >( p );
+    lo = v.x;
+    hi = v.y;
+  }
   __device__ static void load2_cg(const float *p, float &lo, float &hi)
   {
     const float2 v = __ldcg( reinterpret_cast< const float2 * >( p ) );
@@ -584,33 +606,16 @@ __device__ void climb_body(const tree_args &args, uint32_t bid, uint32_t nblk)
   }
 }
 
-// Refit with a fixed topology (one thread per bucket, after k_elem_slabs recomputed the element, bucket and group
-// boxes; elements keep their ranks): the first/second-arrival climb along the stored parent links. exch must
-// hold -1.
+// The climb of one subtree root whose parent node crosses the block: publishes the subtree's slabs in its parent's
+// slot and meets the sibling through the node's exchange word (the protocol of the build's climb); the second
+// arrival merges and goes on. lo/hi hold the subtree's slabs, ps its parent entry (2 * node + side).
 template< int K, typename T >
-__device__ void refit_body(const tree_args &args, uint32_t bid, uint32_t)
+__device__ __forceinline__ void refit_climb_global(T *node_box, const int *__restrict__ parent, int *exch,
+                                                   obj_scalars *__restrict__ sc, int m, int root, int ps,
+                                                   T ( &lo )[K / 2], T ( &hi )[K / 2])
 {
-  const int n = static_cast< int >( args.n );
-  const T *__restrict__ bucket_box = static_cast< const T * >( args.bucket_box );
-  T *node_box = static_cast< T * >( args.node_box );
-  const int *__restrict__ parent = args.parent;
-  int *exch = args.exch;
-  obj_scalars *__restrict__ sc = args.sc;
   constexpr int D = K / 2;
   using io = box_io< T >;
-  const int b = static_cast< int >( bid * blockDim.x + threadIdx.x );
-  const int m = ( n + kLeafSize - 1 ) / kLeafSize;
-  if ( b >= m || m == 1 ) return;  // a one-bucket object's root box came from the slab kernel
-  if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
-  T lo[D], hi[D];
-#pragma unroll
-  for ( int a = 0; a < D; ++a )
-  {
-    lo[a] = bucket_box[( static_cast< size_t >( b ) * D + a ) * 2];
-    hi[a] = bucket_box[( static_cast< size_t >( b ) * D + a ) * 2 + 1];
-  }
-  const int root = sc->root;
-  int ps = __ldg( parent + b );
   while ( true )
   {
     const int par = ps >> 1, side = ps & 1;
@@ -619,12 +624,13 @@ __device__ void refit_body(const tree_args &args, uint32_t bid, uint32_t)
     T *pb = node_box + static_cast< size_t >( par ) * D * 4;
 #pragma unroll
     for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
-    // a sibling that already arrived is seen with one acquire load (see k_build_climb)
+    // a sibling that already arrived is seen with one acquire load; its slabs are read through L2, since another
+    // SM may have written them
     int other = ld_acquire( exch + par );
     if ( other < 0 )
     {
       other = atomic_exch_acq_rel( exch + par, 1 );
-      if ( other < 0 ) return;
+      if ( other < 0 ) return;  // first arrival: the sibling's thread finishes this node
     }
 #pragma unroll
     for ( int a = 0; a < D; ++a )
@@ -641,6 +647,140 @@ __device__ void refit_body(const tree_args &args, uint32_t bid, uint32_t)
     }
     ps = next;
   }
+}
+
+// Refit: new slabs for every node of an unchanged topology. Block `bid` owns buckets [B0, B0 + blockDim.x) and the
+// window of internal nodes with the same indices. Internal node k splits its bucket range [l, r] at k (l <= k < r),
+// so every node whose range lies inside the block's buckets (a local node) is in the window. The local nodes are
+// refit in rounds over shared memory: a subtree [l, r] keeps its slabs in row l - B0 of s_tab (its first bucket's
+// row), and in each round every local node whose children are done merges their rows, writes both children's
+// slabs to its node_box row and leaves the union in its row. Barriers separate the rounds, so no exchange word,
+// atomic or fence is used inside the block. Then every local root (a bucket or local node whose parent crosses the
+// block) climbs through the crossing nodes with the global exchange.
+template< int K, typename T >
+__device__ void refit_body(const tree_args &args, uint32_t bid, uint32_t)
+{
+  const int n = static_cast< int >( args.n );
+  const T *__restrict__ bucket_box = static_cast< const T * >( args.bucket_box );
+  T *node_box = static_cast< T * >( args.node_box );
+  const int2 *__restrict__ child = args.child;
+  const int *__restrict__ parent = args.parent;
+  const int2 *__restrict__ range = args.range;
+  int *exch = args.exch;
+  obj_scalars *__restrict__ sc = args.sc;
+  constexpr int D = K / 2;
+  constexpr int C = 2 * D;
+  using io = box_io< T >;
+  static_assert( ( C * sizeof( T ) ) % 8 == 0, "rows of slab pairs" );
+  __shared__ alignas( 16 ) T s_tab[kBuildThreads * C];  // bucket rows (contiguous, as in bucket_box), then subtrees
+  __shared__ int2 s_child[kBuildThreads];
+  __shared__ int2 s_rng[kBuildThreads];
+  __shared__ int s_up[kBuildThreads];
+  __shared__ unsigned char s_done[kBuildThreads];
+  __shared__ int s_list[kBuildThreads];
+  __shared__ int s_wcnt[kBuildThreads / 32];
+  const int B0 = static_cast< int >( bid * blockDim.x );
+  const int tid = static_cast< int >( threadIdx.x );
+  const int m = ( n + kLeafSize - 1 ) / kLeafSize;
+  // a one-bucket object's root box came from the slab kernel; a failed sort leaves nothing to refit (both uniform)
+  if ( m == 1 || *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
+  const int rows = min( static_cast< int >( blockDim.x ), m - B0 );
+  const int nodes_here = min( static_cast< int >( blockDim.x ), m - 1 - B0 );  // internal nodes of the window
+  {
+    // the block's bucket rows: 16-byte asynchronous copies (the block's first row starts on a 16-byte boundary:
+    // B0 * C * sizeof(T) is a multiple of 128 * 8), the last few bytes of a ragged block by plain loads
+    const int bytes = rows * C * static_cast< int >( sizeof( T ) );
+    const unsigned char *src = reinterpret_cast< const unsigned char * >( bucket_box + static_cast< size_t >( B0 ) * C );
+    unsigned char *dst = reinterpret_cast< unsigned char * >( s_tab );
+    for ( int o = tid * 16; o + 16 <= bytes; o += blockDim.x * 16 ) cp_async16( dst + o, src + o );
+    const int tail = bytes & ~15;
+    for ( int o = tail + tid * static_cast< int >( sizeof( T ) ); o < bytes; o += blockDim.x * sizeof( T ) )
+      *reinterpret_cast< T * >( dst + o ) = *reinterpret_cast< const T * >( src + o );
+  }
+  if ( tid < nodes_here )
+  {
+    s_child[tid] = __ldg( child + B0 + tid );
+    s_rng[tid] = __ldg( range + B0 + tid );
+    s_up[tid] = __ldg( parent + m + B0 + tid );
+  }
+  const int root = sc->root;
+  int pb_entry = tid < rows ? __ldg( parent + B0 + tid ) : 0;  // this thread's bucket's parent entry
+  cp_async_wait_all();
+  __syncthreads();
+  auto is_local = [&](int node) {
+    if ( node < B0 || node - B0 >= nodes_here ) return false;
+    const int2 rg = s_rng[node - B0];
+    return rg.x >= B0 && rg.y < B0 + static_cast< int >( blockDim.x );
+  };
+  const bool mine = is_local( B0 + tid );  // this thread owns node B0 + tid, refit in the rounds
+  bool pending = mine;
+  s_done[tid] = 0;
+  // rounds: the nodes whose children are buckets or done nodes are listed, then merged by groups of D lanes (lane
+  // a: axis a of both children, so a node's node_box row is written by one coalesced store per group); barriers
+  // order one round's rows and flags before the next round's reads
+  constexpr int G = 32 / D;  // node groups per warp
+  const int lane = tid & 31, warp = tid >> 5, nwarps = static_cast< int >( blockDim.x ) >> 5;
+  while ( __syncthreads_or( pending ) )
+  {
+    bool ready = false;
+    if ( pending )
+    {
+      const int2 c = s_child[tid];
+      ready = ( c.x < 0 || s_done[c.x - B0] ) && ( c.y < 0 || s_done[c.y - B0] );
+    }
+    const unsigned bal = __ballot_sync( 0xffffffffu, ready );
+    if ( lane == 0 ) s_wcnt[warp] = __popc( bal );
+    __syncthreads();
+    int off = 0, total = 0;
+    for ( int w = 0; w < nwarps; ++w )
+    {
+      const int c = s_wcnt[w];
+      off += w < warp ? c : 0;
+      total += c;
+    }
+    if ( ready ) s_list[off + __popc( bal & ( ( 1u << lane ) - 1u ) )] = tid;
+    __syncthreads();
+    if ( lane < G * D )
+    {
+      const int a = lane % D;
+      for ( int e = warp * G + lane / D; e < total; e += nwarps * G )
+      {
+        const int q = s_list[e];
+        const int node = B0 + q;
+        T *L = s_tab + ( s_rng[q].x - B0 ) * C;  // the left child's row (its range starts at the node's)
+        const T *R = s_tab + ( node + 1 - B0 ) * C;  // the right child's row
+        T ll, lh, rlo, rhi;
+        io::load2( L + 2 * a, ll, lh );
+        io::load2( R + 2 * a, rlo, rhi );
+        io::store4( node_box + static_cast< size_t >( node ) * D * 4 + a * 4, ll, lh, rlo, rhi );
+        io::store2( L + 2 * a, io::mn( ll, rlo ), io::mx( lh, rhi ) );
+      }
+    }
+    __syncthreads();
+    if ( ready )
+    {
+      if ( B0 + tid == root )
+      {
+        const T *L = s_tab + ( s_rng[tid].x - B0 ) * C;
+        T lo[D], hi[D];
+#pragma unroll
+        for ( int a = 0; a < D; ++a ) io::load2( L + 2 * a, lo[a], hi[a] );
+        store_root( sc, lo, hi );
+      }
+      s_done[tid] = 1;
+      pending = false;
+    }
+  }
+  // local roots climb through the crossing nodes: this thread's bucket when its parent is not local, and its node
+  // when it is local and its parent is not
+  auto climb_from = [&](int ps, int row) {
+    T lo[D], hi[D];
+#pragma unroll
+    for ( int a = 0; a < D; ++a ) io::load2( s_tab + row * C + 2 * a, lo[a], hi[a] );
+    refit_climb_global< K, T >( node_box, parent, exch, sc, m, root, ps, lo, hi );
+  };
+  if ( tid < rows && !is_local( pb_entry >> 1 ) ) climb_from( pb_entry, tid );
+  if ( mine && B0 + tid != root && !is_local( s_up[tid] >> 1 ) ) climb_from( s_up[tid], s_rng[tid].x - B0 );
 }
 
 uint32_t slab_grid(uint64_t n) { return static_cast< uint32_t >( ( n + kSlabThreads - 1 ) / kSlabThreads ); }
@@ -882,11 +1022,11 @@ cudaError_t launch_climb_batch(int K, bool fp32, const batch_launch &b, cudaStre
 #undef D
 }
 
-cudaError_t launch_refit(int K, bool fp32, uint64_t n, const void *bucket_box, void *node_box, const int *parent,
-                         int *exch, obj_scalars *sc, cudaStream_t s)
+cudaError_t launch_refit(int K, bool fp32, uint64_t n, const void *bucket_box, void *node_box, const int2 *child,
+                         const int2 *range, const int *parent, int *exch, obj_scalars *sc, cudaStream_t s)
 {
-  const tree_args a{ n, nullptr, nullptr, bucket_box, node_box, nullptr, nullptr, const_cast< int * >( parent ), exch,
-                     nullptr, sc };
+  const tree_args a{ n, nullptr, nullptr, bucket_box, node_box, const_cast< int2 * >( child ), const_cast< int2 * >( range ),
+                     const_cast< int * >( parent ), exch, nullptr, sc };
 #define F( KK ) launch_refit_t< KK, float >( a, s )
 #define D( KK ) launch_refit_t< KK, double >( a, s )
   BVHG_BY_K( F, D )

@@ -330,6 +330,25 @@ def test_refit_after_motion(precision):
             assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b2, 18))
 
 
+@pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
+@pytest.mark.parametrize("k", [6, 18, 26])
+def test_refit_after_deformation_over_many_blocks(k, precision):
+    """A non-rigid motion over 25,000 buckets (196 refit blocks, the last one ragged): every node's slabs after the
+    refit are the exact unions of what they cover, whether the node lies inside one block's buckets or crosses
+    blocks, and the pair set is the oracle's for the moved vertices."""
+    a = meshes.random_soup(150000, 3, seed=103, size=0.004)
+    b = meshes.random_soup(199993, 3, seed=104, size=0.004, stream=1)
+    with bvhg.Context(k=k, precision=precision) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        for step in range(2):
+            w = 0.01 * (step + 1)
+            b2 = b + w * np.sin(7.0 * b[..., ::-1] + step)
+            ctx.set_elements(ob, b2)
+            ctx.build(ob, bvhg.REFIT)
+            ctx.validate_tree(ob)
+            assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b2, k))
+
+
 def test_stage_timing_and_launch_count():
     a = meshes.random_soup(10000, 3, seed=111, size=0.02)
     with bvhg.Context(k=18, stage_timing=True) as ctx:
