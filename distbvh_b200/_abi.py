@@ -202,15 +202,22 @@ class Context:
         return out[: cnt.value]
 
     def sort_and_sweep(self, a, b, axis=-1):
-        """Sort-and-sweep pairs (gid in a, gid in b) as an (m, 2) uint64 array, and the axis swept."""
+        """Sort-and-sweep pairs (gid in a, gid in b) as an (m, 2) uint64 array, and the axis swept. The sweep runs
+        once into a buffer sized by the last call's count (at least 65,536 pairs); only a larger result runs it
+        again, into a buffer of the exact size."""
         cnt = ctypes.c_uint64()
         used = ctypes.c_int32()
-        st = lib.bvhg_sort_and_sweep(self._h, a, b, axis, None, 0, ctypes.byref(cnt), ctypes.byref(used), MEM_HOST)
-        if st not in (OK, ERR_OVERFLOW):
-            self._check(st)
-        out = np.empty((max(cnt.value, 1), 2), dtype=np.uint64)
-        self._check(lib.bvhg_sort_and_sweep(self._h, a, b, axis, out.ctypes.data, cnt.value, ctypes.byref(cnt),
-                                            ctypes.byref(used), MEM_HOST))
+        cap = max(65536, getattr(self, "_sweep_cap", 0))
+        out = np.empty((cap, 2), dtype=np.uint64)
+        st = lib.bvhg_sort_and_sweep(self._h, a, b, axis, out.ctypes.data, cap, ctypes.byref(cnt), ctypes.byref(used),
+                                     MEM_HOST)
+        if st == ERR_OVERFLOW:
+            cap = cnt.value
+            out = np.empty((cap, 2), dtype=np.uint64)
+            st = lib.bvhg_sort_and_sweep(self._h, a, b, axis, out.ctypes.data, cap, ctypes.byref(cnt),
+                                         ctypes.byref(used), MEM_HOST)
+        self._check(st)
+        self._sweep_cap = max(cap, cnt.value)
         return out[: cnt.value], used.value
 
     def sort_and_sweep_raw(self, a, b, axis, out_ptr, capacity, mem):

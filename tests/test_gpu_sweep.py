@@ -92,6 +92,22 @@ def test_precision_form_gives_the_same_set():
         assert np.array_equal(orc.canonical(got), want)
 
 
+def test_python_call_grows_its_buffer_once():
+    """More pairs than the binding's first buffer (65,536): the sweep runs again into a buffer of the reported size;
+    the next call starts with that size and runs once."""
+    m = 40
+    xyz = meshes.tet_lattice(m)
+    even = meshes.checkerboard(m)
+    a, b = np.ascontiguousarray(xyz[even]), np.ascontiguousarray(xyz[~even])
+    want = orc.pair_set(a, b, 18)
+    assert want.shape[0] > 65536
+    with bvhg.Context(k=18) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        for _ in range(2):
+            got, _ = ctx.sort_and_sweep(oa, ob, -1)
+            assert np.array_equal(orc.canonical(got), want)
+
+
 def test_device_output_overflow_and_errors():
     torch = pytest.importorskip("torch")
     a = meshes.random_soup(3000, 3, seed=1201, size=0.03)
