@@ -1472,6 +1472,20 @@ bvhg_status bvhg_broadphase(bvhg_ctx *ctx, int32_t obj_a, int32_t obj_b, uint64_
   return emit_pairs( ctx, a, b, false, lp, np, pairs, capacity, count, mem );
 }
 
+namespace {
+// True when p is device memory of any GPU (managed memory counts as host here: the host may access it).
+bool is_device_pointer(const void *p)
+{
+  cudaPointerAttributes at{};
+  if ( cudaPointerGetAttributes( &at, p ) != cudaSuccess )
+  {
+    cudaGetLastError();  // not a pointer CUDA knows: host memory (the error is not sticky; clear it)
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice;
+}
+}  // namespace
+
 bvhg_status bvhg_batch_broadphase(bvhg_ctx *ctx, uint32_t nscenes, const int32_t *obj_a, const int32_t *obj_b,
                                   int32_t mode, uint64_t *pairs, uint64_t capacity, uint64_t *counts,
                                   uint64_t *offsets, int32_t mem)
@@ -1483,6 +1497,10 @@ bvhg_status bvhg_batch_broadphase(bvhg_ctx *ctx, uint32_t nscenes, const int32_t
   if ( capacity > 0 && !pairs ) return fail( ctx, BVHG_ERR_ARG, "null pair buffer" );
   if ( nscenes == 0 ) return BVHG_OK;
   cudaSetDevice( ctx->cfg.device );
+  // the scene arrays, counts and offsets are host memory: a device pointer is refused, not dereferenced
+  for ( const void *h : { static_cast< const void * >( obj_a ), static_cast< const void * >( obj_b ),
+                          static_cast< const void * >( counts ), static_cast< const void * >( offsets ) } )
+    if ( h && is_device_pointer( h ) ) return fail( ctx, BVHG_ERR_ARG, "scene arrays, counts and offsets must be host memory" );
   const batch_args x{ nscenes, obj_a, obj_b, mode };
   bvhg_status st = run_batch( ctx, x, counts );
   if ( st != BVHG_OK ) return st;

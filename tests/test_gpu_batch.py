@@ -95,3 +95,28 @@ def test_batch_autotune_picks_a_configuration():
         got = ctx.batch_broadphase(objs)
         for s, (a, b) in enumerate(bodies):
             assert np.array_equal(orc.canonical(got[s]), orc.pair_set(a, b, 18))
+
+
+def test_batch_refuses_device_memory_for_host_arrays():
+    """Scene arrays, counts and offsets are host memory: a device pointer among them is an argument error (the call
+    must not write through it), and the context stays usable."""
+    a = meshes.random_soup(2000, 3, seed=71, size=0.04)
+    b = meshes.random_soup(1500, 3, seed=72, size=0.04, stream=1)
+    with bvhg.Context(k=18) as ctx:
+        oa, ob = ctx.object(), ctx.object()
+        ctx.set_elements(oa, a)
+        ctx.set_elements(ob, b)
+        ia = np.array([oa], dtype=np.int32)
+        ib = np.array([ob], dtype=np.int32)
+        out = torch.empty((1 << 16, 2), dtype=torch.int64, device="cuda")
+        d_counts = torch.zeros(1, dtype=torch.int64, device="cuda")
+        st = ctx.batch_broadphase_raw(ia.ctypes.data, ib.ctypes.data, 1, bvhg.REBUILD, out.data_ptr(), out.shape[0],
+                                      d_counts.data_ptr(), bvhg.MEM_DEVICE)
+        assert st == bvhg._abi.ERR_ARG
+        d_ia = torch.from_numpy(ia).cuda()
+        counts = np.zeros(1, dtype=np.uint64)
+        st = ctx.batch_broadphase_raw(d_ia.data_ptr(), ib.ctypes.data, 1, bvhg.REBUILD, out.data_ptr(), out.shape[0],
+                                      counts.ctypes.data, bvhg.MEM_DEVICE)
+        assert st == bvhg._abi.ERR_ARG
+        got = ctx.batch_broadphase([(oa, ob)])
+        assert np.array_equal(orc.canonical(got[0]), orc.pair_set(a, b, 18))
