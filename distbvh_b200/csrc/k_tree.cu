@@ -553,55 +553,79 @@ __device__ void climb_body(const tree_args &args, uint32_t bid, uint32_t nblk)
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout ) return;
   const int m = ( n + kLeafSize - 1 ) / kLeafSize;
   const unsigned count = *reinterpret_cast< volatile unsigned * >( &sc->climb_count );
+  // A first arrival publishes the end of its range the sibling needs (its first bucket as a left child, its last as
+  // a right one) together with that end's boundary dissimilarity, packed as (end << 7 | byte) while bucket indices
+  // fit 24 bits: the second arrival then chooses the next parent without loading bdel.
+  const bool packed = m < ( 1 << 24 );
   for ( unsigned q = bid * blockDim.x + threadIdx.x; q < count; q += nblk * blockDim.x )
   {
     const int4 w = queue[q];
     int par = w.x >> 1, side = w.x & 1, l = w.y, r = w.z;
     T lo[D], hi[D];
-    T *pb = node_box + static_cast< size_t >( par ) * D * 4;
+    {
+      const T *pb = node_box + static_cast< size_t >( par ) * D * 4;
 #pragma unroll
-    for ( int a = 0; a < D; ++a ) io::load2_cg( pb + a * 4 + side * 2, lo[a], hi[a] );
+      for ( int a = 0; a < D; ++a ) io::load2_cg( pb + a * 4 + side * 2, lo[a], hi[a] );
+    }
+    int dl = l > 0 ? __ldg( bdel + l - 1 ) : 0;      // dissimilarity across the range's left boundary
+    int dr = r < m - 1 ? __ldg( bdel + r ) : 0;      // and across its right boundary
+    // A sibling that already arrived is seen with one acquire load (its slab stores were released by its
+    // exchange); only when the slot looks empty does this thread publish through the exchange itself, whose
+    // release also covers its own slab stores. The next level's acquire load is issued before the sibling's slabs
+    // are merged, so the two round trips of a level overlap.
+    int other = ld_acquire( exch + par );
     while ( true )
     {
-      // A sibling that already arrived is seen with one acquire load (its slab stores were released by its
-      // exchange); only when the slot looks empty does this thread publish through the exchange itself, whose
-      // release also covers its own slab stores. A late second arrival thus waits for no store of its own.
-      int other = ld_acquire( exch + par );
       if ( other < 0 )
       {
-        other = atomic_exch_acq_rel( exch + par, side == 0 ? l : r );
+        const int end = side == 0 ? l : r, dend = side == 0 ? dl : dr;
+        other = atomic_exch_acq_rel( exch + par, packed ? ( end << 7 ) | dend : end );
         if ( other < 0 ) break;  // first arrival: the sibling's thread finishes this node
       }
-      if ( side == 0 ) r = other;
-      else l = other;
-#pragma unroll
-      for ( int a = 0; a < D; ++a )
+      const int oend = packed ? other >> 7 : other;
+      if ( side == 0 )
       {
-        T sl, sh;
-        io::load2_cg( pb + a * 4 + ( 1 - side ) * 2, sl, sh );
-        lo[a] = io::mn( lo[a], sl );
-        hi[a] = io::mx( hi[a], sh );
+        r = oend;
+        dr = packed ? ( other & 127 ) : ( r < m - 1 ? __ldg( bdel + r ) : 0 );
+      } else {
+        l = oend;
+        dl = packed ? ( other & 127 ) : ( l > 0 ? __ldg( bdel + l - 1 ) : 0 );
       }
+      const T *pb = node_box + static_cast< size_t >( par ) * D * 4 + ( 1 - side ) * 2;
+      T sl[D], sh[D];
+#pragma unroll
+      for ( int a = 0; a < D; ++a ) io::load2_cg( pb + a * 4, sl[a], sh[a] );
       range[par] = make_int2( l, r );
       if ( l == 0 && r == m - 1 )
       {
+#pragma unroll
+        for ( int a = 0; a < D; ++a )
+        {
+          lo[a] = io::mn( lo[a], sl[a] );
+          hi[a] = io::mx( hi[a], sh[a] );
+        }
         sc->root = par;
         store_root( sc, lo, hi );
         break;
       }
       const int node = par;
-      const int self_slot = m + par;
-      bool left_child;
-      if ( l == 0 ) left_child = true;
-      else if ( r == m - 1 ) left_child = false;
-      else left_child = cdelta( bdel, r ) < cdelta( bdel, l - 1 );
+      // cdelta(r) against cdelta(l - 1): (byte << 32 | boundary index)
+      const bool left_child = l == 0 || ( r != m - 1 && ( ( static_cast< long long >( dr ) << 32 ) | r ) <
+                                                            ( ( static_cast< long long >( dl ) << 32 ) | ( l - 1 ) ) );
       par = left_child ? r : l - 1;
       side = left_child ? 0 : 1;
-      pb = node_box + static_cast< size_t >( par ) * D * 4;
+      other = ld_acquire( exch + par );
 #pragma unroll
-      for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, lo[a], hi[a] );
+      for ( int a = 0; a < D; ++a )
+      {
+        lo[a] = io::mn( lo[a], sl[a] );
+        hi[a] = io::mx( hi[a], sh[a] );
+      }
+      T *qb = node_box + static_cast< size_t >( par ) * D * 4 + side * 2;
+#pragma unroll
+      for ( int a = 0; a < D; ++a ) io::store2( qb + a * 4, lo[a], hi[a] );
       child[2 * par + side] = node;
-      parent[self_slot] = 2 * par + side;
+      parent[m + node] = 2 * par + side;
     }
   }
 }
@@ -875,14 +899,14 @@ uint32_t climb_grid(uint64_t n)
 template< int K, typename T >
 cudaError_t launch_climb_t(const tree_args &a, cudaStream_t s)
 {
-  k_single< tree_args, climb_body< K, T >, 128, 7 ><<< climb_grid( a.n ), 128, 0, s >>>( a );
+  k_single< tree_args, climb_body< K, T >, 128, 4 ><<< climb_grid( a.n ), 128, 0, s >>>( a );
   return cudaGetLastError();
 }
 
 template< int K, typename T >
 cudaError_t launch_climb_batch_t(const batch_launch &b, cudaStream_t s)
 {
-  k_batched< tree_args, climb_body< K, T >, 128, 7 ><<< b.blocks, 128, 0, s >>>( static_cast< const tree_args * >( b.items ),
+  k_batched< tree_args, climb_body< K, T >, 128, 4 ><<< b.blocks, 128, 0, s >>>( static_cast< const tree_args * >( b.items ),
                                                                                b.starts, b.nitems );
   return cudaGetLastError();
 }
