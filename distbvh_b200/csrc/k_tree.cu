@@ -635,6 +635,64 @@ __device__ void climb_body(const tree_args &args, uint32_t bid, uint32_t nblk)
 // arrival merges and goes on. lo/hi hold the subtree's slabs, ps its parent entry (2 * node + side).
 template< int K, typename T >
 __device__ __forceinline__ void refit_climb_global(T *node_box, const int *__restrict__ parent, int *exch,
+                                                   obj_scalars *__restrict__ sc, int m, int root, int ps, T *row)
+{
+  constexpr int D = K / 2;
+  using io = box_io< T >;
+  int par = ps >> 1, side = ps & 1;
+  // FP64 form. The subtree's slabs stay in its shared-memory row (registers hold only the sibling's slabs in
+  // flight). The next level's parent link and this level's exchange word are read ahead: the acquire load of a level
+  // is issued before the previous level's sibling slabs are merged, so the two round trips overlap.
+  int nxt = par == root ? 0 : __ldg( parent + m + par );
+  int other = ld_acquire( exch + par );
+  while ( true )
+  {
+    T *pb = node_box + static_cast< size_t >( par ) * D * 4;
+#pragma unroll
+    for ( int a = 0; a < D; ++a ) io::store2( pb + a * 4 + side * 2, row[2 * a], row[2 * a + 1] );
+    if ( other < 0 )
+    {
+      // the exchange's release covers the slab stores above
+      other = atomic_exch_acq_rel( exch + par, 1 );
+      if ( other < 0 ) return;  // first arrival: the sibling's thread finishes this node
+    }
+    // the sibling's slabs are read through L2, since another SM may have written them
+    T sl[D], sh[D];
+#pragma unroll
+    for ( int a = 0; a < D; ++a ) io::load2_cg( pb + a * 4 + ( 1 - side ) * 2, sl[a], sh[a] );
+    const bool at_root = par == root;
+    if ( !at_root )
+    {
+      par = nxt >> 1;
+      side = nxt & 1;
+      nxt = par == root ? 0 : __ldg( parent + m + par );
+      other = ld_acquire( exch + par );
+    }
+#pragma unroll
+    for ( int a = 0; a < D; ++a )
+    {
+      row[2 * a] = io::mn( row[2 * a], sl[a] );
+      row[2 * a + 1] = io::mx( row[2 * a + 1], sh[a] );
+    }
+    if ( at_root )
+    {
+      T lo[D], hi[D];
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
+      {
+        lo[a] = row[2 * a];
+        hi[a] = row[2 * a + 1];
+      }
+      store_root( sc, lo, hi );
+      return;
+    }
+  }
+}
+
+// The same climb with the subtree's slabs in registers and no read-ahead of the exchange word (the FP32 form: there
+// the read-ahead measured slower).
+template< int K, typename T >
+__device__ __forceinline__ void refit_climb_global_regs(T *node_box, const int *__restrict__ parent, int *exch,
                                                    obj_scalars *__restrict__ sc, int m, int root, int ps,
                                                    T ( &lo )[K / 2], T ( &hi )[K / 2])
 {
@@ -797,11 +855,17 @@ __device__ void refit_body(const tree_args &args, uint32_t bid, uint32_t)
   }
   // local roots climb through the crossing nodes: this thread's bucket when its parent is not local, and its node
   // when it is local and its parent is not
+  // (each local root's row belongs to its climbing thread alone)
   auto climb_from = [&](int ps, int row) {
-    T lo[D], hi[D];
+    if constexpr ( sizeof( T ) == 8 )
+    {
+      refit_climb_global< K, T >( node_box, parent, exch, sc, m, root, ps, s_tab + row * C );
+    } else {
+      T lo[D], hi[D];
 #pragma unroll
-    for ( int a = 0; a < D; ++a ) io::load2( s_tab + row * C + 2 * a, lo[a], hi[a] );
-    refit_climb_global< K, T >( node_box, parent, exch, sc, m, root, ps, lo, hi );
+      for ( int a = 0; a < D; ++a ) io::load2( s_tab + row * C + 2 * a, lo[a], hi[a] );
+      refit_climb_global_regs< K, T >( node_box, parent, exch, sc, m, root, ps, lo, hi );
+    }
   };
   if ( tid < rows && !is_local( pb_entry >> 1 ) ) climb_from( pb_entry, tid );
   if ( mine && B0 + tid != root && !is_local( s_up[tid] >> 1 ) ) climb_from( s_up[tid], s_rng[tid].x - B0 );
