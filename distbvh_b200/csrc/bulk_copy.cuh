@@ -18,7 +18,15 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
   asm volatile( "cp.async.ca.shared.global [%0], [%1], 16;" ::"r"( smem_addr( dst ) ), "l"( src ) : "memory" );
 }
 
-// Waits for all of this thread's cp_async16 copies (a __syncwarp / __syncthreads then publishes them to the others).
+// 4 or 8 bytes global -> shared without a register round trip; both addresses aligned to the size.
+template< int BYTES >
+__device__ __forceinline__ void cp_async_small(void *dst, const void *src)
+{
+  static_assert( BYTES == 4 || BYTES == 8, "cp.async.ca copies 4, 8 or 16 bytes" );
+  asm volatile( "cp.async.ca.shared.global [%0], [%1], %2;" ::"r"( smem_addr( dst ) ), "l"( src ), "n"( BYTES ) : "memory" );
+}
+
+// Waits for all of this thread's cp_async16 / cp_async_small copies (a __syncwarp / __syncthreads then publishes them to the others).
 __device__ __forceinline__ void cp_async_wait_all()
 {
   asm volatile( "cp.async.wait_all;" ::: "memory" );

@@ -318,14 +318,15 @@ __device__ void build_leaf_body(const tree_args &args, uint32_t bid, uint32_t)
   if ( *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout || m == 1 ) return;  // uniform
   bool active = b < m;
 
-  // a. the block's bucket boxes into the table (coalesced rows)
+  // a. the block's bucket boxes into the table (coalesced rows), by asynchronous copies: every copy of the thread is
+  // in flight at once, and it waits for them before the barrier below
   {
     const int rows = min( kBuildThreads, m - bbase );
     const T *src = bucket_box + static_cast< size_t >( bbase ) * C;
     for ( int k = tid; k < rows * C; k += kBuildThreads )
     {
       const int row = k / C;
-      box( row, k - row * C ) = src[k];
+      cp_async_small< sizeof( T ) >( &box( row, k - row * C ), src + k );
     }
   }
   const long long dself = ( b + 1 < m ) ? bdelta( keys, b ) : 0ll;
@@ -345,6 +346,7 @@ __device__ void build_leaf_body(const tree_args &args, uint32_t bid, uint32_t)
     s_root_ref = -1;
     s_delta[0] = ( bbase >= 1 && bbase < m ) ? bdelta( keys, bbase - 1 ) : 0ll;
   }
+  cp_async_wait_all();
   __syncthreads();  // the returns above are uniform over the grid
 
   int l = b, r = b;
