@@ -85,7 +85,7 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned k, unsigned 
 }
 
 // Slabs of element e straight into a shared-memory row (C = 2 D values: min, max per slab), slab by slab so that
-// only the vertices stay in registers: the same FP64 slabs, or the same FP32 enclosures, that k_elem_slabs unites
+// only the vertices stay in registers: the same FP64 slabs, or the same FP32 enclosures, that slabs_body unites
 // into the bucket boxes.
 template< int K, typename T, int VT >
 __device__ __forceinline__ void slabs_to_row(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
@@ -126,7 +126,7 @@ __device__ __forceinline__ void slabs_to_row(const double *__restrict__ verts, u
   }
 }
 
-// Everything one query packet needs besides the tree (see k_traverse).
+// Everything one query packet needs besides the tree (see traverse_body).
 template< typename T >
 struct trav_args
 {
@@ -223,7 +223,7 @@ __device__ __forceinline__ void test_bucket(const trav_args< T > &x, const T *ql
   __syncwarp();  // the cache is refilled by the next leaf
 }
 
-// One packet: the union box of ranks pk*32 .. pk*32 + 31 against the target root, then the walk (see k_traverse).
+// One packet: the union box of ranks pk*32 .. pk*32 + 31 against the target root, then the walk (see traverse_body).
 template< int K, typename T, int VT >
 __device__ __forceinline__ void traverse_packet(const trav_args< T > &x, const uint32_t i, const unsigned lane,
                                                 int2 *stack, T *cache, const T *rb)

@@ -255,7 +255,7 @@ __device__ void slabs_body(const slabs_args &args, uint32_t bid, uint32_t)
 
 // Phase 1 (one thread per leaf bucket b, blocks of 128 consecutive buckets).
 //
-// a. The block loads its 128 bucket boxes (k_elem_slabs wrote them) into a shared box table, one row per bucket
+// a. The block loads its 128 bucket boxes (slabs_body wrote them) into a shared box table, one row per bucket
 //    (C = 2 D components, padded to C + 1 against bank conflicts). A subtree's box lives in the row of its first
 //    bucket: merging two subtrees writes the parent's node_box row (both children's slabs, with the lanes of a
 //    warp acting as slab components) straight to global memory and leaves the union in the left child's row.
