@@ -69,6 +69,8 @@ def parse():
     p.add_argument("--lattice", type=int, default=256, help="tet_lattice cells per axis (256 = 16,777,216 tets)")
     p.add_argument("--kdop", type=int, default=26, choices=[6, 18, 26], help="tet_lattice k-DOP (26 = the precision case)")
     p.add_argument("--no-oracle", action="store_true", help="skip the full-size oracle pair-set check")
+    p.add_argument("--batch-form", default=None, metavar="GROUPS,LANES",
+                   help="batch: run this form (groups 0 = per-object launches) instead of the autotuner's choice")
     return p.parse_args()
 
 
@@ -503,7 +505,12 @@ def run_batch_form(args, world, rank, local):
         ctx.set_elements(ob, db, mem=bvhg.MEM_DEVICE)
         tensors += [da, db]
         objs.append((oa, ob))
-    groups, lanes, tune_ms = ctx.batch_autotune(objs)
+    if args.batch_form:
+        groups, lanes = (int(v) for v in args.batch_form.split(","))
+        ctx.test_batch_form(groups, lanes)
+        tune_ms = None
+    else:
+        groups, lanes, tune_ms = ctx.batch_autotune(objs)
     ia = np.ascontiguousarray([o[0] for o in objs], dtype=np.int32)
     ib = np.ascontiguousarray([o[1] for o in objs], dtype=np.int32)
     counts = np.zeros(len(objs), dtype=np.uint64)
