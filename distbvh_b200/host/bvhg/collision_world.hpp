@@ -33,6 +33,8 @@
 #include "../../../include/bvhg.h"
 
 #include <algorithm>
+#include <array>
+#include <cfloat>
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -92,12 +94,106 @@ private:
 
 class collision_object;
 
-// Patch metadata (src/bvh/patch.hpp:55-123, without its k-DOP and centroid).
+// Patch metadata handed to the narrowphase functor (the id and size of src/bvh/patch.hpp:55-123).
 struct patch_meta
 {
   std::size_t gid;
   std::size_t size;
   std::size_t global_id() const { return gid; }
+};
+
+// A patch of an object (src/bvh/patch.hpp:55-123): its global id, element count, k-DOP (the union of its elements'
+// slabs: kdop()[2 a] the minimum and kdop()[2 a + 1] the maximum of slab a) and centroid (the mean of its
+// elements' centroids, summed in the patch's element order as std::accumulate does there). An empty patch has the
+// default k-DOP of the reference (every slab [DBL_MAX, lowest]) and centroid (0, 0, 0).
+class patch
+{
+public:
+  patch() = default;
+  patch(std::size_t id, std::size_t size, std::vector< double > kdop, std::array< double, 3 > centroid)
+      : m_global_id( id ), m_size( size ), m_kdop( std::move( kdop ) ), m_centroid( centroid )
+  {}
+  std::size_t global_id() const noexcept { return m_global_id; }
+  const std::vector< double > &kdop() const noexcept { return m_kdop; }
+  const std::array< double, 3 > &centroid() const noexcept { return m_centroid; }
+  bool empty() const noexcept { return m_size == 0; }
+  std::size_t size() const noexcept { return m_size; }
+
+private:
+  std::size_t m_global_id = static_cast< std::size_t >( -1 );
+  std::size_t m_size = 0;
+  std::vector< double > m_kdop;
+  std::array< double, 3 > m_centroid{};
+};
+
+// The tree over an object's non-empty patches that for_each_tree hands out (the snapshot_tree of
+// src/bvh/collision_object.hpp:59, built top-down as src/bvh/bvh_build.hpp:55-139 builds it: split at the mean
+// centroid along the longest cardinal axis of the node's k-DOP, halves when one side would be empty). nodes()[0] is
+// the root; a leaf holds one patch (index into patches()); count() is the number of leaves.
+class snapshot_tree
+{
+public:
+  struct node
+  {
+    std::vector< double > kdop;  // union of the patches below, as patch::kdop()
+    int child[2] = { -1, -1 };   // node indices, -1 at a leaf
+    std::size_t patch = 0;       // a leaf's index into patches()
+    bool leaf() const noexcept { return child[0] < 0; }
+  };
+  std::size_t count() const noexcept { return m_patches.size(); }
+  bool empty() const noexcept { return m_nodes.empty(); }
+  const node *root() const noexcept { return m_nodes.empty() ? nullptr : &m_nodes[0]; }
+  const std::vector< node > &nodes() const noexcept { return m_nodes; }
+  const std::vector< patch > &patches() const noexcept { return m_patches; }
+
+  explicit snapshot_tree(std::vector< patch > non_empty, int k) : m_patches( std::move( non_empty ) )
+  {
+    if ( m_patches.empty() ) return;
+    std::vector< std::size_t > idx( m_patches.size() );
+    for ( std::size_t i = 0; i < idx.size(); ++i ) idx[i] = i;
+    m_nodes.reserve( 2 * idx.size() );
+    build( idx, 0, idx.size(), k );
+  }
+
+private:
+  // node over idx[lo, hi); returns its index
+  int build(std::vector< std::size_t > &idx, std::size_t lo, std::size_t hi, int k)
+  {
+    const int me = static_cast< int >( m_nodes.size() );
+    m_nodes.emplace_back();
+    std::vector< double > box( m_patches[idx[lo]].kdop() );
+    for ( std::size_t i = lo + 1; i < hi; ++i )
+      for ( int a = 0; a < k / 2; ++a )
+      {
+        box[2 * a] = std::min( box[2 * a], m_patches[idx[i]].kdop()[2 * a] );
+        box[2 * a + 1] = std::max( box[2 * a + 1], m_patches[idx[i]].kdop()[2 * a + 1] );
+      }
+    m_nodes[me].kdop = box;
+    if ( hi - lo == 1 )
+    {
+      m_nodes[me].patch = idx[lo];
+      return me;
+    }
+    // the first three slabs are the cardinal axes in every k-DOP of the library
+    int axis = 0;
+    for ( int a = 1; a < 3; ++a )
+      if ( box[2 * a + 1] - box[2 * a] > box[2 * axis + 1] - box[2 * axis] ) axis = a;
+    double mean = 0.0;
+    for ( std::size_t i = lo; i < hi; ++i ) mean += m_patches[idx[i]].centroid()[axis];
+    mean /= static_cast< double >( hi - lo );
+    auto mid = std::partition( idx.begin() + static_cast< std::ptrdiff_t >( lo ), idx.begin() + static_cast< std::ptrdiff_t >( hi ),
+                               [&](std::size_t i) { return m_patches[i].centroid()[axis] < mean; } );
+    std::size_t m = static_cast< std::size_t >( mid - idx.begin() );
+    if ( m == lo || m == hi ) m = lo + ( hi - lo ) / 2;
+    const int l = build( idx, lo, m, k );
+    const int r = build( idx, m, hi, k );
+    m_nodes[me].child[0] = l;
+    m_nodes[me].child[1] = r;
+    return me;
+  }
+
+  std::vector< patch > m_patches;
+  std::vector< node > m_nodes;
 };
 
 // src/bvh/collision_query.hpp:50-64, plus the exact element pairs of the patch pair.
@@ -272,6 +368,22 @@ public:
   // The exact element pairs (global ids) of the last broadphase with `other`.
   const std::vector< std::pair< uint64_t, uint64_t > > &last_pairs() const { return m_last_pairs; }
 
+  // collision_object::local_patches (src/bvh/collision_object.hpp:189): this object's od_factor patches (after
+  // init_broadphase), global ids id() * od_factor + p.
+  const std::vector< patch > &local_patches() const noexcept { return m_patches; }
+
+  // collision_object::for_each_tree (src/bvh/collision_object.hpp:164-168): f(const snapshot_tree &) with the tree
+  // over this object's non-empty patches (one rank: the reference's tree spans every rank's patches).
+  template< typename F >
+  void for_each_tree(F &&f) const
+  {
+    std::vector< patch > non_empty;
+    for ( const auto &p : m_patches )
+      if ( !p.empty() ) non_empty.push_back( p );
+    const snapshot_tree tree( std::move( non_empty ), world_k() );
+    f( tree );
+  }
+
   // Global ids of each patch's elements, in the patch order (after init_broadphase).
   std::vector< std::vector< uint64_t > > patch_global_ids() const
   {
@@ -310,6 +422,8 @@ private:
   std::vector< std::size_t > m_pbeg;   // patch p = positions [m_pbeg[p], m_pbeg[p + 1])
   std::vector< narrowphase_result > m_results;
   std::vector< std::pair< uint64_t, uint64_t > > m_last_pairs;
+  std::vector< patch > m_patches;      // local_patches()
+  int world_k() const;
 };
 
 class collision_world
@@ -398,6 +512,7 @@ inline collision_object::collision_object(collision_world &w, std::size_t id) : 
 inline bvhg_ctx *collision_object::ctx() const { return m_world.ctx(); }
 inline int collision_object::overdecomposition_factor() const noexcept { return static_cast< int >( m_world.m_od ); }
 inline std::size_t collision_object::num_patches() const noexcept { return m_world.m_od; }
+inline int collision_object::world_k() const { return m_world.m_cfg.k; }
 
 inline void collision_object::init_broadphase()
 {
@@ -416,6 +531,34 @@ inline void collision_object::init_broadphase()
   for ( std::size_t r = 0; r < m_n; ++r )
     std::memcpy( m_elems.bytes.data() + r * m_elems.elem_size, m_src.data() + order[r] * m_elems.elem_size,
                  m_elems.elem_size );
+  // the patches' k-DOPs from the device (bvhg_patch_kdops), their centroids from the elements' (the library's
+  // centroids are the reference's bit for bit), summed in patch order
+  const int D = m_world.m_cfg.k / 2;
+  std::vector< double > boxes( P * D * 2 );
+  detail::check( ctx(), bvhg_patch_kdops( ctx(), m_obj, boxes.data(), BVHG_MEM_HOST ), "init_broadphase" );
+  std::vector< double > cent( 3 * std::max< std::size_t >( m_n, 1 ) );
+  if ( m_n ) detail::check( ctx(), bvhg_get_centroids( ctx(), m_obj, cent.data() ), "init_broadphase" );
+  m_patches.clear();
+  for ( std::size_t p = 0; p < P; ++p )
+  {
+    const std::size_t size = m_pbeg[p + 1] - m_pbeg[p];
+    std::vector< double > box( boxes.begin() + static_cast< std::ptrdiff_t >( p * D * 2 ),
+                               boxes.begin() + static_cast< std::ptrdiff_t >( ( p + 1 ) * D * 2 ) );
+    std::array< double, 3 > c{ 0.0, 0.0, 0.0 };
+    if ( size == 0 )
+    {
+      for ( int a = 0; a < D; ++a )
+      {
+        box[2 * a] = DBL_MAX;
+        box[2 * a + 1] = -DBL_MAX;
+      }
+    } else {
+      for ( std::size_t r = m_pbeg[p]; r < m_pbeg[p + 1]; ++r )
+        for ( int a = 0; a < 3; ++a ) c[a] += cent[3 * order[r] + a];
+      for ( int a = 0; a < 3; ++a ) c[a] /= static_cast< double >( size );
+    }
+    m_patches.emplace_back( m_id * P + p, size, std::move( box ), c );
+  }
   m_built = true;
 }
 

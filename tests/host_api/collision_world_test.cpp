@@ -7,7 +7,9 @@
 
 #include <algorithm>
 #include <array>
+#include <cfloat>
 #include <cstdio>
+#include <string>
 #include <vector>
 
 namespace
@@ -45,8 +47,30 @@ std::vector< tri_element > read_elements(const char *path, std::size_t gid_base)
 }
 }  // namespace
 
+// "empty <od>": an object without elements (the reference's set_empty_data section,
+// tests/collision_object_test.cpp:207-240): od empty patches with the default k-DOP, an empty tree.
+int empty_object(std::size_t od)
+{
+  bvhg::collision_world world( od );
+  auto &obj = world.create_collision_object();
+  obj.set_entity_data( std::vector< tri_element >{}, bvhg::split_algorithm::clustering );
+  obj.init_broadphase();
+  if ( obj.local_patches().size() != od ) return 4;
+  for ( const auto &p : obj.local_patches() )
+  {
+    if ( !p.empty() || p.size() != 0 ) return 5;
+    for ( std::size_t a = 0; a < p.kdop().size(); a += 2 )
+      if ( p.kdop()[a] != DBL_MAX || p.kdop()[a + 1] != -DBL_MAX ) return 6;
+  }
+  std::size_t count = 1;
+  obj.for_each_tree( [&](const bvhg::snapshot_tree &t) { count = t.count() + ( t.empty() ? 0 : 1 ); } );
+  std::printf( "empty %zu\n", count );
+  return count == 0 ? 0 : 7;
+}
+
 int main(int argc, char **argv)
 {
+  if ( argc == 3 && std::string( argv[1] ) == "empty" ) return empty_object( static_cast< std::size_t >( std::atoi( argv[2] ) ) );
   if ( argc < 5 ) return 2;
   const std::size_t od = static_cast< std::size_t >( std::atoi( argv[3] ) );
   bvhg::world_config cfg;
@@ -90,5 +114,19 @@ int main(int argc, char **argv)
   if ( got.size() != obj.last_pairs().size() ) return 3;
   std::printf( "pairs %zu calls %zu\n", got.size(), calls );
   for ( const auto &p : got ) std::printf( "%zu %zu\n", p.first, p.second );
+  // the first object's patches (local_patches) and the tree over them (for_each_tree), as in the reference's
+  // collision_object init test (tests/collision_object_test.cpp:136-170): exact values in hexadecimal floats
+  for ( const auto &p : obj.local_patches() )
+  {
+    std::printf( "patch %zu %zu", p.global_id(), p.size() );
+    for ( double v : p.kdop() ) std::printf( " %a", v );
+    for ( double v : p.centroid() ) std::printf( " %a", v );
+    std::printf( "\n" );
+  }
+  obj.for_each_tree( [](const bvhg::snapshot_tree &t) {
+    std::size_t leaves = 0;
+    for ( const auto &n : t.nodes() ) leaves += n.leaf() ? 1 : 0;
+    std::printf( "tree %zu %zu %zu\n", t.count(), t.nodes().size(), leaves );
+  } );
   return 0;
 }

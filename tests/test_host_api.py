@@ -49,9 +49,48 @@ def test_host_api_pairs_match_the_oracle(tmp_path, od, k):
                          capture_output=True, text=True).stdout.split("\n")
     head = out[0].split()
     count, calls = int(head[1]), int(head[3])
-    got = np.array([[int(x) for x in line.split()] for line in out[1:] if line.strip()], dtype=np.int64).reshape(-1, 2)
+    body = [line for line in out[1:] if line.strip()]
+    got = np.array([[int(x) for x in line.split()] for line in body if line[0].isdigit()],
+                   dtype=np.int64).reshape(-1, 2)
     want = orc.pair_set(a, b, k).astype(np.int64)
     want[:, 1] += 1000000
     assert count == want.shape[0] > 0
     assert 1 <= calls <= od * od
     assert np.array_equal(got, want[np.lexsort((want[:, 1], want[:, 0]))])
+    # local_patches: the oracle's Morton clustering, the union of its element slabs per patch, and the mean of its
+    # element centroids summed in patch order; for_each_tree: one leaf per non-empty patch
+    patches = [line.split()[1:] for line in body if line.startswith("patch")]
+    order, bounds = orc.morton_cluster(a, k, od)
+    slabs, cent = orc.kdops(a, k), orc.centroids(a)
+    assert len(patches) == od
+    for p, rec in enumerate(patches):
+        gid, size = int(rec[0]), int(rec[1])
+        vals = [float.fromhex(x) for x in rec[2:]]
+        idx = order[int(bounds[p]):int(bounds[p + 1])].astype(np.int64)
+        assert gid == p and size == idx.size
+        if size == 0:
+            continue
+        box = np.empty((k // 2, 2))
+        box[:, 0] = slabs[idx, :, 0].min(axis=0)
+        box[:, 1] = slabs[idx, :, 1].max(axis=0)
+        assert vals[:k] == box.reshape(-1).tolist()
+        c = [0.0, 0.0, 0.0]
+        for e in idx:
+            for ax in range(3):
+                c[ax] += float(cent[e, ax])
+        assert vals[k:] == [x / size for x in c]
+    tree = [line.split()[1:] for line in body if line.startswith("tree")]
+    nonempty = int(np.count_nonzero(np.diff(bounds.astype(np.int64))))
+    assert tree and int(tree[0][0]) == nonempty and int(tree[0][2]) == nonempty
+    assert int(tree[0][1]) == 2 * nonempty - 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("od", [1, 8, 64])
+def test_host_api_empty_object(tmp_path, od):
+    """An object without elements: od empty patches with the reference's default k-DOP and an empty tree."""
+    exe = str(tmp_path / "cw")
+    compile_driver(exe)
+    out = subprocess.run([exe, "empty", str(od)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.split() == ["empty", "0"]
