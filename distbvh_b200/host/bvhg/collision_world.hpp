@@ -94,14 +94,6 @@ private:
 
 class collision_object;
 
-// Patch metadata handed to the narrowphase functor (the id and size of src/bvh/patch.hpp:55-123).
-struct patch_meta
-{
-  std::size_t gid;
-  std::size_t size;
-  std::size_t global_id() const { return gid; }
-};
-
 // A patch of an object (src/bvh/patch.hpp:55-123): its global id, element count, k-DOP (the union of its elements'
 // slabs: kdop()[2 a] the minimum and kdop()[2 a + 1] the maximum of slab a) and centroid (the mean of its
 // elements' centroids, summed in the patch's element order as std::accumulate does there). An empty patch has the
@@ -201,7 +193,7 @@ template< typename T >
 struct broadphase_collision
 {
   collision_object &object;
-  patch_meta meta;
+  const patch &meta;
   std::size_t patch_id;
   span< const T > elements;
   span< const std::pair< uint32_t, uint32_t > > candidates;  // (index in this span, index in the other span)
@@ -393,6 +385,10 @@ public:
     return out;
   }
 
+  // collision_object::end_phase (src/bvh/collision_object.cpp:400-403) closes a vt phase of the object's task
+  // chains; one rank with no chains has nothing to close. The results and patches stay as they are.
+  void end_phase() noexcept {}
+
   std::size_t id() const noexcept { return m_id; }
   int overdecomposition_factor() const noexcept;
   std::size_t num_patches() const noexcept;
@@ -468,11 +464,11 @@ public:
   void set_narrowphase_functor(narrowphase_functor< T > fun)
   {
     m_functor_type = detail::type_id< T >();
-    m_functor = [fun](collision_object &oa, const patch_meta &ma, const void *ea, std::size_t na, collision_object &ob,
-                      const patch_meta &mb, const void *eb, std::size_t nb,
+    m_functor = [fun](collision_object &oa, const patch &ma, const void *ea, std::size_t na, collision_object &ob,
+                      const patch &mb, const void *eb, std::size_t nb,
                       span< const std::pair< uint32_t, uint32_t > > cand) {
-      broadphase_collision< T > a{ oa, ma, ma.gid, span< const T >( static_cast< const T * >( ea ), na ), cand };
-      broadphase_collision< T > b{ ob, mb, mb.gid, span< const T >( static_cast< const T * >( eb ), nb ), cand };
+      broadphase_collision< T > a{ oa, ma, ma.global_id(), span< const T >( static_cast< const T * >( ea ), na ), cand };
+      broadphase_collision< T > b{ ob, mb, mb.global_id(), span< const T >( static_cast< const T * >( eb ), nb ), cand };
       return fun( a, b );
     };
   }
@@ -498,8 +494,8 @@ private:
   std::unique_ptr< bvhg_ctx, ctx_deleter > m_ctx;
   std::vector< std::unique_ptr< collision_object > > m_objects;
   const void *m_functor_type = nullptr;
-  std::function< narrowphase_result_pair( collision_object &, const patch_meta &, const void *, std::size_t,
-                                          collision_object &, const patch_meta &, const void *, std::size_t,
+  std::function< narrowphase_result_pair( collision_object &, const patch &, const void *, std::size_t,
+                                          collision_object &, const patch &, const void *, std::size_t,
                                           span< const std::pair< uint32_t, uint32_t > > ) >
     m_functor;
 };
@@ -598,9 +594,8 @@ inline void collision_object::broadphase(collision_object &other)
     for ( std::size_t q = 0; q < cnt; ++q ) cand[q] = { pairs[2 * ( first + q )], pairs[2 * ( first + q ) + 1] };
     const std::size_t a0 = patch_begin( pa ), a1 = patch_begin( pa + 1 );
     const std::size_t b0 = other.patch_begin( pb ), b1 = other.patch_begin( pb + 1 );
-    const patch_meta ma{ m_id * m_world.m_od + pa, a1 - a0 }, mb{ other.m_id * m_world.m_od + pb, b1 - b0 };
     narrowphase_result_pair res = m_world.m_functor(
-      *this, ma, m_elems.bytes.data() + a0 * m_elems.elem_size, a1 - a0, other, mb,
+      *this, m_patches[pa], m_elems.bytes.data() + a0 * m_elems.elem_size, a1 - a0, other, other.m_patches[pb],
       other.m_elems.bytes.data() + b0 * other.m_elems.elem_size, b1 - b0,
       span< const std::pair< uint32_t, uint32_t > >( cand.data(), cand.size() ) );
     if ( res.a.size() ) m_results.push_back( std::move( res.a ) );

@@ -95,6 +95,10 @@ int main(int argc, char **argv)
       res.b = bvhg::narrowphase_result( sizeof( detailed_result ) );
       auto &ra = static_cast< bvhg::typed_narrowphase_result< detailed_result > & >( res.a );
       if ( a.object.id() != 0 || b.object.id() != 1 ) throw std::runtime_error( "object ids" );
+      // the functor's patches are the objects' own (local_patches), with their elements
+      if ( &a.meta != &a.object.local_patches()[a.meta.global_id() % od] || a.meta.size() != a.elements.size() ||
+           &b.meta != &b.object.local_patches()[b.meta.global_id() % od] || b.meta.size() != b.elements.size() )
+        throw std::runtime_error( "patch metadata" );
       for ( const auto &c : a.candidates )
         ra.emplace_back( detailed_result{ a.meta.global_id(), a.elements[c.first].global_id(), b.meta.global_id(),
                                           b.elements[c.second].global_id() } );
@@ -128,5 +132,7 @@ int main(int argc, char **argv)
     for ( const auto &n : t.nodes() ) leaves += n.leaf() ? 1 : 0;
     std::printf( "tree %zu %zu %zu\n", t.count(), t.nodes().size(), leaves );
   } );
+  obj.end_phase();
+  obj2.end_phase();
   return 0;
 }
