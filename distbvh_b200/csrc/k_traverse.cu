@@ -409,10 +409,10 @@ __device__ void traverse_body(const trav_item &item, uint32_t, uint32_t)
 //
 // In dense contact a packet's walk visits a few hundred internal nodes and tens of leaf buckets, each shared by only
 // a fraction of the packet's 32 queries. Two changes over the walk of traverse_packet:
-//   - Nodes in batches. Each step pops up to kDenseBatch (node, lane mask) entries from the stack; the warp copies
-//     their rows (both children's slabs) into shared memory with one round of 16-byte asynchronous copies, and every
-//     lane tests its query against the children of each popped node whose mask holds it, from shared memory. One
-//     global round trip serves the whole batch instead of one per chunk of slabs per node.
+//   - Nodes in batches. Each step pops up to kDenseBatch (4 or 6) (node, lane mask) entries from the stack; the
+//     warp copies their rows (both children's slabs) into shared memory with one round of 16-byte asynchronous
+//     copies, and every lane tests its query against the children of each popped node whose mask holds it, from
+//     shared memory. One global round trip serves the whole batch instead of one per chunk of slabs per node.
 //   - Leaves in batches. The walk only queues (bucket, lane mask) entries; a flush spreads all (query, element)
 //     tests of the queued entries over the warp's lanes, 32 at a time, with every query's slabs staged in shared
 //     memory and the target elements' stored rows read from global memory. Hits leave through one ballot and one
@@ -447,7 +447,10 @@ __device__ __forceinline__ void shared_pair(const float *p, float &lo, float &hi
   lo = v.x;
   hi = v.y;
 }
-constexpr int kDenseBatch = 4;  // nodes popped per step
+// Nodes popped per step: 6 for 26-DOP FP64 rows (measured 6% faster there, at 4 resident blocks per SM instead of
+// 5), 4 otherwise (6 measured 1-6% slower for the other k-DOPs and the FP32 rows).
+template< int K, typename T >
+constexpr int kDenseBatch = ( K == 26 && sizeof( T ) == 8 ) ? 6 : 4;
 constexpr int kDenseStack = 256;
 
 template< int K, typename T >
@@ -456,7 +459,7 @@ struct dense_smem
   // every array starts on a 16-byte boundary: rows[] receives 16-byte asynchronous copies, and q[] and rows[] are
   // read as 8- or 16-byte (min, max) pairs
   alignas( 16 ) T q[32][K];                  // query slabs of the packet, (min, max) per slab
-  alignas( 16 ) T rows[kDenseBatch][2 * K];  // node rows of the batch: [slab][child][min, max]
+  alignas( 16 ) T rows[kDenseBatch< K, T >][2 * K];  // node rows of the batch: [slab][child][min, max]
   alignas( 16 ) uint32_t qe[32];             // query element indices
   alignas( 16 ) int2 stack[kDenseStack];     // (node, lane mask)
   alignas( 16 ) int2 leaf[kLeafQueue];       // (bucket, lane mask)
@@ -609,7 +612,7 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
   while ( sp > 0 )
   {
     __syncwarp();
-    const int nb = sp < kDenseBatch ? sp : kDenseBatch;
+    const int nb = sp < kDenseBatch< K, T > ? sp : kDenseBatch< K, T >;
     sp -= nb;
     // the batch's node rows into shared memory (one round of asynchronous copies), their links into registers
     for ( int t = static_cast< int >( lane ); t < nb * R16; t += 32 )
@@ -626,14 +629,14 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
       links = __ldg( x.child + node );
       if ( x.self ) span = make_int2( node, __ldg( &x.range[node].y ) );
     }
-    unsigned emask[kDenseBatch];
+    unsigned emask[kDenseBatch< K, T >];
 #pragma unroll
-    for ( int k = 0; k < kDenseBatch; ++k ) emask[k] = k < nb ? static_cast< unsigned >( sm.stack[sp + k].y ) : 0u;
+    for ( int k = 0; k < kDenseBatch< K, T >; ++k ) emask[k] = k < nb ? static_cast< unsigned >( sm.stack[sp + k].y ) : 0u;
     cp_async_wait_all();
     __syncwarp();
-    unsigned m0[kDenseBatch], m1[kDenseBatch];
+    unsigned m0[kDenseBatch< K, T >], m1[kDenseBatch< K, T >];
 #pragma unroll
-    for ( int k = 0; k < kDenseBatch; ++k )
+    for ( int k = 0; k < kDenseBatch< K, T >; ++k )
     {
       bool o0 = ( emask[k] >> lane ) & 1u, o1 = o0;
       if ( x.self )
@@ -670,7 +673,7 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
     }
     // children: buckets to the leaf queue, internal nodes onto the stack (warp-uniform; lane 0 writes)
 #pragma unroll
-    for ( int k = 0; k < kDenseBatch; ++k )
+    for ( int k = 0; k < kDenseBatch< K, T >; ++k )
     {
       const int cx = __shfl_sync( 0xffffffffu, links.x, k ), cy = __shfl_sync( 0xffffffffu, links.y, k );
 #pragma unroll
@@ -694,7 +697,7 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
         }
       }
     }
-    if ( nleaf > kLeafQueue - 2 * kDenseBatch )
+    if ( nleaf > kLeafQueue - 2 * kDenseBatch< K, T > )
     {
       flush_leaves< K, T >( x, sm, nleaf, i0, lane );
       nleaf = 0;
