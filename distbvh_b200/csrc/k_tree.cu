@@ -11,7 +11,9 @@
 // No thread ever waits. Nodes whose two children close inside a block of 128 buckets are merged in shared memory
 // (warp rounds, then block rounds) and written out coalesced; the rest use a global exchange slot per node: the
 // first arrival's slab stores are ordered before its acq_rel atomic exchange, and the second arrival, which sees
-// the slot taken with an acquire load (or learns it from its own exchange), reads them through L2 after it.
+// the slot taken with an acquire load (or learns it from its own exchange), reads them through L2 after it. The
+// refit keeps the topology and splits the same way: the nodes inside a block in barrier-separated rounds over
+// shared memory, then the block's local roots climb through the crossing nodes with the same exchange.
 #include "bvhg_internal.cuh"
 #include "bulk_copy.cuh"
 #include "kdop_math.cuh"
