@@ -84,9 +84,9 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned k, unsigned 
   return base + pre;
 }
 
-// Slabs of element e straight into a shared-memory row (C = 2 D values: min, max per slab), slab by slab so that
-// only the vertices stay in registers: the same FP64 slabs, or the same FP32 enclosures, that slabs_body unites
-// into the bucket boxes.
+// Slabs of element e straight into a shared-memory row (C = 2 D values: min, max per slab): the same FP64 slabs
+// (slab by slab, so that only the vertices stay in registers), or the same FP32 enclosures, that slabs_body
+// unites into the bucket boxes.
 template< int K, typename T, int VT >
 __device__ __forceinline__ void slabs_to_row(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
                                              float eps_hi, T *row)
@@ -98,20 +98,24 @@ __device__ __forceinline__ void slabs_to_row(const double *__restrict__ verts, u
     const double *src = verts + static_cast< size_t >( e ) * VT * 3;
 #pragma unroll
     for ( int k = 0; k < VT * 3; ++k ) p[k] = __ldg( src + k );
-#pragma unroll
-    for ( int a = 0; a < D; ++a )
+    if constexpr ( sizeof( T ) == 8 )
     {
-      if constexpr ( sizeof( T ) == 8 )
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
       {
         double l, h;
         slab64< K >( p, VT, a, eps, l, h );
         row[2 * a] = l;
         row[2 * a + 1] = h;
-      } else {
-        float l, h;
-        slab32< K >( p, VT, a, eps_hi, l, h );
-        row[2 * a] = l;
-        row[2 * a + 1] = h;
+      }
+    } else {
+      float lo[D], hi[D];
+      slabs32_all< K, VT >( p, eps_hi, lo, hi );
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
+      {
+        row[2 * a] = lo[a];
+        row[2 * a + 1] = hi[a];
       }
     }
   } else {
@@ -415,12 +419,14 @@ __device__ void traverse_body(const trav_item &item, uint32_t, uint32_t)
 //     shared memory. One global round trip serves the whole batch instead of one per chunk of slabs per node.
 //   - Leaves in batches. The walk only queues (bucket, lane mask) entries; a flush spreads all (query, element)
 //     tests of the queued entries over the warp's lanes, 32 at a time, with every query's slabs staged in shared
-//     memory and the target elements' stored rows read from global memory. Hits leave through one ballot and one
-//     atomic per 32 tests.
+//     memory and the target elements' stored rows read from global memory. Hits collect in a per-warp buffer in
+//     shared memory (one ballot per 32 tests); a full buffer leaves through one atomic reservation and coalesced
+//     stores, so a warp pays an atomic's round trip per 33-64 pairs instead of per round of tests with a hit.
 // The stack grows by at most kDenseBatch entries per step, so its depth bound is kDenseStack; a walk that would pass
 // it raises kErrOverflowStack, and the host then runs the pair search again with the single-node walk (whose stack
 // is bounded by the tree depth).
 constexpr int kLeafQueue = 32;  // queued (bucket, mask) entries per warp
+constexpr int kPairBuf = 64;    // buffered pairs per warp: drained once more than 32 are held
 
 // A (min, max) pair: from global memory (read-only path) or from shared memory, as one vector load.
 __device__ __forceinline__ void load_pair(const double *p, double &lo, double &hi)
@@ -464,6 +470,7 @@ struct dense_smem
   alignas( 16 ) int2 stack[kDenseStack];     // (node, lane mask)
   alignas( 16 ) int2 leaf[kLeafQueue];       // (bucket, lane mask)
   alignas( 16 ) uint32_t pre[kLeafQueue];    // exclusive prefix of the entries' test counts (8 per query)
+  alignas( 16 ) uint2 out[kPairBuf];         // pairs found and not yet written
 };
 
 template< int K, typename T >
@@ -478,10 +485,27 @@ static_assert( dense_smem_aligned< 6, double >() && dense_smem_aligned< 18, doub
                  dense_smem_aligned< 18, float >() && dense_smem_aligned< 26, float >(),
                "dense walk shared memory must keep 16-byte alignment" );
 
-// Tests every (query, element) pair of the queued entries; i0 = the packet's first query rank.
+// Writes the warp's buffered pairs: one atomic reservation for all of them, then coalesced stores (a count past
+// the capacity is still counted, so the host learns the size it needs).
+template< int K, typename T >
+__device__ __forceinline__ void drain_pairs(const trav_args< T > &x, dense_smem< K, T > &sm, uint32_t &nout,
+                                            unsigned lane)
+{
+  __syncwarp();
+  unsigned long long base = 0;
+  if ( lane == 0 && nout ) base = atomicAdd( &x.ps->count, static_cast< unsigned long long >( nout ) );
+  base = __shfl_sync( 0xffffffffu, base, 0 );
+  for ( uint32_t j = lane; j < nout; j += 32 )
+    if ( base + j < x.cap ) x.pairs[base + j] = sm.out[j];
+  __syncwarp();
+  nout = 0;
+}
+
+// Tests every (query, element) pair of the queued entries; i0 = the packet's first query rank. Hits are appended to
+// the warp's pair buffer (nout pairs held).
 template< int K, typename T >
 __device__ __forceinline__ void flush_leaves(const trav_args< T > &x, dense_smem< K, T > &sm, int nleaf, uint32_t i0,
-                                             unsigned lane)
+                                             unsigned lane, uint32_t &nout)
 {
   constexpr int D = K / 2;
   __syncwarp();
@@ -548,10 +572,9 @@ __device__ __forceinline__ void flush_leaves(const trav_args< T > &x, dense_smem
     const unsigned bal = __ballot_sync( 0xffffffffu, hit );
     if ( bal )
     {
-      unsigned long long pos = 0;
-      if ( lane == 0 ) pos = atomicAdd( &x.ps->count, static_cast< unsigned long long >( __popc( bal ) ) );
-      pos = __shfl_sync( 0xffffffffu, pos, 0 ) + static_cast< unsigned >( __popc( bal & lt ) );
-      if ( hit && pos < x.cap ) x.pairs[pos] = make_uint2( sm.qe[q], __ldg( x.tperm + r ) );
+      if ( hit ) sm.out[nout + static_cast< unsigned >( __popc( bal & lt ) )] = make_uint2( sm.qe[q], __ldg( x.tperm + r ) );
+      nout += static_cast< uint32_t >( __popc( bal ) );
+      if ( nout > kPairBuf - 32 ) drain_pairs< K, T >( x, sm, nout, lane );
     }
   }
   __syncwarp();
@@ -601,10 +624,12 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
   if ( !mask ) return;
   const int root = x.tsc->root;
   int nleaf = 0;
+  uint32_t nout = 0;
   if ( root < 0 )
   {
     if ( lane == 0 ) sm.leaf[0] = make_int2( ~root, static_cast< int >( mask ) );
-    flush_leaves< K, T >( x, sm, 1, i0, lane );
+    flush_leaves< K, T >( x, sm, 1, i0, lane, nout );
+    drain_pairs< K, T >( x, sm, nout, lane );
     return;
   }
   if ( lane == 0 ) sm.stack[0] = make_int2( root, static_cast< int >( mask ) );
@@ -690,6 +715,7 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
           if ( sp >= x.dense_stack )
           {
             if ( lane == 0 ) atomicCAS( &x.ps->error, 0, kErrOverflowStack );
+            drain_pairs< K, T >( x, sm, nout, lane );
             return;
           }
           if ( lane == 0 ) sm.stack[sp] = make_int2( ch, static_cast< int >( m ) );
@@ -699,20 +725,25 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
     }
     if ( nleaf > kLeafQueue - 2 * kDenseBatch< K, T > )
     {
-      flush_leaves< K, T >( x, sm, nleaf, i0, lane );
+      flush_leaves< K, T >( x, sm, nleaf, i0, lane, nout );
       nleaf = 0;
     }
   }
-  if ( nleaf > 0 ) flush_leaves< K, T >( x, sm, nleaf, i0, lane );
+  if ( nleaf > 0 ) flush_leaves< K, T >( x, sm, nleaf, i0, lane, nout );
+  drain_pairs< K, T >( x, sm, nout, lane );
 }
 
 // Resident blocks per SM of the dense walk: as many as its shared memory allows (228 KB per SM, 1 KB of it reserved
-// per block), at most 6; the register budget follows from it.
+// per block), at most kDenseBlockCap; the register budget follows from it. 18-DOP FP64 rows run at 5 blocks (96
+// registers, no spills): at 6 they were squeezed into 80 registers with spills, and the walk was 16% slower.
+template< int K, typename T >
+constexpr int kDenseBlockCap = ( K == 18 && sizeof( T ) == 8 ) ? 5 : 6;
+template< int K, typename T >
+constexpr int kDenseBlocksBySmem =
+  ( 228 * 1024 ) / ( ( kTravThreads / 32 ) * static_cast< int >( sizeof( dense_smem< K, T > ) ) + 1024 );
 template< int K, typename T >
 constexpr int kDenseBlocksPerSM =
-  ( 228 * 1024 ) / ( ( kTravThreads / 32 ) * static_cast< int >( sizeof( dense_smem< K, T > ) ) + 1024 ) < 6
-    ? ( 228 * 1024 ) / ( ( kTravThreads / 32 ) * static_cast< int >( sizeof( dense_smem< K, T > ) ) + 1024 )
-    : 6;
+  kDenseBlocksBySmem< K, T > < kDenseBlockCap< K, T > ? kDenseBlocksBySmem< K, T > : kDenseBlockCap< K, T >;
 
 // Dense contact: one warp per packet of 32 query ranks (the hardware balances the walks).
 template< int K, typename T >
@@ -826,7 +857,12 @@ cudaError_t launch_trav_batch_t(bool dense, uint32_t V, const batch_launch &b, c
   return cudaGetLastError();
 }
 
-// K7: FP64 slabs of both elements from their vertices, slab by slab with early exit.
+constexpr int kRecheckThreads = 256;
+constexpr int kRecheckBuf = 128;  // buffered pairs per warp: drained once more than 96 are held
+
+// K7: FP64 overlap of both elements from their vertices. With both vertex counts known at compile time, the
+// comparison-only projections of overlap64 (shared products, no products by 0 or 1, one epsilon shift per slab);
+// otherwise slab64 slab by slab with early exit. Both give the outcome of comparing the FP64 slabs.
 template< int K, int VA, int VB >
 __device__ void recheck_body(const recheck_args &args, uint32_t bid, uint32_t nblk)
 {
@@ -846,28 +882,43 @@ __device__ void recheck_body(const recheck_args &args, uint32_t bid, uint32_t nb
                               cand_cap );
   const int Va = VA > 0 ? VA : static_cast< int >( Var );
   const int Vb = VB > 0 ? VB : static_cast< int >( Vbr );
-  for ( uint64_t p = static_cast< uint64_t >( bid ) * blockDim.x + threadIdx.x; p < ncand;
-        p += static_cast< uint64_t >( nblk ) * blockDim.x )
+  // Confirmed pairs collect in a per-warp buffer in shared memory and leave through one atomic reservation per
+  // 97-128 pairs, with coalesced stores (one same-address atomic per 32 candidates made the kernel wait on the
+  // counter's round trip).
+  __shared__ uint2 s_out[kRecheckThreads / 32][kRecheckBuf];
+  const unsigned lane = threadIdx.x & 31u, lt = ( 1u << lane ) - 1u;
+  uint2 *wout = s_out[threadIdx.x >> 5];
+  uint32_t nout = 0;
+  auto drain = [&]() {
+    __syncwarp();
+    unsigned long long base = 0;
+    if ( lane == 0 && nout ) base = atomicAdd( &ps->count2, static_cast< unsigned long long >( nout ) );
+    base = __shfl_sync( 0xffffffffu, base, 0 );
+    for ( uint32_t j = lane; j < nout; j += 32 )
+      if ( base + j < cap ) out[base + j] = wout[j];
+    __syncwarp();
+    nout = 0;
+  };
+  // warp-uniform trips: lane l of a warp takes candidate p0 + l
+  for ( uint64_t p0 = static_cast< uint64_t >( bid ) * blockDim.x + ( threadIdx.x & ~31u ); p0 < ncand;
+        p0 += static_cast< uint64_t >( nblk ) * blockDim.x )
   {
-    const uint2 c = __ldg( cand + p );
+    const uint64_t p = p0 + lane;
+    const bool valid = p < ncand;
+    const uint2 c = valid ? __ldg( cand + p ) : make_uint2( 0u, 0u );
+    bool ok = valid;
     const double *pa = va + static_cast< size_t >( c.x ) * Va * 3;
     const double *pb = vb + static_cast< size_t >( c.y ) * Vb * 3;
     double xa[VA > 0 ? VA * 3 : 24], xb[VB > 0 ? VB * 3 : 24];
-    bool ok = true;
     if constexpr ( VA > 0 && VB > 0 )
     {
-#pragma unroll
-      for ( int k = 0; k < VA * 3; ++k ) xa[k] = __ldg( pa + k );
-#pragma unroll
-      for ( int k = 0; k < VB * 3; ++k ) xb[k] = __ldg( pb + k );
-#pragma unroll
-      for ( int a = 0; a < D; ++a )
+      if ( valid )
       {
-        if ( !ok ) break;
-        double alo, ahi, blo, bhi;
-        slab64< K >( xa, VA, a, eps, alo, ahi );
-        slab64< K >( xb, VB, a, eps, blo, bhi );
-        ok = alo < bhi && blo < ahi;
+#pragma unroll
+        for ( int k = 0; k < VA * 3; ++k ) xa[k] = __ldg( pa + k );
+#pragma unroll
+        for ( int k = 0; k < VB * 3; ++k ) xb[k] = __ldg( pb + k );
+        ok = overlap64< K, VA, VB >( xa, xb, eps );
       }
     } else {
       (void)xa;
@@ -896,15 +947,18 @@ __device__ void recheck_body(const recheck_args &args, uint32_t bid, uint32_t nb
         ok = alo < bhi && blo < ahi;
       }
     }
-    const unsigned long long o = warp_reserve( ok ? 1u : 0u, &ps->count2 );
-    if ( ok && o < cap ) out[o] = c;
+    const unsigned bal = __ballot_sync( 0xffffffffu, ok );
+    if ( ok ) wout[nout + static_cast< unsigned >( __popc( bal & lt ) )] = c;
+    nout += static_cast< uint32_t >( __popc( bal ) );
+    if ( nout > kRecheckBuf - 32 ) drain();
   }
+  drain();
 }
 
 // grid-stride over the candidates (their count is read on the device): at most 4 blocks per SM
 uint32_t recheck_grid(uint64_t ncand)
 {
-  const uint64_t blocks = ( ncand + 255 ) / 256;
+  const uint64_t blocks = ( ncand + kRecheckThreads - 1 ) / kRecheckThreads;
   const uint64_t capb = static_cast< uint64_t >( device_sm_count() ) * 4;
   return static_cast< uint32_t >( blocks < capb ? ( blocks ? blocks : 1 ) : capb );
 }
@@ -913,10 +967,10 @@ template< int K >
 cudaError_t recheck_k(const recheck_args &a, cudaStream_t s)
 {
   const uint32_t grid = recheck_grid( a.cand_cap );
-  if ( a.Va == 3 && a.Vb == 3 ) k_single< recheck_args, recheck_body< K, 3, 3 >, 256, 2 ><<< grid, 256, 0, s >>>( a );
-  else if ( a.Va == 4 && a.Vb == 4 ) k_single< recheck_args, recheck_body< K, 4, 4 >, 256, 2 ><<< grid, 256, 0, s >>>( a );
-  else if ( a.Va == 8 && a.Vb == 8 ) k_single< recheck_args, recheck_body< K, 8, 8 >, 256, 2 ><<< grid, 256, 0, s >>>( a );
-  else k_single< recheck_args, recheck_body< K, 0, 0 >, 256, 2 ><<< grid, 256, 0, s >>>( a );
+  if ( a.Va == 3 && a.Vb == 3 ) k_single< recheck_args, recheck_body< K, 3, 3 >, kRecheckThreads, 2 ><<< grid, kRecheckThreads, 0, s >>>( a );
+  else if ( a.Va == 4 && a.Vb == 4 ) k_single< recheck_args, recheck_body< K, 4, 4 >, kRecheckThreads, 2 ><<< grid, kRecheckThreads, 0, s >>>( a );
+  else if ( a.Va == 8 && a.Vb == 8 ) k_single< recheck_args, recheck_body< K, 8, 8 >, kRecheckThreads, 2 ><<< grid, kRecheckThreads, 0, s >>>( a );
+  else k_single< recheck_args, recheck_body< K, 0, 0 >, kRecheckThreads, 2 ><<< grid, kRecheckThreads, 0, s >>>( a );
   return cudaGetLastError();
 }
 
@@ -924,10 +978,10 @@ template< int K >
 cudaError_t recheck_batch_k(uint32_t V, const batch_launch &b, cudaStream_t s)
 {
   const recheck_args *it = static_cast< const recheck_args * >( b.items );
-  if ( V == 3 ) k_batched< recheck_args, recheck_body< K, 3, 3 >, 256, 2 ><<< b.blocks, 256, 0, s >>>( it, b.starts, b.nitems );
-  else if ( V == 4 ) k_batched< recheck_args, recheck_body< K, 4, 4 >, 256, 2 ><<< b.blocks, 256, 0, s >>>( it, b.starts, b.nitems );
-  else if ( V == 8 ) k_batched< recheck_args, recheck_body< K, 8, 8 >, 256, 2 ><<< b.blocks, 256, 0, s >>>( it, b.starts, b.nitems );
-  else k_batched< recheck_args, recheck_body< K, 0, 0 >, 256, 2 ><<< b.blocks, 256, 0, s >>>( it, b.starts, b.nitems );
+  if ( V == 3 ) k_batched< recheck_args, recheck_body< K, 3, 3 >, kRecheckThreads, 2 ><<< b.blocks, kRecheckThreads, 0, s >>>( it, b.starts, b.nitems );
+  else if ( V == 4 ) k_batched< recheck_args, recheck_body< K, 4, 4 >, kRecheckThreads, 2 ><<< b.blocks, kRecheckThreads, 0, s >>>( it, b.starts, b.nitems );
+  else if ( V == 8 ) k_batched< recheck_args, recheck_body< K, 8, 8 >, kRecheckThreads, 2 ><<< b.blocks, kRecheckThreads, 0, s >>>( it, b.starts, b.nitems );
+  else k_batched< recheck_args, recheck_body< K, 0, 0 >, kRecheckThreads, 2 ><<< b.blocks, kRecheckThreads, 0, s >>>( it, b.starts, b.nitems );
   return cudaGetLastError();
 }
 

@@ -80,6 +80,97 @@ __device__ __forceinline__ void slab64(const double *p, int V, int a, double eps
   }
 }
 
+// ---- FP64 overlap outcome (no slab bits) ---------------------------------------------------------------
+//
+// The recheck of the precision form needs the outcome of the strict overlap test, not the slab bits. The
+// projections below equal project64's in value; they may differ only in the sign of a zero, which no comparison
+// sees. A product by 0 is a zero that the sums absorb (t + (+-0) == t), a product by 1 is the coordinate, a
+// product by -c is -(v * c) exactly, and each product v_k * c shared by several normals is rounded once. The
+// epsilon shift is monotone under round-to-nearest, so min over vertices of (p - eps) == (min p) - eps, and it is
+// applied once per slab. Per tetrahedron at K = 26 this is 72 FP64 operations for the projections instead of 260.
+
+// Projections of one vertex onto the normals of group G: 0 = the axes (normals 0..2), 1 = the edge normals
+// (r,r,0) (r,0,r) (0,r,r) (r,-r,0) (r,0,-r) (0,r,-r), 2 = the corner normals (s,s,s) (s,-s,s) (s,s,-s) (s,-s,-s),
+// in normal_comp's order within the group.
+template< int G >
+__device__ __forceinline__ void project_group(const double v0, const double v1, const double v2, double *p)
+{
+  if constexpr ( G == 0 )
+  {
+    p[0] = v0;
+    p[1] = v1;
+    p[2] = v2;
+  } else if constexpr ( G == 1 ) {
+    const double m0 = __dmul_rn( v0, kOverRoot2 ), m1 = __dmul_rn( v1, kOverRoot2 ), m2 = __dmul_rn( v2, kOverRoot2 );
+    p[0] = __dadd_rn( m0, m1 );
+    p[1] = __dadd_rn( m0, m2 );
+    p[2] = __dadd_rn( m1, m2 );
+    p[3] = __dsub_rn( m0, m1 );
+    p[4] = __dsub_rn( m0, m2 );
+    p[5] = __dsub_rn( m1, m2 );
+  } else {
+    const double c0 = __dmul_rn( v0, kOverRoot3 ), c1 = __dmul_rn( v1, kOverRoot3 ), c2 = __dmul_rn( v2, kOverRoot3 );
+    const double s = __dadd_rn( c0, c1 ), d = __dsub_rn( c0, c1 );
+    p[0] = __dadd_rn( s, c2 );
+    p[1] = __dadd_rn( d, c2 );
+    p[2] = __dsub_rn( s, c2 );
+    p[3] = __dsub_rn( d, c2 );
+  }
+}
+
+template< int G >
+constexpr int group_size = G == 0 ? 3 : ( G == 1 ? 6 : 4 );
+
+// Strict overlap of two elements (V* vertices each at x*[3 v + c]) over the slabs of group G, with the same
+// outcome as comparing slab64's values.
+template< int G, int VA, int VB >
+__device__ __forceinline__ bool group_overlap64(const double *xa, const double *xb, double eps)
+{
+  constexpr int N = group_size< G >;
+  double alo[N], ahi[N], blo[N], bhi[N];
+#pragma unroll
+  for ( int v = 0; v < VA; ++v )
+  {
+    double p[N];
+    project_group< G >( xa[3 * v], xa[3 * v + 1], xa[3 * v + 2], p );
+#pragma unroll
+    for ( int k = 0; k < N; ++k )
+    {
+      alo[k] = v ? fmin( alo[k], p[k] ) : p[k];
+      ahi[k] = v ? fmax( ahi[k], p[k] ) : p[k];
+    }
+  }
+#pragma unroll
+  for ( int v = 0; v < VB; ++v )
+  {
+    double p[N];
+    project_group< G >( xb[3 * v], xb[3 * v + 1], xb[3 * v + 2], p );
+#pragma unroll
+    for ( int k = 0; k < N; ++k )
+    {
+      blo[k] = v ? fmin( blo[k], p[k] ) : p[k];
+      bhi[k] = v ? fmax( bhi[k], p[k] ) : p[k];
+    }
+  }
+  bool ok = true;
+#pragma unroll
+  for ( int k = 0; k < N; ++k )
+    ok = ok && __dsub_rn( alo[k], eps ) < __dadd_rn( bhi[k], eps ) && __dsub_rn( blo[k], eps ) < __dadd_rn( ahi[k], eps );
+  return ok;
+}
+
+// Strict overlap of two elements over all K/2 slabs (the FP64 pair-set test), group by group.
+template< int K, int VA, int VB >
+__device__ __forceinline__ bool overlap64(const double *xa, const double *xb, double eps)
+{
+  bool ok = group_overlap64< 0, VA, VB >( xa, xb, eps );
+  if constexpr ( K >= 18 )
+    if ( ok ) ok = group_overlap64< 1, VA, VB >( xa, xb, eps );
+  if constexpr ( K == 26 )
+    if ( ok ) ok = group_overlap64< 2, VA, VB >( xa, xb, eps );
+  return ok;
+}
+
 // ---- FP32 enclosure ------------------------------------------------------------------------------------
 
 // Error bound constant: the FP64 value of ((t0 + t1) + t2), t_k = fl(v_k n_k), differs from the exact sum by
@@ -197,6 +288,92 @@ __device__ __forceinline__ void slab32(const double *p, int V, int a, float eps_
   }
 }
 
+// All K/2 FP32 enclosures of one element with V vertices, bit for bit the values slab32 gives slab by slab, with
+// the shared work done once per vertex: each coordinate is rounded down and up once, and the product interval of a
+// coordinate by a normal magnitude is formed once for all normals that use it (a component -c gives the negated
+// interval exactly, because directed rounding is symmetric under negation: rd(-z) = -ru(z)). Sums, magnitudes,
+// the widening and the epsilon step run in slab32's order.
+template< int K, int V >
+__device__ __forceinline__ void slabs32_all(const double *p, float eps_hi, float *lo, float *hi)
+{
+  constexpr int D = K / 2;
+  const float inf = __int_as_float( 0x7f800000 );
+#pragma unroll
+  for ( int a = 0; a < D; ++a )
+  {
+    lo[a] = inf;
+    hi[a] = -inf;
+  }
+  // widening by the FP64 evaluation error (not for the axes, whose projection is the coordinate), the epsilon
+  // step, and the running min / max over the vertices: slab32's tail
+  auto finish = [&](int a, float slo, float shi, float mag, bool exact) {
+    if ( !exact )
+    {
+      const float e = __fmul_ru( mag, kTwoPowM51 );
+      slo = __fsub_rd( slo, e );
+      shi = __fadd_ru( shi, e );
+    }
+    if ( eps_hi != 0.f )
+    {
+      const float m2 = __fadd_ru( fmaxf( fabsf( slo ), fabsf( shi ) ), eps_hi );
+      const float e2 = __fmul_ru( m2, kTwoPowM52 );
+      slo = __fsub_rd( __fsub_rd( slo, eps_hi ), e2 );
+      shi = __fadd_ru( __fadd_ru( shi, eps_hi ), e2 );
+    }
+    lo[a] = fminf( lo[a], slo );
+    hi[a] = fmaxf( hi[a], shi );
+  };
+#pragma unroll
+  for ( int v = 0; v < V; ++v )
+  {
+    float xl[3], xh[3];
+#pragma unroll
+    for ( int c = 0; c < 3; ++c )
+    {
+      xl[c] = __double2float_rd( p[3 * v + c] );
+      xh[c] = __double2float_ru( p[3 * v + c] );
+    }
+#pragma unroll
+    for ( int c = 0; c < 3; ++c ) finish( c, xl[c], xh[c], 0.f, true );
+    if constexpr ( K == 26 )
+    {
+      // corners (s,s,s) (s,-s,s) (s,s,-s) (s,-s,-s): normals 3..6
+      float tl[3], th[3];
+#pragma unroll
+      for ( int c = 0; c < 3; ++c ) mul_interval( xl[c], xh[c], kOverRoot3Lo, kOverRoot3Hi, true, tl[c], th[c] );
+      const float mag = __fadd_ru( __fadd_ru( fmaxf( fabsf( tl[0] ), fabsf( th[0] ) ), fmaxf( fabsf( tl[1] ), fabsf( th[1] ) ) ),
+                                   fmaxf( fabsf( tl[2] ), fabsf( th[2] ) ) );
+#pragma unroll
+      for ( int q = 0; q < 4; ++q )
+      {
+        const float l1 = ( q & 1 ) ? -th[1] : tl[1], h1 = ( q & 1 ) ? -tl[1] : th[1];
+        const float l2 = ( q & 2 ) ? -th[2] : tl[2], h2 = ( q & 2 ) ? -tl[2] : th[2];
+        finish( 3 + q, __fadd_rd( __fadd_rd( tl[0], l1 ), l2 ), __fadd_ru( __fadd_ru( th[0], h1 ), h2 ), mag, false );
+      }
+    }
+    if constexpr ( K >= 18 )
+    {
+      // edges (r,r,0) (r,0,r) (0,r,r) (r,-r,0) (r,0,-r) (0,r,-r): normals 3..8 (K = 18) or 7..12 (K = 26)
+      constexpr int E = K == 18 ? 3 : 7;
+      float tl[3], th[3], tm[3];
+#pragma unroll
+      for ( int c = 0; c < 3; ++c )
+      {
+        mul_interval( xl[c], xh[c], kOverRoot2Lo, kOverRoot2Hi, true, tl[c], th[c] );
+        tm[c] = fmaxf( fabsf( tl[c] ), fabsf( th[c] ) );
+      }
+#pragma unroll
+      for ( int e = 0; e < 6; ++e )
+      {
+        const int c1 = ( e % 3 == 2 ) ? 1 : 0, c2 = ( e % 3 == 0 ) ? 1 : 2;
+        const bool neg = e >= 3;
+        const float l2 = neg ? -th[c2] : tl[c2], h2 = neg ? -tl[c2] : th[c2];
+        finish( E + e, __fadd_rd( tl[c1], l2 ), __fadd_ru( th[c1], h2 ), __fadd_ru( tm[c1], tm[c2] ), false );
+      }
+    }
+  }
+}
+
 // Slabs of element e (gathered vertices) into lo/hi.
 template< int K, typename T, int VT >
 __device__ __forceinline__ void leaf_slabs(const double *__restrict__ verts, uint32_t Vrt, uint32_t e, double eps,
@@ -211,21 +388,18 @@ __device__ __forceinline__ void leaf_slabs(const double *__restrict__ verts, uin
   {
 #pragma unroll
     for ( int k = 0; k < VT * 3; ++k ) p[k] = __ldg( src + k );
-#pragma unroll
-    for ( int a = 0; a < D; ++a )
+    if constexpr ( sizeof( T ) == 8 )
     {
-      if constexpr ( sizeof( T ) == 8 )
+#pragma unroll
+      for ( int a = 0; a < D; ++a )
       {
         double l, h;
         slab64< K >( p, VT, a, eps, l, h );
         lo[a] = l;
         hi[a] = h;
-      } else {
-        float l, h;
-        slab32< K >( p, VT, a, eps_hi, l, h );
-        lo[a] = l;
-        hi[a] = h;
       }
+    } else {
+      slabs32_all< K, VT >( p, eps_hi, lo, hi );
     }
   } else {
     (void)VMAX;

@@ -476,6 +476,50 @@ def test_signed_zeros_and_exact_cancellations(k, V, eps):
         assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), orc.pair_set(a, b, k, eps))
 
 
+@pytest.mark.parametrize("k", [6, 18, 26])
+@pytest.mark.parametrize("V", [3, 4, 8])
+@pytest.mark.parametrize("eps", [0.0, 0.25])
+def test_signed_zeros_filter_form_recheck(k, V, eps):
+    """The same coordinates through the precision form: the FP32 candidates are rechecked in FP64 by projections
+    that skip products by 0 and 1 and share the products by the normal magnitudes. Many slabs touch exactly
+    (strict overlap fails by equality) or meet at signed zeros, so the recheck's outcome must be the FP64 one on
+    every candidate: the pair set equals the oracle's, in both roles and for self-collision."""
+    rng = np.random.default_rng(2000 + 10 * k + V)
+    values = np.array([-0.0, 0.0, 0.25, -0.25, 1.0, -1.0])
+    a = values[rng.integers(0, len(values), size=(1500, V, 3))]
+    b = values[rng.integers(0, len(values), size=(1200, V, 3))]
+    with bvhg.Context(k=k, epsilon=eps, precision=bvhg.FILTER_FP32) as ctx:
+        oa, ob = build_pair(ctx, a, b)
+        want = orc.pair_set(a, b, k, eps)
+        assert np.array_equal(orc.canonical(ctx.broadphase(oa, ob)), want)
+        assert np.array_equal(orc.canonical(ctx.broadphase(ob, oa)), orc.pair_set(b, a, k, eps))
+        assert np.array_equal(orc.canonical(ctx.self_collision(oa)), orc.self_pair_set(a, k, eps))
+
+
+@pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
+@pytest.mark.parametrize("k", [6, 18, 26])
+@pytest.mark.parametrize("V", [3, 4, 8])
+def test_slab_paths_agree_bitwise(precision, k, V):
+    """Elements of 3, 4 and 8 vertices take the kernels' unrolled slab code (FP32: every enclosure of an element
+    from shared per-vertex roundings and products); any other vertex count takes the generic code, one vertex and
+    one slab at a time. The same elements with their first vertex repeated (V + 1 vertices, the same slabs) must
+    give the same bits through both, for random coordinates over many magnitudes and for cancelling ones."""
+    rng = np.random.default_rng(3000 + 10 * k + V)
+    soup = meshes.random_soup(4000, V, seed=40 + V, size=0.01)
+    scaled = soup * (10.0 ** rng.integers(-20, 20, size=(4000, 1, 1)))
+    values = np.array([-0.0, 0.0, 0.25, -0.25, 1.0, -1.0, 1e-40, -3e38])
+    special = values[rng.integers(0, len(values), size=(2000, V, 3))]
+    for xyz in (soup, scaled, special):
+        padded = np.ascontiguousarray(np.concatenate([xyz, xyz[:, :1, :]], axis=1))
+        for eps in (0.0, 0.003):
+            with bvhg.Context(k=k, epsilon=eps, precision=precision) as ctx:
+                o1, o2 = ctx.object(), ctx.object()
+                ctx.set_elements(o1, xyz)
+                ctx.set_elements(o2, padded)
+                s1, s2 = ctx.kdops(o1, xyz.shape[0]), ctx.kdops(o2, xyz.shape[0])
+                assert np.array_equal(s1.view(np.uint8), s2.view(np.uint8)), (eps, np.argwhere(s1 != s2)[:4])
+
+
 @pytest.mark.parametrize("precision", [bvhg.PLAIN_FP64, bvhg.FILTER_FP32])
 def test_dense_walk_stack_bound_falls_back(precision):
     """The dense-contact walk pops several nodes per step, so its stack can grow past the tree depth; when it
