@@ -54,7 +54,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *s
 // retire in program order within the warp, and hands the base back by shuffle), per-digit tile counts published
 // for the decoupled look-back, the tile reordered in the shared buffer it came from, contiguous digit runs
 // written out. Every wait is bounded (look-back polls and mbarrier waits); on a timeout the block raises the
-// object's error word and stops, and blocks that may have read a garbage prefix write nothing.
+// object's error word and stops, and blocks that may have read a garbage prefix write only inside the output.
 template< int BITS >
 __device__ void onesweep_body(const sort_pass_args &a, uint32_t, uint32_t)
 {
@@ -269,13 +269,16 @@ __device__ void onesweep_body(const sort_pass_args &a, uint32_t, uint32_t)
     }
     __syncthreads();
     // A block that timed out published a garbage prefix (so that no successor waits forever) and raised the
-    // object's error word before doing so; every block that could have read such a prefix sees it here, writes
-    // nothing and stops (no bulk copy is in flight at this point).
+    // object's error word. A block that sees the error here writes nothing and stops (no bulk copy is in flight
+    // at this point); one that read a garbage prefix without seeing the error yet writes only inside [0, n) (the
+    // bound on every output position below), and the host reports the error for the whole sort. The error word
+    // and the next tile are fetched together: the fence that used to order them cost the tile two more round trips
+    // to L2 on its critical path (one pass 54.4 -> 52.4 us).
     if ( tid == 0 )
     {
-      __threadfence();
+      const uint32_t nx = atomicAdd( &sc->sort_tile_counter[pass], 1u );
       s_err = *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout;
-      s_next = static_cast< int >( atomicAdd( &sc->sort_tile_counter[pass], 1u ) );
+      s_next = static_cast< int >( nx );
     }
     __syncthreads();
     if ( s_err ) return;
