@@ -268,27 +268,6 @@ __device__ void onesweep_body(const sort_pass_args &a, uint32_t, uint32_t)
       s_lstart[tid] = lexcl;
     }
     __syncthreads();
-    // A block that timed out published a garbage prefix (so that no successor waits forever) and raised the
-    // object's error word. A block that sees the error here writes nothing and stops (no bulk copy is in flight
-    // at this point); one that read a garbage prefix without seeing the error yet writes only inside [0, n) (the
-    // bound on every output position below), and the host reports the error for the whole sort. The error word
-    // and the next tile are fetched together: the fence that used to order them cost the tile two more round trips
-    // to L2 on its critical path (one pass 54.4 -> 52.4 us).
-    if ( tid == 0 )
-    {
-      const uint32_t nx = atomicAdd( &sc->sort_tile_counter[pass], 1u );
-      s_err = *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout;
-      s_next = static_cast< int >( nx );
-    }
-    __syncthreads();
-    if ( s_err ) return;
-    const uint32_t next = static_cast< uint32_t >( s_next );
-    // the other stage was drained by the previous iteration's write-out (barrier below): refill it
-    if ( tid == 0 && next < tiles && tma_tile( next ) )
-    {
-      fence_proxy_async_smem();
-      issue( next, st ^ 1 );
-    }
     // reorder the tile into its own stage buffer (its data now lives in registers)
 #pragma unroll
     for ( int j = 0; j < kSortItems; ++j )
@@ -303,6 +282,25 @@ __device__ void onesweep_body(const sort_pass_args &a, uint32_t, uint32_t)
       }
     }
     __syncthreads();
+    // While the tile is written out, thread 0 claims the next tile, reads the error word and starts the next copy
+    // into the other stage (drained by the previous iteration's write-out). Claiming here, not before the reorder,
+    // keeps a claimed tile's wait for its block short: every successor's look-back waits for that tile's counts.
+    // A block that timed out published a garbage prefix (so that no successor waits forever) and raised the
+    // object's error word. A block that sees the error stops after this tile (no copy is then in flight); a block
+    // that read a garbage prefix writes only inside [0, n) (the bound on every output position below), and the
+    // host reports the error for the whole sort.
+    if ( tid == 0 )
+    {
+      const uint32_t nx = atomicAdd( &sc->sort_tile_counter[pass], 1u );
+      const bool err = *reinterpret_cast< volatile int * >( &sc->error ) == kErrTimeout;
+      s_next = static_cast< int >( nx );
+      s_err = err;
+      if ( !err && nx < tiles && tma_tile( nx ) )
+      {
+        fence_proxy_async_smem();
+        issue( nx, st ^ 1 );
+      }
+    }
     // the warp histograms were last read by the reorder above: clear them for the next tile
     for ( int q = tid; q < ( kWarps / 2 ) * RADIX; q += kSortThreads ) ( &s_whist[0][0] )[q] = 0;
     for ( uint32_t i = tid; i < cnt; i += kSortThreads )
@@ -316,8 +314,9 @@ __device__ void onesweep_body(const sort_pass_args &a, uint32_t, uint32_t)
       }
     }
     __syncthreads();  // the stage is drained: the next iteration may refill it
+    if ( s_err ) return;
     st ^= 1;
-    tile = next;
+    tile = static_cast< uint32_t >( s_next );
   }
 }
 
