@@ -469,7 +469,6 @@ struct dense_smem
   alignas( 16 ) uint32_t qe[32];             // query element indices
   alignas( 16 ) int2 stack[kDenseStack];     // (node, lane mask)
   alignas( 16 ) int2 leaf[kLeafQueue];       // (bucket, lane mask)
-  alignas( 16 ) uint32_t pre[kLeafQueue];    // exclusive prefix of the entries' test counts (8 per query)
   alignas( 16 ) uint2 out[kPairBuf];         // pairs found and not yet written
 };
 
@@ -518,8 +517,9 @@ __device__ __forceinline__ void flush_leaves(const trav_args< T > &x, dense_smem
     const uint32_t y = __shfl_up_sync( 0xffffffffu, inc, o );
     if ( lane >= static_cast< unsigned >( o ) ) inc += y;
   }
-  if ( static_cast< int >( lane ) < nleaf ) sm.pre[lane] = inc - c;
   const uint32_t total = __shfl_sync( 0xffffffffu, inc, 31 );
+  const bool is_entry = static_cast< int >( lane ) < nleaf;
+  const uint32_t mypre = inc - c;
   __syncwarp();
   const unsigned lt = ( 1u << lane ) - 1u;
   for ( uint32_t base = 0; base < total; base += 32 )
@@ -527,17 +527,19 @@ __device__ __forceinline__ void flush_leaves(const trav_args< T > &x, dense_smem
     const uint32_t g = base + lane;
     bool hit = false;
     uint32_t q = 0, r = 0;
+    // the entry of test g: the last entry whose prefix is <= g, from the entries that start before this round and
+    // the starts inside it (entries have distinct prefixes: every entry holds at least 8 tests)
+    const unsigned before = __ballot_sync( 0xffffffffu, is_entry && mypre < base );
+    const unsigned inround = ( is_entry && mypre >= base && mypre - base < 32u ) ? ( 1u << ( mypre - base ) ) : 0u;
+    const unsigned starts = __reduce_or_sync( 0xffffffffu, inround );
+    int lo = __popc( before ) + __popc( starts & ( ( 2u << lane ) - 1u ) ) - 1;
+    lo = lo < 0 ? 0 : lo;
+    const uint32_t lpre = __shfl_sync( 0xffffffffu, mypre, lo );
+    const int enx = __shfl_sync( 0xffffffffu, ent.x, lo ), eny = __shfl_sync( 0xffffffffu, ent.y, lo );
     if ( g < total )
     {
-      int lo = 0, hi = nleaf - 1;  // the last entry whose prefix is <= g
-      while ( lo < hi )
-      {
-        const int mid = ( lo + hi + 1 ) >> 1;
-        if ( sm.pre[mid] <= g ) lo = mid;
-        else hi = mid - 1;
-      }
-      const uint32_t rr = g - sm.pre[lo];
-      const int2 en = sm.leaf[lo];
+      const uint32_t rr = g - lpre;
+      const int2 en = make_int2( enx, eny );
       unsigned m = static_cast< unsigned >( en.y );
       for ( uint32_t k = rr >> 3; k > 0; --k ) m &= m - 1;  // the (rr / 8)-th query of the entry's mask
       q = static_cast< uint32_t >( __ffs( m ) - 1 );
@@ -663,6 +665,7 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
 #pragma unroll
     for ( int k = 0; k < kDenseBatch< K, T >; ++k )
     {
+      if ( k >= nb ) break;
       bool o0 = ( emask[k] >> lane ) & 1u, o1 = o0;
       if ( x.self )
       {
@@ -700,6 +703,7 @@ __device__ __forceinline__ void traverse_packet_stored(const trav_args< T > &x, 
 #pragma unroll
     for ( int k = 0; k < kDenseBatch< K, T >; ++k )
     {
+      if ( k >= nb ) break;
       const int cx = __shfl_sync( 0xffffffffu, links.x, k ), cy = __shfl_sync( 0xffffffffu, links.y, k );
 #pragma unroll
       for ( int side = 0; side < 2; ++side )
