@@ -7,10 +7,12 @@
 // of (node, lane mask) entries: both children of a node are tested from one row holding their slabs (one 32-byte
 // FP64 / 16-byte FP32 sector per slab, loaded a chunk of slabs at a time), and a child is entered with the mask of
 // the lanes that overlap it. At a leaf bucket each lane of the mask tests its query against the bucket's
-// elements. Overlaps are emitted as (query element, tree element) local indices through one warp-aggregated
-// reservation per bucket visit; pairs beyond capacity are counted but not stored, so the host can grow the buffer
-// and retry. In sparse contact the grid is persistent and culls 32 packets per warp step against the target root
-// before walking the survivors; in dense contact it is one warp per packet.
+// elements. Overlaps are emitted as (query element, tree element) local indices: through one warp-aggregated
+// reservation per bucket visit in sparse contact, through a per-warp buffer in shared memory in dense contact;
+// pairs beyond capacity are counted but not stored, so the host can grow the buffer and retry. In sparse contact
+// the grid is persistent and culls 32 packets per warp step against the target root before walking the
+// survivors; in dense contact it is one warp per packet. The FP64 recheck of the precision form reads both
+// elements' vertices per candidate and decides the overlap by comparison-only projections (kdop_math.cuh).
 //
 // Self-collision (self_collision_set, collision_query.hpp:331-368): the query of rank i only visits subtrees
 // holding ranks > i (internal node k splits its bucket range [l, r] into [l, k] and [k + 1, r]) and tests only
@@ -419,7 +421,8 @@ __device__ void traverse_body(const trav_item &item, uint32_t, uint32_t)
 //     shared memory. One global round trip serves the whole batch instead of one per chunk of slabs per node.
 //   - Leaves in batches. The walk only queues (bucket, lane mask) entries; a flush spreads all (query, element)
 //     tests of the queued entries over the warp's lanes, 32 at a time, with every query's slabs staged in shared
-//     memory and the target elements' stored rows read from global memory. Hits collect in a per-warp buffer in
+//     memory and the target elements' stored rows read from global memory. A lane finds the entry of its test from
+//     two warp votes per round and reads it from the lane that holds it. Hits collect in a per-warp buffer in
 //     shared memory (one ballot per 32 tests); a full buffer leaves through one atomic reservation and coalesced
 //     stores, so a warp pays an atomic's round trip per 33-64 pairs instead of per round of tests with a hit.
 // The stack grows by at most kDenseBatch entries per step, so its depth bound is kDenseStack; a walk that would pass
